@@ -1,0 +1,451 @@
+"""Benchmark: partial-wave H solves/s (FP64) and R^k table GB/s on B200.
+
+One step = the whole hot path for one LS partial wave of the production-size
+workload (ks=10, ns=200, Rmax=40, k=0..8, 30 orbitals, 40 channels, 2 %
+angular coefficients; H and S 8000 x 8000): R^k cell tables for every
+multipole, channel-block assembly (bsr_mat) and the diag_hd generalized
+eigensolve with eigenvectors (bsr_hd).  Inputs are seeded synthetic data.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank solves its own partial wave (different seed): the
+work shards by partial wave with no collective in the data path (weak
+scaling); rank 0 prints one JSON line.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "partial-wave H solves/sec & R^k GB/s, mixed vs FP64 at 1e-10 rel eigenvalue err"
+WORKLOAD = "config2"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_desc(pw, khm=None):
+    d = {
+        "workload": "%s: one LS partial wave, ks=%d ns=%d Rmax=%g k=0..%d, %d orbitals, %d channels "
+                    "(H %dx%d), %.0f%% angular coefficients, FP64 assembly + diag_hd eigensolve with vectors"
+                    % (pw["name"], pw["ks"], pw["ns"], pw["t"][-1], pw["kmax"], pw["norb"], pw["nch"],
+                       pw["nch"] * pw["ns"], pw["nch"] * pw["ns"], 100 * {"config1": 0.05, "config2": 0.02}.get(
+                           pw["name"], 0.0)),
+        "seed": pw["seed"], "ncoef": int(len(pw["coefs"]["c"])), "knot_scale": round(pw["knot_scale"], 6),
+        "l2": "working set above L2 (H 262 MB, A 488 MB at config2); L2 flushed between steps",
+    }
+    if khm is not None:
+        d["khm"] = int(khm)
+    return d
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference path (the oracle restating the reference's routines)
+# ---------------------------------------------------------------------------
+def _assemble_groups_worker(args):
+    """One process of the CPU assembly sample: the I_data groups of one multipole
+    for a slice of channel pairs (the block distribution of bsr_mat3_mpi)."""
+    pw, k, chans_slice = args
+    from oracle import oracle as O
+    ob = O.Basis(pw["ks"], pw["t"])
+    rkb = ob.mrk_cell(k)
+    ns, ks = ob.ns, ob.ks
+    rkb_all = np.zeros((ns, ns, ks, ks, pw["kmax"] + 1), order="F")
+    rkb_all[..., k] = rkb
+    c = pw["coefs"]
+    sel = (c["k"] == k) & np.isin(c["ich"], chans_slice)
+    sub = {kk: v[sel] for kk, v in c.items()}
+    t0 = time.perf_counter()
+    O.assemble(ob, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], rkb_all, sub, want_s=False,
+               want_acf=True)
+    return time.perf_counter() - t0
+
+
+def cpu_reference_step(pw, threads):
+    """Time a bounded sample of one config-2 solve on the CPU, extrapolated per stage.
+
+    Sample (about 20-40 s of CPU work):
+      R^k tables   mrk_cell for 2 of the kmax+1 multipoles            -> x (kmax+1)/2
+      assembly     every I_data group of one multipole (k = kmax/2),
+                   channel pairs dealt over `threads` processes     -> x (kmax+1)
+      channel eig  DSYGV for 4 channels                              -> x nch/4
+      transforms   bb^T H_ij bb for nch-1 off-diagonal blocks        -> x nb/(nch-1)
+      DSYEV('V')   the leading khm/4 principal submatrix             -> x 64 (n^3)
+    Returns (seconds per solve, stage seconds, description)."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+    from scipy.linalg import lapack
+
+    ks, ns, kmax, nch = pw["ks"], pw["ns"], pw["kmax"], pw["nch"]
+    ob = O.Basis(ks, pw["t"])
+    st = {}
+    t0 = time.perf_counter()
+    for k in (0, kmax):
+        ob.mrk_cell(k)
+    st["rk_tables"] = (time.perf_counter() - t0) * (kmax + 1) / 2
+    kmid = kmax // 2
+    chans = np.arange(1, nch + 1)
+    nproc = max(1, threads)
+    slices = [chans[q::nproc] for q in range(nproc)]
+    # the parallel assembly time is the slowest process's own compute time
+    # (process start-up and table set-up are not charged to the reference)
+    if nproc == 1:
+        wt = [_assemble_groups_worker((pw, kmid, slices[0]))]
+    else:
+        with ProcessPoolExecutor(max_workers=nproc, mp_context=mp.get_context("spawn")) as ex:
+            wt = list(ex.map(_assemble_groups_worker, [(pw, kmid, s) for s in slices]))
+    st["assembly"] = max(wt) * (kmax + 1)
+    # diag_hd pieces on the oracle's restatement, H built blockwise on the CPU for 4 channels
+    rng = np.random.default_rng(0)
+    sb = ob.band("sb")
+    S = np.zeros((ns, ns))
+    for jc in range(ks):
+        for i in range(ks - 1 - jc, ns):
+            j = i + jc - ks + 1
+            S[i, j] = S[j, i] = sb[i, jc]
+    hl = [ob.hl_full(l, pw["z"]) for l in range(pw["lch"].max() + 1)]
+    t0 = time.perf_counter()
+    bbs = []
+    for ich in range(4):
+        l = min(pw["lch"][ich], ks - 2)
+        i1 = l + 1
+        Hd = -0.5 * hl[pw["lch"][ich]] + pw["ech"][ich] * S
+        w, v, info = lapack.dsygv(Hd[i1:, i1:].copy(), S[i1:, i1:].copy(), itype=1, jobz="V", uplo="U")[:3]
+        bb = np.zeros((ns, len(w)))
+        bb[i1:, :] = v
+        bbs.append(bb)
+    st["channel_eig"] = (time.perf_counter() - t0) * nch / 4
+    Hx = rng.standard_normal((ns, ns))
+    t0 = time.perf_counter()
+    for q in range(nch - 1):
+        _ = bbs[q % 4].T @ Hx @ bbs[(q + 1) % 4]
+    nb = nch * (nch - 1) // 2
+    st["transform"] = (time.perf_counter() - t0) * nb / (nch - 1)
+    khm = nch * ns - int(np.sum(np.minimum(pw["lch"], ks - 2) + 1))
+    n4 = khm // 4
+    A = rng.standard_normal((n4, n4))
+    A = np.tril(A + A.T)
+    t0 = time.perf_counter()
+    lapack.dsyev(A, compute_v=1, lower=1)
+    st["dense_eig"] = (time.perf_counter() - t0) * (khm / n4) ** 3
+    total = sum(st.values())
+    desc = ("bounded sample of one %s solve, extrapolated per stage: mrk_cell for 2/%d multipoles; all I_data "
+            "groups of multipole %d over %d processes; DSYGV for 4/%d channels; %d/%d block transforms; "
+            "DSYEV('V') at n=%d scaled by (khm/n)^3 to khm=%d" % (pw["name"], kmax + 1, kmid, nproc, nch,
+                                                                 nch - 1, nb, n4, khm))
+    return total, st, desc
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from bsr_b200 import workload as W
+    pw = W.partial_wave(args.workload)
+    threads = os.cpu_count() or 1
+    for _ in range(max(0, min(args.warmup, 1))):
+        pass        # the CPU path has no warm-up state; a sample is timed directly
+    secs = []
+    stages = None
+    desc = ""
+    for _ in range(args.steps):
+        total, stages, desc = cpu_reference_step(pw, threads)
+        secs.append(total)
+    spp = statistics.mean(secs)
+    value = 1.0 / spp
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": spp * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_desc(pw),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": desc,
+                         "stage_seconds": {k: round(v, 3) for k, v in stages.items()}},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Fortran with no compiler in this image; its routines are timed through the "
+                "C restatement (oracle/) with LAPACK from scipy's OpenBLAS on all host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 path
+# ---------------------------------------------------------------------------
+def fp64_peak_tflops(torch):
+    """Measured FP64 GEMM rate (cuBLAS, 8192^3): the denominator for FP64 kernels."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    import bsr_b200 as bsr
+    from bsr_b200 import workload as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    pw = W.partial_wave(args.workload, seed=W.CONFIGS[args.workload]["seed"] + rank)
+    ctx = bsr.Context()
+    basis = bsr.define_spline(pw["t"], pw["ks"])
+    P = bsr.as_fortran(pw["P"])
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        H = bsr.assemble(ctx, basis, pw["z"], pw["lch"], pw["ech"], P, pw["kmax"], pw["coefs"])
+        res = bsr.diag_hd(ctx, basis, pw["lch"], H["hcc"], want_vectors=True)
+        return res
+
+    for _ in range(args.warmup):
+        res = step()
+    torch.cuda.synchronize()
+    khm = res["khm"]
+    # ---- timed region: K steps, L2 flushed between steps (outside the events) ----
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ms = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        res = step()
+        e.record(stream)
+        e.synchronize()
+        ms += s.elapsed_time(e)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_total = float(t_max.item())
+    value = world * args.steps / (ms_total * 1e-3)
+    # ---- stage breakdown (separate pass with stage events on) ----
+    ctx.set_timing(True)
+    ctx.stage_times()
+    nst = max(1, min(args.steps, 2))
+    for _ in range(nst):
+        flush.fill_(1.0)
+        step()
+    torch.cuda.synchronize()
+    stages = ctx.stage_times()
+    ctx.set_timing(False)
+    own_launches = sum(n for _, n in stages.values()) / nst
+    # ---- e2e: host buffers through the C ABI (bsrg_partial_wave_solve) ----
+    e2e_ms = 0.0
+    ne2e = max(1, min(args.steps, 3))
+    bsr.partial_wave_solve(ctx, pw, want_vectors=True)
+    torch.cuda.synchronize()
+    for _ in range(ne2e):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev = bsr.partial_wave_solve(ctx, pw, want_vectors=True)
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+    c = pw["coefs"]
+    h2d = (pw["t"].nbytes + pw["P"].nbytes + sum(np.asarray(c[k]).nbytes for k in c) + pw["lch"].nbytes
+           + pw["ech"].nbytes)
+    d2h = int(len(ev)) * 8
+    e2e_t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * ne2e / (float(e2e_t.item()) * 1e-3)
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    # ---- roofline figures (algorithmic work per launch / measured launch time) ----
+    import json as _json
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = _json.load(open(pp))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    fp64 = fp64_peak_tflops(torch)
+    ns, ks, kmax = pw["ns"], pw["ks"], pw["kmax"]
+    nk = kmax + 1
+    rkb_bytes = ns * ns * ks * ks * 8
+    exp_ms, exp_n = stages["rk_expand"]
+    exp_launch_ms = exp_ms / max(exp_n, 1)
+    rk_gbs = rkb_bytes / (exp_launch_ms * 1e-3) / 1e9
+    # exchange: per group ns^2 outputs x (2ks-1)^2 multiply-adds
+    ngx = int(np.sum(_group_counts(c, 1)))
+    ngd = int(np.sum(_group_counts(c, 0)))
+    x_flops = 2.0 * ngx * ns * ns * (2 * ks - 1) ** 2 / nk          # per launch (one launch per k)
+    x_ms, x_n = stages["exchange"]
+    x_launch_ms = x_ms / max(x_n, 1)
+    d_flops = 2.0 * ngd * (ns * ks) ** 2 / nk
+    d_ms, d_n = stages["direct"]
+    d_launch_ms = d_ms / max(nk, 1)
+    eig_ms, _ = stages["dense_eig"]
+    eig_ms /= nst
+    eig_flops = (4.0 / 3.0 + 2.0 + 4.0) * khm ** 3     # tridiagonalisation + D&C + back-transform, rough
+    by_stage = {
+        "rk_expand": {"bound": "hbm", "achieved": rk_gbs, "peak": hbm_peak, "unit": "GB/s",
+                      "frac": rk_gbs / hbm_peak, "launch_ms": exp_launch_ms,
+                      "algorithmic": "%d bytes written per launch (rkb ns^2 ks^2 doubles, one multipole)" % rkb_bytes},
+        "exchange": {"bound": "tensor", "achieved": x_flops / (x_launch_ms * 1e-3) / 1e12, "peak": fp64,
+                     "unit": "TFLOP/s", "launch_ms": x_launch_ms,
+                     "algorithmic": "2*ns^2*(2ks-1)^2 flop per exchange group, %d groups over %d launches"
+                                    % (ngx, nk)},
+        "direct": {"bound": "tensor", "achieved": d_flops / (d_launch_ms * 1e-3) / 1e12, "peak": fp64,
+                   "unit": "TFLOP/s", "launch_ms": d_launch_ms,
+                   "algorithmic": "2*(ns ks)^2 flop per direct group, %d groups" % ngd},
+        "dense_eig": {"bound": "tensor", "achieved": eig_flops / (eig_ms * 1e-3) / 1e12, "peak": fp64,
+                      "unit": "TFLOP/s", "launch_ms": eig_ms, "library": "cuSOLVER Xsyevd",
+                      "algorithmic": "~7.3 khm^3 flop (sytrd + stedc + ormtr)"},
+    }
+    for v in by_stage.values():
+        v["frac"] = v["achieved"] / v["peak"]
+    own = {k: v for k, v in by_stage.items() if "library" not in v}
+    per_step_ms = {k: v[0] / nst for k, v in stages.items()}
+    dom_own = max(own, key=lambda k: per_step_ms[k])
+    r = dict(by_stage[dom_own])
+    r["kernel"] = dom_own
+    r["traffic"] = None
+    r["peak_source"] = (hbm_src + " (MEASURED_PEAKS.json hbm_gbs)") if r["unit"] == "GB/s" else \
+        "measured in this run: cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)"
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; see config)",
+        "config": dict(workload_desc(pw, khm), parallelism="one partial wave per GPU, no collective"),
+        "rk_gbs": {"value": rk_gbs, "unit": "GB/s", "frac_of_hbm": rk_gbs / hbm_peak,
+                   "what": "mrk_cell rkb expansion: ns^2 ks^2 doubles written per multipole"},
+        "stages_ms_per_step": {k: round(v, 4) for k, v in per_step_ms.items()},
+        "roofline": r,
+        "roofline_by_stage": by_stage,
+        "fp64_gemm_tflops_measured": fp64,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
+                "api": "bsrg_partial_wave_solve (host buffers: knots, orbitals, coefficient records in; "
+                       "eigenvalues out)"},
+        "gpu_launches": int(round(own_launches * args.steps)),
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        total, st, desc = cpu_reference_step(pw, threads)
+        line["cpu_baseline"] = {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
+                                "sample": desc, "stage_seconds": {k: round(v, 3) for k, v in st.items()}}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _group_counts(c, ty):
+    """Number of (k, ich, jch) groups of structure ty, per multipole."""
+    sel = c["type"] == ty
+    key = (c["k"][sel].astype(np.int64) * 100000 + c["ich"][sel] * 1000 + c["jch"][sel])
+    return np.array([len(np.unique(key))])
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

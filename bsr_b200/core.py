@@ -1,0 +1,302 @@
+"""Host-side mirror of the reference's routines on the hot path, backed by libbsrgpu.
+
+Names, argument meaning and error behaviour follow the Fortran routines of
+jagot/bsr (src/libs/BS and src/bsr/BSR_MAT3, BSR_HD3); arrays are torch CUDA
+tensors whose memory is the Fortran column-major layout of the reference's
+arrays (a tensor of shape (ns, ks) here has strides (1, ns)).  A reference
+'Stop' becomes a BsrgError exception.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from ._lib import BsrgError, call, lib
+
+__all__ = ["BsrgError", "define_grid", "define_spline", "Basis", "rk_moments", "mrk_cell", "density", "convol",
+           "sum_amb", "Context", "assemble", "diag_hd", "partial_wave_solve", "fortran_empty", "as_fortran"]
+
+
+# ---------------------------------------------------------------------------
+# layout helpers
+# ---------------------------------------------------------------------------
+def fortran_empty(shape, device="cuda", dtype=torch.float64):
+    """Uninitialised tensor of `shape` with column-major (Fortran) memory."""
+    t = torch.empty(tuple(reversed(shape)), device=device, dtype=dtype)
+    return t.permute(*reversed(range(len(shape))))
+
+
+def fortran_zeros(shape, device="cuda", dtype=torch.float64):
+    t = torch.zeros(tuple(reversed(shape)), device=device, dtype=dtype)
+    return t.permute(*reversed(range(len(shape))))
+
+
+def _is_fortran(x):
+    st, sz = x.stride(), x.shape
+    exp = 1
+    for d in range(x.dim()):
+        if sz[d] != 1 and st[d] != exp:
+            return False
+        exp *= sz[d]
+    return True
+
+
+def as_fortran(x, device="cuda"):
+    """Column-major float64 CUDA tensor with the values of x (numpy or torch)."""
+    if isinstance(x, np.ndarray):
+        x = torch.from_numpy(np.ascontiguousarray(x.T)).permute(*reversed(range(x.ndim)))
+    x = x.to(device=device, dtype=torch.float64)
+    if not _is_fortran(x):
+        rev = tuple(reversed(range(x.dim())))
+        x = x.permute(*rev).contiguous().permute(*rev)
+    return x
+
+
+def _ptr(x):
+    return ctypes.c_void_p(x.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+# ---------------------------------------------------------------------------
+# grid and basis: define_grid.f90, define_spline.f90
+# ---------------------------------------------------------------------------
+def define_grid(grid_type, ks, z, h, hmax, rmax):
+    """Knot sequence of define_grid (grid_type 0: mkgrid, 1: mkgrid1).
+
+    Returns dict(t, ns, ml, me, h) with the spline_param values the reference
+    leaves in its module."""
+    cap = int((rmax * z / h + 1 + ks) * 2) + 4 * ks + 64
+    t = np.zeros(cap)
+    ns, ml, me = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    hh = ctypes.c_double()
+    call("bsrg_mkgrid", grid_type, ks, z, h, hmax, rmax, _dptr(t), cap, ctypes.byref(ns), ctypes.byref(ml),
+         ctypes.byref(me), ctypes.byref(hh))
+    n = ns.value
+    return {"t": t[: n + ks].copy(), "ns": n, "ml": ml.value, "me": me.value, "h": hh.value, "ks": ks}
+
+
+class Basis:
+    """define_spline's module state, resident on the GPU (spline_grid + spline_galerkin)."""
+
+    _WHICH = {"gr": 0, "grm": 1, "grw": 2, "bsp": 3, "bsq": 4, "bspd": 5, "sb": 6, "r1": 7, "rm1": 8, "rm2": 9,
+              "rm3": 10, "db1": 11, "db2": 12, "t": 13}
+
+    def __init__(self, t, ks, ml=0, me=0, h=0.0):
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        self.ks = int(ks)
+        self.ns = len(t) - self.ks
+        self.nv = self.ns - self.ks + 1
+        self.ml, self.me, self.h = int(ml), int(me), float(h)
+        self.t = t
+        handle = ctypes.c_void_p()
+        call("bsrg_define_spline", self.ks, self.ns, _dptr(t), self.ml, self.me, self.h, _stream(),
+             ctypes.byref(handle))
+        self.handle = handle
+
+    def free(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            torch.cuda.current_stream().synchronize()
+            lib().bsrg_basis_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def get(self, name):
+        """Module array `name` as a Fortran-layout CUDA tensor (gr, bsp, sb, db2, ...)."""
+        ks, ns, nv = self.ks, self.ns, self.nv
+        shapes = {"gr": (nv, ks), "grm": (nv, ks), "grw": (nv, ks), "bsp": (nv + 1, ks, ks),
+                  "bsq": (nv + 1, ks, ks), "bspd": (nv + 1, ks, ks, 2), "t": (ns + ks,)}
+        out = fortran_empty(shapes.get(name, (ns, ks)))
+        call("bsrg_basis_get", self.handle, self._WHICH[name], _ptr(out), _stream())
+        return out
+
+    def mrm(self, mm):
+        """mrm.f90: <B_i|r^mm|B_j> band (ns, ks)."""
+        out = fortran_empty((self.ns, self.ks))
+        call("bsrg_mrm", self.handle, mm, _ptr(out), _stream())
+        return out
+
+
+def define_spline(t, ks, ml=0, me=0, h=0.0):
+    return Basis(t, ks, ml, me, h)
+
+
+# ---------------------------------------------------------------------------
+# R^k tables: rk_moments.f90, mrk_cell.f90
+# ---------------------------------------------------------------------------
+def rk_moments(basis, k):
+    """(rkd1 (ik,nv), rkd2 (ik,nv), rkd (ik,ik,nv)) for multipole k."""
+    ik = basis.ks * (basis.ks + 1) // 2
+    rkd1 = fortran_empty((ik, basis.nv))
+    rkd2 = fortran_empty((ik, basis.nv))
+    rkd = fortran_empty((ik, ik, basis.nv))
+    call("bsrg_rk_moments", basis.handle, k, _ptr(rkd1), _ptr(rkd2), _ptr(rkd), _stream())
+    return rkd1, rkd2, rkd
+
+
+def mrk_cell(basis, k, ldp=None, out=None):
+    """rkb(ns,ns,ldp,ldp) = R^k(B_i B_j; B_{i+ip-1} B_{j+jp-1}) (ldp defaults to ks)."""
+    ldp = basis.ks if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mrk_cell", basis.handle, k, _ptr(out), ldp, _stream())
+    return out
+
+
+# ---------------------------------------------------------------------------
+# density.f90, convol.f90, sum_amb.f90
+# ---------------------------------------------------------------------------
+def density(ns, ks, p1, p2, type):
+    cols = {"s": ks, "n": 2 * ks - 1}.get(type, ns)
+    d = fortran_empty((ns, cols))
+    p1, p2 = as_fortran(p1), as_fortran(p2)
+    call("bsrg_density", ns, ks, _ptr(d), _ptr(p1), _ptr(p2), type.encode(), _stream())
+    return d
+
+
+def convol(ns, ks, d, rkb, icase, sym_i, sym_j):
+    """a(ns, *) = convol of rkb with density d (band result for icase 1,2; full for 3,4).
+
+    Entries of a band result outside the band are left zero."""
+    d = as_fortran(d)
+    rkb = as_fortran(rkb)
+    ldp = rkb.shape[2]
+    a = fortran_zeros((ns, ns))
+    call("bsrg_convol", ns, ks, _ptr(a), _ptr(d), _ptr(rkb), ldp, icase, sym_i.encode(), sym_j.encode(),
+         _stream())
+    if icase <= 2:
+        so = sym_i if icase == 1 else sym_j
+        return a[:, : (ks if so == "s" else 2 * ks - 1)]
+    return a
+
+
+def sum_amb(ns, ks, a, b, sym):
+    a, b = as_fortran(a), as_fortran(b)
+    out = torch.empty(1, device="cuda", dtype=torch.float64)
+    call("bsrg_sum_amb", ns, ks, _ptr(a), _ptr(b), sym.encode(), _ptr(out), _stream())
+    return out
+
+
+# ---------------------------------------------------------------------------
+# bsr_mat assembly and bsr_hd diagonalisation
+# ---------------------------------------------------------------------------
+class Context:
+    """Stream + cuBLAS/cuSOLVER handles + device workspace (bsrg_ctx)."""
+
+    def __init__(self, device=None, stream=None):
+        device = torch.cuda.current_device() if device is None else device
+        self.stream = stream if stream is not None else torch.cuda.current_stream(device)
+        h = ctypes.c_void_p()
+        call("bsrg_ctx_create", device, ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(h))
+        self.handle = h
+
+    def workspace_bytes(self):
+        return lib().bsrg_ctx_workspace_bytes(self.handle)
+
+    STAGES = ("rk_moments", "direct", "exchange", "one_electron", "channel_eig", "transform", "dense_eig",
+              "rk_expand")
+
+    def set_timing(self, on=True):
+        call("bsrg_ctx_set_timing", self.handle, 1 if on else 0)
+
+    def stage_times(self):
+        """Per-stage device time (ms) and launch counts since the last read (then reset)."""
+        ms = np.zeros(len(self.STAGES))
+        n = np.zeros(len(self.STAGES), dtype=np.int32)
+        call("bsrg_ctx_stage_times", self.handle, _dptr(ms), _iptr(n), len(self.STAGES))
+        return {s: (float(ms[i]), int(n[i])) for i, s in enumerate(self.STAGES)}
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            lib().bsrg_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _coef_arrays(coefs):
+    out = {k: np.ascontiguousarray(coefs[k], dtype=np.int32) for k in ("k", "type", "ich", "jch", "a", "b")}
+    out["c"] = np.ascontiguousarray(coefs["c"], dtype=np.float64)
+    return out
+
+
+def assemble(ctx, basis, z, lch, ech, P, kmax, coefs, want_s=False, want_acf=False):
+    """bsr_mat SUB1 for one partial wave: H blocks hcc (ns, ns, nch(nch+1)/2) on the device."""
+    ns = basis.ns
+    lch_a = np.ascontiguousarray(lch, dtype=np.int32)
+    ech_a = np.ascontiguousarray(ech, dtype=np.float64)
+    nch = len(lch_a)
+    nblk = nch * (nch + 1) // 2
+    Pd = as_fortran(P)
+    c = _coef_arrays(coefs)
+    hcc = fortran_empty((ns, ns, nblk))
+    scc = fortran_empty((ns, ns, nblk)) if want_s else None
+    acf = fortran_empty((nch, nch, kmax + 1)) if want_acf else None
+    call("bsrg_assemble", ctx.handle, basis.handle, float(z), nch, _iptr(lch_a), _dptr(ech_a), Pd.shape[1],
+         _ptr(Pd), kmax, len(c["c"]), _iptr(c["k"]), _iptr(c["type"]), _iptr(c["ich"]), _iptr(c["jch"]),
+         _iptr(c["a"]), _iptr(c["b"]), _dptr(c["c"]), _ptr(hcc), _ptr(scc) if want_s else None,
+         _ptr(acf) if want_acf else None)
+    out = {"hcc": hcc}
+    if want_s:
+        out["scc"] = scc
+    if want_acf:
+        out["acf"] = acf
+    return out
+
+
+def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001, want_vectors=True,
+            want_bb=False):
+    """bsr_hd diag_hd for a block-diagonal overlap: eigenvalues (khm,) [+ vectors (khm,khm), bb]."""
+    lch_a = np.ascontiguousarray(lch, dtype=np.int32)
+    nch = len(lch_a)
+    ns = basis.ns
+    ev = torch.empty(nch * ns, device="cuda", dtype=torch.float64)
+    vecs = torch.empty((nch * ns) ** 2, device="cuda", dtype=torch.float64) if want_vectors else None
+    bb = fortran_empty((ns, nch * ns)) if want_bb else None
+    khm = ctypes.c_int()
+    call("bsrg_diag_hd", ctx.handle, basis.handle, nch, _iptr(lch_a), _ptr(as_fortran(hcc)), itype, ilzero, ibzero,
+         float(Edmax), float(Egap), 1 if want_vectors else 0, _ptr(ev), ctypes.byref(khm),
+         _ptr(vecs) if want_vectors else None, _ptr(bb) if want_bb else None)
+    n = khm.value
+    out = {"eval": ev[:n], "khm": n}
+    if want_vectors:
+        out["vectors"] = vecs[: n * n].view(n, n).t()      # column-major (khm, khm)
+    if want_bb:
+        out["bb"] = bb
+    return out
+
+
+def partial_wave_solve(ctx, pw, want_vectors=True):
+    """The whole path with host buffers (e2e): knots, orbitals, coefficients in; eigenvalues out."""
+    t = np.ascontiguousarray(pw["t"], dtype=np.float64)
+    P = np.asfortranarray(pw["P"], dtype=np.float64)
+    lch = np.ascontiguousarray(pw["lch"], dtype=np.int32)
+    ech = np.ascontiguousarray(pw["ech"], dtype=np.float64)
+    c = _coef_arrays(pw["coefs"])
+    nch, ns, ks = len(lch), len(t) - pw["ks"], pw["ks"]
+    ev = np.zeros(nch * ns)
+    khm = ctypes.c_int()
+    call("bsrg_partial_wave_solve", ctx.handle, ks, ns, _dptr(t), float(pw["z"]), nch, _iptr(lch), _dptr(ech),
+         P.shape[1], P.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), pw["kmax"], len(c["c"]), _iptr(c["k"]),
+         _iptr(c["type"]), _iptr(c["ich"]), _iptr(c["jch"]), _iptr(c["a"]), _iptr(c["b"]), _dptr(c["c"]),
+         1 if want_vectors else 0, _dptr(ev), ctypes.byref(khm))
+    return ev[: khm.value].copy()

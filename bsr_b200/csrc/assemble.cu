@@ -1,0 +1,622 @@
+// Channel-block assembly of one partial wave on the GPU (the bsr_mat hot path).
+//
+// Reference (src/bsr/BSR_MAT3): SUB1 (sub1.f90:72-191) drives, per partial wave,
+//   L_data Case(6..9) (L_data.f90:131-150) with hl_core from INT_core
+//   (l_core.f90:174-270): H_ii += -1/2 hl_l  (no closed shells),
+//   I_data Case(6..9) (I_data.f90:192-218): for each coefficient group of one
+//   channel pair, multipole k and structure, xx = sum_t c_t density(p_a,p_b),
+//   dd = convol(xx) and UPDATE_HX (mod_intmat.f90:69) into the block,
+//   UPDATE_CF (mod_intmat.f90:245) for the asymptotic coefficients,
+//   UPDATE_HL(i,i,sb,Etarg) (sub1.f90:178) and the symmetrisation of the
+//   diagonal blocks (sub1.f90:187-191).
+//
+// B200 layout of the work, per multipole k (all on one stream):
+//   rk moments -> rkb_k (ns,ns,ks,ks) in HBM (32 MB at ns=200, ks=10, stays in L2)
+//   direct groups:   Xd_g = sum_t c_t density_s(p_a,p_b)          (band (ns,ks))
+//                    Out[g,(i,ip)] = sum_(j,jp) Xd_g(j,jp) rkb(i,j,ip,jp)
+//                    a register-tiled FP64 GEMM (groups x (ns ks) x (ns ks)) whose
+//                    epilogue is UPDATE_HX 's' into the channel block
+//   exchange groups: the group density D_g = sum_t c_t p_a p_b^T is built in
+//                    shared memory tile by tile (never written to HBM) and the
+//                    convol icase-3 gather runs on it for several groups at once,
+//                    so every rkb value read from L2 feeds all of them; the
+//                    epilogue is UPDATE_HX 'x'.
+// A block receives at most one group per (k, structure), so no two CTAs of one
+// launch update the same H element and no atomics are needed.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+
+namespace bsrg {
+
+// ---------------------------------------------------------------------------
+// one-electron blocks: hcc_ii = -1/2 * hl_core(l_i)  (hcc zeroed beforehand)
+// hl = db2 - l(l+1) rm2 + 2z rm1 with the Bloch fix of INT_core at (ns, ks-1/ks)
+// ---------------------------------------------------------------------------
+__global__ void one_electron_kernel(int ns, int ks, int nch, const int *__restrict__ lch, double z,
+                                    const double *__restrict__ db2, const double *__restrict__ rm2,
+                                    const double *__restrict__ rm1, double *hcc)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ks || ich >= nch) return;
+    int i = tid % ns, jp = tid / ns;            // band (i, jp): element (i, j = i + jp - (ks-1))
+    int j = i + jp - (ks - 1);
+    if (j < 0) return;
+    int l = lch[ich];
+    double c1 = (double)(l * (l + 1)), c2 = 2 * z;
+    double v = db2[tid] - c1 * rm2[tid] + c2 * rm1[tid];
+    if (i == ns - 1 && (jp == ks - 2 || jp == ks - 1)) {
+        double cb = db2[0] - db2[(ns - 1) + (size_t)ns * (ks - 2)];
+        v = jp == ks - 2 ? v + cb : v - cb;
+    }
+    double *blk = hcc + ((size_t)(ich + 1) * (ich + 2) / 2 - 1) * ns * ns;
+    double x = -0.5 * v;
+    blk[i + (size_t)ns * j] += x;
+    if (i != j) blk[j + (size_t)ns * i] += x;
+}
+
+// UPDATE_HL(ich,ich,sb,c_ich) for all channels; optionally also writes S blocks.
+__global__ void sb_update_kernel(int ns, int ks, int nch, const double *__restrict__ ech,
+                                 const double *__restrict__ sb, double *hcc, double *scc)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ks || ich >= nch) return;
+    int i = tid % ns, ith = tid / ns;
+    int j = i + ith - (ks - 1);
+    if (j < 0) return;
+    size_t off = ((size_t)(ich + 1) * (ich + 2) / 2 - 1) * ns * ns;
+    double s = sb[tid];
+    if (hcc) {
+        double v = ech[ich] * s;
+        hcc[off + i + (size_t)ns * j] += v;
+        if (i != j) hcc[off + j + (size_t)ns * i] += v;
+    }
+    if (scc) {
+        scc[off + i + (size_t)ns * j] = s;
+        if (i != j) scc[off + j + (size_t)ns * i] = s;
+    }
+}
+
+__global__ void symmetrize_diag_kernel(int ns, int nch, double *hcc)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ns || ich >= nch) return;
+    int i = tid % ns, j = tid / ns;
+    if (j > i) return;
+    double *blk = hcc + ((size_t)(ich + 1) * (ich + 2) / 2 - 1) * ns * ns;
+    double c = blk[i + (size_t)ns * j] + blk[j + (size_t)ns * i];
+    blk[i + (size_t)ns * j] = c / 2.0;
+    blk[j + (size_t)ns * i] = c / 2.0;
+}
+
+// ---------------------------------------------------------------------------
+// direct groups
+// ---------------------------------------------------------------------------
+struct GroupDesc {
+    int start, end;   // coefficient range
+    int blk;          // 0-based block index i(i-1)/2 + j - 1
+    int ich, jch;     // 1-based channels
+};
+
+// Xd_g(j,jp) = sum_t c_t * density_s(p_a,p_b)(j,jp)   (I_data.f90:198-199)
+__global__ void direct_density_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd,
+                                      const int *__restrict__ ca, const int *__restrict__ cb,
+                                      const double *__restrict__ cv, const double *__restrict__ P,
+                                      double *__restrict__ Xd)
+{
+    int g = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng || tid >= ns * ks) return;
+    int i = tid % ns, jp = tid / ns;
+    GroupDesc G = gd[g];
+    double acc = 0.0;
+    if (i + jp < ns) {
+        for (int t = G.start; t < G.end; t++) {
+            const double *pa = P + (size_t)ns * ca[t], *pb = P + (size_t)ns * cb[t];
+            double dd = jp == 0 ? pa[i] * pb[i] : pa[i] * pb[i + jp] + pa[i + jp] * pb[i];
+            acc = fma(cv[t], dd, acc);
+        }
+    }
+    Xd[(size_t)g * ns * ks + tid] = acc;
+}
+
+// Out[g,(i,ip)] = sum_(jp,j) Xd[g,(j,jp)] * rkb(i,j,ip,jp); epilogue UPDATE_HX 's'.
+// CTA tile: 64 groups x 64 rows i (one ip); 256 threads with 4x4 outputs each.
+constexpr int DG_TM = 64, DG_TN = 64, DG_TK = 16;
+
+__global__ void __launch_bounds__(256)
+direct_gemm_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, const double *__restrict__ Xd,
+                   const double *__restrict__ rkb, double *hcc)
+{
+    __shared__ double As[DG_TK][DG_TM + 1];
+    __shared__ double Bs[DG_TK][DG_TN];
+    int i0 = blockIdx.x * DG_TN;
+    int ip = blockIdx.y;
+    int g0 = blockIdx.z * DG_TM;
+    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4] = {};
+    size_t nn = (size_t)ns * ns;
+    size_t ldx = (size_t)ns * ks;
+    for (int jp = 0; jp < ks; jp++) {
+        const double *R = rkb + nn * (ip + (size_t)ks * jp);
+        int jmax = ns - jp;                       // Xd(j,jp) = 0 beyond
+        for (int j0 = 0; j0 < jmax; j0 += DG_TK) {
+            // A tile: As[kk][gg] = Xd[g0+gg][(j0+kk) + ns*jp]
+            for (int q = threadIdx.x; q < DG_TK * DG_TM; q += 256) {
+                int kk = q % DG_TK, gg = q / DG_TK;
+                int g = g0 + gg, j = j0 + kk;
+                As[kk][gg] = (g < ng && j < jmax) ? Xd[(size_t)g * ldx + j + (size_t)ns * jp] : 0.0;
+            }
+            // B tile: Bs[kk][ii] = rkb(i0+ii, j0+kk, ip, jp)
+            for (int q = threadIdx.x; q < DG_TK * DG_TN; q += 256) {
+                int ii = q % DG_TN, kk = q / DG_TN;
+                int i = i0 + ii, j = j0 + kk;
+                Bs[kk][ii] = (i < ns && j < jmax) ? R[i + (size_t)ns * j] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < DG_TK; kk++) {
+                double a[4], b[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) a[r] = As[kk][ty * 4 + r];
+#pragma unroll
+                for (int c = 0; c < 4; c++) b[c] = Bs[kk][tx + 16 * c];
+#pragma unroll
+                for (int r = 0; r < 4; r++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+            }
+            __syncthreads();
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        int g = g0 + ty * 4 + r;
+        if (g >= ng) continue;
+        double *blk = hcc + (size_t)gd[g].blk * nn;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int i = i0 + tx + 16 * c;
+            if (i + ip >= ns) continue;
+            double v = acc[r][c];
+            blk[i + (size_t)ns * (i + ip)] += v;
+            if (ip > 0) blk[(i + ip) + (size_t)ns * i] += v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// exchange groups: a(x,y') = sum_(x',y) R(x,x',y,y') D_g(x',y), D_g = sum c p_a p_b^T
+// One CTA per (32x32 output tile, XG_G groups).  256 threads: thread (tx,ty)
+// owns rows x0+tx, columns y0+ty+8q (q<4), for each of the CTA's groups.
+// ---------------------------------------------------------------------------
+constexpr int XT = 32, XG_G = 4;
+
+__global__ void __launch_bounds__(256)
+exchange_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, const int *__restrict__ ca,
+                const int *__restrict__ cb, const double *__restrict__ cv, const double *__restrict__ P,
+                const double *__restrict__ rkb, double *hcc)
+{
+    extern __shared__ double Dsm[];            // XG_G tiles of (XT+2h) x (XT+2h), h = ks-1
+    const int hw = ks - 1, W = XT + 2 * hw;
+    int tiles_x = (ns + XT - 1) / XT;
+    int x0 = (blockIdx.x % tiles_x) * XT, y0 = (blockIdx.x / tiles_x) * XT;
+    int gbase = blockIdx.y * XG_G;
+    int ngl = ng - gbase < XG_G ? ng - gbase : XG_G;
+    // build the group densities with halo: D(x', y), x' = x0-hw+r, y = y0-hw+c
+    for (int gl = 0; gl < XG_G; gl++) {
+        double *D = Dsm + (size_t)gl * W * W;
+        GroupDesc G = gl < ngl ? gd[gbase + gl] : GroupDesc{0, 0, 0, 0, 0};
+        for (int q = threadIdx.x; q < W * W; q += blockDim.x) {
+            int r = q % W, c = q / W;
+            int xp = x0 - hw + r, y = y0 - hw + c;
+            double acc = 0.0;
+            if (xp >= 0 && xp < ns && y >= 0 && y < ns) {
+                for (int t = G.start; t < G.end; t++)
+                    acc = fma(cv[t], P[(size_t)ns * ca[t] + xp] * P[(size_t)ns * cb[t] + y], acc);
+            }
+            D[r + (size_t)W * c] = acc;
+        }
+    }
+    __syncthreads();
+    int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+    int x = x0 + tx;
+    double acc[XG_G][4];
+#pragma unroll
+    for (int gl = 0; gl < XG_G; gl++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[gl][q] = 0.0;
+    size_t nn = (size_t)ns * ns;
+    if (x < ns) {
+        for (int e = -hw; e <= hw; e++) {
+            int xp = x + e;
+            if (xp < 0 || xp >= ns) continue;
+            int r1 = e >= 0 ? x : xp, c1 = e >= 0 ? e : -e;
+            int rr = tx + hw + e;                        // smem row of x'
+            for (int f = -hw; f <= hw; f++) {
+                int c2 = f >= 0 ? f : -f;
+                const double *R = rkb + nn * (c1 + (size_t)ks * c2) + r1;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    int yp = y0 + ty + 8 * q;                // output column y'
+                    int y = yp + f;                          // summed index y
+                    if (yp >= ns || y < 0 || y >= ns) continue;
+                    int r2 = f >= 0 ? yp : y;
+                    double rv = R[(size_t)ns * r2];
+                    int cc = ty + 8 * q + hw + f;            // smem column of y
+#pragma unroll
+                    for (int gl = 0; gl < XG_G; gl++)
+                        acc[gl][q] = fma(rv, Dsm[(size_t)gl * W * W + rr + (size_t)W * cc], acc[gl][q]);
+                }
+            }
+        }
+    }
+    if (x >= ns) return;
+    for (int gl = 0; gl < ngl; gl++) {
+        double *blk = hcc + (size_t)gd[gbase + gl].blk * nn;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int yp = y0 + ty + 8 * q;
+            if (yp < ns) blk[x + (size_t)ns * yp] += acc[gl][q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// asymptotic coefficients (UPDATE_CF): acf(ich,jch,k) = sum_t c_t <p_a|r^k|p_b>
+// one warp per direct group; bvmv (bvmv.f90:2, 's') as a warp reduction.
+// ---------------------------------------------------------------------------
+__global__ void acf_kernel(int ns, int ks, int nch, int k, int ng, const GroupDesc *__restrict__ gd,
+                           const int *__restrict__ ca, const int *__restrict__ cb,
+                           const double *__restrict__ cv, const double *__restrict__ P,
+                           const double *__restrict__ rmk, double *acf)
+{
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x % 32;
+    if (warp >= ng) return;
+    GroupDesc G = gd[warp];
+    double CA = 0.0;
+    for (int t = G.start; t < G.end; t++) {
+        const double *x = P + (size_t)ns * ca[t], *y = P + (size_t)ns * cb[t];
+        double s = 0.0;
+        for (int q = lane; q < ns * ks; q += 32) {
+            int i = q % ns, jp = q / ns;           // band (i, jp), element (i, i+jp-(ks-1))
+            int j = i + jp - (ks - 1);
+            if (j < 0) continue;
+            double a = rmk[q];
+            s += jp == ks - 1 ? a * x[i] * y[i] : a * (x[i] * y[j] + x[j] * y[i]);
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        CA += cv[t] * s;
+    }
+    if (lane == 0) acf[(G.ich - 1) + (size_t)nch * ((G.jch - 1) + (size_t)nch * k)] += CA;
+}
+
+// ---------------------------------------------------------------------------
+// workspace helpers
+// ---------------------------------------------------------------------------
+int ctx_reserve(bsrg_ctx *c, size_t bytes)
+{
+    if (c->ws_bytes >= bytes) return BSRG_OK;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "workspace sync");
+    if (c->ws) cudaFree(c->ws);
+    c->ws = nullptr;
+    c->ws_bytes = 0;
+    size_t want = bytes + (bytes >> 3);
+    e = cudaMalloc(&c->ws, want);
+    if (e != cudaSuccess) return cuda_fail(e, "workspace alloc");
+    c->ws_bytes = want;
+    return BSRG_OK;
+}
+
+int ctx_reserve_pinned(bsrg_ctx *c, size_t bytes)
+{
+    if (c->pinned_bytes >= bytes) {
+        cudaError_t e = cudaEventSynchronize(c->ev_stage);
+        return cuda_fail(e, "pinned staging wait");
+    }
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "pinned sync");
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_bytes = 0;
+    size_t want = bytes + (bytes >> 3);
+    e = cudaMallocHost(&c->pinned, want);
+    if (e != cudaSuccess) return cuda_fail(e, "pinned alloc");
+    c->pinned_bytes = want;
+    return BSRG_OK;
+}
+
+void stage_begin(bsrg_ctx *c, int stage)
+{
+    if (!c->timing) return;
+    cudaEvent_t a, b;
+    for (cudaEvent_t *ev : {&a, &b}) {
+        if (!c->pool->empty()) { *ev = c->pool->back(); c->pool->pop_back(); }
+        else cudaEventCreate(ev);
+    }
+    cudaEventRecord(a, c->stream);
+    c->events->push_back({stage, a, b});
+}
+
+void stage_end(bsrg_ctx *c, int stage, int launches)
+{
+    if (!c->timing) return;
+    for (auto it = c->events->rbegin(); it != c->events->rend(); ++it)
+        if (it->stage == stage) {
+            cudaEventRecord(it->stop, c->stream);
+            break;
+        }
+    c->stage_launches[stage] += launches;
+}
+
+int stage_collect(bsrg_ctx *c)
+{
+    if (!c->timing || c->events->empty()) return BSRG_OK;
+    for (auto &e : *c->events) {
+        cudaError_t err = cudaEventSynchronize(e.stop);
+        if (err != cudaSuccess) return cuda_fail(err, "stage timing");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e.start, e.stop);
+        c->stage_ms[e.stage] += ms;
+        c->pool->push_back(e.start);
+        c->pool->push_back(e.stop);
+    }
+    c->events->clear();
+    return BSRG_OK;
+}
+
+}  // namespace bsrg
+
+using namespace bsrg;
+
+extern "C" {
+
+int bsrg_ctx_set_timing(bsrg_ctx *c, int on)
+{
+    if (!c) { set_error("ctx_set_timing: null context"); return BSRG_ERR_ARG; }
+    int rc = stage_collect(c);
+    c->timing = on ? 1 : 0;
+    return rc;
+}
+
+int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n)
+{
+    if (!c || !ms) { set_error("ctx_stage_times: null argument"); return BSRG_ERR_ARG; }
+    int rc = stage_collect(c);
+    for (int q = 0; q < n && q < BSRG_NSTAGE; q++) {
+        ms[q] = c->stage_ms[q];
+        if (launches) launches[q] = c->stage_launches[q];
+    }
+    for (int q = 0; q < BSRG_NSTAGE; q++) { c->stage_ms[q] = 0.0; c->stage_launches[q] = 0; }
+    return rc;
+}
+
+int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
+{
+    if (!out) { set_error("ctx_create: null output"); return BSRG_ERR_ARG; }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "ctx_create setDevice");
+    bsrg_ctx *c = new bsrg_ctx();
+    std::memset(c, 0, sizeof *c);
+    c->device = device;
+    c->stream = (cudaStream_t)stream;
+    if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) {
+        delete c;
+        set_error("ctx_create: cublasCreate failed");
+        return BSRG_ERR_SOLVER;
+    }
+    cublasSetStream(c->blas, c->stream);
+    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS) {
+        cublasDestroy(c->blas);
+        delete c;
+        set_error("ctx_create: cusolverDnCreate failed");
+        return BSRG_ERR_SOLVER;
+    }
+    cusolverDnSetStream(c->solver, c->stream);
+    cudaEventCreateWithFlags(&c->ev_stage, cudaEventDisableTiming);
+    cudaEventRecord(c->ev_stage, c->stream);
+    c->events = new std::vector<bsrg_stage_event>();
+    c->pool = new std::vector<cudaEvent_t>();
+    *out = c;
+    return BSRG_OK;
+}
+
+int bsrg_ctx_destroy(bsrg_ctx *c)
+{
+    if (!c) return BSRG_OK;
+    cudaStreamSynchronize(c->stream);
+    if (c->ws) cudaFree(c->ws);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    cudaEventDestroy(c->ev_stage);
+    for (auto &e : *c->events) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
+    for (auto ev : *c->pool) cudaEventDestroy(ev);
+    delete c->events;
+    delete c->pool;
+    cusolverDnDestroy(c->solver);
+    cublasDestroy(c->blas);
+    delete c;
+    return BSRG_OK;
+}
+
+size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c) { return c ? c->ws_bytes : 0; }
+
+int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int *lch, const double *ech,
+                  int norb, const double *P, int kmax, int ncoef, const int *ck, const int *ctype,
+                  const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
+                  double *hcc, double *scc, double *acf)
+{
+    if (!c || !b || !lch || !ech || !P || !hcc || (ncoef > 0 && (!ck || !ctype || !cich || !cjch || !ca || !cb || !cval))) {
+        set_error("assemble: null argument");
+        return BSRG_ERR_ARG;
+    }
+    if (nch < 1 || norb < 1 || kmax < 0 || ncoef < 0) {
+        set_error("assemble: bad sizes nch=%d norb=%d kmax=%d ncoef=%d", nch, norb, kmax, ncoef);
+        return BSRG_ERR_ARG;
+    }
+    const int ns = b->ns, ks = b->ks, nv = b->nv, ik = ik_of(ks);
+    cudaStream_t s = c->stream;
+    // ---- group the coefficient records (the cmdata blocks of State_res) ----
+    std::vector<std::vector<GroupDesc>> dgroups(kmax + 1), xgroups(kmax + 1);
+    for (int t = 0; t < ncoef;) {
+        int k = ck[t], ty = ctype[t], i = cich[t], j = cjch[t];
+        if (k < 0 || k > kmax || (ty != 0 && ty != 1) || i < 1 || i > nch || j < 1 || j > i) {
+            set_error("assemble: coefficient %d out of range (k=%d type=%d ich=%d jch=%d)", t, k, ty, i, j);
+            return BSRG_ERR_ARG;
+        }
+        int t0 = t;
+        while (t < ncoef && ck[t] == k && ctype[t] == ty && cich[t] == i && cjch[t] == j) {
+            if (ca[t] < 0 || ca[t] >= norb || cb[t] < 0 || cb[t] >= norb) {
+                set_error("assemble: orbital index out of range at coefficient %d", t);
+                return BSRG_ERR_ARG;
+            }
+            t++;
+        }
+        if (t < ncoef) {
+            long a0 = ((long)k * 2 + ty) * (long)(nch + 1) * (nch + 1) + (long)i * (nch + 1) + j;
+            long a1 = ((long)ck[t] * 2 + ctype[t]) * (long)(nch + 1) * (nch + 1) + (long)cich[t] * (nch + 1) + cjch[t];
+            if (a1 < a0) {
+                set_error("assemble: coefficients not sorted by (k,type,ich,jch) at %d", t);
+                return BSRG_ERR_ARG;
+            }
+        }
+        GroupDesc g{t0, t, i * (i - 1) / 2 + j - 1, i, j};
+        (ty == 0 ? dgroups : xgroups)[k].push_back(g);
+    }
+    size_t ngroups = 0, maxgd = 0;
+    for (int k = 0; k <= kmax; k++) {
+        ngroups += dgroups[k].size() + xgroups[k].size();
+        maxgd = std::max(maxgd, dgroups[k].size());
+    }
+    // ---- workspace ----
+    size_t nn = (size_t)ns * ns;
+    size_t need = 0;
+    auto add = [&](size_t bytes) { need += ((bytes + 255) & ~(size_t)255) + 256; };
+    add(sizeof(int) * (size_t)ncoef * 2);
+    add(sizeof(double) * (size_t)ncoef);
+    add(sizeof(GroupDesc) * ngroups);
+    add(sizeof(int) * nch);
+    add(sizeof(double) * nch);
+    add(sizeof(double) * (size_t)ik * nv * 2);
+    add(sizeof(double) * (size_t)ik * ik * nv);
+    add(sizeof(double) * nn * ks * ks);
+    add(sizeof(double) * maxgd * ns * ks);
+    add(sizeof(double) * (size_t)ns * ks);
+    int rc = ctx_reserve(c, need);
+    if (rc != BSRG_OK) return rc;
+    size_t host_bytes = sizeof(int) * (size_t)ncoef * 2 + sizeof(double) * (size_t)ncoef +
+                        sizeof(GroupDesc) * ngroups + sizeof(int) * nch + sizeof(double) * nch + 64;
+    rc = ctx_reserve_pinned(c, host_bytes);
+    if (rc != BSRG_OK) return rc;
+    Arena ar{(char *)c->ws, 0, c->ws_bytes};
+    int *d_ca = ar.take<int>(ncoef), *d_cb = ar.take<int>(ncoef);
+    double *d_cv = ar.take<double>(ncoef);
+    GroupDesc *d_gd = ar.take<GroupDesc>(ngroups);
+    int *d_lch = ar.take<int>(nch);
+    double *d_ech = ar.take<double>(nch);
+    double *rkd1 = ar.take<double>((size_t)ik * nv), *rkd2 = ar.take<double>((size_t)ik * nv);
+    double *rkd = ar.take<double>((size_t)ik * ik * nv);
+    double *rkb = ar.take<double>(nn * ks * ks);
+    double *Xd = ar.take<double>(std::max<size_t>(maxgd, 1) * ns * ks);
+    double *rmk = ar.take<double>((size_t)ns * ks);
+    // stage host metadata through pinned memory, one copy
+    char *hp = (char *)c->pinned;
+    size_t o = 0;
+    auto stage = [&](const void *src, size_t bytes) { std::memcpy(hp + o, src, bytes); size_t r = o; o += bytes; return r; };
+    size_t o_ca = stage(ca, sizeof(int) * ncoef), o_cb = stage(cb, sizeof(int) * ncoef);
+    size_t o_cv = stage(cval, sizeof(double) * ncoef);
+    size_t o_gd = o;
+    std::vector<size_t> doff(kmax + 1), xoff(kmax + 1);
+    for (int k = 0; k <= kmax; k++) {
+        doff[k] = (o - o_gd) / sizeof(GroupDesc);
+        stage(dgroups[k].data(), sizeof(GroupDesc) * dgroups[k].size());
+        xoff[k] = (o - o_gd) / sizeof(GroupDesc);
+        stage(xgroups[k].data(), sizeof(GroupDesc) * xgroups[k].size());
+    }
+    size_t o_lch = stage(lch, sizeof(int) * nch), o_ech = stage(ech, sizeof(double) * nch);
+    cudaError_t e;
+#define CP(dst, off, bytes) \
+    if ((bytes) > 0 && (e = cudaMemcpyAsync(dst, hp + (off), bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
+        return cuda_fail(e, "assemble upload");
+    CP(d_ca, o_ca, sizeof(int) * ncoef);
+    CP(d_cb, o_cb, sizeof(int) * ncoef);
+    CP(d_cv, o_cv, sizeof(double) * ncoef);
+    CP(d_gd, o_gd, sizeof(GroupDesc) * ngroups);
+    CP(d_lch, o_lch, sizeof(int) * nch);
+    CP(d_ech, o_ech, sizeof(double) * nch);
+#undef CP
+    cudaEventRecord(c->ev_stage, s);
+    // ---- one-electron part ----
+    size_t nblk = (size_t)nch * (nch + 1) / 2;
+    if ((e = cudaMemsetAsync(hcc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset hcc");
+    if (scc && (e = cudaMemsetAsync(scc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset scc");
+    if (acf && (e = cudaMemsetAsync(acf, 0, sizeof(double) * nch * nch * (kmax + 1), s)) != cudaSuccess)
+        return cuda_fail(e, "memset acf");
+    stage_begin(c, 3);
+    {
+        dim3 g((ns * ks + 127) / 128, nch);
+        one_electron_kernel<<<g, 128, 0, s>>>(ns, ks, nch, d_lch, z, b->db2, b->rm2, b->rm1, hcc);
+    }
+    stage_end(c, 3);
+    // ---- two-electron groups, one multipole at a time ----
+    const int W = XT + 2 * (ks - 1);
+    size_t xsm = sizeof(double) * XG_G * W * W;
+    if (xsm > 48 * 1024) {
+        e = cudaFuncSetAttribute(exchange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
+        if (e != cudaSuccess) return cuda_fail(e, "exchange smem");
+    }
+    for (int k = 0; k <= kmax; k++) {
+        int nd = (int)dgroups[k].size(), nx = (int)xgroups[k].size();
+        if (nd == 0 && nx == 0) continue;
+        stage_begin(c, 0);
+        rc = launch_rk_moments(b, k, rkd1, rkd2, rkd, s);
+        if (rc != BSRG_OK) return rc;
+        stage_end(c, 0, 3);
+        stage_begin(c, 7);
+        rc = launch_mrk_cell(b, rkd1, rkd2, rkd, rkb, ks, s);
+        if (rc != BSRG_OK) return rc;
+        stage_end(c, 7, 1);
+        if (nd > 0) {
+            stage_begin(c, 1);
+            const GroupDesc *gdd = d_gd + doff[k];
+            dim3 g1((ns * ks + 127) / 128, nd);
+            direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
+            dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
+            direct_gemm_kernel<<<g2, 256, 0, s>>>(ns, ks, nd, gdd, Xd, rkb, hcc);
+            if (acf) {
+                rc = launch_mrm(b, k, rmk, s);
+                if (rc != BSRG_OK) return rc;
+                acf_kernel<<<(nd * 32 + 127) / 128, 128, 0, s>>>(ns, ks, nch, k, nd, gdd, d_ca, d_cb, d_cv, P,
+                                                                 rmk, acf);
+            }
+            stage_end(c, 1, acf ? 4 : 2);
+        }
+        if (nx > 0) {
+            stage_begin(c, 2);
+            int tiles = ((ns + XT - 1) / XT) * ((ns + XT - 1) / XT);
+            dim3 g3(tiles, (nx + XG_G - 1) / XG_G);
+            exchange_kernel<<<g3, 256, xsm, s>>>(ns, ks, nx, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkb, hcc);
+            stage_end(c, 2, 1);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "assemble k-loop");
+    }
+    // ---- target energies, overlap, symmetrisation ----
+    stage_begin(c, 3);
+    {
+        dim3 g((ns * ks + 127) / 128, nch);
+        sb_update_kernel<<<g, 128, 0, s>>>(ns, ks, nch, d_ech, b->sb, hcc, scc);
+        dim3 g2((ns * ns + 127) / 128, nch);
+        symmetrize_diag_kernel<<<g2, 128, 0, s>>>(ns, nch, hcc);
+    }
+    stage_end(c, 3, 2);
+    rc = cuda_fail(cudaGetLastError(), "assemble");
+    if (rc == BSRG_OK) rc = stage_collect(c);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,48 @@
+// Internal declarations shared by the bsrgpu translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/bsr_b200.h"
+
+#define BSRG_MAXKS 16
+
+// Device-resident B-spline basis (spline_param + spline_grid + spline_galerkin
+// module state of the reference, libs/BS/spline_*.f90).  All arrays keep the
+// Fortran column-major layout, 0-based:
+//   t[ns+ks]; gr/grm/grw (nv,ks) at [iv + nv*m];
+//   bsp/bsq (nv+1,ks,ks) at [iv + (nv+1)*(m + ks*ith)], bspd adds index d (0,1);
+//   band matrices (ns,ks) at [i + ns*jcol] (lower-column storage).
+struct bsrg_basis {
+    int ks, ns, nv, ml, me;
+    double h;
+    double gx[BSRG_MAXKS], gw[BSRG_MAXKS];    // host copies of the Gauss rule
+    double *t, *gr, *grm, *grw, *bsp, *bsq, *bspd;
+    double *sb, *r1, *rm1, *rm2, *rm3, *db1, *db2;
+    int device;
+};
+
+namespace bsrg {
+
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *where);
+
+inline int ik_of(int ks) { return ks * (ks + 1) / 2; }
+
+// Gauss-Legendre nodes/weights on [0,1], ascending (Newton on P_k).
+void gauss_legendre(int k, double *x, double *w);
+
+// kernels launched by the C-ABI layer
+int launch_basis_tables(bsrg_basis *b, cudaStream_t s);
+int launch_mrm(const bsrg_basis *b, int mm, double *rm, cudaStream_t s);
+int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s);
+int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                    double *rkb, int ldp, cudaStream_t s);
+int launch_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, cudaStream_t s);
+int launch_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp, int icase,
+                  char si, char sj, cudaStream_t s);
+int launch_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, cudaStream_t s);
+
+}  // namespace bsrg

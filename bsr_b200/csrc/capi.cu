@@ -1,0 +1,308 @@
+// C ABI entry points (include/bsr_b200.h): argument checks, error reporting,
+// basis lifecycle and the thin wrappers around the table and convolution
+// kernels.  The assembly and eigensolve entry points live in assemble.cu and
+// diag_hd.cu.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bsrg_internal.h"
+
+namespace bsrg {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    if (e == cudaSuccess) return BSRG_OK;
+    set_error("%s: %s", where, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? BSRG_ERR_NOMEM : BSRG_ERR_CUDA;
+}
+
+// Gauss-Legendre rule on [0,1] by Newton iteration on the Legendre polynomial
+// (the reference tabulates the same nodes to 15 digits, gauss.f90:2).
+void gauss_legendre(int k, double *x, double *w)
+{
+    for (int i = 0; i < k; i++) {
+        double z = std::cos(M_PI * (i + 0.75) / (k + 0.5));
+        double dp = 1.0;
+        for (int it = 0; it < 200; it++) {
+            double p0 = 1.0, p1 = z;
+            for (int j = 2; j <= k; j++) {
+                double p2 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p0) / j;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = k * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) <= 1e-17) break;
+        }
+        double p0 = 1.0, p1 = z;
+        for (int j = 2; j <= k; j++) {
+            double p2 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p0) / j;
+            p0 = p1;
+            p1 = p2;
+        }
+        if (k == 1) { p1 = z; p0 = 1.0; }
+        dp = k * (z * p1 - p0) / (z * z - 1.0);
+        x[i] = 0.5 * (1.0 - z);
+        w[i] = 1.0 / ((1.0 - z * z) * dp * dp);
+    }
+}
+
+}  // namespace bsrg
+
+using namespace bsrg;
+
+#define CHECK_ARG(cond, ...)              \
+    do {                                  \
+        if (!(cond)) {                    \
+            set_error(__VA_ARGS__);       \
+            return BSRG_ERR_ARG;          \
+        }                                 \
+    } while (0)
+
+extern "C" {
+
+const char *bsrg_last_error(void) { return bsrg::g_err; }
+int bsrg_version(void) { return 1; }
+
+// define_grid.f90:86 (grid_type 0) and :213 (grid_type 1)
+int bsrg_mkgrid(int grid_type, int ks, double z, double h, double hmax, double rmax, double *t, int cap,
+                int *ns_out, int *ml_out, int *me_out, double *h_out)
+{
+    CHECK_ARG(t && ns_out && ml_out && me_out && h_out, "mkgrid: null output");
+    CHECK_ARG(ks >= 2 && ks <= BSRG_MAXKS, "mkgrid: ks=%d out of range", ks);
+    CHECK_ARG(z > 0 && h > 0 && hmax > 0 && rmax > 0, "mkgrid: non-positive parameter");
+    if (grid_type == 0) {
+        double h0 = h;
+        int ml = (int)(1.0 / h + 0.1);
+        CHECK_ARG(ml >= 1, "mkgrid: h too large");
+        h = 1.0 / ml;
+        double hp1 = 1.0 + h, tmax = z * rmax, hmx = z * hmax;
+        double a = std::log(hmx / h) / std::log(hp1) + 1.0;
+        int me1 = (int)(a > 0.0 ? a : 0.0);
+        int me2 = (int)(std::log(tmax) / std::log(hp1) + 1.0);
+        int me, m;
+        double h2 = 0.0;
+        if (me2 <= me1) { me = me2; m = 0; }
+        else {
+            me = me1;
+            double tx = 1.0;
+            for (int i = 0; i < me; i++) tx *= hp1;
+            h2 = h * tx / hp1;
+            m = (int)std::lround((tmax - tx) / h2);
+        }
+        int n = ml + me + m + ks - 1, nt = n + ks;
+        CHECK_ARG(nt <= cap, "mkgrid: capacity %d < %d", cap, nt);
+        for (int i = 0; i < nt; i++) t[i] = 0.0;
+        for (int i = ks + 1; i <= ks + ml; i++) t[i - 1] = t[i - 2] + h0;
+        for (int i = ks + ml + 1; i <= ks + me + ml; i++) t[i - 1] = t[i - 2] * hp1;
+        for (int i = ks + me + ml + 1; i <= n + 1; i++) t[i - 1] = t[i - 2] + h2;
+        for (int i = n + 2; i <= nt; i++) t[i - 1] = t[n];
+        for (int i = 0; i < nt; i++) t[i] = t[i] / z;
+        *ns_out = n; *ml_out = ml; *me_out = me; *h_out = h;
+        return BSRG_OK;
+    }
+    CHECK_ARG(grid_type == 1, "mkgrid: unknown grid_type %d", grid_type);
+    rmax = rmax * z;
+    hmax = hmax * z;
+    int nt = (int)((rmax / h + 1 + ks) * 2);
+    CHECK_ARG(nt + ks <= cap, "mkgrid: capacity %d < %d", cap, nt + ks);
+    std::vector<double> tt(nt + ks + 2, 0.0);
+#define T1(i) tt[(i) - 1]
+    int ns = ks;
+    int ml = (int)(1.0 / h + 0.5);
+    h = 1.0 / ml;
+    for (int i = 1; i <= ml; i++) { ns++; T1(ns) = T1(ns - 1) + h; }
+    if (hmax < h) hmax = h;
+    int me = 0;
+    for (;;) {
+        CHECK_ARG(ns + 1 < nt, "mkgrid: grid overflow");
+        T1(ns + 1) = T1(ns) * (1.0 + h);
+        if (T1(ns + 1) - T1(ns) > hmax) break;
+        ns++;
+        if (T1(ns) > rmax) break;
+        me++;
+    }
+    if (T1(ns) < rmax) {
+        for (;;) {
+            CHECK_ARG(ns + 1 < nt, "mkgrid: grid overflow");
+            T1(ns + 1) = T1(ns) + hmax;
+            ns++;
+            if (T1(ns) >= rmax) break;
+        }
+    }
+    if (T1(ns) > rmax) {
+        ns--; me--;
+        for (int i = ns + 1; i <= ns + ks; i++) T1(i) = rmax;
+        T1(ns) = (T1(ns + 1) + T1(ns - 1)) / 2.0;
+    }
+#undef T1
+    CHECK_ARG(ns + ks <= cap, "mkgrid: capacity %d < %d", cap, ns + ks);
+    for (int i = 0; i < ns + ks; i++) t[i] = tt[i] / z;
+    *ns_out = ns; *ml_out = ml; *me_out = me; *h_out = h;
+    return BSRG_OK;
+}
+
+int bsrg_define_spline(int ks, int ns, const double *t_host, int ml, int me, double h, void *stream,
+                       bsrg_basis **out)
+{
+    CHECK_ARG(out && t_host, "define_spline: null argument");
+    CHECK_ARG(ks >= 2 && ks <= BSRG_MAXKS, "define_spline: ks=%d out of range 2..%d", ks, BSRG_MAXKS);
+    CHECK_ARG(ns >= ks, "define_spline: ns=%d < ks=%d", ns, ks);
+    for (int i = 1; i < ns + ks; i++)
+        CHECK_ARG(t_host[i] >= t_host[i - 1], "define_spline: knots not non-decreasing at %d", i);
+    for (int iv = 0; iv < ns - ks + 1; iv++)
+        CHECK_ARG(t_host[iv + ks] > t_host[iv + ks - 1], "define_spline: empty interval %d", iv);
+    cudaStream_t s = (cudaStream_t)stream;
+    bsrg_basis *b = new bsrg_basis();
+    std::memset(b, 0, sizeof *b);
+    b->ks = ks; b->ns = ns; b->nv = ns - ks + 1; b->ml = ml; b->me = me; b->h = h;
+    cudaGetDevice(&b->device);
+    gauss_legendre(ks, b->gx, b->gw);
+    size_t nvk = (size_t)b->nv * ks, nb = (size_t)(b->nv + 1) * ks * ks, nband = (size_t)ns * ks;
+    double **bufs[] = {&b->t, &b->gr, &b->grm, &b->grw, &b->bsp, &b->bsq, &b->bspd,
+                       &b->sb, &b->r1, &b->rm1, &b->rm2, &b->rm3, &b->db1, &b->db2};
+    size_t sizes[] = {(size_t)(ns + ks), nvk, nvk, nvk, nb, nb, 2 * nb,
+                      nband, nband, nband, nband, nband, nband, nband};
+    for (int q = 0; q < 14; q++) {
+        cudaError_t e = cudaMalloc((void **)bufs[q], sizes[q] * sizeof(double));
+        if (e != cudaSuccess) { bsrg_basis_free(b); return cuda_fail(e, "define_spline alloc"); }
+    }
+    cudaError_t e = cudaMemcpyAsync(b->t, t_host, sizeof(double) * (ns + ks), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) { bsrg_basis_free(b); return cuda_fail(e, "define_spline copy"); }
+    int rc = launch_basis_tables(b, s);
+    if (rc != BSRG_OK) { bsrg_basis_free(b); return rc; }
+    *out = b;
+    return BSRG_OK;
+}
+
+int bsrg_basis_free(bsrg_basis *b)
+{
+    if (!b) return BSRG_OK;
+    double *bufs[] = {b->t, b->gr, b->grm, b->grw, b->bsp, b->bsq, b->bspd,
+                      b->sb, b->r1, b->rm1, b->rm2, b->rm3, b->db1, b->db2};
+    for (double *p : bufs)
+        if (p) cudaFree(p);
+    delete b;
+    return BSRG_OK;
+}
+
+int bsrg_basis_dims(const bsrg_basis *b, int *dims)
+{
+    CHECK_ARG(b && dims, "basis_dims: null argument");
+    dims[0] = b->ks; dims[1] = b->ns; dims[2] = b->nv; dims[3] = b->ml; dims[4] = b->me;
+    return BSRG_OK;
+}
+
+int bsrg_basis_get(const bsrg_basis *b, int which, double *dst, void *stream)
+{
+    CHECK_ARG(b && dst, "basis_get: null argument");
+    size_t nvk = (size_t)b->nv * b->ks, nb = (size_t)(b->nv + 1) * b->ks * b->ks,
+           nband = (size_t)b->ns * b->ks;
+    const double *src;
+    size_t n;
+    switch (which) {
+    case 0: src = b->gr; n = nvk; break;
+    case 1: src = b->grm; n = nvk; break;
+    case 2: src = b->grw; n = nvk; break;
+    case 3: src = b->bsp; n = nb; break;
+    case 4: src = b->bsq; n = nb; break;
+    case 5: src = b->bspd; n = 2 * nb; break;
+    case 6: src = b->sb; n = nband; break;
+    case 7: src = b->r1; n = nband; break;
+    case 8: src = b->rm1; n = nband; break;
+    case 9: src = b->rm2; n = nband; break;
+    case 10: src = b->rm3; n = nband; break;
+    case 11: src = b->db1; n = nband; break;
+    case 12: src = b->db2; n = nband; break;
+    case 13: src = b->t; n = (size_t)(b->ns + b->ks); break;
+    default: set_error("basis_get: unknown array %d", which); return BSRG_ERR_ARG;
+    }
+    return cuda_fail(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     (cudaStream_t)stream), "basis_get");
+}
+
+int bsrg_mrm(const bsrg_basis *b, int mm, double *rm, void *stream)
+{
+    CHECK_ARG(b && rm, "mrm: null argument");
+    return launch_mrm(b, mm, rm, (cudaStream_t)stream);
+}
+
+int bsrg_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream)
+{
+    CHECK_ARG(b, "rk_moments: null basis");
+    CHECK_ARG(k >= 0 && k <= 64, "rk_moments: k=%d out of range", k);
+    return launch_rk_moments(b, k, rkd1, rkd2, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_mrk_cell_from_moments(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                               double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkd1 && rkd2 && rkd && rkb, "mrk_cell: null argument");
+    CHECK_ARG(ldp >= b->ks, "mrk_cell: ldp=%d < ks=%d", ldp, b->ks);
+    return launch_mrk_cell(b, rkd1, rkd2, rkd, rkb, ldp, (cudaStream_t)stream);
+}
+
+int bsrg_mrk_cell(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkb, "mrk_cell: null argument");
+    CHECK_ARG(ldp >= b->ks, "mrk_cell: ldp=%d < ks=%d", ldp, b->ks);
+    CHECK_ARG(k >= 0 && k <= 64, "mrk_cell: k=%d out of range", k);
+    cudaStream_t s = (cudaStream_t)stream;
+    int ik = ik_of(b->ks);
+    size_t n1 = (size_t)ik * b->nv, n3 = (size_t)ik * ik * b->nv;
+    double *buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * n1 + n3) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "mrk_cell scratch");
+    int rc = launch_rk_moments(b, k, buf, buf + n1, buf + 2 * n1, s);
+    if (rc == BSRG_OK) rc = launch_mrk_cell(b, buf, buf + n1, buf + 2 * n1, rkb, ldp, s);
+    cudaFreeAsync(buf, s);
+    return rc;
+}
+
+int bsrg_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, void *stream)
+{
+    CHECK_ARG(d && p1 && p2, "density: null argument");
+    CHECK_ARG(ns >= ks && ks >= 1, "density: bad ns/ks");
+    CHECK_ARG(type == 's' || type == 'n' || type == 'x', "density: unknown type '%c'", type);
+    return launch_density(ns, ks, d, p1, p2, type, (cudaStream_t)stream);
+}
+
+int bsrg_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp, int icase, char sym_i,
+                char sym_j, void *stream)
+{
+    CHECK_ARG(a && d && rkb, "convol: null argument");
+    CHECK_ARG(ns >= ks && ks >= 1, "convol: bad ns/ks");
+    if (!((sym_i == 's' || sym_i == 'n') && (sym_j == 's' || sym_j == 'n') && icase >= 1 && icase <= 4)) {
+        set_error(" CONVOL:  unknown case (icase=%d sym_i=%c sym_j=%c)", icase, sym_i, sym_j);
+        return BSRG_ERR_CASE;
+    }
+    int need = (sym_i == 'n' || sym_j == 'n') ? 2 * ks - 1 : ks;
+    CHECK_ARG(ldp >= need, "convol: ldp=%d < %d", ldp, need);
+    return launch_convol(ns, ks, a, d, rkb, ldp, icase, sym_i, sym_j, (cudaStream_t)stream);
+}
+
+int bsrg_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, void *stream)
+{
+    CHECK_ARG(a && b && out, "sum_amb: null argument");
+    if (!(sym == 's' || sym == 'l' || sym == 'n' || sym == 'x')) {
+        set_error(" SUM_AmB:  unknown symmetry '%c'", sym);
+        return BSRG_ERR_CASE;
+    }
+    return launch_sum_amb(ns, ks, a, b, sym, out, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,58 @@
+// bsrg_ctx: stream, solver handles and a growable device workspace.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <vector>
+
+#include "bsrg_internal.h"
+
+struct bsrg_stage_event {
+    int stage;
+    cudaEvent_t start, stop;
+};
+
+struct bsrg_ctx {
+    int device;
+    cudaStream_t stream;
+    cublasHandle_t blas;
+    cusolverDnHandle_t solver;
+    void *ws;                 // device workspace
+    size_t ws_bytes;
+    void *pinned;             // pinned host staging buffer
+    size_t pinned_bytes;
+    cudaEvent_t ev_stage;     // guards reuse of the pinned buffer
+    // stage timing (off unless bsrg_ctx_set_timing)
+    int timing;
+    std::vector<bsrg_stage_event> *events;   // recorded, not yet read
+    std::vector<cudaEvent_t> *pool;          // free events
+    double stage_ms[BSRG_NSTAGE];
+    int stage_launches[BSRG_NSTAGE];
+};
+
+namespace bsrg {
+
+// carve aligned sub-buffers out of one allocation
+struct Arena {
+    char *base;
+    size_t off, cap;
+    template <class T> T *take(size_t n)
+    {
+        off = (off + 255) & ~(size_t)255;
+        T *p = (T *)(base + off);
+        off += n * sizeof(T);
+        return p;
+    }
+};
+
+// make sure the context workspace holds at least `bytes`; synchronises the
+// stream before replacing a smaller buffer.
+int ctx_reserve(bsrg_ctx *c, size_t bytes);
+int ctx_reserve_pinned(bsrg_ctx *c, size_t bytes);
+
+// stage timing helpers: no-ops unless timing is on
+void stage_begin(bsrg_ctx *c, int stage);
+void stage_end(bsrg_ctx *c, int stage, int launches = 1);
+int stage_collect(bsrg_ctx *c);   // waits for recorded events and accumulates
+
+}  // namespace bsrg

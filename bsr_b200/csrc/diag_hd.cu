@@ -1,0 +1,391 @@
+// bsr_hd's diagonalisation of one partial wave on the GPU.
+//
+// Reference: src/bsr/BSR_HD3/diag_hd.f90 for the case the assembly produces,
+// an overlap S = blockdiag(sb) (diag_ovl /= 0, "reduced to a STANDARD
+// eigenvalue problem", :68-71):
+//   1. per channel, drop the first l+1 splines (l capped at ks-2, :83) and the
+//      last one if itype = -1, DSYGV('V','U') of (H_ii, S_ii) (:82-111);
+//      keep eigenpairs with w <= Edmax (if Edmax /= 0) and |w| >= Egap;
+//   2. A = diag(bval) + bb_i^T H_ij bb_j for every stored off-diagonal block
+//      (:188-219);
+//   3. DSYEV('V','L') of A (:312, LAPACK_calls.f90:54).
+// Step 1 runs cuSOLVER's sygvd per channel, the filter and compaction run on
+// the device (one small host read of the per-channel counts fixes khm), step 2
+// is two batched FP64 GEMMs over all blocks, step 3 is cuSOLVER's syevd.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+
+namespace bsrg {
+
+// AA[ich](r,c) = H_ii(s0+r, s0+c), CC[ich](r,c) = sb(s0+r, s0+c), leading dimension ns
+__global__ void extract_channel_kernel(int ns, int ks, const int *__restrict__ s0v, const int *__restrict__ nsolv,
+                                       const double *__restrict__ hcc, const double *__restrict__ sb,
+                                       double *AA, double *CC)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ns) return;
+    int r = tid % ns, c = tid / ns;
+    int s0 = s0v[ich], n = nsolv[ich];
+    size_t o = (size_t)ich * ns * ns + tid;
+    if (r >= n || c >= n) { AA[o] = 0.0; CC[o] = 0.0; return; }
+    int i = s0 + r, j = s0 + c;
+    const double *H = hcc + ((size_t)(ich + 1) * (ich + 2) / 2 - 1) * ns * ns;
+    AA[o] = H[i + (size_t)ns * j];
+    int hi = i > j ? i : j, lo = i > j ? j : i;
+    double sv = 0.0;
+    if (hi - lo < ks) sv = sb[hi + (size_t)ns * (lo - hi + ks - 1)];
+    CC[o] = sv;
+}
+
+__global__ void keep_count_kernel(int ns, int nch, const int *__restrict__ nsolv, const double *__restrict__ W,
+                                  double edmax, double egap, int *counts)
+{
+    int ich = blockIdx.x;
+    if (ich >= nch) return;
+    int n = nsolv[ich], cnt = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double w = W[(size_t)ich * ns + i];
+        bool keep = !(edmax != 0.0 && w > edmax) && !(egap > 0.0 && fabs(w) < egap);
+        cnt += keep;
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    __shared__ int part[32];
+    if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int q = 0; q < (int)(blockDim.x + 31) / 32; q++) s += part[q];
+        counts[ich] = s;
+    }
+}
+
+// bval[ipsol[ich]+q] and BB[ich](:, q) for the q-th kept solution (ascending order kept)
+__global__ void compact_kernel(int ns, const int *__restrict__ s0v, const int *__restrict__ nsolv,
+                               const int *__restrict__ ipsol, const double *__restrict__ W,
+                               const double *__restrict__ AA, double edmax, double egap, double *bval, double *BB)
+{
+    int ich = blockIdx.x;
+    __shared__ int rank[1024];
+    int n = nsolv[ich], s0 = s0v[ich];
+    if (threadIdx.x == 0) {
+        int q = 0;
+        for (int i = 0; i < n; i++) {
+            double w = W[(size_t)ich * ns + i];
+            bool keep = !(edmax != 0.0 && w > edmax) && !(egap > 0.0 && fabs(w) < egap);
+            rank[i] = keep ? q++ : -1;
+        }
+    }
+    __syncthreads();
+    double *B = BB + (size_t)ich * ns * ns;
+    // zero the whole padded block first
+    for (int q = threadIdx.x; q < ns * ns; q += blockDim.x) B[q] = 0.0;
+    __syncthreads();
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        int r = q % n, i = q / n;
+        int dst = rank[i];
+        if (dst < 0) continue;
+        B[(s0 + r) + (size_t)ns * dst] = AA[(size_t)ich * ns * ns + r + (size_t)ns * i];
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (rank[i] >= 0) bval[ipsol[ich] + rank[i]] = W[(size_t)ich * ns + i];
+}
+
+struct BlockMap { int ic, jc; };   // 0-based channels, ic > jc
+
+__global__ void scatter_blocks_kernel(int ns, long lda, const BlockMap *__restrict__ bm, const int *__restrict__ ipsol,
+                                      const double *__restrict__ T, double *A)
+{
+    int b = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ns) return;
+    int r = tid % ns, c = tid / ns;
+    BlockMap m = bm[b];
+    int nr = ipsol[m.ic + 1] - ipsol[m.ic], nc = ipsol[m.jc + 1] - ipsol[m.jc];
+    if (r >= nr || c >= nc) return;
+    A[(size_t)(ipsol[m.ic] + r) + (size_t)lda * (ipsol[m.jc] + c)] = T[(size_t)b * ns * ns + tid];
+}
+
+__global__ void set_diag_kernel(long n, const double *__restrict__ bval, double *A)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) A[i + n * i] = bval[i];
+}
+
+}  // namespace bsrg
+
+using namespace bsrg;
+
+extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                            int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
+                            double *eval, int *khm_out, double *vecs, double *bbout)
+{
+    if (!c || !b || !lch || !hcc || !eval || !khm_out) {
+        set_error("diag_hd: null argument");
+        return BSRG_ERR_ARG;
+    }
+    if (nch < 1) { set_error("diag_hd: nch=%d", nch); return BSRG_ERR_ARG; }
+    const int ns = b->ns, ks = b->ks;
+    if (ns > 1024) { set_error("diag_hd: ns=%d above 1024", ns); return BSRG_ERR_ARG; }
+    cudaStream_t s = c->stream;
+    cudaError_t e;
+    // ---- per-channel geometry (diag_hd.f90:83-86) ----
+    std::vector<int> s0v(nch), nsolv(nch);
+    for (int ich = 0; ich < nch; ich++) {
+        int l = lch[ich];
+        if (l > ks - 2) l = ks - 2;
+        if (ilzero == 0) l = 0;
+        int i1 = l + 2, i2 = ns;
+        if (itype == -1) i2 = ns - ibzero;
+        s0v[ich] = i1 - 1;
+        nsolv[ich] = i2 - i1 + 1;
+        if (nsolv[ich] < 1) { set_error("diag_hd: channel %d has no solutions", ich + 1); return BSRG_ERR_ARG; }
+    }
+    int nb = nch * (nch - 1) / 2;
+    std::vector<BlockMap> bmap;
+    bmap.reserve(nb);
+    for (int ic = 1; ic < nch; ic++)
+        for (int jc = 0; jc < ic; jc++) bmap.push_back({ic, jc});
+    // ---- workspace: phase 1 ----
+    size_t nn = (size_t)ns * ns;
+    int lwork1 = 0;
+    if (cusolverDnDsygvd_bufferSize(c->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER,
+                                    ns, nullptr, ns, nullptr, ns, nullptr, &lwork1) != CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: sygvd_bufferSize failed");
+        return BSRG_ERR_SOLVER;
+    }
+    // worst case khm for sizing the dense phase up front
+    int khm_max = 0;
+    for (int ich = 0; ich < nch; ich++) khm_max += nsolv[ich];
+    cusolverDnParams_t params;
+    if (cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: cusolverDnCreateParams failed");
+        return BSRG_ERR_SOLVER;
+    }
+    cusolverEigMode_t jobz = want_vectors ? CUSOLVER_EIG_MODE_VECTOR : CUSOLVER_EIG_MODE_NOVECTOR;
+    size_t dws = 0, hws = 0;
+    if (cusolverDnXsyevd_bufferSize(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm_max, CUDA_R_64F, nullptr,
+                                    khm_max, CUDA_R_64F, nullptr, CUDA_R_64F, &dws, &hws) != CUSOLVER_STATUS_SUCCESS) {
+        cusolverDnDestroyParams(params);
+        set_error("diag_hd: syevd_bufferSize failed");
+        return BSRG_ERR_SOLVER;
+    }
+    size_t need = 0;
+    auto add = [&](size_t bytes) { need += ((bytes + 255) & ~(size_t)255) + 256; };
+    add(sizeof(int) * nch * 3 + 64);      // s0, nsol, counts
+    add(sizeof(int) * (nch + 1));         // ipsol
+    add(sizeof(int) * (nch + 1));         // infos
+    add(sizeof(double) * nn * nch * 3);   // AA, CC, BB
+    add(sizeof(double) * (size_t)ns * nch * 2);  // W, bval
+    add(sizeof(double) * (size_t)lwork1);
+    add(sizeof(BlockMap) * std::max(nb, 1));
+    add(sizeof(double *) * std::max(nb, 1) * 6);
+    add(sizeof(double) * nn * std::max(nb, 1) * 2);   // Wt, T
+    if (!vecs) add(sizeof(double) * (size_t)khm_max * khm_max);
+    add(dws + 16);
+    int rc = ctx_reserve(c, need);
+    if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
+    // pinned staging layout (ints): s0 | nsol | info | cnt | ipsol | final info, then block maps and pointers
+    const size_t o_s0 = 0, o_nsol = nch, o_info = 2 * (size_t)nch, o_cnt = 3 * (size_t)nch, o_ip = 4 * (size_t)nch,
+                 o_fin = 5 * (size_t)nch + 1;
+    size_t o_bm_bytes = ((o_fin + 1) * sizeof(int) + 15) & ~(size_t)15;
+    size_t o_ptr_bytes = (o_bm_bytes + sizeof(BlockMap) * nb + 15) & ~(size_t)15;
+    rc = ctx_reserve_pinned(c, o_ptr_bytes + sizeof(double *) * nb * 5 + 64);
+    if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
+    Arena ar{(char *)c->ws, 0, c->ws_bytes};
+    int *d_s0 = ar.take<int>(nch), *d_nsol = ar.take<int>(nch), *d_cnt = ar.take<int>(nch);
+    int *d_ipsol = ar.take<int>(nch + 1), *d_info = ar.take<int>(nch + 1);
+    double *AA = ar.take<double>(nn * nch), *CC = ar.take<double>(nn * nch), *BB = ar.take<double>(nn * nch);
+    double *Wv = ar.take<double>((size_t)ns * nch), *bval = ar.take<double>((size_t)ns * nch);
+    double *work1 = ar.take<double>(std::max(lwork1, 1));
+    BlockMap *d_bm = ar.take<BlockMap>(std::max(nb, 1));
+    double **d_ptrs = ar.take<double *>((size_t)std::max(nb, 1) * 6);
+    double *Wt = ar.take<double>(nn * std::max(nb, 1)), *T = ar.take<double>(nn * std::max(nb, 1));
+    double *Abuf = vecs ? nullptr : ar.take<double>((size_t)khm_max * khm_max);
+    void *dwork = ar.take<char>(dws + 16);
+    int *hi = (int *)c->pinned;
+    std::memcpy(hi + o_s0, s0v.data(), sizeof(int) * nch);
+    std::memcpy(hi + o_nsol, nsolv.data(), sizeof(int) * nch);
+    if ((e = cudaMemcpyAsync(d_s0, hi + o_s0, sizeof(int) * nch, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d_nsol, hi + o_nsol, sizeof(int) * nch, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+        cusolverDnDestroyParams(params);
+        return cuda_fail(e, "diag_hd upload");
+    }
+    // ---- 1. channel problems ----
+    stage_begin(c, 4);
+    {
+        dim3 g((unsigned)((nn + 127) / 128), nch);
+        extract_channel_kernel<<<g, 128, 0, s>>>(ns, ks, d_s0, d_nsol, hcc, b->sb, AA, CC);
+    }
+    for (int ich = 0; ich < nch; ich++) {
+        cusolverStatus_t st = cusolverDnDsygvd(c->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                               CUBLAS_FILL_MODE_UPPER, nsolv[ich], AA + nn * ich, ns, CC + nn * ich,
+                                               ns, Wv + (size_t)ns * ich, work1, lwork1, d_info + ich);
+        if (st != CUSOLVER_STATUS_SUCCESS) {
+            cusolverDnDestroyParams(params);
+            set_error("diag_hd: sygvd failed to launch for channel %d (status %d)", ich + 1, (int)st);
+            return BSRG_ERR_SOLVER;
+        }
+    }
+    keep_count_kernel<<<nch, 256, 0, s>>>(ns, nch, d_nsol, Wv, edmax, egap, d_cnt);
+    stage_end(c, 4, 2);   // extract + keep_count (the sygvd calls are cuSOLVER's)
+    if ((e = cudaMemcpyAsync(hi + o_info, d_info, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(hi + o_cnt, d_cnt, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
+        cusolverDnDestroyParams(params);
+        return cuda_fail(e, "diag_hd readback");
+    }
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) {
+        cusolverDnDestroyParams(params);
+        return cuda_fail(e, "diag_hd channel solves");
+    }
+    for (int ich = 0; ich < nch; ich++)
+        if (hi[o_info + ich] != 0) {
+            cusolverDnDestroyParams(params);
+            set_error("BSR_HD: channel diagonalization failed, channel = %d (info %d)", ich + 1, hi[o_info + ich]);
+            return BSRG_ERR_INFO;
+        }
+    std::vector<int> ipsol(nch + 1, 0);
+    for (int ich = 0; ich < nch; ich++) ipsol[ich + 1] = ipsol[ich] + hi[o_cnt + ich];
+    const int khm = ipsol[nch];
+    *khm_out = khm;
+    if (khm == 0) {
+        cusolverDnDestroyParams(params);
+        set_error("diag_hd: no channel solutions survive the filter");
+        return BSRG_ERR_INFO;
+    }
+    const size_t dws_cap = dws;
+    if (cusolverDnXsyevd_bufferSize(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm, CUDA_R_64F, nullptr, khm,
+                                    CUDA_R_64F, nullptr, CUDA_R_64F, &dws, &hws) != CUSOLVER_STATUS_SUCCESS ||
+        dws > dws_cap) {
+        cusolverDnDestroyParams(params);
+        set_error("diag_hd: syevd_bufferSize failed");
+        return BSRG_ERR_SOLVER;
+    }
+    size_t asz = (size_t)khm * khm;
+    double *A = vecs ? vecs : Abuf;
+    std::vector<char> hwork(hws + 16);
+    // ---- compaction ----
+    int *h_ip = hi + o_ip;
+    std::memcpy(h_ip, ipsol.data(), sizeof(int) * (nch + 1));
+    BlockMap *h_bm = (BlockMap *)((char *)c->pinned + o_bm_bytes);
+    if (nb > 0) std::memcpy(h_bm, bmap.data(), sizeof(BlockMap) * nb);
+    double **h_ptrs = (double **)((char *)c->pinned + o_ptr_bytes);
+    for (int q = 0; q < nb; q++) {
+        const BlockMap &m = bmap[q];
+        h_ptrs[q] = (double *)(hcc + ((size_t)(m.ic + 1) * m.ic / 2 + m.jc) * nn);   // H_ij, i = ic+1 (1-based)
+        h_ptrs[nb + q] = BB + nn * m.jc;
+        h_ptrs[2 * nb + q] = Wt + nn * q;
+        h_ptrs[3 * nb + q] = BB + nn * m.ic;
+        h_ptrs[4 * nb + q] = T + nn * q;
+    }
+    if ((e = cudaMemcpyAsync(d_ipsol, h_ip, sizeof(int) * (nch + 1), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+        cusolverDnDestroyParams(params);
+        return cuda_fail(e, "diag_hd ipsol upload");
+    }
+    if (nb > 0) {
+        if ((e = cudaMemcpyAsync(d_bm, h_bm, sizeof(BlockMap) * nb, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_ptrs, h_ptrs, sizeof(double *) * nb * 5, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+            cusolverDnDestroyParams(params);
+            return cuda_fail(e, "diag_hd block upload");
+        }
+    }
+    cudaEventRecord(c->ev_stage, s);
+    stage_begin(c, 5);
+    compact_kernel<<<nch, 256, 0, s>>>(ns, d_s0, d_nsol, d_ipsol, Wv, AA, edmax, egap, bval, BB);
+    // ---- 2. A = diag(bval) + bb^T H_ij bb ----
+    if ((e = cudaMemsetAsync(A, 0, sizeof(double) * asz, s)) != cudaSuccess) {
+        cusolverDnDestroyParams(params);
+        return cuda_fail(e, "memset A");
+    }
+    set_diag_kernel<<<(khm + 255) / 256, 256, 0, s>>>(khm, bval, A);
+    if (nb > 0) {
+        const double one = 1.0, zero = 0.0;
+        double **pH = d_ptrs, **pBj = d_ptrs + nb, **pW = d_ptrs + 2 * nb, **pBi = d_ptrs + 3 * nb,
+               **pT = d_ptrs + 4 * nb;
+        cublasStatus_t bs1 = cublasDgemmBatched(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, ns, ns, ns, &one,
+                                                (const double *const *)pH, ns, (const double *const *)pBj, ns,
+                                                &zero, pW, ns, nb);
+        cublasStatus_t bs2 = cublasDgemmBatched(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, ns, ns, ns, &one,
+                                                (const double *const *)pBi, ns, (const double *const *)pW, ns,
+                                                &zero, pT, ns, nb);
+        if (bs1 != CUBLAS_STATUS_SUCCESS || bs2 != CUBLAS_STATUS_SUCCESS) {
+            cusolverDnDestroyParams(params);
+            set_error("diag_hd: block transform GEMM failed (%d, %d)", (int)bs1, (int)bs2);
+            return BSRG_ERR_SOLVER;
+        }
+        dim3 g((unsigned)((nn + 127) / 128), nb);
+        scatter_blocks_kernel<<<g, 128, 0, s>>>(ns, khm, d_bm, d_ipsol, T, A);
+    }
+    stage_end(c, 5, nb > 0 ? 3 : 2);   // compact, set_diag, scatter (GEMMs are cuBLAS's)
+    // ---- 3. eigensolve ----
+    stage_begin(c, 6);
+    cusolverStatus_t st = cusolverDnXsyevd(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm, CUDA_R_64F, A, khm,
+                                           CUDA_R_64F, eval, CUDA_R_64F, dwork, dws, hwork.data(), hws,
+                                           d_info + nch);
+    cusolverDnDestroyParams(params);
+    stage_end(c, 6, 0);
+    if (st != CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: syevd failed to launch (status %d)", (int)st);
+        return BSRG_ERR_SOLVER;
+    }
+    if (bbout && (e = cudaMemcpyAsync(bbout, BB, sizeof(double) * nn * nch, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd bb copy");
+    if ((e = cudaMemcpyAsync(hi + o_fin, d_info + nch, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd info");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diag_hd syevd");
+    int hinfo = hi[o_fin];
+    if (hinfo != 0) {
+        set_error("LAP_DSYEV: DSYEV(lapack) gives INFO = %d", hinfo);
+        return BSRG_ERR_INFO;
+    }
+    return stage_collect(c);
+}
+
+// whole path with host buffers: bsr_mat SUB1 followed by bsr_hd's diag_hd
+extern "C" int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double *t, double z, int nch,
+                                       const int *lch, const double *ech, int norb, const double *P, int kmax,
+                                       int ncoef, const int *ck, const int *ctype, const int *cich,
+                                       const int *cjch, const int *ca, const int *cb, const double *cval,
+                                       int want_vectors, double *eval, int *khm)
+{
+    if (!c || !t || !P || !eval || !khm) { set_error("partial_wave_solve: null argument"); return BSRG_ERR_ARG; }
+    cudaStream_t s = c->stream;
+    bsrg_basis *b = nullptr;
+    int rc = bsrg_define_spline(ks, ns, t, 0, 0, 0.0, s, &b);
+    if (rc != BSRG_OK) return rc;
+    size_t nn = (size_t)ns * ns, nblk = (size_t)nch * (nch + 1) / 2;
+    double *dP = nullptr, *hcc = nullptr, *dev_eval = nullptr;
+    cudaError_t e;
+    if ((e = cudaMallocAsync((void **)&dP, sizeof(double) * ns * norb, s)) != cudaSuccess ||
+        (e = cudaMallocAsync((void **)&hcc, sizeof(double) * nn * nblk, s)) != cudaSuccess ||
+        (e = cudaMallocAsync((void **)&dev_eval, sizeof(double) * (size_t)nch * ns, s)) != cudaSuccess) {
+        rc = cuda_fail(e, "partial_wave_solve alloc");
+    }
+    if (rc == BSRG_OK && (e = cudaMemcpyAsync(dP, P, sizeof(double) * ns * norb, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        rc = cuda_fail(e, "partial_wave_solve upload");
+    if (rc == BSRG_OK)
+        rc = bsrg_assemble(c, b, z, nch, lch, ech, norb, dP, kmax, ncoef, ck, ctype, cich, cjch, ca, cb, cval, hcc,
+                           nullptr, nullptr);
+    double *vecs = nullptr;
+    if (rc == BSRG_OK && want_vectors) {
+        size_t n = (size_t)nch * ns;
+        if ((e = cudaMallocAsync((void **)&vecs, sizeof(double) * n * n, s)) != cudaSuccess)
+            rc = cuda_fail(e, "partial_wave_solve vecs");
+    }
+    if (rc == BSRG_OK)
+        rc = bsrg_diag_hd(c, b, nch, lch, hcc, 0, 1, 1, 0.0, 0.001, want_vectors, dev_eval, khm, vecs, nullptr);
+    if (rc == BSRG_OK &&
+        (e = cudaMemcpyAsync(eval, dev_eval, sizeof(double) * (*khm), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        rc = cuda_fail(e, "partial_wave_solve download");
+    if (rc == BSRG_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "partial_wave_solve sync");
+    if (vecs) cudaFreeAsync(vecs, s);
+    if (dP) cudaFreeAsync(dP, s);
+    if (hcc) cudaFreeAsync(hcc, s);
+    if (dev_eval) cudaFreeAsync(dev_eval, s);
+    cudaStreamSynchronize(s);
+    bsrg_basis_free(b);
+    return rc;
+}

@@ -1,0 +1,440 @@
+// B-spline basis tables and R^k cell tables on the GPU.
+//
+// Replaces, for the reference's B-spline library (src/libs/BS):
+//   initvb  (define_spline.f90:67)  -> basis_points_kernel
+//   mdb1/mdb2/mrm (define_spline.f90:184,214, mrm.f90:2) -> band_kernel
+//   moments/moment (moments.f90:2,76) -> moments_kernel
+//   rk_triang/rk_pdiag (rk_moments.f90:56,105) -> diag_cell_kernel
+//   mrk_cell (mrk_cell.f90:2) -> rkb_expand_kernel
+//
+// This file is compiled with --fmad=false: every sum is accumulated in the
+// reference's order with separately rounded multiplies and adds, so the tables
+// equal the Fortran restatement's bit for bit.  All of it is one-shot or
+// HBM-write bound (the rkb expansion), so giving up FMA costs nothing measurable.
+#include "bsrg_internal.h"
+
+namespace bsrg {
+
+// de Boor's bsplvb/bsplvd (vbsplvd.f90:3,170) for one point.  left is the
+// 0-based knot index with t[left] <= x <= t[left+1].  db[j + k*m] = m-th
+// derivative of the j-th of the k B-splines nonzero on that interval.
+struct BvbState {
+    int j;
+    double deltal[BSRG_MAXKS + 1], deltar[BSRG_MAXKS + 1];
+};
+
+__device__ static void bsplvb_dev(const double *t, int jhigh, int index, double x, int left,
+                                           double *biatx, BvbState &st)
+{
+    if (index == 1) {
+        st.j = 1;
+        biatx[0] = 1.0;
+        if (st.j >= jhigh) return;
+    }
+    for (;;) {
+        int j = st.j, jp1 = j + 1;
+        st.deltar[j - 1] = t[left + j] - x;
+        st.deltal[j - 1] = x - t[left + 1 - j];
+        double saved = 0.0;
+        for (int i = 1; i <= j; i++) {
+            double term = biatx[i - 1] / (st.deltar[i - 1] + st.deltal[jp1 - i - 1]);
+            biatx[i - 1] = saved + st.deltar[i - 1] * term;
+            saved = st.deltal[jp1 - i - 1] * term;
+        }
+        biatx[jp1 - 1] = saved;
+        st.j = jp1;
+        if (st.j >= jhigh) break;
+    }
+}
+
+__device__ static void bsplvd_dev(const double *t, int k, double x, int left, int nderiv, double *db)
+{
+    BvbState st;
+    int mhigh = nderiv < k ? nderiv : k;
+    if (mhigh < 1) mhigh = 1;
+    int kp1 = k + 1;
+    bsplvb_dev(t, kp1 - mhigh, 1, x, left, db, st);
+    if (mhigh == 1) return;
+    int ideriv = mhigh;
+    for (int m = 2; m <= mhigh; m++) {
+        int jp1mid = 1;
+        for (int j = ideriv; j <= k; j++) {
+            db[(j - 1) + k * (ideriv - 1)] = db[jp1mid - 1];
+            jp1mid++;
+        }
+        ideriv--;
+        bsplvb_dev(t, kp1 - ideriv, 2, x, left, db, st);
+    }
+    double a[BSRG_MAXKS * BSRG_MAXKS];
+#define A(i, j) a[((i) - 1) + k * ((j) - 1)]
+    int jlow = 1;
+    for (int i = 1; i <= k; i++) {
+        for (int j = jlow; j <= k; j++) A(j, i) = 0.0;
+        jlow = i;
+        A(i, i) = 1.0;
+    }
+    for (int m = 2; m <= mhigh; m++) {
+        int kp1mm = kp1 - m;
+        double fk = (double)kp1mm;
+        int il = left, i = k;
+        for (int ld = 1; ld <= kp1mm; ld++) {
+            double factor = fk / (t[il + kp1mm] - t[il]);
+            for (int j = 1; j <= i; j++) A(i, j) = (A(i, j) - A(i - 1, j)) * factor;
+            il--;
+            i--;
+        }
+        for (int ii = 1; ii <= k; ii++) {
+            double sum = 0.0;
+            int jl = ii > m ? ii : m;
+            for (int j = jl; j <= k; j++) sum = sum + A(j, ii) * db[(j - 1) + k * (m - 1)];
+            db[(ii - 1) + k * (m - 1)] = sum;
+        }
+    }
+#undef A
+}
+
+// values of the ks B-splines at x (nderiv = 1), no derivative work array
+__device__ static void bspl_values(const double *t, int k, double x, int left, double *v)
+{
+    BvbState st;
+    bsplvb_dev(t, k, 1, x, left, v, st);
+}
+
+// ---------------------------------------------------------------------------
+// initvb: one thread per (interval, Gauss point); thread nv*ks does the last knot.
+// ---------------------------------------------------------------------------
+struct GaussRule { double x[BSRG_MAXKS], w[BSRG_MAXKS]; };
+
+__global__ void basis_points_kernel(int ks, int ns, int nv, const double *__restrict__ t, GaussRule g,
+                                    double *gr, double *grm, double *grw, double *bsp, double *bsq,
+                                    double *bspd)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    double db[BSRG_MAXKS * 3];
+    size_t ld = (size_t)(nv + 1);
+    if (tid < nv * ks) {
+        int iv = tid % nv, m = tid / nv;
+        double tl = t[iv + ks - 1], tr = t[iv + ks];
+        double x = (tr - tl) * g.x[m] + tl;
+        double xm = 1.0 / x;
+        gr[iv + (size_t)nv * m] = x;
+        grm[iv + (size_t)nv * m] = xm;
+        grw[iv + (size_t)nv * m] = (tr - tl) * g.w[m];
+        bsplvd_dev(t, ks, x, iv + ks - 1, 3, db);
+        for (int ith = 0; ith < ks; ith++) {
+            size_t o = iv + ld * (m + (size_t)ks * ith);
+            double v = db[ith], d1 = db[ith + ks], d2 = db[ith + 2 * ks];
+            bsp[o] = v;
+            bspd[o] = d1;
+            bspd[o + ld * ks * ks] = d2;
+            bsq[o] = d1 - xm * v;
+        }
+    } else if (tid == nv * ks) {
+        double x = t[ns];
+        bsplvd_dev(t, ks, x, ns - 1, 3, db);
+        for (int ith = 0; ith < ks; ith++) {
+            size_t o = nv + ld * (0 + (size_t)ks * ith);
+            double v = db[ith], d1 = db[ith + ks], d2 = db[ith + 2 * ks];
+            bsp[o] = v;
+            bspd[o] = d1;
+            bspd[o + ld * ks * ks] = d2;
+            bsq[o] = d1 - v / x;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Band operator matrices in lower-column storage, one thread per (irow, jcol):
+//   kind 0: <B_i|r^mm|B_j> (mrm.f90), kind 1: <B_i|B'_j> (mdb1), kind 2: <B_i|B''_j> (mdb2).
+// The reference accumulates over ith = 1..ks (outer loop) for a fixed element.
+// ---------------------------------------------------------------------------
+__device__ static double rpow_dev(double g, int p)
+{
+    double r = g;
+    for (int q = 1; q < p; q++) r = r * g;
+    return r;
+}
+
+__global__ void band_kernel(int ks, int ns, int nv, int kind, int mm, const double *__restrict__ gr,
+                            const double *__restrict__ grm, const double *__restrict__ grw,
+                            const double *__restrict__ bsp, const double *__restrict__ bspd, double *out)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ks) return;
+    int irow = tid % ns, jcol = tid / ns;
+    size_t ld = (size_t)(nv + 1);
+    double acc = 0.0;
+    for (int ith = 0; ith < ks; ith++) {
+        int iv = irow - ith;
+        int jth = jcol + ith - (ks - 1);
+        if (iv < 0 || iv >= nv || jth < 0 || jth > ith) continue;
+        double s = 0.0;
+        for (int m = 0; m < ks; m++) {
+            double w = grw[iv + (size_t)nv * m];
+            double bi = bsp[iv + ld * (m + (size_t)ks * ith)];
+            double wb = w * bi, v;
+            if (kind == 0) {
+                double bj = bsp[iv + ld * (m + (size_t)ks * jth)];
+                if (mm == 0) v = wb * bj;
+                else if (mm == -1) v = wb * grm[iv + (size_t)nv * m] * bj;
+                else if (mm <= -2) v = wb * rpow_dev(grm[iv + (size_t)nv * m], -mm) * bj;
+                else if (mm == 1) v = wb * gr[iv + (size_t)nv * m] * bj;
+                else v = wb * rpow_dev(gr[iv + (size_t)nv * m], mm) * bj;
+            } else {
+                double dj = bspd[iv + ld * (m + (size_t)ks * (jth + (size_t)ks * (kind - 1)))];
+                v = wb * dj;
+            }
+            s = s + v;
+        }
+        acc = acc + s;
+    }
+    if (kind == 2 && tid == 0) {
+        // db2(1,1) holds <B_{ns-1}|B''_{ns}> over the last interval (define_spline.f90:238)
+        int iv = nv - 1;
+        double s = 0.0;
+        for (int m = 0; m < ks; m++)
+            s = s + grw[iv + (size_t)nv * m] * bsp[iv + ld * (m + (size_t)ks * (ks - 2))] *
+                        bspd[iv + ld * (m + (size_t)ks * ((ks - 1) + (size_t)ks * 1))];
+        acc = acc + s;
+    }
+    out[irow + (size_t)ns * jcol] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// moments (moments.f90:2,76), sym 's', dir 'b': rkm(ii, iv), one thread each.
+// With me > 0 the geometric region repeats the reference's scaling chain
+// rkm(:,iv) = rkm(:,iv-1)*hp starting from the last directly computed cell.
+// ---------------------------------------------------------------------------
+__device__ static double moment_one(int ks, int nv, int iv, int k, int i, int j, const double *gr,
+                                    const double *grm, const double *grw, const double *bsp)
+{
+    size_t ld = (size_t)(nv + 1);
+    double s = 0.0;
+    for (int m = 0; m < ks; m++) {
+        double gw = grw[iv + (size_t)nv * m];
+        if (k > 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(gr[iv + (size_t)nv * m], k);
+        if (k < 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], -k);
+        double bj = bsp[iv + ld * (m + (size_t)ks * j)] * gw;
+        s = s + bsp[iv + ld * (m + (size_t)ks * i)] * bj;
+    }
+    return s;
+}
+
+__global__ void moments_kernel(int ks, int nv, int ml, int me, double hp, int k, const double *gr,
+                               const double *grm, const double *grw, const double *bsp, double *rkm)
+{
+    int ik = ks * (ks + 1) / 2;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ik * nv) return;
+    int ii = tid % ik, iv = tid / ik;
+    // unpack ii -> (i, j), i <= j
+    int i = 0, rem = ii;
+    while (rem >= ks - i) { rem -= ks - i; i++; }
+    int j = i + rem;
+    int iv1 = iv + 1;                        // 1-based
+    int s0 = ml + ks, s1 = ml + me - ks + 2;  // scaled range (1-based), empty when me == 0
+    double v;
+    if (me != 0 && iv1 >= s0 && iv1 <= s1) {
+        v = moment_one(ks, nv, s0 - 2, k, i, j, gr, grm, grw, bsp);
+        for (int q = s0; q <= iv1; q++) v = v * hp;
+    } else {
+        v = moment_one(ks, nv, iv, k, i, j, gr, grm, grw, bsp);
+    }
+    rkm[ii + (size_t)ik * iv] = v;
+}
+
+// ---------------------------------------------------------------------------
+// rk_triang (rk_moments.f90:105): one CTA per diagonal cell.  With me > 0 the
+// cells of the geometric region repeat rk_pdiag's chain rkd(iv) = rkd(iv-1)*(1+h).
+// ---------------------------------------------------------------------------
+__global__ void diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+                                 const double *__restrict__ t, GaussRule g, const double *gr,
+                                 const double *grm, const double *grw, const double *bsp, double *rkd)
+{
+    extern __shared__ double sm[];
+    const int ik = ks * (ks + 1) / 2;
+    double *bt = sm;                          // [m][i][j] : ks*ks*ks  B-spline values at inner points
+    double *wx = bt + ks * ks * ks;           // [m][i]   : weights * x^k at inner points
+    double *INT = wx + ks * ks;               // [m][jj]  : ks*ik
+    double *a = INT + ks * ik;                // [jj][ii] : ik*ik  (column-major a(ii,jj))
+    int iv_out = blockIdx.x;
+    int iv1 = iv_out + 1;
+    int s0 = ml + ks, s1 = ml + me - ks + 2;
+    int nscale = 0, iv = iv_out;
+    if (me != 0 && iv1 >= s0 && iv1 <= s1) { iv = s0 - 2; nscale = iv1 - s0 + 1; }
+    int left = iv + ks - 1;
+    double xbase = t[left];
+    size_t ld = (size_t)(nv + 1);
+    // inner points: for each outer Gauss point m, ks points on [t_left, gr(iv,m)]
+    for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) {
+        int m = q / ks, i = q % ks;
+        double span = gr[iv + (size_t)nv * m] - xbase;
+        double x = span * g.x[i] + xbase;
+        double v[BSRG_MAXKS];
+        bspl_values(t, ks, x, left, v);
+        for (int j = 0; j < ks; j++) bt[(m * ks + i) * ks + j] = v[j];
+        double w = span * g.w[i];
+        double xk;
+        if (k > 1) xk = w * rpow_dev(x, k);
+        else if (k == 1) xk = w * x;
+        else xk = w;
+        wx[m * ks + i] = xk;
+    }
+    __syncthreads();
+    // INT(j,jp,m) = SUM_i (wx_i * bt(i,j)) * bt(i,jp)
+    for (int q = threadIdx.x; q < ks * ik; q += blockDim.x) {
+        int m = q / ik, jj = q % ik;
+        int j = 0, rem = jj;
+        while (rem >= ks - j) { rem -= ks - j; j++; }
+        int jp = j + rem;
+        double s = 0.0;
+        for (int i = 0; i < ks; i++) {
+            double tmp = wx[m * ks + i] * bt[(m * ks + i) * ks + j];
+            s = s + tmp * bt[(m * ks + i) * ks + jp];
+        }
+        INT[m * ik + jj] = s;
+    }
+    __syncthreads();
+    // a(ii,jj) = SUM_m bi(m) * INT(jj,m), bi = bsp(i)*bsp(ip)*grw*grm^(k+1)
+    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
+        int ii = q % ik, jj = q / ik;
+        int i = 0, rem = ii;
+        while (rem >= ks - i) { rem -= ks - i; i++; }
+        int ip = i + rem;
+        double s = 0.0;
+        for (int m = 0; m < ks; m++) {
+            double g2;
+            if (k != 0) g2 = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], k + 1);
+            else g2 = grw[iv + (size_t)nv * m] * grm[iv + (size_t)nv * m];
+            double bi = bsp[iv + ld * (m + (size_t)ks * i)] * bsp[iv + ld * (m + (size_t)ks * ip)] * g2;
+            s = s + bi * INT[m * ik + jj];
+        }
+        a[ii + ik * jj] = s;
+    }
+    __syncthreads();
+    double *out = rkd + (size_t)ik * ik * iv_out;
+    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
+        int r = q % ik, c = q / ik;
+        double v = a[r + ik * c] + a[c + ik * r];
+        for (int n = 0; n < nscale; n++) v = v * hscale;
+        out[r + (size_t)ik * c] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mrk_cell (mrk_cell.f90:2): rkb(i,j,ip,jp) = sum over cells, jv outer and iv
+// inner in ascending order as the reference accumulates.  One thread per
+// element; threadIdx.x runs along i (the contiguous index).  Elements with
+// ip or jp >= ks (ldp > ks) or past the last spline are written as zero.
+// ---------------------------------------------------------------------------
+__global__ void rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rkd1,
+                                  const double *__restrict__ rkd2, const double *__restrict__ rkd,
+                                  double *__restrict__ rkb)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int ipjp = blockIdx.z;
+    int ip = ipjp % ldp, jp = ipjp / ldp;
+    if (i >= ns || j >= ns) return;
+    const int ik = ks * (ks + 1) / 2;
+    double acc = 0.0;
+    if (ip < ks && jp < ks && i + ip < ns && j + jp < ns) {
+        int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
+        int iv_hi = i < nv - 1 ? i : nv - 1;
+        int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = j < nv - 1 ? j : nv - 1;
+        for (int jv = jv_lo; jv <= jv_hi; jv++) {
+            int jh = j - jv;                       // 0-based position of B_j in cell jv
+            int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+            double r2j = rkd2[jj + (size_t)ik * jv];
+            double r1j = rkd1[jj + (size_t)ik * jv];
+            for (int iv = iv_lo; iv <= iv_hi; iv++) {
+                int ih = i - iv;
+                int ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                double c;
+                if (iv < jv) c = rkd1[ii + (size_t)ik * iv] * r2j;
+                else if (iv > jv) c = r1j * rkd2[ii + (size_t)ik * iv];
+                else c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                acc = acc + c;
+            }
+        }
+    }
+    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static GaussRule rule_of(const bsrg_basis *b)
+{
+    GaussRule g;
+    for (int i = 0; i < BSRG_MAXKS; i++) { g.x[i] = i < b->ks ? b->gx[i] : 0.0; g.w[i] = i < b->ks ? b->gw[i] : 0.0; }
+    return g;
+}
+
+int launch_basis_tables(bsrg_basis *b, cudaStream_t s)
+{
+    int n = b->nv * b->ks + 1;
+    basis_points_kernel<<<(n + 127) / 128, 128, 0, s>>>(b->ks, b->ns, b->nv, b->t, rule_of(b), b->gr, b->grm,
+                                                         b->grw, b->bsp, b->bsq, b->bspd);
+    int nb = b->ns * b->ks, bl = (nb + 127) / 128;
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 1, 0, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->db1);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 2, 0, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->db2);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, 0, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->sb);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, 1, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->r1);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, -1, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->rm1);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, -2, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->rm2);
+    band_kernel<<<bl, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, -3, b->gr, b->grm, b->grw, b->bsp, b->bspd, b->rm3);
+    return cuda_fail(cudaGetLastError(), "basis tables");
+}
+
+int launch_mrm(const bsrg_basis *b, int mm, double *rm, cudaStream_t s)
+{
+    int nb = b->ns * b->ks;
+    band_kernel<<<(nb + 127) / 128, 128, 0, s>>>(b->ks, b->ns, b->nv, 0, mm, b->gr, b->grm, b->grw, b->bsp,
+                                                 b->bspd, rm);
+    return cuda_fail(cudaGetLastError(), "mrm");
+}
+
+static double ipow_host(double q, int k)
+{
+    double hp = 1.0;
+    if (k >= 0) { for (int i = 0; i < k; i++) hp *= q; }
+    else { double p = 1.0; for (int i = 0; i < -k; i++) p *= q; hp = 1.0 / p; }
+    return hp;
+}
+
+int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s)
+{
+    int ks = b->ks, nv = b->nv, ik = ik_of(ks);
+    double q = 1.0 + b->h;
+    int n = ik * nv;
+    if (rkd1)
+        moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k) * q, k, b->gr,
+                                                       b->grm, b->grw, b->bsp, rkd1);
+    if (rkd2)
+        moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 1)) * q,
+                                                       -(k + 1), b->gr, b->grm, b->grw, b->bsp, rkd2);
+    if (rkd) {
+        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik + (size_t)ik * ik);
+        if (shm > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)shm);
+            if (e != cudaSuccess) return cuda_fail(e, "diag_cell smem");
+        }
+        diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
+                                             b->grm, b->grw, b->bsp, rkd);
+    }
+    return cuda_fail(cudaGetLastError(), "rk_moments");
+}
+
+int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                    double *rkb, int ldp, cudaStream_t s)
+{
+    dim3 blk(32, 8);
+    dim3 grd((b->ns + 31) / 32, (b->ns + 7) / 8, ldp * ldp);
+    rkb_expand_kernel<<<grd, blk, 0, s>>>(b->ks, b->ns, b->nv, ldp, rkd1, rkd2, rkd, rkb);
+    return cuda_fail(cudaGetLastError(), "mrk_cell");
+}
+
+}  // namespace bsrg

@@ -1,0 +1,165 @@
+/*
+ * bsr_b200.h -- C ABI of the B200 (sm_100a) implementation of the BSR radial,
+ * assembly and eigensolve hot path.
+ *
+ * Every entry point returns an int status (BSRG_OK = 0, negative on error) and
+ * never terminates the process; bsrg_last_error() gives the message of the
+ * last failure on the calling thread.  Array arguments keep the layouts of the
+ * reference's Fortran arrays (column-major, the first index fastest), so a
+ * Fortran ISO_C_BINDING shim can pass its module arrays through unchanged.
+ * Unless an argument says "host", pointers are device pointers and the call is
+ * asynchronous on the given stream (a cudaStream_t passed as void*; NULL is
+ * the legacy default stream).  Memory passed in is owned by the caller; the
+ * library never frees it.
+ *
+ * Each declaration cites the reference routine it stands behind (paths within
+ * the jagot/bsr tree).
+ */
+#ifndef BSR_B200_H
+#define BSR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSRG_OK            0
+#define BSRG_ERR_ARG      -1   /* bad argument (the reference's Stop on a range check) */
+#define BSRG_ERR_CUDA     -2   /* CUDA runtime error */
+#define BSRG_ERR_SOLVER   -3   /* cuSOLVER / cuBLAS error */
+#define BSRG_ERR_INFO     -4   /* factorisation failed (LAPACK info /= 0 in the reference) */
+#define BSRG_ERR_NOMEM    -5   /* device allocation failed */
+#define BSRG_ERR_CASE     -6   /* unknown convol / SUM_AmB case */
+
+typedef struct bsrg_basis bsrg_basis;   /* device-resident B-spline basis */
+typedef struct bsrg_ctx bsrg_ctx;       /* stream + solver handles + workspace */
+
+const char *bsrg_last_error(void);
+int bsrg_version(void);
+
+/* ---- knot grid: src/libs/BS/define_grid.f90:86 (mkgrid, grid_type 0) and
+ *      :213 (mkgrid1, grid_type 1).  Host only.  t (host) must hold cap
+ *      doubles; returns ns, ml, me and the adjusted h of spline_param. */
+int bsrg_mkgrid(int grid_type, int ks, double z, double h, double hmax, double rmax,
+                double *t, int cap, int *ns, int *ml, int *me, double *h_out);
+
+/* ---- basis: src/libs/BS/define_spline.f90:15 (define_spline: initvb :67,
+ *      initas :133, mdb1 :184, mdb2 :214, mrm.f90:2).  t is a host array of
+ *      ns+ks knots; ml, me, h are spline_param's (me > 0 enables the
+ *      scaling-law shortcut of moments.f90:45-61 and rk_moments.f90:74-91). */
+int bsrg_define_spline(int ks, int ns, const double *t_host, int ml, int me, double h,
+                       void *stream, bsrg_basis **out);
+int bsrg_basis_free(bsrg_basis *b);
+/* dims[0..4] = ks, ns, nv, ml, me (host) */
+int bsrg_basis_dims(const bsrg_basis *b, int *dims);
+/* Copy one module array to dst (device).  which: 0 gr, 1 grm, 2 grw (nv,ks);
+ * 3 bsp, 4 bsq (nv+1,ks,ks); 5 bspd (nv+1,ks,ks,2); 6 sb, 7 r1, 8 rm1, 9 rm2,
+ * 10 rm3, 11 db1, 12 db2 (ns,ks); 13 t (ns+ks). */
+int bsrg_basis_get(const bsrg_basis *b, int which, double *dst, void *stream);
+/* src/libs/BS/mrm.f90:2: <B_i|r^mm|B_j> band (ns,ks) into rm (device). */
+int bsrg_mrm(const bsrg_basis *b, int mm, double *rm, void *stream);
+
+/* ---- R^k cell moments: src/libs/BS/rk_moments.f90:2 (moments.f90:2 for
+ *      rkd1 = <B_i|r^k|B_j>, rkd2 = <B_i|r^-(k+1)|B_j> per interval, packed
+ *      ik = ks(ks+1)/2 pairs; rk_triang :105 for the diagonal cells).
+ *      rkd1, rkd2: (ik, nv); rkd: (ik, ik, nv).  Device. */
+int bsrg_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
+
+/* ---- R^k B-spline integral table: src/libs/BS/mrk_cell.f90:2.
+ *      rkb(i,j,ip,jp) = R^k(B_i B_j; B_{i+ip-1} B_{j+jp-1}), stored as
+ *      (ns, ns, ldp, ldp) with ldp >= ks (the reference's module array uses
+ *      ldp = 2ks-1); entries with ip or jp > ks are zero.  Device.  The
+ *      moments are computed into scratch that the call allocates and frees. */
+int bsrg_mrk_cell(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream);
+/* Same, from moments already computed by bsrg_rk_moments (no allocation). */
+int bsrg_mrk_cell_from_moments(const bsrg_basis *b, const double *rkd1, const double *rkd2,
+                               const double *rkd, double *rkb, int ldp, void *stream);
+
+/* ---- src/libs/BS/density.f90:2.  type 's' -> d (ns,ks); 'n' -> (ns,2ks-1);
+ *      'x' -> (ns,ns).  Device. */
+int bsrg_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, void *stream);
+
+/* ---- src/libs/BS/convol.f90:2.  a (ns, *) receives the contraction of rkb
+ *      (ns,ns,ldp,ldp) with d over electron 2 (icase 1), electron 1 (icase 2),
+ *      or the exchange pairings (icase 3, 4; a is then a full (ns,ns) matrix).
+ *      sym_i/sym_j in {'s','n'}; 'n' needs ldp >= 2ks-1.  Device. */
+int bsrg_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp,
+                int icase, char sym_i, char sym_j, void *stream);
+
+/* ---- src/libs/BS/sum_amb.f90:2.  *out (device, one double) = SUM(a*b) over
+ *      the storage mode sym in {'s','l','n','x'}. */
+int bsrg_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, void *stream);
+
+/* ---- context: stream, cuBLAS/cuSOLVER handles and a growable workspace. */
+int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out);
+int bsrg_ctx_destroy(bsrg_ctx *c);
+/* bytes of device workspace the context currently holds */
+size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c);
+/* Stage timing (the reference's per-stage CPU_time lines in mat_log / bsr_hd
+ * logs, sub1.f90:68-202): when on, the assembly and diagonalisation calls
+ * bracket each stage with CUDA events on the context stream and add the
+ * elapsed device time to per-stage totals; bsrg_ctx_stage_times copies the
+ * BSRG_NSTAGE totals (ms) and the counts of this library's own kernel launches
+ * (library calls such as cuSOLVER's are timed but not counted), then resets
+ * them.  Stages: 0 R^k cell moments, 1 direct groups, 2 exchange groups,
+ * 3 one-electron / overlap / symmetrisation, 4 channel eigenproblems,
+ * 5 block transforms, 6 dense eigensolve, 7 rkb expansion (mrk_cell). */
+#define BSRG_NSTAGE 8
+int bsrg_ctx_set_timing(bsrg_ctx *c, int on);
+int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n);
+
+/* ---- channel-block assembly of one partial wave (bsr_mat):
+ *      src/bsr/BSR_MAT3/sub1.f90:72-191 (SUB1), L_data.f90:131-150 and
+ *      l_core.f90:174-270 (one-electron block -1/2*hl_core, no closed shells),
+ *      I_data.f90:192-218 (Case 6..9 two-electron groups: density ->
+ *      convol -> UPDATE_HX), mod_intmat.f90:69,131,245 (UPDATE_HX/HL/CF).
+ *
+ *      H  = blockdiag(-1/2 hl_{l_ch} + E_ch sb) + sum over coefficient groups,
+ *      hcc (device) has nch(nch+1)/2 blocks of (ns,ns), block ij = i(i-1)/2+j
+ *      (1-based, i >= j), diagonal blocks symmetrised as in SUB1.
+ *      Coefficient records (host arrays, ncoef long) are sorted by
+ *      (k, type, ich, jch) exactly like the cmdata blocks of State_res:
+ *        ck    multipole 0..kmax
+ *        ctype 0 = direct  Rk(i . j .) (I_data jtype 6, jcase 1)
+ *              1 = exchange Rk(i . . j) (I_data jtype 8, jcase 3)
+ *        cich, cjch 1-based channels with cich >= cjch
+ *        ca, cb 0-based orbital columns of P (ns, norb) (device)
+ *        cval the angular coefficient
+ *      lch, ech: host arrays of channel l and target energy (EC = 0).
+ *      acf (device, (nch,nch,kmax+1)) or NULL receives UPDATE_CF's sums.
+ *      scc (device) or NULL receives the overlap blocks blockdiag(sb). */
+int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int *lch, const double *ech,
+                  int norb, const double *P, int kmax, int ncoef, const int *ck, const int *ctype,
+                  const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
+                  double *hcc, double *scc, double *acf);
+
+/* ---- src/bsr/BSR_HD3/diag_hd.f90:2-340 for a block-diagonal S (diag_ovl /= 0):
+ *      per-channel DSYGV on the diagonal blocks with the first l+1 splines
+ *      dropped (:82-111), Egap/Edmax filter, transform of the off-diagonal
+ *      blocks to the channel eigenbasis (:188-219), DSYEV('V','L') of the
+ *      khm x khm matrix (:312).
+ *      hcc (device) as written by bsrg_assemble; sb blocks are taken from b.
+ *      lch (host).  eval (device) must hold nch*ns doubles; *khm (host) gets
+ *      the dimension.  vecs (device, khm*khm, may be NULL): eigenvectors in the
+ *      channel eigenbasis (the reference's a(:,:) after DSYEV); bb (device,
+ *      (ns, nch*ns), may be NULL): the channel eigenbasis, columns packed.
+ *      want_vectors = 0 computes eigenvalues only. */
+int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                 int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
+                 double *eval, int *khm, double *vecs, double *bb);
+
+/* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
+ *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.
+ *      t (ns+ks), P (ns,norb), coefficient arrays as in bsrg_assemble, all
+ *      host; eval (host) must hold nch*ns doubles. */
+int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double *t, double z, int nch,
+                            const int *lch, const double *ech, int norb, const double *P, int kmax,
+                            int ncoef, const int *ck, const int *ctype, const int *cich, const int *cjch,
+                            const int *ca, const int *cb, const double *cval, int want_vectors,
+                            double *eval, int *khm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSR_B200_H */

@@ -1,0 +1,317 @@
+"""ctypes front end of the CPU oracle (oracle/liboracle.so) plus the diag_hd restatement.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's cpu_baseline / reference leg as the checker.  The product
+(bsr_b200/) never imports this module.
+
+The C part restates the reference's B-spline radial library (src/libs/BS) and
+the bsr_mat channel-block assembly (src/bsr/BSR_MAT3); the diag_hd part below
+restates src/bsr/BSR_HD3/diag_hd.f90 with scipy's LAPACK (DSYGV, DSYEV) as the
+stand-in for the system LAPACK the reference links.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_gauss.argtypes = [ctypes.c_int, _D, _D]
+        L.orc_mkgrid0.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4 + [_D, ctypes.c_int, _I, _I, _I, _D]
+        L.orc_mkgrid1.argtypes = L.orc_mkgrid0.argtypes
+        L.orc_basis_new.restype = ctypes.c_void_p
+        L.orc_basis_new.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.orc_basis_free.argtypes = [ctypes.c_void_p]
+        L.orc_basis_get.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
+        L.orc_mrm.argtypes = [ctypes.c_void_p, ctypes.c_int, _D]
+        L.orc_bhwf.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, _D]
+        L.orc_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_char, ctypes.c_char]
+        L.orc_rk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.orc_mrk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, ctypes.c_int]
+        L.orc_density.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, ctypes.c_char]
+        L.orc_convol.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_char, ctypes.c_char]
+        L.orc_sum_amb.restype = ctypes.c_double
+        L.orc_sum_amb.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, ctypes.c_char]
+        L.orc_bav.argtypes = [ctypes.c_int, ctypes.c_int, _D, _D, _D, ctypes.c_char, ctypes.c_char]
+        L.orc_bvmv.restype = ctypes.c_double
+        L.orc_bvmv.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_char, _D, _D]
+        L.orc_quadr.restype = ctypes.c_double
+        L.orc_quadr.argtypes = [ctypes.c_void_p, _D, _D, ctypes.c_int]
+        for f in ("orc_rk", "orc_rkd", "orc_rke", "orc_rkv"):
+            getattr(L, f).restype = ctypes.c_double
+            getattr(L, f).argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
+        L.orc_hl_full.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D]
+        L.orc_assemble.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _I, _D,
+                                   ctypes.c_int, _D, ctypes.c_int, _D,
+                                   ctypes.c_int, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D]
+        _LIB = L
+    return _LIB
+
+
+def build():
+    import subprocess
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_I)
+
+
+def gauss(k):
+    x = np.zeros(k)
+    w = np.zeros(k)
+    lib().orc_gauss(k, _p(x), _p(w))
+    return x, w
+
+
+def mkgrid(grid_type, ks, z, h, hmax, rmax):
+    """define_grid (define_grid.f90:2): returns dict(t, ns, ml, me, h)."""
+    cap = int((rmax * z / h + 1 + ks) * 2) + 4 * ks + 64
+    t = np.zeros(cap)
+    ns = ctypes.c_int()
+    ml = ctypes.c_int()
+    me = ctypes.c_int()
+    hh = ctypes.c_double()
+    f = lib().orc_mkgrid0 if grid_type == 0 else lib().orc_mkgrid1
+    rc = f(ks, z, h, hmax, rmax, _p(t), cap, ctypes.byref(ns), ctypes.byref(ml), ctypes.byref(me),
+           ctypes.byref(hh))
+    if rc != 0:
+        raise RuntimeError("mkgrid failed")
+    n = ns.value
+    return {"t": t[: n + ks].copy(), "ns": n, "ml": ml.value, "me": me.value, "h": hh.value, "ks": ks}
+
+
+class Basis:
+    """define_spline (define_spline.f90:15) state on the CPU."""
+
+    NAMES = {"gr": 0, "grm": 1, "grw": 2, "bsp": 3, "bsq": 4, "bspd": 5, "sb": 6, "r1": 7,
+             "rm1": 8, "rm2": 9, "rm3": 10, "db1": 11, "db2": 12, "gx": 13, "gw": 14}
+
+    def __init__(self, ks, t, ml=0, me=0, h=0.0):
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        self.ks = ks
+        self.ns = len(t) - ks
+        self.nv = self.ns - ks + 1
+        self.ml, self.me, self.h = ml, me, h
+        self.t = t
+        self._h = lib().orc_basis_new(ks, self.ns, _p(t), ml, me, h)
+        if not self._h:
+            raise ValueError("bad basis")
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.orc_basis_free(self._h)
+            self._h = None
+
+    def get(self, name):
+        ks, ns, nv = self.ks, self.ns, self.nv
+        shapes = {"gr": (ks, nv), "grm": (ks, nv), "grw": (ks, nv), "bsp": (ks, ks, nv + 1),
+                  "bsq": (ks, ks, nv + 1), "bspd": (2, ks, ks, nv + 1), "gx": (ks,), "gw": (ks,)}
+        shp = shapes.get(name, (ks, ns))
+        out = np.zeros(shp)
+        lib().orc_basis_get(self._h, self.NAMES[name], _p(out))
+        return out  # C-order view of the Fortran column-major array: reversed index order
+
+    def band(self, name):
+        """(ns, ks) Fortran band matrix as a numpy array indexed [i, jcol]."""
+        return self.get(name).T.copy()
+
+    def mrm(self, mm):
+        out = np.zeros((self.ks, self.ns))
+        lib().orc_mrm(self._h, mm, _p(out))
+        return out.T.copy()
+
+    def bhwf(self, n, l, z):
+        c = np.zeros(self.ns)
+        rc = lib().orc_bhwf(self._h, n, l, z, _p(c))
+        if rc != 0:
+            raise RuntimeError("bhwf: Cholesky failed")
+        return c
+
+    def rk_moments(self, k):
+        ik = self.ks * (self.ks + 1) // 2
+        rkd1 = np.zeros((self.nv, ik))
+        rkd2 = np.zeros((self.nv, ik))
+        rkd = np.zeros((self.nv, ik, ik))
+        lib().orc_rk_moments(self._h, k, _p(rkd1), _p(rkd2), _p(rkd))
+        # Fortran (ik,nv) and (ik,ik,nv) column-major -> return [iv, ii] and [iv, jj, ii]
+        return rkd1, rkd2, rkd
+
+    def mrk_cell(self, k, ldp=None):
+        """rkb (ns,ns,ldp,ldp) Fortran order, returned as a flat Fortran-ordered array."""
+        ldp = ldp or self.ks
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mrk_cell(self._h, k, _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
+
+    def quadr(self, p1, p2, m):
+        p1 = np.ascontiguousarray(p1, dtype=np.float64)
+        p2 = np.ascontiguousarray(p2, dtype=np.float64)
+        return lib().orc_quadr(self._h, _p(p1), _p(p2), m)
+
+    def hl_full(self, l, z):
+        out = np.zeros((self.ns, self.ns))
+        lib().orc_hl_full(self._h, l, z, _p(out))
+        return out.T.copy()
+
+
+def density(ns, ks, p1, p2, typ):
+    cols = {"s": ks, "n": 2 * ks - 1}.get(typ, ns)
+    d = np.zeros(ns * max(cols, ns))
+    lib().orc_density(ns, ks, _p(d), _p(np.ascontiguousarray(p1, dtype=np.float64)),
+                      _p(np.ascontiguousarray(p2, dtype=np.float64)), typ.encode())
+    return d.reshape((ns, -1), order="F")[:, :cols].copy(order="F")
+
+
+def convol(ns, ks, d, rkb, icase, sym_i, sym_j):
+    """convol.f90:2.  d (ns, *) Fortran-ordered; rkb (ns,ns,ldp,ldp) Fortran-ordered."""
+    ldp = rkb.shape[2]
+    dd = np.zeros((ns, ns), order="F")
+    dd[:, : d.shape[1]] = d
+    a = np.zeros((ns, ns), order="F")
+    rk = np.asfortranarray(rkb)
+    rc = lib().orc_convol(ns, ks, a.ctypes.data_as(_D), dd.ctypes.data_as(_D), rk.ctypes.data_as(_D),
+                          ldp, icase, sym_i.encode(), sym_j.encode())
+    if rc != 0:
+        raise ValueError("convol: unknown case")
+    return a
+
+
+def sum_amb(ns, ks, a, b, sym):
+    cols = ns
+    aa = np.zeros((ns, cols), order="F")
+    bb = np.zeros((ns, cols), order="F")
+    aa[:, : a.shape[1]] = a
+    bb[:, : b.shape[1]] = b
+    return lib().orc_sum_amb(ns, ks, aa.ctypes.data_as(_D), bb.ctypes.data_as(_D), sym.encode())
+
+
+def rk_routes(ns, ks, rkb, pi1, pj1, pi2, pj2):
+    """R^k(i1,j1;i2,j2) by the table (rk.f90), direct (rkd), exchange (rke) and vector (rkv) routes."""
+    rk = np.asfortranarray(rkb)
+    ldp = rkb.shape[2]
+    args = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
+    L = lib()
+    out = {}
+    for name, f in (("RK_cell", L.orc_rk), ("RKd", L.orc_rkd), ("RKe", L.orc_rke), ("RKv", L.orc_rkv)):
+        out[name] = f(ns, ks, rk.ctypes.data_as(_D), ldp, *[_p(a) for a in args])
+    return out
+
+
+def assemble(basis, z, lch, ech, P, kmax, rkb_all, coefs, want_s=True, want_acf=True):
+    """bsr_mat SUB1 for one partial wave (channel-channel part).
+
+    rkb_all: (ns,ns,ks,ks,kmax+1) Fortran-ordered.  coefs: dict of int arrays
+    k, type, ich, jch, a, b and float array c, sorted by (k, type, ich, jch).
+    Returns hcc (nblk, ns, ns) with hcc[ij] the Fortran (ns,ns) block as a
+    C-order array indexed [col, row] -> we transpose to [row, col].
+    """
+    ns, ks = basis.ns, basis.ks
+    nch = len(lch)
+    nblk = nch * (nch + 1) // 2
+    hcc = np.zeros(nblk * ns * ns)
+    scc = np.zeros(nblk * ns * ns) if want_s else None
+    acf = np.zeros(nch * nch * (kmax + 1)) if want_acf else None
+    lch_a = np.ascontiguousarray(lch, dtype=np.int32)
+    ech_a = np.ascontiguousarray(ech, dtype=np.float64)
+    Pf = np.asfortranarray(P, dtype=np.float64)
+    rk = np.asfortranarray(rkb_all)
+    c = {kk: np.ascontiguousarray(coefs[kk], dtype=np.int32) for kk in ("k", "type", "ich", "jch", "a", "b")}
+    cv = np.ascontiguousarray(coefs["c"], dtype=np.float64)
+    rc = lib().orc_assemble(basis._h, z, nch, _pi(lch_a), _p(ech_a), P.shape[1], Pf.ctypes.data_as(_D),
+                            kmax, rk.ctypes.data_as(_D), len(cv), _pi(c["k"]), _pi(c["type"]),
+                            _pi(c["ich"]), _pi(c["jch"]), _pi(c["a"]), _pi(c["b"]), _p(cv), _p(hcc),
+                            _p(scc) if want_s else None, _p(acf) if want_acf else None)
+    if rc != 0:
+        raise ValueError("assemble: coefficient out of range")
+    out = {"hcc": hcc.reshape(nblk, ns, ns).transpose(0, 2, 1).copy()}
+    if want_s:
+        out["scc"] = scc.reshape(nblk, ns, ns).transpose(0, 2, 1).copy()
+    if want_acf:
+        out["acf"] = acf.reshape(kmax + 1, nch, nch).transpose(0, 2, 1).copy()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# diag_hd restatement (src/bsr/BSR_HD3/diag_hd.f90:2-340) with scipy LAPACK
+# ---------------------------------------------------------------------------
+def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001,
+            want_vectors=False):
+    """Solve H c = E S c the way bsr_hd does for one partial wave.
+
+    hcc, scc: (nch(nch+1)/2, ns, ns) lower-triangle channel blocks [row, col]
+    as written by Record_matrix (record_matrix.f90:2).  S must be block
+    diagonal here (diag_ovl /= 0): the reference then solves a standard
+    problem after the per-channel pre-diagonalisation (diag_hd.f90:68-71).
+    Returns dict(eval, khm, bval, ipsol, [a_vectors]).
+    """
+    from scipy.linalg import lapack
+
+    nch = len(lch)
+    blk = lambda i, j: hcc[i * (i + 1) // 2 + j]   # 0-based i >= j
+    sblk = lambda i, j: scc[i * (i + 1) // 2 + j]
+    for i in range(nch):
+        for j in range(i):
+            if np.any(sblk(i, j) != 0):
+                raise NotImplementedError("generalized path (S with off-diagonal blocks)")
+    bb = []
+    bval = []
+    ipsol = [0]
+    for ich in range(nch):
+        l = lch[ich]
+        if l > ks - 2:
+            l = ks - 2
+        if ilzero == 0:
+            l = 0
+        i1 = l + 2
+        i2 = ns - ibzero if itype == -1 else ns
+        aa = blk(ich, ich)[i1 - 1: i2, i1 - 1: i2].copy()
+        cc = sblk(ich, ich)[i1 - 1: i2, i1 - 1: i2].copy()
+        w, v, info = lapack.dsygv(aa, cc, itype=1, jobz="V", uplo="U")[:3]
+        if info != 0:
+            raise RuntimeError("BSR_HD: channel diagonalization failed, channel %d" % (ich + 1))
+        keep = np.ones(len(w), dtype=bool)
+        if Edmax != 0.0:
+            keep &= ~(w > Edmax)
+        if Egap > 0.0:
+            keep &= ~(np.abs(w) < Egap)
+        vv = np.zeros((ns, int(keep.sum())))
+        vv[i1 - 1: i2, :] = v[:, keep]
+        bb.append(vv)
+        bval.extend(w[keep].tolist())
+        ipsol.append(ipsol[-1] + int(keep.sum()))
+    khm = ipsol[-1]
+    a = np.zeros((khm, khm), order="F")
+    a[np.arange(khm), np.arange(khm)] = bval
+    for ic in range(nch):
+        for jc in range(ic):
+            h = blk(ic, jc)
+            if not np.any(h != 0):
+                continue
+            w = bb[ic].T @ h          # rows: solutions of ic, cols: B-splines
+            a[ipsol[ic]: ipsol[ic + 1], ipsol[jc]: ipsol[jc + 1]] = w @ bb[jc]
+    ev, vec, info = lapack.dsyev(a, compute_v=1 if want_vectors else 0, lower=1)[:3]
+    if info != 0:
+        raise RuntimeError("DSYEV info %d" % info)
+    out = {"eval": ev, "khm": khm, "bval": np.array(bval), "ipsol": np.array(ipsol)}
+    if want_vectors:
+        out["vectors"] = vec
+        out["bb"] = bb
+    return out

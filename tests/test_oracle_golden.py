@@ -1,0 +1,68 @@
+"""The oracle against the reference's own known answers (src/libs/BS/TEST_BS).
+
+int_out holds the reference's 16-digit outputs of R^k integrals by several
+routes on the TEST_BS grid; int_inp1 holds exact hydrogenic rationals."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def test_gauss_matches_reference_table(golden):
+    for k, tab in golden["gauss"].items():
+        x, w = O.gauss(int(k))
+        assert np.max(np.abs(x - np.array(tab["x"]))) < 2e-15
+        assert np.max(np.abs(w - np.array(tab["w"]))) < 2e-15
+
+
+def test_test_bs_grid(test_bs):
+    g = test_bs["grid"]
+    assert (g["ns"], g["ml"], g["me"]) == (64, 8, 49)
+    assert g["t"][8] == 0.0625 and abs(g["t"][-1] - 160.48838) < 1e-5
+
+
+@pytest.mark.parametrize("route", ["RK_cell", "RKd", "RKe", "RKv"])
+def test_int_out_routes(test_bs, golden, route):
+    B, orbs = test_bs["basis"], test_bs["orbs"]
+    worst = 0.0
+    for e in golden["int_out"]:
+        rkb = B.mrk_cell(e["k"])
+        p = [orbs[o] for o in e["orbs"]]
+        got = O.rk_routes(B.ns, B.ks, rkb, *p)[route]
+        ref = e["routes"][route]
+        worst = max(worst, abs(got - ref) / abs(ref))
+    assert worst < 1e-13, worst
+
+
+def test_int_inp1_analytic_rk(test_bs, golden):
+    """R^k of Z=2 hydrogenic orbitals against the exact rationals (x Z, test_bs.f90:328)."""
+    B = test_bs["basis"]
+    z = test_bs["knot"]["z"]
+    orbs = {}
+    for n in range(1, 6):
+        for l in range(n):
+            orbs["%d%s" % (n, "spdfg"[l])] = B.bhwf(n, l, z)
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "R":
+            continue
+        rkb = B.mrk_cell(e["k"])
+        p = [orbs[o] for o in e["orbs"]]
+        got = O.rk_routes(B.ns, B.ks, rkb, *p)["RK_cell"]
+        sa = e["ratio"] * z
+        assert abs(got - sa) / abs(sa) < 1e-12, (e, got, sa)
+        n += 1
+    assert n >= 7
+
+
+def test_orthogonality_matches_quadr_out(test_bs, golden):
+    """<i|j> - delta_ij (QUADR, quadr.f90) against the 3-digit values of quadr_out,
+    which the reference printed for the t.f90 orbitals (Z=2 for 1s, Z=1 otherwise)."""
+    B, orbs = test_bs["basis"], test_bs["orbs"]
+    for e in golden["quadr_orth"]:
+        v = B.quadr(orbs[e["a"]], orbs[e["b"]], 0) - (1.0 if e["a"] == e["b"] else 0.0)
+        if abs(e["err"]) > 1e-6:
+            half_ulp3 = 0.5 * 10.0 ** (np.floor(np.log10(abs(e["err"]))) - 2)   # printed with 3 digits
+            assert abs(v - e["err"]) <= half_ulp3 * (1 + 1e-9), (e, v)
+        else:
+            assert abs(v) < 1e-12, (e, v)
