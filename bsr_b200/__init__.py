@@ -20,7 +20,13 @@ from . import workload  # noqa: F401
 def __getattr__(name):
     # the torch-backed API is imported lazily so that host-only users
     # (workload generation, the C ABI symbol checks) do not need a GPU
-    from . import core
-    if hasattr(core, name):
+    import importlib
+    if name.startswith("__"):
+        raise AttributeError(name)
+    core = importlib.import_module(__name__ + ".core")
+    if name == "core":
+        return core
+    try:
         return getattr(core, name)
-    raise AttributeError(name)
+    except AttributeError:
+        raise AttributeError("module 'bsr_b200' has no attribute %r" % name) from None

@@ -125,63 +125,120 @@ __global__ void direct_density_kernel(int ns, int ks, int ng, const GroupDesc *_
     Xd[(size_t)g * ns * ks + tid] = acc;
 }
 
-// Out[g,(i,ip)] = sum_(jp,j) Xd[g,(j,jp)] * rkb(i,j,ip,jp); epilogue UPDATE_HX 's'.
-// CTA tile: 64 groups x 64 rows i (one ip); 256 threads with 4x4 outputs each.
-constexpr int DG_TM = 64, DG_TN = 64, DG_TK = 16;
+constexpr int XTX = 32;                  // exchange tile rows (lanes)
+constexpr int XTYT = 5;                  // exchange columns per thread
+constexpr int XTY = 8 * XTYT;            // exchange tile columns (8 warps)
 
-__global__ void __launch_bounds__(256)
-direct_gemm_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, const double *__restrict__ Xd,
-                   const double *__restrict__ rkb, double *hcc)
+struct PadLayout {
+    int PL, NP;
+    size_t slice;                        // NP*NP
+    __host__ __device__ size_t at(int i, int j, int ip, int jp, int ks) const
+    {
+        return (size_t)(i + PL) + (size_t)NP * (j + PL) + slice * (ip + (size_t)ks * jp);
+    }
+};
+
+static PadLayout pad_layout(int ns, int ks)
 {
-    __shared__ double As[DG_TK][DG_TM + 1];
-    __shared__ double Bs[DG_TK][DG_TN];
-    int i0 = blockIdx.x * DG_TN;
-    int ip = blockIdx.y;
-    int g0 = blockIdx.z * DG_TM;
-    int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4] = {};
-    size_t nn = (size_t)ns * ns;
-    size_t ldx = (size_t)ns * ks;
-    for (int jp = 0; jp < ks; jp++) {
-        const double *R = rkb + nn * (ip + (size_t)ks * jp);
-        int jmax = ns - jp;                       // Xd(j,jp) = 0 beyond
-        for (int j0 = 0; j0 < jmax; j0 += DG_TK) {
-            // A tile: As[kk][gg] = Xd[g0+gg][(j0+kk) + ns*jp]
-            for (int q = threadIdx.x; q < DG_TK * DG_TM; q += 256) {
-                int kk = q % DG_TK, gg = q / DG_TK;
-                int g = g0 + gg, j = j0 + kk;
-                As[kk][gg] = (g < ng && j < jmax) ? Xd[(size_t)g * ldx + j + (size_t)ns * jp] : 0.0;
-            }
-            // B tile: Bs[kk][ii] = rkb(i0+ii, j0+kk, ip, jp)
-            for (int q = threadIdx.x; q < DG_TK * DG_TN; q += 256) {
-                int ii = q % DG_TN, kk = q / DG_TN;
-                int i = i0 + ii, j = j0 + kk;
-                Bs[kk][ii] = (i < ns && j < jmax) ? R[i + (size_t)ns * j] : 0.0;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int kk = 0; kk < DG_TK; kk++) {
-                double a[4], b[4];
-#pragma unroll
-                for (int r = 0; r < 4; r++) a[r] = As[kk][ty * 4 + r];
-#pragma unroll
-                for (int c = 0; c < 4; c++) b[c] = Bs[kk][tx + 16 * c];
-#pragma unroll
-                for (int r = 0; r < 4; r++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
-            }
-            __syncthreads();
+    PadLayout L;
+    L.PL = ks - 1;
+    L.NP = ns + L.PL + XTY + L.PL;
+    L.slice = (size_t)L.NP * L.NP;
+    return L;
+}
+
+// 8-byte asynchronous global->shared copy; a false predicate writes zero.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool pred)
+{
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Out[g,(i,ip)] = sum_(jp,j) Xd[g,(j,jp)] * rkb(i,j,ip,jp); epilogue UPDATE_HX 's'.
+// A register-tiled FP64 GEMM: CTA tile 128 groups x 64 rows i of one ip, K = (j,jp)
+// in steps of 16; 128 threads with 8x8 outputs each; operands double-buffered in
+// shared memory by cp.async; the sum over K runs in the reference's order
+// (jp outer, j inner) for every output.
+constexpr int DG_TM = 128, DG_TN = 64, DG_TK = 16, DG_THREADS = 128;
+
+__global__ void __launch_bounds__(DG_THREADS)
+direct_gemm_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, const double *__restrict__ Xd,
+                   const double *__restrict__ rkbp, PadLayout L, double *hcc)
+{
+    __shared__ __align__(16) double As[2][DG_TK][DG_TM];
+    __shared__ __align__(16) double Bs[2][DG_TK][DG_TN];
+    const int i0 = blockIdx.x * DG_TN;
+    const int ip = blockIdx.y;
+    const int g0 = blockIdx.z * DG_TM;
+    const int tx = threadIdx.x % 8, ty = threadIdx.x / 8;      // i: tx*8.., groups: ty*8..
+    const size_t nn = (size_t)ns * ns, ldx = (size_t)ns * ks;
+    // K steps: (jp, j0) with j0 < ns - jp
+    int nsteps = 0;
+    for (int jp = 0; jp < ks; jp++) nsteps += (ns - jp + DG_TK - 1) / DG_TK;
+    auto load = [&](int buf, int step) {
+        int jp = 0, s = step;
+        for (;;) {
+            int n = (ns - jp + DG_TK - 1) / DG_TK;
+            if (s < n) break;
+            s -= n;
+            jp++;
         }
+        int j0 = s * DG_TK, jmax = ns - jp;
+        for (int q = threadIdx.x; q < DG_TK * DG_TM; q += DG_THREADS) {
+            int kk = q % DG_TK, gg = q / DG_TK;
+            int g = g0 + gg, j = j0 + kk;
+            bool ok = g < ng && j < jmax;
+            cp_async8(&As[buf][kk][gg], ok ? (const void *)(Xd + (size_t)g * ldx + j + (size_t)ns * jp) : (const void *)Xd, ok);
+        }
+        const double *R = rkbp + L.at(0, 0, ip, jp, ks);
+        for (int q = threadIdx.x; q < DG_TK * DG_TN; q += DG_THREADS) {
+            int ii = q % DG_TN, kk = q / DG_TN;
+            int i = i0 + ii, j = j0 + kk;
+            bool ok = i < ns && j < jmax;
+            cp_async8(&Bs[buf][kk][ii], ok ? (const void *)(R + i + (size_t)L.NP * j) : (const void *)rkbp, ok);
+        }
+        cp_async_commit();
+    };
+    double acc[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; r++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc[r][c] = 0.0;
+    load(0, 0);
+    for (int st = 0; st < nsteps; st++) {
+        int buf = st & 1;
+        if (st + 1 < nsteps) { load(buf ^ 1, st + 1); cp_async_wait<1>(); }
+        else cp_async_wait<0>();
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < DG_TK; kk++) {
+            double a[8], b[8];
+            const double2 *ap = reinterpret_cast<const double2 *>(&As[buf][kk][ty * 8]);
+            const double2 *bp = reinterpret_cast<const double2 *>(&Bs[buf][kk][tx * 8]);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                double2 va = ap[q], vb = bp[q];
+                a[2 * q] = va.x; a[2 * q + 1] = va.y;
+                b[2 * q] = vb.x; b[2 * q + 1] = vb.y;
+            }
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+#pragma unroll
+                for (int c = 0; c < 8; c++) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+        __syncthreads();
     }
 #pragma unroll
-    for (int r = 0; r < 4; r++) {
-        int g = g0 + ty * 4 + r;
+    for (int r = 0; r < 8; r++) {
+        int g = g0 + ty * 8 + r;
         if (g >= ng) continue;
         double *blk = hcc + (size_t)gd[g].blk * nn;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            int i = i0 + tx + 16 * c;
+        for (int c = 0; c < 8; c++) {
+            int i = i0 + tx * 8 + c;
             if (i + ip >= ns) continue;
             double v = acc[r][c];
             blk[i + (size_t)ns * (i + ip)] += v;
@@ -191,79 +248,224 @@ direct_gemm_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, con
 }
 
 // ---------------------------------------------------------------------------
-// exchange groups: a(x,y') = sum_(x',y) R(x,x',y,y') D_g(x',y), D_g = sum c p_a p_b^T
-// One CTA per (32x32 output tile, XG_G groups).  256 threads: thread (tx,ty)
-// owns rows x0+tx, columns y0+ty+8q (q<4), for each of the CTA's groups.
+// The R^k table of the assembly pipeline, in a zero-margined layout:
+//   rkbp[(i+PL) + NP*((j+PL) + NP*(ip + ks*jp))],  PL = ks-1 low margin,
+//   NP = ns + PL + PH with PH = XTY + PL high margin (tile overhang),
+// so the exchange kernel reads R for any shifted index of its tiles without
+// bounds tests.  Values equal mrk_cell's (mrk_cell.f90:2): the cells of two
+// disjoint interval ranges factorise, sum_iv sum_jv rkd1(iv) rkd2(jv) =
+// M1(i,ip) M2(j,jp) with the band moments M1 = <B_i|r^k|B_i'>, M2 =
+// <B_i|r^-(k+1)|B_i'>; only pairs whose interval ranges overlap (|i-j| < ks)
+// sum cell by cell.  All terms are positive, so the regrouping changes the
+// result by a few ulp at most.
 // ---------------------------------------------------------------------------
-constexpr int XT = 32, XG_G = 4;
+// M1(i,ip) = sum over cells of rkd1, M2 likewise (ascending interval order)
+__global__ void band_moment_kernel(int ks, int ns, int nv, const double *__restrict__ rkd1,
+                                   const double *__restrict__ rkd2, double *M1, double *M2)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * ks) return;
+    int i = tid % ns, ip = tid / ns;
+    const int ik = ks * (ks + 1) / 2;
+    double a = 0.0, b = 0.0;
+    if (i + ip < ns) {
+        int lo = i + ip - (ks - 1); if (lo < 0) lo = 0;
+        int hi = i < nv - 1 ? i : nv - 1;
+        for (int iv = lo; iv <= hi; iv++) {
+            int ih = i - iv, ii = ih * ks - ih * (ih - 1) / 2 + ip;
+            a += rkd1[ii + (size_t)ik * iv];
+            b += rkd2[ii + (size_t)ik * iv];
+        }
+    }
+    M1[tid] = a;
+    M2[tid] = b;
+}
 
 __global__ void __launch_bounds__(256)
-exchange_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, const int *__restrict__ ca,
-                const int *__restrict__ cb, const double *__restrict__ cv, const double *__restrict__ P,
-                const double *__restrict__ rkb, double *hcc)
+rkb_pad_kernel(int ks, int ns, int nv, PadLayout L, const double *__restrict__ rkd1, const double *__restrict__ rkd2,
+               const double *__restrict__ rkd, const double *__restrict__ M1, const double *__restrict__ M2,
+               double *__restrict__ rkbp)
 {
-    extern __shared__ double Dsm[];            // XG_G tiles of (XT+2h) x (XT+2h), h = ks-1
-    const int hw = ks - 1, W = XT + 2 * hw;
-    int tiles_x = (ns + XT - 1) / XT;
-    int x0 = (blockIdx.x % tiles_x) * XT, y0 = (blockIdx.x / tiles_x) * XT;
-    int gbase = blockIdx.y * XG_G;
-    int ngl = ng - gbase < XG_G ? ng - gbase : XG_G;
-    // build the group densities with halo: D(x', y), x' = x0-hw+r, y = y0-hw+c
-    for (int gl = 0; gl < XG_G; gl++) {
-        double *D = Dsm + (size_t)gl * W * W;
-        GroupDesc G = gl < ngl ? gd[gbase + gl] : GroupDesc{0, 0, 0, 0, 0};
-        for (int q = threadIdx.x; q < W * W; q += blockDim.x) {
-            int r = q % W, c = q / W;
-            int xp = x0 - hw + r, y = y0 - hw + c;
-            double acc = 0.0;
-            if (xp >= 0 && xp < ns && y >= 0 && y < ns) {
-                for (int t = G.start; t < G.end; t++)
-                    acc = fma(cv[t], P[(size_t)ns * ca[t] + xp] * P[(size_t)ns * cb[t] + y], acc);
+    const int ipjp = blockIdx.z, ip = ipjp % ks, jp = ipjp / ks;
+    const int pr = blockIdx.x * 32 + threadIdx.x, pc = blockIdx.y * 8 + threadIdx.y;
+    if (pr >= L.NP || pc >= L.NP) return;
+    const int i = pr - L.PL, j = pc - L.PL;
+    double v = 0.0;
+    if (i >= 0 && j >= 0 && i + ip < ns && j + jp < ns) {
+        int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
+        int iv_hi = i < nv - 1 ? i : nv - 1;
+        int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = j < nv - 1 ? j : nv - 1;
+        if (iv_hi < jv_lo) v = M1[i + (size_t)ns * ip] * M2[j + (size_t)ns * jp];
+        else if (jv_hi < iv_lo) v = M1[j + (size_t)ns * jp] * M2[i + (size_t)ns * ip];
+        else {
+            const int ik = ks * (ks + 1) / 2;
+            for (int jv = jv_lo; jv <= jv_hi; jv++) {
+                int jh = j - jv, jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                for (int iv = iv_lo; iv <= iv_hi; iv++) {
+                    int ih = i - iv, ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                    double c;
+                    if (iv < jv) c = rkd1[ii + (size_t)ik * iv] * rkd2[jj + (size_t)ik * jv];
+                    else if (iv > jv) c = rkd1[jj + (size_t)ik * jv] * rkd2[ii + (size_t)ik * iv];
+                    else c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                    v += c;
+                }
             }
-            D[r + (size_t)W * c] = acc;
+        }
+    }
+    rkbp[(size_t)pr + (size_t)L.NP * pc + L.slice * ipjp] = v;
+}
+
+// ---------------------------------------------------------------------------
+// exchange groups: a(x,y') = sum_(x',y) R(x,x',y,y') D_g(x',y), D_g = sum c p_a p_b^T
+//
+// One CTA per (XTX x XTY output tile, G groups), 8 warps.  Lane l owns row
+// x = x0 + l (the contiguous rkb index, so R loads coalesce); warp w owns the
+// XTYT columns y' = y0 + XTYT w + j.  For each row shift e the thread walks the
+// column shift f with a sliding window of D values held in registers: per f
+// step it loads XTYT R values (shared by its G groups, from L2, no bounds
+// tests thanks to the zero margins) and one new D value per group from shared
+// memory, and issues G*XTYT FMAs.  The group densities (with halo) are built
+// once per CTA in shared memory from staged term vectors and never touch HBM.
+// ---------------------------------------------------------------------------
+constexpr int XTC = 16;                  // terms staged per chunk in the density build
+
+template <int KS, int G>
+__global__ void __launch_bounds__(256, 2)
+exchange_kernel(int ns, int ng, PadLayout L, const GroupDesc *__restrict__ gd, const int *__restrict__ ca,
+                const int *__restrict__ cb, const double *__restrict__ cv, const double *__restrict__ P,
+                const double *__restrict__ rkbp, double *hcc)
+{
+    constexpr int HW = KS - 1, WX = XTX + 2 * HW, WY = XTY + 2 * HW;
+    constexpr int NQ = (WX * WY + 255) / 256;          // density entries per thread
+    extern __shared__ double sm[];
+    double *Dsm = sm;                                   // [G][WY cols (y)][WX rows (x')]
+    double *U = Dsm + (size_t)G * WX * WY;              // [XTC][WX]
+    double *V = U + XTC * WX;                           // [XTC][WY]
+    const int tiles_x = (ns + XTX - 1) / XTX;
+    const int x0 = (blockIdx.x % tiles_x) * XTX, y0 = (blockIdx.x / tiles_x) * XTY;
+    const int gbase = blockIdx.y * G;
+    const int ngl = ng - gbase < G ? ng - gbase : G;
+    // ---- group densities D(x', y) = sum_t (c_t p_a(x')) p_b(y) ----
+    for (int gl = 0; gl < G; gl++) {
+        double *D = Dsm + (size_t)gl * WX * WY;
+        int ts = 0, te = 0;
+        if (gl < ngl) { ts = gd[gbase + gl].start; te = gd[gbase + gl].end; }
+        double acc[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+        for (int t0 = ts; t0 < te; t0 += XTC) {
+            int nt = te - t0 < XTC ? te - t0 : XTC;
+            __syncthreads();
+            for (int q = threadIdx.x; q < nt * WX; q += 256) {
+                int t = q / WX, r = q % WX, xp = x0 - HW + r;
+                U[t * WX + r] = (xp >= 0 && xp < ns) ? cv[t0 + t] * P[(size_t)ns * ca[t0 + t] + xp] : 0.0;
+            }
+            for (int q = threadIdx.x; q < nt * WY; q += 256) {
+                int t = q / WY, c = q % WY, y = y0 - HW + c;
+                V[t * WY + c] = (y >= 0 && y < ns) ? P[(size_t)ns * cb[t0 + t] + y] : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                int e = threadIdx.x + 256 * q;
+                if (e < WX * WY) {
+                    int r = e % WX, c = e / WX;
+                    double a = acc[q];
+                    for (int t = 0; t < nt; t++) a = fma(U[t * WX + r], V[t * WY + c], a);
+                    acc[q] = a;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            int e = threadIdx.x + 256 * q;
+            if (e < WX * WY) D[e] = acc[q];
         }
     }
     __syncthreads();
-    int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
-    int x = x0 + tx;
-    double acc[XG_G][4];
+    // ---- main loop ----
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x = x0 + lane, yb = y0 + XTYT * w;
+    const size_t NPs = (size_t)L.NP;
+    double acc[G][XTYT];
 #pragma unroll
-    for (int gl = 0; gl < XG_G; gl++)
+    for (int gl = 0; gl < G; gl++)
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[gl][q] = 0.0;
-    size_t nn = (size_t)ns * ns;
-    if (x < ns) {
-        for (int e = -hw; e <= hw; e++) {
-            int xp = x + e;
-            if (xp < 0 || xp >= ns) continue;
-            int r1 = e >= 0 ? x : xp, c1 = e >= 0 ? e : -e;
-            int rr = tx + hw + e;                        // smem row of x'
-            for (int f = -hw; f <= hw; f++) {
-                int c2 = f >= 0 ? f : -f;
-                const double *R = rkb + nn * (c1 + (size_t)ks * c2) + r1;
+        for (int j = 0; j < XTYT; j++) acc[gl][j] = 0.0;
+    // R(x,x',y,y') at rkbp[(min(x,x')+PL) + NP*(min(y,y')+PL) + slice*(|e| + KS|f|)]
+    const double *Rbase = rkbp + L.PL + NPs * (yb + L.PL);
+    for (int e = -HW; e <= HW; e++) {
+        const int r1 = e >= 0 ? x : x + e;
+        const int rr = lane + e + HW;
+        const double *Re = Rbase + r1 + L.slice * (e >= 0 ? e : -e);
+        double dwin[G][XTYT];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    int yp = y0 + ty + 8 * q;                // output column y'
-                    int y = yp + f;                          // summed index y
-                    if (yp >= ns || y < 0 || y >= ns) continue;
-                    int r2 = f >= 0 ? yp : y;
-                    double rv = R[(size_t)ns * r2];
-                    int cc = ty + 8 * q + hw + f;            // smem column of y
+        for (int gl = 0; gl < G; gl++)
 #pragma unroll
-                    for (int gl = 0; gl < XG_G; gl++)
-                        acc[gl][q] = fma(rv, Dsm[(size_t)gl * W * W + rr + (size_t)W * cc], acc[gl][q]);
+            for (int j = 0; j < XTYT; j++) dwin[gl][j] = Dsm[(size_t)gl * WX * WY + (XTYT * w + j) * WX + rr];
+#pragma unroll
+        for (int f = -HW; f <= HW; f++) {
+            const double *Rp = Re + L.slice * KS * (f >= 0 ? f : -f) + (f < 0 ? (long)f * (long)NPs : 0);
+            double R[XTYT];
+#pragma unroll
+            for (int j = 0; j < XTYT; j++) R[j] = __ldg(Rp + NPs * j);
+#pragma unroll
+            for (int gl = 0; gl < G; gl++)
+#pragma unroll
+                for (int j = 0; j < XTYT; j++) acc[gl][j] = fma(R[j], dwin[gl][j], acc[gl][j]);
+            if (f < HW) {
+#pragma unroll
+                for (int gl = 0; gl < G; gl++) {
+#pragma unroll
+                    for (int j = 0; j < XTYT - 1; j++) dwin[gl][j] = dwin[gl][j + 1];
+                    dwin[gl][XTYT - 1] = Dsm[(size_t)gl * WX * WY + (XTYT * w + XTYT + f + HW) * WX + rr];
                 }
             }
         }
     }
     if (x >= ns) return;
+    const size_t nn = (size_t)ns * ns;
     for (int gl = 0; gl < ngl; gl++) {
         double *blk = hcc + (size_t)gd[gbase + gl].blk * nn;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            int yp = y0 + ty + 8 * q;
-            if (yp < ns) blk[x + (size_t)ns * yp] += acc[gl][q];
+        for (int j = 0; j < XTYT; j++) {
+            const int yp = yb + j;
+            if (yp < ns) blk[x + (size_t)ns * yp] += acc[gl][j];
         }
+    }
+}
+
+static int exchange_groups_per_cta(int ks) { return ks <= 12 ? 4 : 2; }
+
+static size_t exchange_smem(int ks)
+{
+    int WX = XTX + 2 * (ks - 1), WY = XTY + 2 * (ks - 1);
+    return sizeof(double) * ((size_t)exchange_groups_per_cta(ks) * WX * WY + (size_t)XTC * (WX + WY));
+}
+
+typedef void (*exchange_fn)(int, int, PadLayout, const GroupDesc *, const int *, const int *, const double *,
+                            const double *, const double *, double *);
+
+static exchange_fn exchange_kernel_for(int ks)
+{
+    switch (ks) {
+    case 2: return exchange_kernel<2, 4>;
+    case 3: return exchange_kernel<3, 4>;
+    case 4: return exchange_kernel<4, 4>;
+    case 5: return exchange_kernel<5, 4>;
+    case 6: return exchange_kernel<6, 4>;
+    case 7: return exchange_kernel<7, 4>;
+    case 8: return exchange_kernel<8, 4>;
+    case 9: return exchange_kernel<9, 4>;
+    case 10: return exchange_kernel<10, 4>;
+    case 11: return exchange_kernel<11, 4>;
+    case 12: return exchange_kernel<12, 4>;
+    case 13: return exchange_kernel<13, 2>;
+    case 14: return exchange_kernel<14, 2>;
+    case 15: return exchange_kernel<15, 2>;
+    case 16: return exchange_kernel<16, 2>;
+    default: return nullptr;
     }
 }
 
@@ -504,9 +706,10 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
     add(sizeof(double) * nch);
     add(sizeof(double) * (size_t)ik * nv * 2);
     add(sizeof(double) * (size_t)ik * ik * nv);
-    add(sizeof(double) * nn * ks * ks);
+    const PadLayout PL = pad_layout(ns, ks);
+    add(sizeof(double) * PL.slice * ks * ks);
     add(sizeof(double) * maxgd * ns * ks);
-    add(sizeof(double) * (size_t)ns * ks);
+    add(sizeof(double) * (size_t)ns * ks * 3);
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) return rc;
     size_t host_bytes = sizeof(int) * (size_t)ncoef * 2 + sizeof(double) * (size_t)ncoef +
@@ -521,9 +724,10 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
     double *d_ech = ar.take<double>(nch);
     double *rkd1 = ar.take<double>((size_t)ik * nv), *rkd2 = ar.take<double>((size_t)ik * nv);
     double *rkd = ar.take<double>((size_t)ik * ik * nv);
-    double *rkb = ar.take<double>(nn * ks * ks);
+    double *rkbp = ar.take<double>(PL.slice * ks * ks);
     double *Xd = ar.take<double>(std::max<size_t>(maxgd, 1) * ns * ks);
     double *rmk = ar.take<double>((size_t)ns * ks);
+    double *M1 = ar.take<double>((size_t)ns * ks), *M2 = ar.take<double>((size_t)ns * ks);
     // stage host metadata through pinned memory, one copy
     char *hp = (char *)c->pinned;
     size_t o = 0;
@@ -564,12 +768,12 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
     }
     stage_end(c, 3);
     // ---- two-electron groups, one multipole at a time ----
-    const int W = XT + 2 * (ks - 1);
-    size_t xsm = sizeof(double) * XG_G * W * W;
-    if (xsm > 48 * 1024) {
-        e = cudaFuncSetAttribute(exchange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm);
-        if (e != cudaSuccess) return cuda_fail(e, "exchange smem");
-    }
+    const size_t xsm = exchange_smem(ks);
+    const int xg = exchange_groups_per_cta(ks);
+    exchange_fn xk = exchange_kernel_for(ks);
+    if (!xk) { set_error("assemble: ks=%d unsupported", ks); return BSRG_ERR_ARG; }
+    if ((e = cudaFuncSetAttribute(xk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm)) != cudaSuccess)
+        return cuda_fail(e, "exchange smem");
     for (int k = 0; k <= kmax; k++) {
         int nd = (int)dgroups[k].size(), nx = (int)xgroups[k].size();
         if (nd == 0 && nx == 0) continue;
@@ -578,16 +782,19 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
         if (rc != BSRG_OK) return rc;
         stage_end(c, 0, 3);
         stage_begin(c, 7);
-        rc = launch_mrk_cell(b, rkd1, rkd2, rkd, rkb, ks, s);
-        if (rc != BSRG_OK) return rc;
-        stage_end(c, 7, 1);
+        band_moment_kernel<<<(ns * ks + 127) / 128, 128, 0, s>>>(ks, ns, nv, rkd1, rkd2, M1, M2);
+        {
+            dim3 gp((PL.NP + 31) / 32, (PL.NP + 7) / 8, ks * ks);
+            rkb_pad_kernel<<<gp, dim3(32, 8), 0, s>>>(ks, ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
+        }
+        stage_end(c, 7, 2);
         if (nd > 0) {
             stage_begin(c, 1);
             const GroupDesc *gdd = d_gd + doff[k];
             dim3 g1((ns * ks + 127) / 128, nd);
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
             dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
-            direct_gemm_kernel<<<g2, 256, 0, s>>>(ns, ks, nd, gdd, Xd, rkb, hcc);
+            direct_gemm_kernel<<<g2, DG_THREADS, 0, s>>>(ns, ks, nd, gdd, Xd, rkbp, PL, hcc);
             if (acf) {
                 rc = launch_mrm(b, k, rmk, s);
                 if (rc != BSRG_OK) return rc;
@@ -598,9 +805,9 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
         }
         if (nx > 0) {
             stage_begin(c, 2);
-            int tiles = ((ns + XT - 1) / XT) * ((ns + XT - 1) / XT);
-            dim3 g3(tiles, (nx + XG_G - 1) / XG_G);
-            exchange_kernel<<<g3, 256, xsm, s>>>(ns, ks, nx, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkb, hcc);
+            int tiles = ((ns + XTX - 1) / XTX) * ((ns + XTY - 1) / XTY);
+            dim3 g3(tiles, (nx + xg - 1) / xg);
+            xk<<<g3, 256, xsm, s>>>(ns, nx, PL, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkbp, hcc);
             stage_end(c, 2, 1);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "assemble k-loop");

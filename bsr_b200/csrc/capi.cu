@@ -180,6 +180,9 @@ int bsrg_define_spline(int ks, int ns, const double *t_host, int ml, int me, dou
     for (int q = 0; q < 14; q++) {
         cudaError_t e = cudaMalloc((void **)bufs[q], sizes[q] * sizeof(double));
         if (e != cudaSuccess) { bsrg_basis_free(b); return cuda_fail(e, "define_spline alloc"); }
+        // allocate_grid / allocate_galerkin zero the module arrays (spline_grid.f90:49)
+        e = cudaMemsetAsync(*bufs[q], 0, sizes[q] * sizeof(double), (cudaStream_t)stream);
+        if (e != cudaSuccess) { bsrg_basis_free(b); return cuda_fail(e, "define_spline zero"); }
     }
     cudaError_t e = cudaMemcpyAsync(b->t, t_host, sizeof(double) * (ns + ks), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) { bsrg_basis_free(b); return cuda_fail(e, "define_spline copy"); }

@@ -41,6 +41,82 @@ __global__ void extract_channel_kernel(int ns, int ks, const int *__restrict__ s
     CC[o] = sv;
 }
 
+// Padded copies for the batched channel solves (all channels in one batch of
+// uniform size n_pad, leading dimension ns):
+//   AG[ich] = diag(H_ii restricted to rows/cols s0.., 0)
+//   LG[q]   = diag(S restricted likewise, I) for each distinct restriction q
+// After the reduction to standard form C = L^-1 H L^-T, pad_shift_kernel puts
+// mu = 2 ||C||_F + 1 on the padded diagonal: above every eigenvalue of the
+// channel block (|lambda| <= ||C||_2 <= ||C||_F), so the padding's eigenpairs
+// sort last, the physical eigenvectors have exactly zero padded components, and
+// the padded matrix keeps the channel's own scale (a much larger mu would
+// drag the eigensolver's norm-relative tolerances with it).
+
+__global__ void extract_padded_kernel(int ns, int npad, const int *__restrict__ s0v, const int *__restrict__ nsolv,
+                                      const double *__restrict__ hcc, double *AG)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * npad) return;
+    int r = tid % ns, c = tid / ns;
+    int n = nsolv[ich], s0 = s0v[ich];
+    const double *H = hcc + ((size_t)(ich + 1) * (ich + 2) / 2 - 1) * ns * ns;
+    double v = 0.0;
+    if (r < n && c < n) v = H[(s0 + r) + (size_t)ns * (s0 + c)];
+    AG[(size_t)ich * ns * npad + tid] = v;
+}
+
+__global__ void pad_shift_kernel(int ns, int npad, const int *__restrict__ nsolv, double *AG)
+{
+    int ich = blockIdx.x, n = nsolv[ich];
+    double *C = AG + (size_t)ich * ns * npad;
+    double ss = 0.0;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        double v = C[(q % n) + (size_t)ns * (q / n)];
+        ss += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    __shared__ double part[32];
+    __shared__ double mu;
+    if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = ss;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x + 31) / 32; w++) t += part[w];
+        mu = 2.0 * sqrt(t) + 1.0;
+    }
+    __syncthreads();
+    for (int r = n + threadIdx.x; r < npad; r += blockDim.x) C[r + (size_t)ns * r] = mu;
+}
+
+__global__ void extract_padded_overlap_kernel(int ns, int ks, int npad, const int *__restrict__ gs0,
+                                              const int *__restrict__ gn, const double *__restrict__ sb, double *LG)
+{
+    int q = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= ns * npad) return;
+    int r = tid % ns, c = tid / ns;
+    int n = gn[q], s0 = gs0[q];
+    double v = 0.0;
+    if (r < n && c < n) {
+        int i = s0 + r, j = s0 + c, hi = i > j ? i : j, lo = i > j ? j : i;
+        if (hi - lo < ks) v = sb[hi + (size_t)ns * (lo - hi + ks - 1)];
+    } else if (r == c && r < npad) v = 1.0;
+    LG[(size_t)q * ns * npad + tid] = v;
+}
+
+// channel solutions back to the per-channel slots read by keep_count/compact
+__global__ void scatter_back_kernel(int ns, int npad, const int *__restrict__ nsolv, const double *__restrict__ AG,
+                                    const double *__restrict__ WG, double *AA, double *Wv)
+{
+    int ich = blockIdx.y;
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = nsolv[ich];
+    if (tid >= ns * n) return;
+    AA[(size_t)ich * ns * ns + tid] = AG[(size_t)ich * ns * npad + tid];
+    if (tid < n) Wv[(size_t)ich * ns + tid] = WG[(size_t)ich * npad + tid];
+}
+
 __global__ void keep_count_kernel(int ns, int nch, const int *__restrict__ nsolv, const double *__restrict__ W,
                                   double edmax, double egap, int *counts)
 {
@@ -115,6 +191,168 @@ __global__ void set_diag_kernel(long n, const double *__restrict__ bval, double 
     if (i < n) A[i + n * i] = bval[i];
 }
 
+struct ChannelGroups {
+    std::vector<int> gs0, gn;                 // first row and size of each group
+    std::vector<std::vector<int>> members;    // channels of each group
+};
+
+static ChannelGroups group_channels(const std::vector<int> &s0v, const std::vector<int> &nsolv)
+{
+    ChannelGroups G;
+    for (size_t ich = 0; ich < s0v.size(); ich++) {
+        int q = -1;
+        for (size_t k = 0; k < G.gs0.size(); k++)
+            if (G.gs0[k] == s0v[ich] && G.gn[k] == nsolv[ich]) { q = (int)k; break; }
+        if (q < 0) {
+            q = (int)G.gs0.size();
+            G.gs0.push_back(s0v[ich]);
+            G.gn.push_back(nsolv[ich]);
+            G.members.emplace_back();
+        }
+        G.members[q].push_back((int)ich);
+    }
+    return G;
+}
+
+// device bytes the batched channel solves take from the arena (0 if unavailable)
+static size_t chan_batched_bytes(bsrg_ctx *c, cusolverDnParams_t params, int ns, const std::vector<int> &s0v,
+                                 const std::vector<int> &nsolv)
+{
+    ChannelGroups G = group_channels(s0v, nsolv);
+    int nch = (int)s0v.size(), ng = (int)G.gs0.size();
+    int npad = *std::max_element(nsolv.begin(), nsolv.end());
+    size_t d1 = 0, h1 = 0;
+    if (cusolverDnXsyevBatched_bufferSize(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, npad,
+                                          CUDA_R_64F, nullptr, ns, CUDA_R_64F, nullptr, CUDA_R_64F, &d1, &h1,
+                                          (int64_t)nch) != CUSOLVER_STATUS_SUCCESS)
+        return 0;
+    size_t bytes = 0;
+    auto add = [&](size_t b) { bytes += ((b + 255) & ~(size_t)255) + 256; };
+    add(sizeof(double) * (size_t)ns * npad * nch);   // AG
+    add(sizeof(double) * (size_t)npad * nch);        // WG
+    add(sizeof(double) * (size_t)ns * npad * ng);    // LG
+    add(d1 + 16);
+    add(sizeof(int) * ng * 2);
+    add(sizeof(double *) * (2 * (size_t)nch + ng));
+    add(sizeof(int) * (nch + ng));
+    return bytes;
+}
+
+// Is cuSOLVER's batched symmetric eigensolver usable for these channel sizes?
+static bool chan_batched_ok(bsrg_ctx *c, cusolverDnParams_t params, int ns, const std::vector<int> &nsolv)
+{
+    if (getenv("BSRG_CHANNEL_SYGVD")) return false;
+    size_t dws = 0, hws = 0;
+    int n = *std::max_element(nsolv.begin(), nsolv.end());
+    cusolverStatus_t st = cusolverDnXsyevBatched_bufferSize(c->solver, params, CUSOLVER_EIG_MODE_VECTOR,
+                                                            CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, nullptr, ns,
+                                                            CUDA_R_64F, nullptr, CUDA_R_64F, &dws, &hws, 1);
+    return st == CUSOLVER_STATUS_SUCCESS;
+}
+
+// The batched channel solves.  Writes eigenvectors (normalised to x^T S x = 1)
+// into AA[ich] (ld ns) and eigenvalues into Wv[ich*ns], like sygvd would: one
+// batched Cholesky of the distinct restricted overlaps (DPOTRF), two batched
+// triangular solves (DSYGST), one batched symmetric eigensolve of all channels
+// (DSYEV) and the batched back-transform x = L^-T y.
+static int solve_channels_batched(bsrg_ctx *c, cusolverDnParams_t params, const bsrg_basis *b, const double *hcc,
+                                  int nch, const std::vector<int> &s0v, const std::vector<int> &nsolv,
+                                  const int *d_s0, const int *d_nsol, double *AA, double *Wv, int *d_info,
+                                  Arena &ar)
+{
+    const int ns = b->ns, ks = b->ks;
+    cudaStream_t s = c->stream;
+    cudaError_t e;
+    ChannelGroups G = group_channels(s0v, nsolv);
+    const int ng = (int)G.gs0.size();
+    const int npad = *std::max_element(nsolv.begin(), nsolv.end());
+    size_t dws = 0, hws = 0;
+    if (cusolverDnXsyevBatched_bufferSize(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, npad,
+                                          CUDA_R_64F, nullptr, ns, CUDA_R_64F, nullptr, CUDA_R_64F, &dws, &hws,
+                                          (int64_t)nch) != CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: syevBatched_bufferSize failed");
+        return BSRG_ERR_SOLVER;
+    }
+    double *AG = ar.take<double>((size_t)ns * npad * nch), *WG = ar.take<double>((size_t)npad * nch);
+    double *LG = ar.take<double>((size_t)ns * npad * ng);
+    void *swork = ar.take<char>(dws + 16);
+    int *d_gs0 = ar.take<int>(ng), *d_gn = ar.take<int>(ng);
+    double **d_ptr = ar.take<double *>(2 * (size_t)nch + ng);    // L per channel | A per channel | L per group
+    int *d_binfo = ar.take<int>((size_t)nch + ng);               // syev info, then potrf info
+    if (ar.off > ar.cap) { set_error("diag_hd: workspace too small for the batched channel solves"); return BSRG_ERR_NOMEM; }
+    std::vector<char> hwork(hws + 16);
+    std::vector<double *> hptr(2 * (size_t)nch + ng);
+    std::vector<int> grp(nch);
+    for (int q = 0; q < ng; q++)
+        for (int ich : G.members[q]) grp[ich] = q;
+    for (int ich = 0; ich < nch; ich++) {
+        hptr[ich] = LG + (size_t)grp[ich] * ns * npad;
+        hptr[nch + ich] = AG + (size_t)ich * ns * npad;
+    }
+    for (int q = 0; q < ng; q++) hptr[2 * (size_t)nch + q] = LG + (size_t)q * ns * npad;
+    if ((e = cudaMemcpyAsync(d_gs0, G.gs0.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d_gn, G.gn.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(d_ptr, hptr.data(), sizeof(double *) * hptr.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd batched upload");
+    {
+        dim3 g((unsigned)((ns * npad + 127) / 128), nch);
+        extract_padded_kernel<<<g, 128, 0, s>>>(ns, npad, d_s0, d_nsol, hcc, AG);
+        dim3 g2((unsigned)((ns * npad + 127) / 128), ng);
+        extract_padded_overlap_kernel<<<g2, 128, 0, s>>>(ns, ks, npad, d_gs0, d_gn, b->sb, LG);
+    }
+    double **Lp = d_ptr, **Ap = d_ptr + nch, **Lg = d_ptr + 2 * nch;
+    if (cusolverDnDpotrfBatched(c->solver, CUBLAS_FILL_MODE_LOWER, npad, Lg, ns, d_binfo + nch, ng) !=
+        CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: potrfBatched failed to launch");
+        return BSRG_ERR_SOLVER;
+    }
+    const double one = 1.0;
+    cublasStatus_t b1 = cublasDtrsmBatched(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N,
+                                           CUBLAS_DIAG_NON_UNIT, npad, npad, &one, (const double *const *)Lp, ns, Ap,
+                                           ns, nch);
+    cublasStatus_t b2 = cublasDtrsmBatched(c->blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                           CUBLAS_DIAG_NON_UNIT, npad, npad, &one, (const double *const *)Lp, ns, Ap,
+                                           ns, nch);
+    if (b1 != CUBLAS_STATUS_SUCCESS || b2 != CUBLAS_STATUS_SUCCESS) {
+        set_error("diag_hd: trsmBatched failed (%d, %d)", (int)b1, (int)b2);
+        return BSRG_ERR_SOLVER;
+    }
+    pad_shift_kernel<<<nch, 256, 0, s>>>(ns, npad, d_nsol, AG);
+    if (cusolverDnXsyevBatched(c->solver, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, npad, CUDA_R_64F,
+                               AG, ns, CUDA_R_64F, WG, CUDA_R_64F, swork, dws, hwork.data(), hws, d_binfo,
+                               nch) != CUSOLVER_STATUS_SUCCESS) {
+        set_error("diag_hd: syevBatched failed to launch");
+        return BSRG_ERR_SOLVER;
+    }
+    cublasStatus_t b3 = cublasDtrsmBatched(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                           CUBLAS_DIAG_NON_UNIT, npad, npad, &one, (const double *const *)Lp, ns, Ap,
+                                           ns, nch);
+    if (b3 != CUBLAS_STATUS_SUCCESS) {
+        set_error("diag_hd: trsmBatched (back-transform) failed (%d)", (int)b3);
+        return BSRG_ERR_SOLVER;
+    }
+    dim3 g((unsigned)((ns * npad + 127) / 128), nch);
+    scatter_back_kernel<<<g, 128, 0, s>>>(ns, npad, d_nsol, AG, WG, AA, Wv);
+    // cuSOLVER needs the host workspace alive until the work is done; check the infos here
+    std::vector<int> hinfo((size_t)nch + ng);
+    if ((e = cudaMemcpyAsync(hinfo.data(), d_binfo, sizeof(int) * (nch + ng), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd batched info");
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diag_hd batched channel solves");
+    for (int q = 0; q < ng; q++)
+        if (hinfo[nch + q] != 0) {
+            set_error("BSR_HD: channel diagonalization failed, overlap of channel = %d not positive definite (info %d)",
+                      G.members[q][0] + 1, hinfo[nch + q]);
+            return BSRG_ERR_INFO;
+        }
+    for (int ich = 0; ich < nch; ich++)
+        if (hinfo[ich] != 0) {
+            set_error("BSR_HD: channel diagonalization failed, channel = %d (info %d)", ich + 1, hinfo[ich]);
+            return BSRG_ERR_INFO;
+        }
+    if ((e = cudaMemsetAsync(d_info, 0, sizeof(int) * nch, s)) != cudaSuccess) return cuda_fail(e, "diag_hd info");
+    return cuda_fail(cudaGetLastError(), "diag_hd batched channel solves");
+}
+
 }  // namespace bsrg
 
 using namespace bsrg;
@@ -186,6 +424,8 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     add(sizeof(double) * nn * std::max(nb, 1) * 2);   // Wt, T
     if (!vecs) add(sizeof(double) * (size_t)khm_max * khm_max);
     add(dws + 16);
+    size_t batched_bytes = chan_batched_bytes(c, params, ns, s0v, nsolv);
+    add(batched_bytes);
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
     // pinned staging layout (ints): s0 | nsol | info | cnt | ipsol | final info, then block maps and pointers
@@ -215,23 +455,34 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         return cuda_fail(e, "diag_hd upload");
     }
     // ---- 1. channel problems ----
+    // Channels with the same l share the restricted overlap S_l.  Per group:
+    // DPOTRF(S_l) once, then for all its channels at once DSYGST as two
+    // batched triangular solves, a batched DSYEV and the back-transform
+    // x = L^-T y (the steps of LAPACK's DSYGV).  If the batched eigensolver is
+    // not available in the loaded cuSOLVER, each channel goes through sygvd.
     stage_begin(c, 4);
-    {
-        dim3 g((unsigned)((nn + 127) / 128), nch);
-        extract_channel_kernel<<<g, 128, 0, s>>>(ns, ks, d_s0, d_nsol, hcc, b->sb, AA, CC);
-    }
-    for (int ich = 0; ich < nch; ich++) {
-        cusolverStatus_t st = cusolverDnDsygvd(c->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
-                                               CUBLAS_FILL_MODE_UPPER, nsolv[ich], AA + nn * ich, ns, CC + nn * ich,
-                                               ns, Wv + (size_t)ns * ich, work1, lwork1, d_info + ich);
-        if (st != CUSOLVER_STATUS_SUCCESS) {
-            cusolverDnDestroyParams(params);
-            set_error("diag_hd: sygvd failed to launch for channel %d (status %d)", ich + 1, (int)st);
-            return BSRG_ERR_SOLVER;
+    bool batched = batched_bytes > 0 && chan_batched_ok(c, params, ns, nsolv);
+    if (batched) {
+        int rcb = solve_channels_batched(c, params, b, hcc, nch, s0v, nsolv, d_s0, d_nsol, AA, Wv, d_info, ar);
+        if (rcb != BSRG_OK) { cusolverDnDestroyParams(params); return rcb; }
+    } else {
+        {
+            dim3 g((unsigned)((nn + 127) / 128), nch);
+            extract_channel_kernel<<<g, 128, 0, s>>>(ns, ks, d_s0, d_nsol, hcc, b->sb, AA, CC);
+        }
+        for (int ich = 0; ich < nch; ich++) {
+            cusolverStatus_t st = cusolverDnDsygvd(c->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR,
+                                                   CUBLAS_FILL_MODE_UPPER, nsolv[ich], AA + nn * ich, ns, CC + nn * ich,
+                                                   ns, Wv + (size_t)ns * ich, work1, lwork1, d_info + ich);
+            if (st != CUSOLVER_STATUS_SUCCESS) {
+                cusolverDnDestroyParams(params);
+                set_error("diag_hd: sygvd failed to launch for channel %d (status %d)", ich + 1, (int)st);
+                return BSRG_ERR_SOLVER;
+            }
         }
     }
     keep_count_kernel<<<nch, 256, 0, s>>>(ns, nch, d_nsol, Wv, edmax, egap, d_cnt);
-    stage_end(c, 4, 2);   // extract + keep_count (the sygvd calls are cuSOLVER's)
+    stage_end(c, 4, batched ? 5 : 2);   // own kernels: extracts, pad shift, scatter-back, keep_count
     if ((e = cudaMemcpyAsync(hi + o_info, d_info, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(hi + o_cnt, d_cnt, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
         cusolverDnDestroyParams(params);

@@ -324,37 +324,75 @@ __global__ void diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, 
 // ---------------------------------------------------------------------------
 // mrk_cell (mrk_cell.f90:2): rkb(i,j,ip,jp) = sum over cells, jv outer and iv
 // inner in ascending order as the reference accumulates.  One thread per
-// element; threadIdx.x runs along i (the contiguous index).  Elements with
-// ip or jp >= ks (ldp > ks) or past the last spline are written as zero.
+// element; a CTA covers 32 rows i (threadIdx.x, the contiguous index) x 8
+// columns j for one (ip, jp).  The interval moments the CTA needs,
+//   u1/u2[ih][iv] = rkd1/rkd2(pair (ih, ih+ip), iv) and w1/w2 likewise for jp,
+// are staged in shared memory once, so the inner loop is two shared loads and
+// a multiply-add per cell; only the diagonal cells (iv == jv) read rkd from
+// global memory.  Elements with ip or jp >= ks (ldp > ks) or past the last
+// spline are written as zero.
 // ---------------------------------------------------------------------------
-__global__ void rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rkd1,
-                                  const double *__restrict__ rkd2, const double *__restrict__ rkd,
-                                  double *__restrict__ rkb)
+constexpr int EXP_TI = 32, EXP_TJ = 8;
+
+__global__ void __launch_bounds__(EXP_TI * EXP_TJ)
+rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rkd1,
+                  const double *__restrict__ rkd2, const double *__restrict__ rkd, double *__restrict__ rkb)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y * blockDim.y + threadIdx.y;
-    int ipjp = blockIdx.z;
-    int ip = ipjp % ldp, jp = ipjp / ldp;
-    if (i >= ns || j >= ns) return;
+    extern __shared__ double sm[];
+    const int ip = blockIdx.z % ldp, jp = blockIdx.z / ldp;
+    const int i0 = blockIdx.x * EXP_TI, j0 = blockIdx.y * EXP_TJ;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
     const int ik = ks * (ks + 1) / 2;
+    const int LI = EXP_TI + ks - 1, LJ = EXP_TJ + ks - 1;     // interval windows
+    const int ivb = i0 - (ks - 1), jvb = j0 - (ks - 1);       // first interval of each window
+    double *u1 = sm, *u2 = u1 + ks * LI, *w1 = u2 + ks * LI, *w2 = w1 + ks * LJ;
+    const bool active = ip < ks && jp < ks;
+    if (active) {
+        const int tid = threadIdx.y * EXP_TI + threadIdx.x, nt = EXP_TI * EXP_TJ;
+        for (int q = tid; q < ks * LI; q += nt) {
+            int ih = q / LI, iv = ivb + q % LI;
+            double a = 0.0, b = 0.0;
+            if (ih + ip < ks && iv >= 0 && iv < nv) {
+                int ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                a = rkd1[ii + (size_t)ik * iv];
+                b = rkd2[ii + (size_t)ik * iv];
+            }
+            u1[q] = a;
+            u2[q] = b;
+        }
+        for (int q = tid; q < ks * LJ; q += nt) {
+            int jh = q / LJ, jv = jvb + q % LJ;
+            double a = 0.0, b = 0.0;
+            if (jh + jp < ks && jv >= 0 && jv < nv) {
+                int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                a = rkd1[jj + (size_t)ik * jv];
+                b = rkd2[jj + (size_t)ik * jv];
+            }
+            w1[q] = a;
+            w2[q] = b;
+        }
+    }
+    __syncthreads();
+    if (i >= ns || j >= ns) return;
     double acc = 0.0;
-    if (ip < ks && jp < ks && i + ip < ns && j + jp < ns) {
+    if (active && i + ip < ns && j + jp < ns) {
         int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
         int iv_hi = i < nv - 1 ? i : nv - 1;
         int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
         int jv_hi = j < nv - 1 ? j : nv - 1;
         for (int jv = jv_lo; jv <= jv_hi; jv++) {
-            int jh = j - jv;                       // 0-based position of B_j in cell jv
-            int jj = jh * ks - jh * (jh - 1) / 2 + jp;
-            double r2j = rkd2[jj + (size_t)ik * jv];
-            double r1j = rkd1[jj + (size_t)ik * jv];
+            const int jh = j - jv, jl = jh * LJ + (jv - jvb);
+            const double r2j = w2[jl], r1j = w1[jl];
             for (int iv = iv_lo; iv <= iv_hi; iv++) {
-                int ih = i - iv;
-                int ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                const int ih = i - iv, il = ih * LI + (iv - ivb);
                 double c;
-                if (iv < jv) c = rkd1[ii + (size_t)ik * iv] * r2j;
-                else if (iv > jv) c = r1j * rkd2[ii + (size_t)ik * iv];
-                else c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                if (iv < jv) c = u1[il] * r2j;
+                else if (iv > jv) c = r1j * u2[il];
+                else {
+                    int ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                    int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                    c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                }
                 acc = acc + c;
             }
         }
@@ -431,9 +469,10 @@ int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
 int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
                     double *rkb, int ldp, cudaStream_t s)
 {
-    dim3 blk(32, 8);
-    dim3 grd((b->ns + 31) / 32, (b->ns + 7) / 8, ldp * ldp);
-    rkb_expand_kernel<<<grd, blk, 0, s>>>(b->ks, b->ns, b->nv, ldp, rkd1, rkd2, rkd, rkb);
+    dim3 blk(EXP_TI, EXP_TJ);
+    dim3 grd((b->ns + EXP_TI - 1) / EXP_TI, (b->ns + EXP_TJ - 1) / EXP_TJ, ldp * ldp);
+    size_t shm = sizeof(double) * 2 * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
+    rkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, rkd1, rkd2, rkd, rkb);
     return cuda_fail(cudaGetLastError(), "mrk_cell");
 }
 

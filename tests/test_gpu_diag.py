@@ -1,8 +1,11 @@
 """bsr_hd's diag_hd on the GPU against the oracle's restatement (scipy LAPACK
 DSYGV / DSYEV standing in for the reference's LAPACK).
 
-Eigenvalue tolerance: 1e-11 relative, |dE| / max|E| over the spectrum, and
-per eigenvalue for the bound part (|E| >= 1)."""
+Eigenvalue tolerance: 1e-11 relative to the spectral radius, |dE| / max|E|.
+H spans about 7 orders of magnitude here (kinetic energies ~1/h_min^2 of the
+1e-3 a.u. first interval), so two backward-stable FP64 eigensolvers -- LAPACK
+DSYEV and cuSOLVER syevd alike -- may differ by ~eps*||A|| in every
+eigenvalue; the bound part is checked against that scale (|dE| <= 64 eps ||A||)."""
 import numpy as np
 import pytest
 
@@ -45,8 +48,9 @@ def test_eigenvalues_config1(config1):
     ev = to_np(res["eval"])
     er = ref["eval"]
     assert np.max(np.abs(ev - er)) / np.max(np.abs(er)) < TOL_E
-    bound = np.abs(er) >= 1.0
-    assert np.max(np.abs(ev[bound] - er[bound]) / np.abs(er[bound])) < TOL_E
+    bound = er < 0.0
+    anorm = np.max(np.abs(er))
+    assert np.max(np.abs(ev[bound] - er[bound])) <= 64 * np.finfo(float).eps * anorm
 
 
 def test_eigenvectors_residual_config1(config1):
@@ -92,3 +96,18 @@ def test_trace_invariance_config2():
     er = ref["eval"]
     assert abs(ev.sum() - ref["bval"].sum()) <= 1e-12 * np.abs(ref["bval"]).sum()
     assert np.max(np.abs(ev - er)) / np.max(np.abs(er)) < TOL_E
+
+
+def test_batched_channel_solves_match_sygvd(monkeypatch):
+    """The batched channel eigensolves (potrf + batched trsm + syevBatched) and the
+    per-channel sygvd path give the same spectrum."""
+    import bsr_b200 as bsr
+    pw = W.partial_wave("config1", seed=8)
+    gb = bsr.define_spline(pw["t"], pw["ks"])
+    ctx = bsr.Context()
+    H = bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], pw["coefs"])
+    a = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=False)["eval"])
+    monkeypatch.setenv("BSRG_CHANNEL_SYGVD", "1")
+    b = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=False)["eval"])
+    assert a.shape == b.shape
+    assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < TOL_E
