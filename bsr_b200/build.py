@@ -22,6 +22,7 @@ UNITS = {
     "convol.cu": ["--fmad=false"],
     "assemble.cu": [],
     "diag_hd.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -75,6 +75,20 @@ int bsrg_mrk_cell(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream
 /* Same, from moments already computed by bsrg_rk_moments (no allocation). */
 int bsrg_mrk_cell_from_moments(const bsrg_basis *b, const double *rkd1, const double *rkd2,
                                const double *rkd, double *rkb, int ldp, void *stream);
+/* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
+ *      not allocate device memory while they run (a serving process that has
+ *      split all of its HBM among its solves at start-up; loops that cannot
+ *      afford the device-wide stall a cudaMalloc/cudaFree may cause).  The
+ *      interval moments go to a static device array inside the library
+ *      (BSRG_NOALLOC_SCRATCH_DOUBLES doubles = 6 MiB, held by every GPU that
+ *      loads the library until exit), so the call allocates nothing.  Limit:
+ *      (2*ik + ik*ik)*nv <= BSRG_NOALLOC_SCRATCH_DOUBLES with ik = ks(ks+1)/2
+ *      (ks = 10: nv <= 250; ks = 8: nv <= 546); larger bases get BSRG_ERR_ARG.
+ *      The first call on a device looks up the array's device address and
+ *      should come before any stream capture on that device.  Calls share the
+ *      array: calls that overlap on the GPU race and must be serialised. */
+#define BSRG_NOALLOC_SCRATCH_DOUBLES 786432
+int bsrg_mrk_cell_noalloc(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream);
 
 /* ---- src/libs/BS/density.f90:2.  type 's' -> d (ns,ks); 'n' -> (ns,2ks-1);
  *      'x' -> (ns,ns).  Device. */
