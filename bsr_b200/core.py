@@ -14,7 +14,7 @@ import torch
 from ._lib import BsrgError, call, lib
 
 __all__ = ["BsrgError", "define_grid", "define_spline", "Basis", "rk_moments", "mrk_cell", "density", "convol",
-           "sum_amb", "Context", "assemble", "diag_hd", "partial_wave_solve", "fortran_empty", "as_fortran"]
+           "sum_amb", "Context", "assemble", "add_two_electron", "diag_hd", "partial_wave_solve", "fortran_empty", "as_fortran"]
 
 
 # ---------------------------------------------------------------------------
@@ -261,6 +261,16 @@ def assemble(ctx, basis, z, lch, ech, P, kmax, coefs, want_s=False, want_acf=Fal
     if want_acf:
         out["acf"] = acf
     return out
+
+
+def add_two_electron(ctx, basis, nch, P, kmax, coefs, hcc, acf=None):
+    """I_data Case(6..9) alone: accumulate the R^k groups into existing blocks hcc (and acf)."""
+    Pd = as_fortran(P)
+    c = _coef_arrays(coefs)
+    call("bsrg_add_two_electron", ctx.handle, basis.handle, nch, Pd.shape[1], _ptr(Pd), kmax, len(c["c"]),
+         _iptr(c["k"]), _iptr(c["type"]), _iptr(c["ich"]), _iptr(c["jch"]), _iptr(c["a"]), _iptr(c["b"]),
+         _dptr(c["c"]), _ptr(hcc), _ptr(acf) if acf is not None else None)
+    return hcc
 
 
 def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001, want_vectors=True,

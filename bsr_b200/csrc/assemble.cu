@@ -648,12 +648,18 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
 
 size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c) { return c ? c->ws_bytes : 0; }
 
-int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int *lch, const double *ech,
-                  int norb, const double *P, int kmax, int ncoef, const int *ck, const int *ctype,
-                  const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
-                  double *hcc, double *scc, double *acf)
+}  // extern "C"
+
+// full = true: the whole SUB1 of the synthetic partial wave (zeroed blocks, the
+// one-electron part, the groups, E_ch sb, symmetrisation); full = false: only
+// I_data Case(6..9) accumulated into the caller's blocks and acf.
+static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int *lch, const double *ech,
+                         int norb, const double *P, int kmax, int ncoef, const int *ck, const int *ctype,
+                         const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
+                         double *hcc, double *scc, double *acf, bool full)
 {
-    if (!c || !b || !lch || !ech || !P || !hcc || (ncoef > 0 && (!ck || !ctype || !cich || !cjch || !ca || !cb || !cval))) {
+    if (!c || !b || (full && (!lch || !ech)) || !P || !hcc ||
+        (ncoef > 0 && (!ck || !ctype || !cich || !cjch || !ca || !cb || !cval))) {
         set_error("assemble: null argument");
         return BSRG_ERR_ARG;
     }
@@ -742,7 +748,7 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
         xoff[k] = (o - o_gd) / sizeof(GroupDesc);
         stage(xgroups[k].data(), sizeof(GroupDesc) * xgroups[k].size());
     }
-    size_t o_lch = stage(lch, sizeof(int) * nch), o_ech = stage(ech, sizeof(double) * nch);
+    size_t o_lch = full ? stage(lch, sizeof(int) * nch) : 0, o_ech = full ? stage(ech, sizeof(double) * nch) : 0;
     cudaError_t e;
 #define CP(dst, off, bytes) \
     if ((bytes) > 0 && (e = cudaMemcpyAsync(dst, hp + (off), bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
@@ -751,22 +757,25 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
     CP(d_cb, o_cb, sizeof(int) * ncoef);
     CP(d_cv, o_cv, sizeof(double) * ncoef);
     CP(d_gd, o_gd, sizeof(GroupDesc) * ngroups);
-    CP(d_lch, o_lch, sizeof(int) * nch);
-    CP(d_ech, o_ech, sizeof(double) * nch);
+    if (full) {
+        CP(d_lch, o_lch, sizeof(int) * nch);
+        CP(d_ech, o_ech, sizeof(double) * nch);
+    }
 #undef CP
     cudaEventRecord(c->ev_stage, s);
     // ---- one-electron part ----
     size_t nblk = (size_t)nch * (nch + 1) / 2;
-    if ((e = cudaMemsetAsync(hcc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset hcc");
-    if (scc && (e = cudaMemsetAsync(scc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset scc");
-    if (acf && (e = cudaMemsetAsync(acf, 0, sizeof(double) * nch * nch * (kmax + 1), s)) != cudaSuccess)
-        return cuda_fail(e, "memset acf");
-    stage_begin(c, 3);
-    {
+    if (full) {
+        if ((e = cudaMemsetAsync(hcc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset hcc");
+        if (scc && (e = cudaMemsetAsync(scc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess)
+            return cuda_fail(e, "memset scc");
+        if (acf && (e = cudaMemsetAsync(acf, 0, sizeof(double) * nch * nch * (kmax + 1), s)) != cudaSuccess)
+            return cuda_fail(e, "memset acf");
+        stage_begin(c, 3);
         dim3 g((ns * ks + 127) / 128, nch);
         one_electron_kernel<<<g, 128, 0, s>>>(ns, ks, nch, d_lch, z, b->db2, b->rm2, b->rm1, hcc);
+        stage_end(c, 3);
     }
-    stage_end(c, 3);
     // ---- two-electron groups, one multipole at a time ----
     const size_t xsm = exchange_smem(ks);
     const int xg = exchange_groups_per_cta(ks);
@@ -813,6 +822,11 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "assemble k-loop");
     }
     // ---- target energies, overlap, symmetrisation ----
+    if (!full) {
+        rc = cuda_fail(cudaGetLastError(), "add_two_electron");
+        if (rc == BSRG_OK) rc = stage_collect(c);
+        return rc;
+    }
     stage_begin(c, 3);
     {
         dim3 g((ns * ks + 127) / 128, nch);
@@ -824,6 +838,25 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
     rc = cuda_fail(cudaGetLastError(), "assemble");
     if (rc == BSRG_OK) rc = stage_collect(c);
     return rc;
+}
+
+extern "C" {
+
+int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int *lch, const double *ech,
+                  int norb, const double *P, int kmax, int ncoef, const int *ck, const int *ctype,
+                  const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
+                  double *hcc, double *scc, double *acf)
+{
+    return assemble_impl(c, b, z, nch, lch, ech, norb, P, kmax, ncoef, ck, ctype, cich, cjch, ca, cb, cval, hcc,
+                         scc, acf, true);
+}
+
+int bsrg_add_two_electron(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const double *P, int kmax,
+                          int ncoef, const int *ck, const int *ctype, const int *cich, const int *cjch,
+                          const int *ca, const int *cb, const double *cval, double *hcc, double *acf)
+{
+    return assemble_impl(c, b, 0.0, nch, nullptr, nullptr, norb, P, kmax, ncoef, ck, ctype, cich, cjch, ca, cb,
+                         cval, hcc, nullptr, acf, false);
 }
 
 }  // extern "C"

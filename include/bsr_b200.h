@@ -148,6 +148,17 @@ int bsrg_assemble(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, const int
                   const int *cich, const int *cjch, const int *ca, const int *cb, const double *cval,
                   double *hcc, double *scc, double *acf);
 
+/* ---- src/bsr/BSR_MAT3/I_data.f90:192-218 alone (I_data Case 6..9 for the
+ *      Coulomb R^k integrals, icase 5): accumulates the two-electron groups into
+ *      the caller's hcc blocks and, for direct groups, into acf (UPDATE_CF),
+ *      without touching anything else -- the drop-in for the I_data call of
+ *      State_res.  Records as for bsrg_assemble; jtype 6 and 7 records go in as
+ *      type 0 and jtype 8 and 9 as type 1 (for the symmetric R^k table convol
+ *      icase 2 equals icase 1 and icase 4 equals icase 3).  acf may be NULL. */
+int bsrg_add_two_electron(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const double *P, int kmax,
+                          int ncoef, const int *ck, const int *ctype, const int *cich, const int *cjch,
+                          const int *ca, const int *cb, const double *cval, double *hcc, double *acf);
+
 /* ---- src/bsr/BSR_HD3/diag_hd.f90:2-340 for a block-diagonal S (diag_ovl /= 0):
  *      per-channel DSYGV on the diagonal blocks with the first l+1 splines
  *      dropped (:82-111), Egap/Edmax filter, transform of the off-diagonal

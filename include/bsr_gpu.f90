@@ -1,0 +1,234 @@
+!======================================================================
+!     bsr_gpu.f90 -- ISO_C_BINDING interface of libbsrgpu.so for the
+!     BSR Fortran codes (C ABI: include/bsr_b200.h)
+!----------------------------------------------------------------------
+!     Interfaces for the C entry points plus wrappers named after the
+!     routines they stand in for:
+!
+!       gpu_define_spline       after define_grid + define_spline
+!       gpu_mrk_cell(k)         mrk_cell (libs/BS/mrk_cell.f90:2): fills
+!                               module spline_integrals rkb from the GPU
+!       gpu_add_two_electron    the I_data Case(6..9) call for icase 5
+!                               (bsr/BSR_MAT3/I_data.f90:192-218)
+!       gpu_diag_hd             the eigen-solution of diag_hd for a
+!                               block-diagonal overlap (bsr/BSR_HD3/
+!                               diag_hd.f90:82-312)
+!
+!     Device memory is obtained from the CUDA runtime through its C
+!     interface (cudaMalloc / cudaMemcpy / cudaFree) bound below.
+!     A status /= 0 is turned into the reference's Stop with the
+!     library's message, so failures read like the reference's.
+!======================================================================
+      Module bsr_gpu
+
+      Use, intrinsic :: iso_c_binding
+      Implicit none
+
+      Integer(c_int), parameter :: BSRG_OK = 0
+      Integer(c_int), parameter :: cudaMemcpyHostToDevice = 1
+      Integer(c_int), parameter :: cudaMemcpyDeviceToHost = 2
+
+      Type(c_ptr), save :: gpu_basis = c_null_ptr     ! bsrg_basis*
+      Type(c_ptr), save :: gpu_ctx   = c_null_ptr     ! bsrg_ctx*
+      Type(c_ptr), save :: d_rkb     = c_null_ptr     ! device rkb(ns,ns,2ks-1,2ks-1)
+      Integer, save :: gpu_krk = -100                 ! multipole held in rkb
+
+      Interface
+
+       Function bsrg_last_error() bind(C, name="bsrg_last_error")
+        Import :: c_ptr
+        Type(c_ptr) :: bsrg_last_error
+       End Function
+
+       Function bsrg_define_spline(ks, ns, t, ml, me, h, stream, out) &
+                bind(C, name="bsrg_define_spline")
+        Import :: c_int, c_double, c_ptr
+        Integer(c_int), value :: ks, ns, ml, me
+        Real(c_double), intent(in) :: t(*)
+        Real(c_double), value :: h
+        Type(c_ptr), value :: stream
+        Type(c_ptr), intent(out) :: out
+        Integer(c_int) :: bsrg_define_spline
+       End Function
+
+       Function bsrg_mrk_cell(b, k, rkb, ldp, stream) bind(C, name="bsrg_mrk_cell")
+        Import :: c_int, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Integer(c_int) :: bsrg_mrk_cell
+       End Function
+
+       Function bsrg_ctx_create(device, stream, out) bind(C, name="bsrg_ctx_create")
+        Import :: c_int, c_ptr
+        Integer(c_int), value :: device
+        Type(c_ptr), value :: stream
+        Type(c_ptr), intent(out) :: out
+        Integer(c_int) :: bsrg_ctx_create
+       End Function
+
+       Function bsrg_add_two_electron(c, b, nch, norb, P, kmax, ncoef, ck, ctype, &
+                cich, cjch, ca, cb, cval, hcc, acf) bind(C, name="bsrg_add_two_electron")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: c, b, P, hcc, acf
+        Integer(c_int), value :: nch, norb, kmax, ncoef
+        Integer(c_int), intent(in) :: ck(*), ctype(*), cich(*), cjch(*), ca(*), cb(*)
+        Real(c_double), intent(in) :: cval(*)
+        Integer(c_int) :: bsrg_add_two_electron
+       End Function
+
+       Function bsrg_diag_hd(c, b, nch, lch, hcc, itype, ilzero, ibzero, edmax, egap, &
+                want_vectors, eval, khm, vecs, bb) bind(C, name="bsrg_diag_hd")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: c, b, hcc, eval, vecs, bb
+        Integer(c_int), value :: nch, itype, ilzero, ibzero, want_vectors
+        Integer(c_int), intent(in) :: lch(*)
+        Real(c_double), value :: edmax, egap
+        Integer(c_int), intent(out) :: khm
+        Integer(c_int) :: bsrg_diag_hd
+       End Function
+
+       Function cudaMalloc(p, bytes) bind(C, name="cudaMalloc")
+        Import :: c_int, c_ptr, c_size_t
+        Type(c_ptr) :: p
+        Integer(c_size_t), value :: bytes
+        Integer(c_int) :: cudaMalloc
+       End Function
+
+       Function cudaFree(p) bind(C, name="cudaFree")
+        Import :: c_int, c_ptr
+        Type(c_ptr), value :: p
+        Integer(c_int) :: cudaFree
+       End Function
+
+       Function cudaMemcpy(dst, src, bytes, kind) bind(C, name="cudaMemcpy")
+        Import :: c_int, c_ptr, c_size_t
+        Type(c_ptr), value :: dst, src
+        Integer(c_size_t), value :: bytes
+        Integer(c_int), value :: kind
+        Integer(c_int) :: cudaMemcpy
+       End Function
+
+      End Interface
+
+      Contains
+
+!======================================================================
+      Subroutine gpu_check(rc, where)
+!----------------------------------------------------------------------
+!     the reference stops on errors; so does the shim, with the message
+!----------------------------------------------------------------------
+      Integer(c_int), intent(in) :: rc
+      Character(*), intent(in) :: where
+      Character(len=512), pointer :: msg
+      Integer :: n
+      if (rc == BSRG_OK) Return
+      Call c_f_pointer(bsrg_last_error(), msg)
+      n = index(msg, c_null_char) - 1
+      if (n < 0) n = len(msg)
+      write(*,'(a,": ",a)') where, msg(1:n)
+      Stop 'bsr_gpu: GPU call failed'
+      End Subroutine gpu_check
+
+!======================================================================
+      Subroutine gpu_define_spline
+!----------------------------------------------------------------------
+!     after define_grid / define_spline: the same basis on the GPU
+!----------------------------------------------------------------------
+      Use spline_param
+      Use spline_grid, only: t
+      Call gpu_check(bsrg_define_spline(ks, ns, t, ml, me, h, c_null_ptr, gpu_basis), &
+                     'define_spline')
+      if (.not. c_associated(gpu_ctx)) &
+       Call gpu_check(bsrg_ctx_create(0_c_int, c_null_ptr, gpu_ctx), 'ctx_create')
+      gpu_krk = -100
+      End Subroutine gpu_define_spline
+
+!======================================================================
+      Subroutine gpu_mrk_cell(k)
+!----------------------------------------------------------------------
+!     mrk_cell(k) (mrk_cell.f90:2): module rkb filled from the GPU table
+!----------------------------------------------------------------------
+      Use spline_param
+      Use spline_integrals
+      Integer, intent(in) :: k
+      Integer(c_size_t) :: bytes
+      if (itype == 'aaa') Call allocate_integrals
+      if (itype == 'rk ' .and. krk == k) Return
+      bytes = int(ns, c_size_t) * ns * (2*ks-1) * (2*ks-1) * 8
+      if (.not. c_associated(d_rkb)) Call gpu_check(cudaMalloc(d_rkb, bytes), 'cudaMalloc rkb')
+      Call gpu_check(bsrg_mrk_cell(gpu_basis, k, d_rkb, 2*ks-1, c_null_ptr), 'mrk_cell')
+      Call gpu_check(cudaMemcpy(c_loc(rkb), d_rkb, bytes, cudaMemcpyDeviceToHost), 'cudaMemcpy rkb')
+      itype = 'rk '
+      krk = k
+      End Subroutine gpu_mrk_cell
+
+!======================================================================
+      Subroutine gpu_add_two_electron(nch, norb, pbs, kmax, ncoef, ck, ctype, &
+                                      cich, cjch, ca, cb, cval, hcc, acf)
+!----------------------------------------------------------------------
+!     I_data Case(6..9), icase 5: the coefficient records of all R^k
+!     channel-channel groups (sorted by k, type, ich, jch; type 0 for
+!     jtype 6/7, 1 for jtype 8/9; orbitals 0-based) added to hcc and acf
+!----------------------------------------------------------------------
+      Use spline_param, only: ns
+      Integer, intent(in) :: nch, norb, kmax, ncoef
+      Real(8), intent(in), target :: pbs(ns, norb)
+      Integer(c_int), intent(in) :: ck(*), ctype(*), cich(*), cjch(*), ca(*), cb(*)
+      Real(c_double), intent(in) :: cval(*)
+      Real(8), intent(inout), target :: hcc(ns, ns, nch*(nch+1)/2), acf(nch, nch, 0:kmax)
+      Type(c_ptr) :: dP, dH, dA
+      Integer(c_size_t) :: bp, bh, ba
+      bp = int(ns, c_size_t) * norb * 8
+      bh = int(ns, c_size_t) * ns * (nch*(nch+1)/2) * 8
+      ba = int(nch, c_size_t) * nch * (kmax+1) * 8
+      Call gpu_check(cudaMalloc(dP, bp), 'cudaMalloc P')
+      Call gpu_check(cudaMalloc(dH, bh), 'cudaMalloc hcc')
+      Call gpu_check(cudaMalloc(dA, ba), 'cudaMalloc acf')
+      Call gpu_check(cudaMemcpy(dP, c_loc(pbs), bp, cudaMemcpyHostToDevice), 'upload P')
+      Call gpu_check(cudaMemcpy(dH, c_loc(hcc), bh, cudaMemcpyHostToDevice), 'upload hcc')
+      Call gpu_check(cudaMemcpy(dA, c_loc(acf), ba, cudaMemcpyHostToDevice), 'upload acf')
+      Call gpu_check(bsrg_add_two_electron(gpu_ctx, gpu_basis, nch, norb, dP, kmax, ncoef, &
+                     ck, ctype, cich, cjch, ca, cb, cval, dH, dA), 'I_data')
+      Call gpu_check(cudaMemcpy(c_loc(hcc), dH, bh, cudaMemcpyDeviceToHost), 'download hcc')
+      Call gpu_check(cudaMemcpy(c_loc(acf), dA, ba, cudaMemcpyDeviceToHost), 'download acf')
+      Call gpu_check(cudaFree(dP), 'cudaFree'); Call gpu_check(cudaFree(dH), 'cudaFree')
+      Call gpu_check(cudaFree(dA), 'cudaFree')
+      End Subroutine gpu_add_two_electron
+
+!======================================================================
+      Subroutine gpu_diag_hd(nch, lch, hcc, itype, ilzero, ibzero, Edmax, Egap, &
+                             khm, eval, a)
+!----------------------------------------------------------------------
+!     diag_hd steps 1, 2 and 7 (diag_hd.f90:82-312) for diag_ovl /= 0:
+!     eigenvalues eval(1:khm) and eigenvectors a(1:khm,1:khm) in the
+!     channel eigenbasis, as the reference leaves them after LAP_DSYEV
+!----------------------------------------------------------------------
+      Use spline_param, only: ns
+      Integer, intent(in) :: nch, itype, ilzero, ibzero
+      Integer(c_int), intent(in) :: lch(nch)
+      Real(8), intent(in), target :: hcc(ns, ns, nch*(nch+1)/2)
+      Real(8), intent(in) :: Edmax, Egap
+      Integer, intent(out) :: khm
+      Real(8), intent(out), target :: eval(nch*ns), a(*)
+      Type(c_ptr) :: dH, dE, dV
+      Integer(c_size_t) :: bh, be, bv
+      Integer(c_int) :: k
+      bh = int(ns, c_size_t) * ns * (nch*(nch+1)/2) * 8
+      be = int(nch, c_size_t) * ns * 8
+      bv = int(nch, c_size_t) * ns * nch * ns * 8
+      Call gpu_check(cudaMalloc(dH, bh), 'cudaMalloc hcc')
+      Call gpu_check(cudaMalloc(dE, be), 'cudaMalloc eval')
+      Call gpu_check(cudaMalloc(dV, bv), 'cudaMalloc vectors')
+      Call gpu_check(cudaMemcpy(dH, c_loc(hcc), bh, cudaMemcpyHostToDevice), 'upload hcc')
+      Call gpu_check(bsrg_diag_hd(gpu_ctx, gpu_basis, nch, lch, dH, itype, ilzero, ibzero, &
+                     Edmax, Egap, 1_c_int, dE, k, dV, c_null_ptr), 'diag_hd')
+      khm = k
+      Call gpu_check(cudaMemcpy(c_loc(eval), dE, int(khm, c_size_t) * 8, cudaMemcpyDeviceToHost), &
+                     'download eval')
+      Call gpu_check(cudaMemcpy(c_loc(a), dV, int(khm, c_size_t) * khm * 8, cudaMemcpyDeviceToHost), &
+                     'download vectors')
+      Call gpu_check(cudaFree(dH), 'cudaFree'); Call gpu_check(cudaFree(dE), 'cudaFree')
+      Call gpu_check(cudaFree(dV), 'cudaFree')
+      End Subroutine gpu_diag_hd
+
+      End Module bsr_gpu

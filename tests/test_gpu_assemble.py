@@ -115,3 +115,21 @@ def test_config2_blocks_via_subproblem():
         gbk = h[:, :, i * (i - 1) // 2 + j - 1]
         err = np.max(np.abs(gbk - rb)) / np.max(np.abs(rb))
         assert err < TOL_H, ((i, j), err)
+
+
+def test_add_two_electron_is_i_data_alone():
+    """bsrg_add_two_electron accumulates exactly the I_data groups: on zeroed blocks
+    its off-diagonal blocks equal the full assembly's (which holds no other term there)."""
+    import torch
+
+    import bsr_b200 as bsr
+    pw = W.partial_wave("config1", seed=6)
+    gb, ctx, full = gpu_assemble(pw, want=False)
+    nch = pw["nch"]
+    h2 = torch.zeros_like(full["hcc"])
+    bsr.add_two_electron(ctx, gb, nch, pw["P"], pw["kmax"], pw["coefs"], h2)
+    a, b = to_np(h2), to_np(full["hcc"])
+    for i in range(2, nch + 1):
+        for j in range(1, i):
+            q = i * (i - 1) // 2 + j - 1
+            assert np.array_equal(a[:, :, q], b[:, :, q]), (i, j)

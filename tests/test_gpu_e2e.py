@@ -29,3 +29,27 @@ def test_repeatable():
     a = bsr.partial_wave_solve(ctx, pw, want_vectors=False)
     b = bsr.partial_wave_solve(ctx, pw, want_vectors=False)
     assert np.array_equal(a, b)
+
+
+def test_bsr_mat_file_round_trip(tmp_path):
+    """GPU assembly -> bsr_mat.nnn (the reference's file) -> GPU diag_hd gives the same spectrum
+    as solving the in-memory blocks: the file carries everything bsr_hd needs."""
+    import torch
+
+    import bsr_b200 as bsr
+    from bsr_b200 import bsrmat_io as io
+    pw = W.partial_wave("config1", seed=9)
+    ctx = bsr.Context()
+    gb = bsr.define_spline(pw["t"], pw["ks"])
+    H = bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], pw["coefs"], want_s=True,
+                     want_acf=True)
+    ev = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=False)["eval"])
+    hcc = to_np(H["hcc"]).transpose(2, 0, 1)
+    scc = to_np(H["scc"]).transpose(2, 0, 1)
+    p = tmp_path / "bsr_mat.001"
+    io.write_bsr_mat(p, scc, hcc, pw["nch"], gb.ns, to_np(H["acf"]), rmax=pw["t"][-1], etarg=pw["ech"])
+    r = io.read_bsr_mat(p)
+    assert r["diag_ovl"] == 1
+    h2 = bsr.as_fortran(np.ascontiguousarray(r["hcc"].transpose(1, 2, 0)))
+    ev2 = to_np(bsr.diag_hd(ctx, gb, pw["lch"], h2, want_vectors=False)["eval"])
+    assert np.array_equal(ev, ev2)
