@@ -24,6 +24,7 @@
 // A block receives at most one group per (k, structure), so no two CTAs of one
 // launch update the same H element and no atomics are needed.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -436,6 +437,147 @@ exchange_kernel(int ns, int ng, PadLayout L, const GroupDesc *__restrict__ gd, c
     }
 }
 
+// ---------------------------------------------------------------------------
+// Exchange groups through the rank structure of the group densities.
+//
+// D_g = sum_t c_t p_a p_b^T is a sum of outer products, so
+//   a_g(x,y') = sum_(e,f) R(x,x+e,y'+f,y') D_g(x+e,y'+f)
+//             = sum_t c_t Z[y'][x][a_t][b_t]
+// with, for every orbital pair,
+//   W[y'][x][e][b] = sum_f R(x,x+e,y'+f,y') p_b(y'+f)      (19 x norb per output)
+//   Z[y'][x][a][b] = sum_e p_a(x+e) W[y'][x][e][b]         (norb x norb per output)
+// The reference contracts every group separately (convol icase 3 on the group
+// density, (2ks-1)^2 multiply-adds per output and group); here each output
+// costs (2ks-1)^2 norb + (2ks-1) norb^2 multiply-adds once for all groups plus
+// one multiply-add per coefficient -- about 8x fewer at the config-2 sizes.
+// One CTA per (column y', XCH consecutive rows x): R for the CTA goes to shared
+// memory once, W and Z stay in shared memory, and each group's XCH outputs of
+// the row are written side by side.  Same sum as the gather kernel, grouped
+// differently: results agree to rounding.
+// ---------------------------------------------------------------------------
+constexpr int XCH = 4;                  // rows x per CTA
+constexpr int NORB_MAX = 32;            // orbitals the factored kernel handles
+constexpr int ZLD = NORB_MAX + 1;       // padded leading dimension of Z rows
+
+template <int KS>
+__global__ void __launch_bounds__(256)
+exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc *__restrict__ gd,
+                         const unsigned short *__restrict__ zoff, const double *__restrict__ cv,
+                         const double *__restrict__ P, const double *__restrict__ rkbp, double *hcc)
+{
+    constexpr int HW = KS - 1, NE = 2 * KS - 1, PXR = XCH + 2 * HW;
+    extern __shared__ double fsm[];
+    double *Py = fsm;                                    // p_b(y'+f)          [f][b]
+    double *Px = Py + NE * NORB_MAX;                     // p_a(x0-HW+r)       [r][a]
+    double *Rs = Px + PXR * NORB_MAX;                    // R(x,x+e,y'+f,y')   [xi][e][f]
+    double *Ws = Rs + XCH * NE * NE;                     // W                  [xi][e][b]
+    double *Zs = Ws + XCH * NE * NORB_MAX;               // Z                  [xi][a][b]
+    const int yp = blockIdx.y;
+    const int x0 = blockIdx.x * XCH;
+    const int tid = threadIdx.x;
+    // ---- stage p(y'+f), p(x0-HW+r) and the CTA's R values ----
+    for (int q = tid; q < NE * NORB_MAX; q += 256) {
+        int f = q / NORB_MAX - HW, b = q % NORB_MAX, y = yp + f;
+        Py[q] = (b < norb && y >= 0 && y < ns) ? P[y + (size_t)ns * b] : 0.0;
+    }
+    for (int q = tid; q < PXR * NORB_MAX; q += 256) {
+        int r = q / NORB_MAX, a = q % NORB_MAX, xr = x0 - HW + r;
+        Px[q] = (a < norb && xr >= 0 && xr < ns) ? P[xr + (size_t)ns * a] : 0.0;
+    }
+    for (int q = tid; q < XCH * NE * NE; q += 256) {
+        int xi = q % XCH, ef = q / XCH, e = ef / NE - HW, f = ef % NE - HW;
+        int x = x0 + xi;
+        double v = 0.0;
+        if (x < ns) {
+            int r1 = e >= 0 ? x : x + e, r2 = f >= 0 ? yp : yp + f;
+            v = rkbp[(size_t)(r1 + L.PL) + (size_t)L.NP * (r2 + L.PL) + L.slice * ((e >= 0 ? e : -e) + KS * (f >= 0 ? f : -f))];
+        }
+        Rs[(xi * NE + (e + HW)) * NE + (f + HW)] = v;
+    }
+    __syncthreads();
+    // ---- W[xi][e][b] = sum_f R[xi][e][f] Py[f][b] ----
+    for (int q = tid; q < XCH * NE * NORB_MAX; q += 256) {
+        int b = q % NORB_MAX, xe = q / NORB_MAX;            // xe = xi*NE + e
+        const double *r = Rs + xe * NE;
+        double w = 0.0;
+#pragma unroll
+        for (int f = 0; f < NE; f++) w = fma(r[f], Py[f * NORB_MAX + b], w);
+        Ws[q] = w;
+    }
+    __syncthreads();
+    // ---- Z[xi][a][b] = sum_e Px[xi+e][a] W[xi][e][b], 2x4 register tiles ----
+    for (int q = tid; q < XCH * (NORB_MAX / 2) * (NORB_MAX / 4); q += 256) {
+        int xi = q / ((NORB_MAX / 2) * (NORB_MAX / 4)), rem = q % ((NORB_MAX / 2) * (NORB_MAX / 4));
+        int a0 = (rem / (NORB_MAX / 4)) * 2, b0 = (rem % (NORB_MAX / 4)) * 4;
+        double z[2][4] = {};
+#pragma unroll
+        for (int e = 0; e < NE; e++) {
+            const double *pa = Px + (xi + e) * NORB_MAX + a0;
+            const double *wb = Ws + (xi * NE + e) * NORB_MAX + b0;
+            double av[2] = {pa[0], pa[1]};
+            double bv[4] = {wb[0], wb[1], wb[2], wb[3]};
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) z[i][j] = fma(av[i], bv[j], z[i][j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) Zs[(xi * NORB_MAX + a0 + i) * ZLD + b0 + j] = z[i][j];
+    }
+    __syncthreads();
+    // ---- a_g(x, y') = sum_t c_t Z[xi][a_t][b_t]; UPDATE_HX 'x' ----
+    // thread (g, xi): the XCH threads of a group read the same terms (broadcast)
+    const size_t nn = (size_t)ns * ns;
+    for (int q = tid; q < ng * XCH; q += 256) {
+        int g = q / XCH, xi = q % XCH, x = x0 + xi;
+        if (x >= ns) continue;
+        GroupDesc G = gd[g];
+        const double *Z = Zs + xi * NORB_MAX * ZLD;
+        double acc = 0.0;
+        for (int t = G.start; t < G.end; t++) acc = fma(cv[t], Z[zoff[t]], acc);
+        hcc[(size_t)G.blk * nn + x + (size_t)ns * yp] += acc;
+    }
+}
+
+typedef void (*exchange_factored_fn)(int, int, int, PadLayout, const GroupDesc *, const unsigned short *,
+                                     const double *, const double *, const double *, double *);
+
+// Z offset a*ZLD + b of every coefficient, so the term loop of the factored
+// kernel reads 10 bytes per term (all CTAs of a launch re-read the terms)
+__global__ void pack_terms_kernel(int ncoef, const int *__restrict__ ca, const int *__restrict__ cb,
+                                  unsigned short *zoff)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ncoef) zoff[t] = (unsigned short)(ca[t] * ZLD + cb[t]);
+}
+
+static size_t exchange_factored_smem(int ks)
+{
+    int NE = 2 * ks - 1, PXR = XCH + 2 * (ks - 1);
+    return sizeof(double) * ((size_t)NE * NORB_MAX + (size_t)PXR * NORB_MAX + (size_t)XCH * NE * NE +
+                             (size_t)XCH * NE * NORB_MAX + (size_t)XCH * NORB_MAX * ZLD);
+}
+
+static exchange_factored_fn exchange_factored_for(int ks)
+{
+    switch (ks) {
+    case 2: return exchange_factored_kernel<2>;
+    case 3: return exchange_factored_kernel<3>;
+    case 4: return exchange_factored_kernel<4>;
+    case 5: return exchange_factored_kernel<5>;
+    case 6: return exchange_factored_kernel<6>;
+    case 7: return exchange_factored_kernel<7>;
+    case 8: return exchange_factored_kernel<8>;
+    case 9: return exchange_factored_kernel<9>;
+    case 10: return exchange_factored_kernel<10>;
+    case 11: return exchange_factored_kernel<11>;
+    case 12: return exchange_factored_kernel<12>;
+    default: return nullptr;
+    }
+}
+
 static int exchange_groups_per_cta(int ks) { return ks <= 12 ? 4 : 2; }
 
 static size_t exchange_smem(int ks)
@@ -716,6 +858,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     add(sizeof(double) * PL.slice * ks * ks);
     add(sizeof(double) * maxgd * ns * ks);
     add(sizeof(double) * (size_t)ns * ks * 3);
+    add(sizeof(unsigned short) * (size_t)ncoef);
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) return rc;
     size_t host_bytes = sizeof(int) * (size_t)ncoef * 2 + sizeof(double) * (size_t)ncoef +
@@ -734,6 +877,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     double *Xd = ar.take<double>(std::max<size_t>(maxgd, 1) * ns * ks);
     double *rmk = ar.take<double>((size_t)ns * ks);
     double *M1 = ar.take<double>((size_t)ns * ks), *M2 = ar.take<double>((size_t)ns * ks);
+    unsigned short *d_zoff = ar.take<unsigned short>(std::max(ncoef, 1));
     // stage host metadata through pinned memory, one copy
     char *hp = (char *)c->pinned;
     size_t o = 0;
@@ -783,6 +927,18 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     if (!xk) { set_error("assemble: ks=%d unsupported", ks); return BSRG_ERR_ARG; }
     if ((e = cudaFuncSetAttribute(xk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm)) != cudaSuccess)
         return cuda_fail(e, "exchange smem");
+    // the factored exchange handles up to NORB_MAX orbitals; BSRG_EXCHANGE_GATHER selects the gather kernel
+    exchange_factored_fn xf = (norb <= NORB_MAX && !getenv("BSRG_EXCHANGE_GATHER")) ? exchange_factored_for(ks) : nullptr;
+    const size_t xfsm = exchange_factored_smem(ks);
+    if (xf) {
+        if ((e = cudaFuncSetAttribute(xf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xfsm)) != cudaSuccess)
+            return cuda_fail(e, "exchange (factored) smem");
+        if (ncoef > 0) {
+            stage_begin(c, 2);
+            pack_terms_kernel<<<(ncoef + 255) / 256, 256, 0, s>>>(ncoef, d_ca, d_cb, d_zoff);
+            stage_end(c, 2, 1);
+        }
+    }
     for (int k = 0; k <= kmax; k++) {
         int nd = (int)dgroups[k].size(), nx = (int)xgroups[k].size();
         if (nd == 0 && nx == 0) continue;
@@ -814,9 +970,14 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         }
         if (nx > 0) {
             stage_begin(c, 2);
-            int tiles = ((ns + XTX - 1) / XTX) * ((ns + XTY - 1) / XTY);
-            dim3 g3(tiles, (nx + xg - 1) / xg);
-            xk<<<g3, 256, xsm, s>>>(ns, nx, PL, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkbp, hcc);
+            if (xf) {
+                dim3 g3((ns + XCH - 1) / XCH, ns);
+                xf<<<g3, 256, xfsm, s>>>(ns, norb, nx, PL, d_gd + xoff[k], d_zoff, d_cv, P, rkbp, hcc);
+            } else {
+                int tiles = ((ns + XTX - 1) / XTX) * ((ns + XTY - 1) / XTY);
+                dim3 g3(tiles, (nx + xg - 1) / xg);
+                xk<<<g3, 256, xsm, s>>>(ns, nx, PL, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkbp, hcc);
+            }
             stage_end(c, 2, 1);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "assemble k-loop");

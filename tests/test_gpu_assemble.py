@@ -133,3 +133,16 @@ def test_add_two_electron_is_i_data_alone():
         for j in range(1, i):
             q = i * (i - 1) // 2 + j - 1
             assert np.array_equal(a[:, :, q], b[:, :, q]), (i, j)
+
+
+@pytest.mark.parametrize("gather", [False, True])
+def test_exchange_paths_match_oracle(monkeypatch, gather):
+    """Both exchange kernels -- the factored one (default, norb <= 32) and the
+    per-group gather one -- give the oracle's blocks to 1e-12."""
+    if gather:
+        monkeypatch.setenv("BSRG_EXCHANGE_GATHER", "1")
+    pw = W.partial_wave("config1", seed=12)
+    ob, ref = oracle_assemble(pw, want_acf=False)
+    gb, ctx, out = gpu_assemble(pw, want=False)
+    errs = block_errors(to_np(out["hcc"]), ref["hcc"])
+    assert errs.max() < TOL_H, errs.max()
