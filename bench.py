@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched and serving sub-results")
     return ap.parse_args()
 
 
@@ -456,6 +457,10 @@ def run_b200(args):
         "gpu_launches": int(round(own_launches * args.steps)),
         "clocks": clk,
     }
+    if world == 1 and not args.no_batched:
+        del ctx, basis, P, res
+        torch.cuda.empty_cache()
+        line["batched"], line["serving"] = bench_batched_serving(torch, bsr)
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         total, st, desc = cpu_reference_step(pw, threads)
@@ -464,6 +469,84 @@ def run_b200(args):
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def bench_batched_serving(torch, bsr):
+    """Batched (64 symmetries of the config4 distribution, all submitted at once) and
+    served (a Poisson stream of config5 requests) solves on one GPU, FP64, with
+    eigenvectors.  Host wall clock from the first submit to the last result; the
+    plain path (one context, symmetries one after another) is timed beside."""
+    from bsr_b200 import serve
+    from bsr_b200 import workload as W
+
+    b = W.symmetry_batch("config4")
+    syms = b["symmetries"]
+    basis = bsr.define_spline(b["t"], b["ks"])
+    P = bsr.as_fortran(b["P"])
+    ctx = bsr.Context()
+
+    def plain(s):
+        H = bsr.assemble(ctx, basis, b["z"], s["lch"], s["ech"], P, b["kmax"], s["coefs"])
+        return bsr.diag_hd(ctx, basis, s["lch"], H["hcc"], want_vectors=True)["eval"].cpu().numpy()
+
+    for s in syms[:2]:
+        plain(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq = [plain(s) for s in syms]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    del ctx
+    torch.cuda.empty_cache()
+
+    def make(n):
+        return serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=n)
+
+    tune = {}
+    n_best = serve.autotune_streams(make, syms[::4], candidates=(1, 2, 3, 4), cache=tune, key="config4")
+    srv = make(n_best)
+    try:
+        serve.run_stream(srv, syms[:2], [0.0, 0.0])
+        reqs = serve.run_stream(srv, syms, [0.0] * len(syms))
+        st = srv.stats(reqs)
+        res = [r.wait() for r in reqs]
+    finally:
+        srv.close()
+    same = all(np.array_equal(r["eval"], e) for r, e in zip(res, seq))
+    maxrel = max(float(np.max(np.abs(r["eval"] - e)) / np.max(np.abs(e))) for r, e in zip(res, seq))
+    nchs = [s["nch"] for s in syms]
+    batched = {
+        "workload": "config4: %d symmetries, channels %d..%d (log-uniform 4..60), ks=%d ns=%d k=0..%d, FP64 with "
+                    "eigenvectors, all submitted at t=0" % (len(syms), min(nchs), max(nchs), b["ks"], b["ns"], b["kmax"]),
+        "solves_per_s": st["solves_per_s"], "plain_solves_per_s": len(syms) / t_seq,
+        "speedup_vs_plain": st["solves_per_s"] * t_seq / len(syms),
+        "p50_s": st["p50_s"], "p99_s": st["p99_s"], "n_streams": n_best,
+        "autotune_solves_per_s": tune["config4"]["solves_per_s"],
+        "eigenvalues_equal_plain": same, "max_rel_diff_vs_plain": maxrel,
+        "timing": "host wall clock, first submit to last result; resident R^k tables; HBM-budget admission",
+    }
+    del srv
+    torch.cuda.empty_cache()
+    b5, arrivals = W.request_stream("config5")
+    srv = serve.PartialWaveServer(b5["t"], b5["ks"], b5["z"], b5["P"], b5["kmax"], n_streams=n_best)
+    try:
+        serve.run_stream(srv, b5["symmetries"][:2], [0.0, 0.0])
+        reqs = serve.run_stream(srv, b5["symmetries"], arrivals)
+        st5 = srv.stats(reqs)
+        peak = srv.queue.peak
+    finally:
+        srv.close()
+    nch5 = [s["nch"] for s in b5["symmetries"]]
+    serving = {
+        "workload": "config5: %d requests, Poisson arrivals at %.0f/s over %.2f s, channels %d..%d (log-uniform "
+                    "4..80), config4 basis, FP64 with eigenvectors" % (len(nch5), W.CONFIGS["config5"]["rate_per_s"],
+                                                                      float(arrivals[-1]), min(nch5), max(nch5)),
+        "solves_per_s": st5["solves_per_s"], "p50_s": st5["p50_s"], "p99_s": st5["p99_s"], "mean_s": st5["mean_s"],
+        "n_streams": n_best, "peak_admitted_gb": peak / 1e9,
+        "timing": "host wall clock; latency = submit to eigenvalues on the host; offered load is above capacity, "
+                  "so latency includes queueing",
+    }
+    return batched, serving
 
 
 def _group_counts(c, ty):

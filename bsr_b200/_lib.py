@@ -39,6 +39,10 @@ SIGNATURES = [
     ("bsrg_ctx_workspace_bytes", _c_size_t, [_P]),
     ("bsrg_ctx_set_timing", _c_int, [_P, _c_int]),
     ("bsrg_ctx_stage_times", _c_int, [_P, _DP, _IP, _c_int]),
+    ("bsrg_tables_create", _c_int, [_P, _P, _c_int, ctypes.POINTER(_c_void_p)]),
+    ("bsrg_tables_free", _c_int, [_P]),
+    ("bsrg_tables_bytes", _c_size_t, [_P]),
+    ("bsrg_ctx_use_tables", _c_int, [_P, _P]),
     ("bsrg_assemble", _c_int, [_P, _P, _c_double, _c_int, _IP, _DP, _c_int, _P, _c_int, _c_int,
                                _IP, _IP, _IP, _IP, _IP, _IP, _DP, _P, _P, _P]),
     ("bsrg_add_two_electron", _c_int, [_P, _P, _c_int, _c_int, _P, _c_int, _c_int, _IP, _IP, _IP, _IP, _IP,

@@ -14,7 +14,7 @@ import torch
 from ._lib import BsrgError, call, lib
 
 __all__ = ["BsrgError", "define_grid", "define_spline", "Basis", "rk_moments", "mrk_cell", "density", "convol",
-           "sum_amb", "Context", "assemble", "add_two_electron", "diag_hd", "partial_wave_solve", "fortran_empty", "as_fortran"]
+           "sum_amb", "Context", "Tables", "assemble", "add_two_electron", "diag_hd", "partial_wave_solve", "fortran_empty", "as_fortran"]
 
 
 # ---------------------------------------------------------------------------
@@ -208,6 +208,11 @@ class Context:
     def workspace_bytes(self):
         return lib().bsrg_ctx_workspace_bytes(self.handle)
 
+    def use_tables(self, tables):
+        """Use resident R^k tables (Tables) in assemble for their basis; None stops."""
+        call("bsrg_ctx_use_tables", self.handle, tables.handle if tables is not None else None)
+        self._tables = tables
+
     STAGES = ("rk_moments", "direct", "exchange", "one_electron", "channel_eig", "transform", "dense_eig",
               "rk_expand")
 
@@ -229,6 +234,30 @@ class Context:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class Tables:
+    """R^k tables of k = 0..kmax for one basis, resident on the device."""
+
+    def __init__(self, ctx, basis, kmax):
+        h = ctypes.c_void_p()
+        call("bsrg_tables_create", ctx.handle, basis.handle, kmax, ctypes.byref(h))
+        self.handle, self.basis, self.kmax = h, basis, kmax
+
+    def nbytes(self):
+        return lib().bsrg_tables_bytes(self.handle)
+
+    def free(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            torch.cuda.synchronize()
+            lib().bsrg_tables_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
         except Exception:
             pass
 

@@ -578,6 +578,19 @@ static exchange_factored_fn exchange_factored_for(int ks)
     }
 }
 
+// band moments + zero-margined R^k table of multipole k (from its cell moments)
+static int build_padded_table(const bsrg_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
+                              double *M1, double *M2, double *rkbp, cudaStream_t s)
+{
+    const int ns = b->ns, ks = b->ks, nv = b->nv;
+    const PadLayout PL = pad_layout(ns, ks);
+    band_moment_kernel<<<(ns * ks + 127) / 128, 128, 0, s>>>(ks, ns, nv, rkd1, rkd2, M1, M2);
+    dim3 gp((PL.NP + 31) / 32, (PL.NP + 7) / 8, ks * ks);
+    rkb_pad_kernel<<<gp, dim3(32, 8), 0, s>>>(ks, ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
+    (void)k;
+    return cuda_fail(cudaGetLastError(), "R^k table");
+}
+
 static int exchange_groups_per_cta(int ks) { return ks <= 12 ? 4 : 2; }
 
 static size_t exchange_smem(int ks)
@@ -855,7 +868,8 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     add(sizeof(double) * (size_t)ik * nv * 2);
     add(sizeof(double) * (size_t)ik * ik * nv);
     const PadLayout PL = pad_layout(ns, ks);
-    add(sizeof(double) * PL.slice * ks * ks);
+    const bsrg_tables *tabs = (c->tables && c->tables->basis == b && c->tables->kmax >= kmax) ? c->tables : nullptr;
+    if (!tabs) add(sizeof(double) * PL.slice * ks * ks);
     add(sizeof(double) * maxgd * ns * ks);
     add(sizeof(double) * (size_t)ns * ks * 3);
     add(sizeof(unsigned short) * (size_t)ncoef);
@@ -873,7 +887,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     double *d_ech = ar.take<double>(nch);
     double *rkd1 = ar.take<double>((size_t)ik * nv), *rkd2 = ar.take<double>((size_t)ik * nv);
     double *rkd = ar.take<double>((size_t)ik * ik * nv);
-    double *rkbp = ar.take<double>(PL.slice * ks * ks);
+    double *rkbp = tabs ? nullptr : ar.take<double>(PL.slice * ks * ks);
     double *Xd = ar.take<double>(std::max<size_t>(maxgd, 1) * ns * ks);
     double *rmk = ar.take<double>((size_t)ns * ks);
     double *M1 = ar.take<double>((size_t)ns * ks), *M2 = ar.take<double>((size_t)ns * ks);
@@ -942,24 +956,26 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     for (int k = 0; k <= kmax; k++) {
         int nd = (int)dgroups[k].size(), nx = (int)xgroups[k].size();
         if (nd == 0 && nx == 0) continue;
-        stage_begin(c, 0);
-        rc = launch_rk_moments(b, k, rkd1, rkd2, rkd, s);
-        if (rc != BSRG_OK) return rc;
-        stage_end(c, 0, 3);
-        stage_begin(c, 7);
-        band_moment_kernel<<<(ns * ks + 127) / 128, 128, 0, s>>>(ks, ns, nv, rkd1, rkd2, M1, M2);
-        {
-            dim3 gp((PL.NP + 31) / 32, (PL.NP + 7) / 8, ks * ks);
-            rkb_pad_kernel<<<gp, dim3(32, 8), 0, s>>>(ks, ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
+        const double *rkbk = rkbp;
+        if (tabs) {
+            rkbk = tabs->rkbp + tabs->table_doubles * k;        // resident table of this multipole
+        } else {
+            stage_begin(c, 0);
+            rc = launch_rk_moments(b, k, rkd1, rkd2, rkd, s);
+            if (rc != BSRG_OK) return rc;
+            stage_end(c, 0, 3);
+            stage_begin(c, 7);
+            rc = build_padded_table(b, k, rkd1, rkd2, rkd, M1, M2, rkbp, s);
+            if (rc != BSRG_OK) return rc;
+            stage_end(c, 7, 2);
         }
-        stage_end(c, 7, 2);
         if (nd > 0) {
             stage_begin(c, 1);
             const GroupDesc *gdd = d_gd + doff[k];
             dim3 g1((ns * ks + 127) / 128, nd);
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
             dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
-            direct_gemm_kernel<<<g2, DG_THREADS, 0, s>>>(ns, ks, nd, gdd, Xd, rkbp, PL, hcc);
+            direct_gemm_kernel<<<g2, DG_THREADS, 0, s>>>(ns, ks, nd, gdd, Xd, rkbk, PL, hcc);
             if (acf) {
                 rc = launch_mrm(b, k, rmk, s);
                 if (rc != BSRG_OK) return rc;
@@ -972,11 +988,11 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             stage_begin(c, 2);
             if (xf) {
                 dim3 g3((ns + XCH - 1) / XCH, ns);
-                xf<<<g3, 256, xfsm, s>>>(ns, norb, nx, PL, d_gd + xoff[k], d_zoff, d_cv, P, rkbp, hcc);
+                xf<<<g3, 256, xfsm, s>>>(ns, norb, nx, PL, d_gd + xoff[k], d_zoff, d_cv, P, rkbk, hcc);
             } else {
                 int tiles = ((ns + XTX - 1) / XTX) * ((ns + XTY - 1) / XTY);
                 dim3 g3(tiles, (nx + xg - 1) / xg);
-                xk<<<g3, 256, xsm, s>>>(ns, nx, PL, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkbp, hcc);
+                xk<<<g3, 256, xsm, s>>>(ns, nx, PL, d_gd + xoff[k], d_ca, d_cb, d_cv, P, rkbk, hcc);
             }
             stage_end(c, 2, 1);
         }
@@ -1018,6 +1034,53 @@ int bsrg_add_two_electron(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, c
 {
     return assemble_impl(c, b, 0.0, nch, nullptr, nullptr, norb, P, kmax, ncoef, ck, ctype, cich, cjch, ca, cb,
                          cval, hcc, nullptr, acf, false);
+}
+
+int bsrg_tables_create(bsrg_ctx *c, const bsrg_basis *b, int kmax, bsrg_tables **out)
+{
+    if (!c || !b || !out || kmax < 0 || kmax > 64) { set_error("tables_create: bad argument"); return BSRG_ERR_ARG; }
+    const int ns = b->ns, ks = b->ks, nv = b->nv, ik = ik_of(ks);
+    const PadLayout PL = pad_layout(ns, ks);
+    bsrg_tables *t = new bsrg_tables();
+    t->basis = b;
+    t->kmax = kmax;
+    t->table_doubles = PL.slice * ks * ks;
+    cudaError_t e = cudaMalloc((void **)&t->rkbp, sizeof(double) * t->table_doubles * (kmax + 1));
+    if (e != cudaSuccess) { delete t; return cuda_fail(e, "tables_create alloc"); }
+    double *scratch = nullptr;
+    size_t n1 = (size_t)ik * nv, n3 = (size_t)ik * ik * nv;
+    e = cudaMalloc((void **)&scratch, sizeof(double) * (2 * n1 + n3 + 2 * (size_t)ns * ks));
+    if (e != cudaSuccess) { cudaFree(t->rkbp); delete t; return cuda_fail(e, "tables_create scratch"); }
+    int rc = BSRG_OK;
+    for (int k = 0; k <= kmax && rc == BSRG_OK; k++) {
+        rc = launch_rk_moments(b, k, scratch, scratch + n1, scratch + 2 * n1, c->stream);
+        if (rc == BSRG_OK)
+            rc = build_padded_table(b, k, scratch, scratch + n1, scratch + 2 * n1, scratch + 2 * n1 + n3,
+                                    scratch + 2 * n1 + n3 + (size_t)ns * ks, t->rkbp + t->table_doubles * k, c->stream);
+    }
+    cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    cudaFree(scratch);
+    if (rc == BSRG_OK && e2 != cudaSuccess) rc = cuda_fail(e2, "tables_create");
+    if (rc != BSRG_OK) { cudaFree(t->rkbp); delete t; return rc; }
+    *out = t;
+    return BSRG_OK;
+}
+
+int bsrg_tables_free(bsrg_tables *t)
+{
+    if (!t) return BSRG_OK;
+    cudaFree(t->rkbp);
+    delete t;
+    return BSRG_OK;
+}
+
+size_t bsrg_tables_bytes(const bsrg_tables *t) { return t ? sizeof(double) * t->table_doubles * (t->kmax + 1) : 0; }
+
+int bsrg_ctx_use_tables(bsrg_ctx *c, const bsrg_tables *t)
+{
+    if (!c) { set_error("ctx_use_tables: null context"); return BSRG_ERR_ARG; }
+    c->tables = t;
+    return BSRG_OK;
 }
 
 }  // extern "C"

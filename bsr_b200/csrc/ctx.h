@@ -12,6 +12,15 @@ struct bsrg_stage_event {
     cudaEvent_t start, stop;
 };
 
+// R^k tables of one basis for k = 0..kmax, resident in the assembly's
+// zero-margined layout (built once, shared by every partial wave of the basis)
+struct bsrg_tables {
+    const bsrg_basis *basis;
+    int kmax;
+    double *rkbp;            // (kmax+1) consecutive tables
+    size_t table_doubles;    // doubles per multipole
+};
+
 struct bsrg_ctx {
     int device;
     cudaStream_t stream;
@@ -28,6 +37,7 @@ struct bsrg_ctx {
     std::vector<cudaEvent_t> *pool;          // free events
     double stage_ms[BSRG_NSTAGE];
     int stage_launches[BSRG_NSTAGE];
+    const bsrg_tables *tables;               // resident tables to use, or NULL
 };
 
 namespace bsrg {

@@ -23,7 +23,8 @@ import math
 
 def symmetry_dims(nch, ns, lch, ks):
     """(khm upper bound, H bytes, dense bytes) of one symmetry."""
-    khm = nch * ns - sum(min(l, ks - 2) + 1 for l in lch)
+    nch, ns, ks = int(nch), int(ns), int(ks)
+    khm = nch * ns - sum(min(int(l), ks - 2) + 1 for l in lch)
     h_bytes = nch * (nch + 1) // 2 * ns * ns * 8
     dense_bytes = 3 * khm * khm * 8          # A, eigenvectors, eigensolver workspace
     return khm, h_bytes, dense_bytes

@@ -25,6 +25,9 @@ CONFIGS = {
     "config2": dict(ks=10, ns=200, rmin=1e-3, rmax=40.0, kmax=8, norb=30, nch=40, lmod=9, z=18.0, p=0.02, seed=2),
     "config4": dict(ks=8, ns=150, rmin=1e-3, rmax=30.0, kmax=6, norb=20, nch=None, lmod=7, z=10.0, p=0.03, seed=4,
                     nsym=64, nch_lo=4, nch_hi=60),
+    # serving: the config4 basis and orbitals, a Poisson request stream with 4..80 channels
+    "config5": dict(ks=8, ns=150, rmin=1e-3, rmax=30.0, kmax=6, norb=20, nch=None, lmod=7, z=10.0, p=0.03, seed=4,
+                    nsym=64, nch_lo=4, nch_hi=80, sym_seed=5, rate_per_s=50.0),
 }
 
 
@@ -139,6 +142,8 @@ def symmetry_batch(name="config4", seed=None, nsym=None):
     rng = np.random.default_rng(seed)
     t, s = knot_grid(cfg["ks"], cfg["ns"], cfg["rmin"], cfg["rmax"])
     P = orbitals(rng, t, cfg["ks"], cfg["norb"])
+    if "sym_seed" in cfg:                   # shares the basis and orbitals of the seed, own symmetries
+        rng = np.random.default_rng(cfg["sym_seed"] + (seed - cfg["seed"]))
     lo, hi = math.log(cfg["nch_lo"]), math.log(cfg["nch_hi"])
     out = []
     for q in range(nsym):
@@ -149,3 +154,13 @@ def symmetry_batch(name="config4", seed=None, nsym=None):
         out.append({"nch": nch, "lch": lch, "ech": ech, "coefs": coefs})
     return {"name": name, "seed": seed, "ks": cfg["ks"], "ns": cfg["ns"], "t": t, "knot_scale": s,
             "z": cfg["z"], "kmax": cfg["kmax"], "norb": cfg["norb"], "P": P, "symmetries": out}
+
+
+def request_stream(name="config5", seed=None, nreq=None):
+    """Serving workload: symmetries of the config5 distribution with Poisson arrival
+    offsets (s) of the configured mean rate.  Returns (batch, arrivals)."""
+    cfg = CONFIGS[name]
+    b = symmetry_batch(name, seed=seed, nsym=nreq)
+    rng = np.random.default_rng((cfg["sym_seed"] if "sym_seed" in cfg else cfg["seed"]) + 7919)
+    arrivals = np.cumsum(rng.exponential(1.0 / cfg["rate_per_s"], size=len(b["symmetries"])))
+    return b, arrivals

@@ -123,6 +123,19 @@ size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c);
 int bsrg_ctx_set_timing(bsrg_ctx *c, int on);
 int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n);
 
+/* ---- resident R^k tables (the reference keeps one multipole's rkb in module
+ *      memory, mrk_cell.f90:34-35; a serving process keeps all of them): the
+ *      tables of k = 0..kmax for basis b, built once on the context's stream
+ *      and kept on the device.  A context told to use them
+ *      (bsrg_ctx_use_tables; NULL stops) skips the per-call table builds in
+ *      bsrg_assemble / bsrg_add_two_electron for that basis.  The tables must
+ *      outlive their use; several contexts may share one set. */
+typedef struct bsrg_tables bsrg_tables;
+int bsrg_tables_create(bsrg_ctx *c, const bsrg_basis *b, int kmax, bsrg_tables **out);
+int bsrg_tables_free(bsrg_tables *t);
+size_t bsrg_tables_bytes(const bsrg_tables *t);
+int bsrg_ctx_use_tables(bsrg_ctx *c, const bsrg_tables *t);
+
 /* ---- channel-block assembly of one partial wave (bsr_mat):
  *      src/bsr/BSR_MAT3/sub1.f90:72-191 (SUB1), L_data.f90:131-150 and
  *      l_core.f90:174-270 (one-electron block -1/2*hl_core, no closed shells),

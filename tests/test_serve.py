@@ -1,0 +1,78 @@
+"""Serving / batching host logic (bsr_b200/serve.py) without a GPU: the admission
+queue keeps the HBM budget, starts requests in arrival order, never starves."""
+import threading
+import time
+
+import numpy as np
+
+from bsr_b200 import serve
+
+
+class _R:
+    def __init__(self, rid, nbytes):
+        self.rid, self.nbytes = rid, nbytes
+
+
+def _drain(q, n_workers, hold_s, log):
+    def work():
+        while True:
+            r = q.take()
+            if r is None:
+                return
+            log.append(("start", r.rid, q.in_flight))
+            time.sleep(hold_s)
+            q.release(r)
+    ths = [threading.Thread(target=work) for _ in range(n_workers)]
+    for t in ths:
+        t.start()
+    return ths
+
+
+def test_budget_respected_and_fifo():
+    q = serve.AdmissionQueue(100)
+    sizes = [40, 40, 40, 90, 10, 10, 60]
+    log = []
+    for i, s in enumerate(sizes):
+        q.put(_R(i, s))
+    ths = _drain(q, 4, 0.02, log)
+    time.sleep(0.3)
+    q.close()
+    for t in ths:
+        t.join()
+    starts = [rid for kind, rid, _ in log if kind == "start"]
+    assert starts == list(range(len(sizes)))              # arrival order
+    assert q.peak <= 100 and q.in_flight == 0
+
+
+def test_oversized_request_runs_alone():
+    q = serve.AdmissionQueue(50)
+    log = []
+    q.put(_R(0, 10))
+    q.put(_R(1, 500))                                       # above the budget: admitted only when alone
+    ths = _drain(q, 2, 0.02, log)
+    time.sleep(0.2)
+    q.close()
+    for t in ths:
+        t.join()
+    big = [inflight for kind, rid, inflight in log if rid == 1]
+    assert big == [500]
+
+
+def test_request_bytes_grow_with_channels():
+    a = serve.request_bytes(4, 150, [0, 1, 2, 3], 8)
+    b = serve.request_bytes(40, 150, [c % 7 for c in range(40)], 8)
+    assert b > 50 * a
+
+
+def test_poisson_arrivals():
+    rng = np.random.default_rng(0)
+    t = serve.poisson_stream(rng, 50.0, 2000)
+    assert np.all(np.diff(t) > 0)
+    assert abs(2000 / t[-1] - 50.0) < 5.0
+
+
+def test_request_bytes_numpy_ints():
+    """Channel counts and l values arrive as numpy int32: no 32-bit overflow at 80 channels."""
+    lch = np.arange(80, dtype=np.int32) % 7
+    nb = serve.request_bytes(np.int32(80), np.int32(150), lch, 8)
+    assert isinstance(nb, int) and nb > 3 * 11000 ** 2 * 8
