@@ -49,6 +49,7 @@ SIGNATURES = [
                                        _IP, _DP, _P, _P]),
     ("bsrg_diag_hd", _c_int, [_P, _P, _c_int, _IP, _P, _c_int, _c_int, _c_int, _c_double, _c_double,
                               _c_int, _P, _IP, _P, _P]),
+    ("bsrg_dsytrd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _P]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),
 ]

@@ -23,6 +23,7 @@ UNITS = {
     "assemble.cu": [],
     "diag_hd.cu": [],
     "noalloc.cu": [],
+    "eigen.cu": [],
 }
 
 

@@ -324,6 +324,17 @@ def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0
     return out
 
 
+def dsytrd(ctx, A):
+    """LAPACK DSYTRD (lower) on the device: returns (d, e, tau); A (n x n, Fortran
+    layout, overwritten) keeps the reflectors below the subdiagonal."""
+    n = A.shape[0]
+    d = torch.empty(max(n, 1), device="cuda", dtype=torch.float64)
+    e = torch.empty(max(n - 1, 1), device="cuda", dtype=torch.float64)
+    tau = torch.empty(max(n - 1, 1), device="cuda", dtype=torch.float64)
+    call("bsrg_dsytrd", ctx.handle, n, _ptr(A), n, _ptr(d), _ptr(e), _ptr(tau))
+    return d[:n], e[:max(n - 1, 0)], tau[:max(n - 1, 0)]
+
+
 def partial_wave_solve(ctx, pw, want_vectors=True):
     """The whole path with host buffers (e2e): knots, orbitals, coefficients in; eigenvalues out."""
     t = np.ascontiguousarray(pw["t"], dtype=np.float64)

@@ -187,6 +187,14 @@ int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, cons
                  int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
                  double *eval, int *khm, double *vecs, double *bb);
 
+/* ---- LAPACK DSYTRD (uplo 'L') as called inside DSYEV by LAP_DSYEV
+ *      (src/libs/ZCOM/LAPACK_calls.f90:54-76, from diag_hd.f90:312): A (device,
+ *      n x n, lower triangle) is reduced to the symmetric tridiagonal T = Q^T A Q;
+ *      d (n), e (n-1) and tau (n-1) on the device; the reflectors are left in A
+ *      below the subdiagonal (LAPACK layout, so DORMTR applies Q).  Uses the
+ *      context's stream and workspace. */
+int bsrg_dsytrd(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, double *tau);
+
 /* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
  *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.
  *      t (ns+ks), P (ns,norb), coefficient arrays as in bsrg_assemble, all
