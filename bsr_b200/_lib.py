@@ -49,6 +49,9 @@ SIGNATURES = [
                                        _IP, _DP, _P, _P]),
     ("bsrg_diag_hd", _c_int, [_P, _P, _c_int, _IP, _P, _c_int, _c_int, _c_int, _c_double, _c_double,
                               _c_int, _P, _IP, _P, _P]),
+    ("bsrg_bs_orth", _c_int, [_P, _P, _c_int, _c_int, _P, _IP, _IP, _P]),
+    ("bsrg_diag_hd_ipsol", _c_int, [_P, _c_int, _IP]),
+    ("bsrg_rsol_out", _c_int, [_P, _c_int, _c_int, _IP, _P, _c_int, _P, _P, _P]),
     ("bsrg_dsytrd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _P]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),

@@ -24,6 +24,7 @@ UNITS = {
     "diag_hd.cu": [],
     "noalloc.cu": [],
     "eigen.cu": [],
+    "post.cu": [],
 }
 
 

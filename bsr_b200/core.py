@@ -316,12 +316,40 @@ def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0
          float(Edmax), float(Egap), 1 if want_vectors else 0, _ptr(ev), ctypes.byref(khm),
          _ptr(vecs) if want_vectors else None, _ptr(bb) if want_bb else None)
     n = khm.value
-    out = {"eval": ev[:n], "khm": n}
+    ipsol = np.zeros(nch + 1, dtype=np.int32)
+    call("bsrg_diag_hd_ipsol", ctx.handle, nch, _iptr(ipsol))
+    out = {"eval": ev[:n], "khm": n, "ipsol": ipsol}
     if want_vectors:
         out["vectors"] = vecs[: n * n].view(n, n).t()      # column-major (khm, khm)
     if want_bb:
         out["bb"] = bb
     return out
+
+
+def bs_orth(ctx, basis, P, ort_lists, hcc):
+    """BS_ORTH on the device blocks hcc (ns, ns, nblk) in place: channel i made
+    orthogonal to the orbitals (0-based columns of P) in ort_lists[i]."""
+    nch = len(ort_lists)
+    ptr = np.zeros(nch + 1, dtype=np.int32)
+    for i, l in enumerate(ort_lists):
+        ptr[i + 1] = ptr[i] + len(l)
+    idx = np.ascontiguousarray(np.concatenate([np.asarray(l, dtype=np.int32) for l in ort_lists])
+                               if ptr[-1] > 0 else np.zeros(1, dtype=np.int32), dtype=np.int32)
+    Pd = as_fortran(P)
+    call("bsrg_bs_orth", ctx.handle, basis.handle, nch, Pd.shape[1], _ptr(Pd), _iptr(ptr), _iptr(idx), _ptr(hcc))
+    return hcc
+
+
+def rsol_out(ctx, ns, ipsol, bb, vectors, want_v=True):
+    """rsol_out: solutions in the B-spline basis v ((nch*ns) x khm) and surface amplitudes WMAT (nch x khm)."""
+    ipsol = np.ascontiguousarray(ipsol, dtype=np.int32)
+    nch, khm = len(ipsol) - 1, int(ipsol[-1])
+    a = as_fortran(vectors)
+    v = fortran_empty((nch * ns, khm)) if want_v else None
+    w = fortran_empty((nch, khm))
+    call("bsrg_rsol_out", ctx.handle, ns, nch, _iptr(ipsol), _ptr(as_fortran(bb)), khm, _ptr(a),
+         _ptr(v) if want_v else None, _ptr(w))
+    return v, w
 
 
 def dsytrd(ctx, A):

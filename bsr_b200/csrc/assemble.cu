@@ -780,6 +780,7 @@ int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
     cudaEventRecord(c->ev_stage, c->stream);
     c->events = new std::vector<bsrg_stage_event>();
     c->pool = new std::vector<cudaEvent_t>();
+    c->last_ipsol = new std::vector<int>();
     *out = c;
     return BSRG_OK;
 }
@@ -795,6 +796,7 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
     for (auto ev : *c->pool) cudaEventDestroy(ev);
     delete c->events;
     delete c->pool;
+    delete c->last_ipsol;
     cusolverDnDestroy(c->solver);
     cublasDestroy(c->blas);
     delete c;

@@ -38,6 +38,7 @@ struct bsrg_ctx {
     double stage_ms[BSRG_NSTAGE];
     int stage_launches[BSRG_NSTAGE];
     const bsrg_tables *tables;               // resident tables to use, or NULL
+    std::vector<int> *last_ipsol;            // channel solution offsets of the last diag_hd
 };
 
 namespace bsrg {

@@ -502,6 +502,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     for (int ich = 0; ich < nch; ich++) ipsol[ich + 1] = ipsol[ich] + hi[o_cnt + ich];
     const int khm = ipsol[nch];
     *khm_out = khm;
+    *c->last_ipsol = ipsol;
     if (khm == 0) {
         cusolverDnDestroyParams(params);
         set_error("diag_hd: no channel solutions survive the filter");

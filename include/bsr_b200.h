@@ -187,6 +187,31 @@ int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, cons
                  int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
                  double *eval, int *khm, double *vecs, double *bb);
 
+/* ---- src/bsr/BSR_MAT3/bs_orth.f90:2-92 (BS_ORTH, called from sub1.f90:195):
+ *      orthogonality conditions of the channels.  Channel i is made orthogonal
+ *      to the orbitals ort_idx[ort_ptr[i] .. ort_ptr[i+1]-1] (host, 0-based
+ *      columns of P; the reference picks the bound orbitals with the channel's l
+ *      that IBORT does not exempt): every block becomes
+ *      H_ij -> (1 - B zz_i) H_ij (1 - zz_j B), zz_i = sum p p^T, B the full
+ *      B-spline overlap.  hcc (device) is updated in place; P (device, ns x norb).
+ *      Perturber blocks (kcp > 0) are outside this path. */
+int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const double *P, const int *ort_ptr,
+                 const int *ort_idx, double *hcc);
+
+/* ---- the channel solution offsets ipsol(0:nch) of the last bsrg_diag_hd on
+ *      this context (module bsr_hd's ipsol, set in diag_hd.f90:100-111):
+ *      channel i owns rows ipsol[i] .. ipsol[i+1]-1 of the eigenvectors. */
+int bsrg_diag_hd_ipsol(bsrg_ctx *c, int nch, int *ipsol);
+
+/* ---- src/bsr/BSR_HD3/rsol_out.f90:20-36: solutions in the B-spline basis
+ *      v(:, is) = sum_j a(j, is) bb(:, j) channel by channel (device,
+ *      (nch*ns) x khm, may be NULL) and the surface amplitudes
+ *      WMAT(ich, is) = v(ich*ns, is) (device, nch x khm).  bb and a as returned
+ *      by bsrg_diag_hd (bb with ns columns reserved per channel), ipsol (host)
+ *      from bsrg_diag_hd_ipsol. */
+int bsrg_rsol_out(bsrg_ctx *c, int ns, int nch, const int *ipsol, const double *bb, int khm, const double *a,
+                  double *v, double *wmat);
+
 /* ---- LAPACK DSYTRD (uplo 'L') as called inside DSYEV by LAP_DSYEV
  *      (src/libs/ZCOM/LAPACK_calls.f90:54-76, from diag_hd.f90:312): A (device,
  *      n x n, lower triangle) is reduced to the symmetric tridiagonal T = Q^T A Q;

@@ -1290,3 +1290,96 @@ int orc_assemble(const orc_basis *b, double z, int nch, const int *lch, const do
     free(x); free(xx); free(dd); free(hl);
     return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* BS_ORTH (src/bsr/BSR_MAT3/bs_orth.f90:2-92): orthogonality conditions of  */
+/* the channels by Bentley's projection H -> (1 - B zz) H (1 - zz B), zz =  */
+/* Sum_j p_j p_j^T over the orbitals listed for the channel (ort_ptr/ort_idx,*/
+/* 0-based orbital columns of P), B = full overlap (Full_mat_sym of sb, 'l').*/
+/* Channels are processed one after another as in the reference (:38-86).   */
+/* ------------------------------------------------------------------------ */
+static void matmul_nn(int n, const double *a, const double *b, double *c)
+{
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < n; i++) {
+            double s = 0.0;
+            for (int k = 0; k < n; k++) s += a[i + (size_t)n * k] * b[k + (size_t)n * j];
+            c[i + (size_t)n * j] = s;
+        }
+}
+
+int orc_bs_orth(int ns, int ks, const double *sb, int nch, const double *P, const int *ort_ptr, const int *ort_idx,
+                double *hcc)
+{
+    size_t nn = (size_t)ns * ns;
+    double *B = (double *)calloc(nn, sizeof(double));
+    double *zz = (double *)malloc(sizeof(double) * nn);
+    double *x = (double *)malloc(sizeof(double) * nn);
+    double *y = (double *)malloc(sizeof(double) * nn);
+    double *xx = (double *)malloc(sizeof(double) * nn);
+    /* Full_mat_sym(ns,ks,sb,bb,'l') */
+    for (int jp = 1; jp <= ks; jp++)
+        for (int i = ks + 1 - jp; i <= ns; i++) {
+            int j = i + jp - ks;
+            B[(i - 1) + (size_t)ns * (j - 1)] = sb[(i - 1) + (size_t)ns * (jp - 1)];
+            B[(j - 1) + (size_t)ns * (i - 1)] = sb[(i - 1) + (size_t)ns * (jp - 1)];
+        }
+    for (int ich = 1; ich <= nch; ich++) {
+        int nort = ort_ptr[ich] - ort_ptr[ich - 1];
+        if (nort == 0) continue;
+        memset(zz, 0, sizeof(double) * nn);
+        for (int q = ort_ptr[ich - 1]; q < ort_ptr[ich]; q++) {
+            const double *z = P + (size_t)ns * ort_idx[q];
+            for (int ii = 0; ii < ns; ii++)
+                for (int jj = 0; jj < ns; jj++) zz[ii + (size_t)ns * jj] += z[ii] * z[jj];
+        }
+        matmul_nn(ns, B, zz, x);
+        matmul_nn(ns, zz, B, y);
+        for (int jch = 1; jch <= nch; jch++) {
+            size_t ij;
+            double *h;
+            if (ich > jch) {
+                ij = (size_t)ich * (ich - 1) / 2 + jch - 1;
+                h = hcc + ij * nn;
+                matmul_nn(ns, x, h, xx);
+                for (size_t q = 0; q < nn; q++) h[q] -= xx[q];
+            } else if (ich == jch) {
+                ij = (size_t)ich * (ich + 1) / 2 - 1;
+                h = hcc + ij * nn;
+                matmul_nn(ns, x, h, xx);
+                for (size_t q = 0; q < nn; q++) h[q] -= xx[q];
+                matmul_nn(ns, h, y, xx);
+                for (size_t q = 0; q < nn; q++) h[q] -= xx[q];
+            } else {
+                ij = (size_t)jch * (jch - 1) / 2 + ich - 1;
+                h = hcc + ij * nn;
+                matmul_nn(ns, h, y, xx);
+                for (size_t q = 0; q < nn; q++) h[q] -= xx[q];
+            }
+        }
+    }
+    free(B); free(zz); free(x); free(y); free(xx);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* rsol_out (src/bsr/BSR_HD3/rsol_out.f90:20-36): the solutions in the      */
+/* B-spline basis v(:,is) = Sum_j a(j,is) bb(:,j) channel by channel and the*/
+/* surface amplitudes WMAT(ich,is) = v(ich*ns, is).  bb: (ns, nch*ns), the  */
+/* channel eigenbasis with ns columns reserved per channel (ipsol offsets). */
+/* ------------------------------------------------------------------------ */
+void orc_rsol(int ns, int nch, const int *ipsol, const double *bb, int khm, const double *a, double *v, double *wmat)
+{
+    int nhm = nch * ns;
+    for (int is = 0; is < khm; is++) {
+        for (int ich = 0; ich < nch; ich++) {
+            for (int r = 0; r < ns; r++) {
+                double s = 0.0;
+                for (int j = ipsol[ich]; j < ipsol[ich + 1]; j++)
+                    s += a[j + (size_t)khm * is] * bb[r + (size_t)ns * ((size_t)ich * ns + (j - ipsol[ich]))];
+                if (v) v[(size_t)ich * ns + r + (size_t)nhm * is] = s;
+                if (r == ns - 1) wmat[ich + (size_t)nch * is] = s;
+            }
+        }
+    }
+}

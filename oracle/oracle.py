@@ -57,6 +57,8 @@ def lib():
         L.orc_assemble.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _I, _D,
                                    ctypes.c_int, _D, ctypes.c_int, _D,
                                    ctypes.c_int, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D]
+        L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
+        L.orc_rsol.argtypes = [ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int, _D, _D, _D]
         _LIB = L
     return _LIB
 
@@ -315,3 +317,34 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
         out["vectors"] = vec
         out["bb"] = bb
     return out
+
+
+def bs_orth(basis, P, ort_lists, hcc):
+    """BS_ORTH (bs_orth.f90:2-92) on host blocks hcc (nblk, ns, ns) [row, col] (the layout
+    assemble returns), returned as a new array.  ort_lists: per channel, the 0-based
+    orbital columns of P the channel is made orthogonal to."""
+    ns, ks = basis.ns, basis.ks
+    sb = np.ascontiguousarray(basis.get("sb"))          # memory = Fortran (ns, ks)
+    ptr = np.zeros(len(ort_lists) + 1, dtype=np.int32)
+    for i, l in enumerate(ort_lists):
+        ptr[i + 1] = ptr[i] + len(l)
+    idx = np.ascontiguousarray(np.concatenate([np.asarray(l, dtype=np.int32) for l in ort_lists])
+                               if ptr[-1] > 0 else np.zeros(1, dtype=np.int32))
+    h = np.asfortranarray(np.asarray(hcc, dtype=np.float64).transpose(1, 2, 0))   # Fortran (ns, ns, nblk)
+    Pf = np.asfortranarray(P, dtype=np.float64)
+    lib().orc_bs_orth(ns, ks, _p(sb), len(ort_lists), Pf.ctypes.data_as(_D), _pi(ptr), _pi(idx),
+                      h.ctypes.data_as(_D))
+    return h.transpose(2, 0, 1).copy()
+
+
+def rsol(ns, nch, ipsol, bb, a, want_v=True):
+    """rsol_out (rsol_out.f90:20-36): solutions v (nch*ns, khm) and surface amplitudes WMAT (nch, khm)."""
+    ipsol = np.ascontiguousarray(ipsol, dtype=np.int32)
+    khm = int(ipsol[-1])
+    bbf = np.asfortranarray(bb, dtype=np.float64)
+    af = np.asfortranarray(a, dtype=np.float64)
+    v = np.zeros((nch * ns, khm), order="F") if want_v else None
+    w = np.zeros((nch, khm), order="F")
+    lib().orc_rsol(ns, nch, _pi(ipsol), bbf.ctypes.data_as(_D), khm, af.ctypes.data_as(_D),
+                   v.ctypes.data_as(_D) if want_v else None, w.ctypes.data_as(_D))
+    return v, w
