@@ -797,6 +797,7 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
     delete c->events;
     delete c->pool;
     delete c->last_ipsol;
+    if (c->pw_buf) cudaFree(c->pw_buf);
     cusolverDnDestroy(c->solver);
     cublasDestroy(c->blas);
     delete c;

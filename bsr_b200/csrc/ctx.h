@@ -39,6 +39,8 @@ struct bsrg_ctx {
     int stage_launches[BSRG_NSTAGE];
     const bsrg_tables *tables;               // resident tables to use, or NULL
     std::vector<int> *last_ipsol;            // channel solution offsets of the last diag_hd
+    void *pw_buf;                            // device buffers of bsrg_partial_wave_solve (kept between calls)
+    size_t pw_bytes;
 };
 
 namespace bsrg {

@@ -609,34 +609,43 @@ extern "C" int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double
     int rc = bsrg_define_spline(ks, ns, t, 0, 0, 0.0, s, &b);
     if (rc != BSRG_OK) return rc;
     size_t nn = (size_t)ns * ns, nblk = (size_t)nch * (nch + 1) / 2;
-    double *dP = nullptr, *hcc = nullptr, *dev_eval = nullptr;
+    const size_t nh = (size_t)nch * ns;
+    // device buffers live in the context between calls (grown when a larger wave arrives)
+    size_t need = 0;
+    auto add = [&](size_t bytes) { need += (bytes + 255) & ~(size_t)255; };
+    add(sizeof(double) * ns * norb);
+    add(sizeof(double) * nn * nblk);
+    add(sizeof(double) * nh);
+    if (want_vectors) add(sizeof(double) * nh * nh);
     cudaError_t e;
-    if ((e = cudaMallocAsync((void **)&dP, sizeof(double) * ns * norb, s)) != cudaSuccess ||
-        (e = cudaMallocAsync((void **)&hcc, sizeof(double) * nn * nblk, s)) != cudaSuccess ||
-        (e = cudaMallocAsync((void **)&dev_eval, sizeof(double) * (size_t)nch * ns, s)) != cudaSuccess) {
-        rc = cuda_fail(e, "partial_wave_solve alloc");
+    if (c->pw_bytes < need) {
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "partial_wave_solve sync");
+        if (c->pw_buf) cudaFree(c->pw_buf);
+        c->pw_buf = nullptr;
+        c->pw_bytes = 0;
+        if (rc == BSRG_OK && (e = cudaMalloc(&c->pw_buf, need)) != cudaSuccess)
+            rc = cuda_fail(e, "partial_wave_solve alloc");
+        if (rc == BSRG_OK) c->pw_bytes = need;
     }
-    if (rc == BSRG_OK && (e = cudaMemcpyAsync(dP, P, sizeof(double) * ns * norb, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    if (rc != BSRG_OK) {
+        bsrg_basis_free(b);
+        return rc;
+    }
+    Arena ar{(char *)c->pw_buf, 0, c->pw_bytes};
+    double *dP = ar.take<double>((size_t)ns * norb), *hcc = ar.take<double>(nn * nblk);
+    double *dev_eval = ar.take<double>(nh);
+    double *vecs = want_vectors ? ar.take<double>(nh * nh) : nullptr;
+    if ((e = cudaMemcpyAsync(dP, P, sizeof(double) * ns * norb, cudaMemcpyHostToDevice, s)) != cudaSuccess)
         rc = cuda_fail(e, "partial_wave_solve upload");
     if (rc == BSRG_OK)
         rc = bsrg_assemble(c, b, z, nch, lch, ech, norb, dP, kmax, ncoef, ck, ctype, cich, cjch, ca, cb, cval, hcc,
                            nullptr, nullptr);
-    double *vecs = nullptr;
-    if (rc == BSRG_OK && want_vectors) {
-        size_t n = (size_t)nch * ns;
-        if ((e = cudaMallocAsync((void **)&vecs, sizeof(double) * n * n, s)) != cudaSuccess)
-            rc = cuda_fail(e, "partial_wave_solve vecs");
-    }
     if (rc == BSRG_OK)
         rc = bsrg_diag_hd(c, b, nch, lch, hcc, 0, 1, 1, 0.0, 0.001, want_vectors, dev_eval, khm, vecs, nullptr);
     if (rc == BSRG_OK &&
         (e = cudaMemcpyAsync(eval, dev_eval, sizeof(double) * (*khm), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         rc = cuda_fail(e, "partial_wave_solve download");
     if (rc == BSRG_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "partial_wave_solve sync");
-    if (vecs) cudaFreeAsync(vecs, s);
-    if (dP) cudaFreeAsync(dP, s);
-    if (hcc) cudaFreeAsync(hcc, s);
-    if (dev_eval) cudaFreeAsync(dev_eval, s);
     cudaStreamSynchronize(s);
     bsrg_basis_free(b);
     return rc;

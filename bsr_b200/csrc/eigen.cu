@@ -23,8 +23,8 @@ namespace {
 
 constexpr int TRD_NB = 32;                  // panel width
 constexpr int TRD_TT = 64;                  // tile edge of the symmetric product
-constexpr int TRD_BB = 4;                   // tiles per block edge (a work unit is one block)
-constexpr int TRD_BT = TRD_TT * TRD_BB;     // block edge
+constexpr int TRD_BB = 4;                   // largest tiles per block edge (a work unit is one block)
+constexpr int TRD_BT = TRD_TT * TRD_BB;     // largest block edge
 constexpr int TRD_NT = 512;                 // threads per CTA
 constexpr int TRD_CG = TRD_NT / TRD_TT;     // column groups in a tile
 constexpr int TRD_CPT = TRD_TT / TRD_CG;    // columns per thread in a tile
@@ -47,40 +47,57 @@ struct TrdArgs {
     double *red_norm;       // per CTA
     double *red_dot;        // per dot chunk: 2*TRD_NB
     double *red_s1;         // per CTA
-    unsigned *bar;          // [0] arrivals, [1] generation, [2] work counter
+    unsigned *bar;          // [2] dynamic work counter
+    unsigned *arrive;       // per CTA (stride 8): last barrier generation reached
+    unsigned *release;      // generation released by CTA 0
     int *err;
-    int nblk;
+    unsigned gen0;          // barrier generations of this launch start above gen0
 };
 
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, int *err)
+// Grid barrier: every CTA publishes the generation it reached in its own slot;
+// CTA 0 waits for all slots, resets the work counter and publishes the release.
+// Every wait is bounded; on a timeout the error flag ends the kernel.
+__device__ __forceinline__ bool grid_barrier(const TrdArgs &a, unsigned gen)
 {
     __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        volatile int *verr = err;
-        if (*verr == 0) {
-            unsigned g = *gen;
-            __threadfence();
-            unsigned arrived = atomicAdd(bar, 1u);
-            if (arrived == gridDim.x - 1) {
-                atomicExch(bar, 0u);
-                atomicExch(bar + 2, 0u);      // dynamic work counter of the next phase
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            } else {
-                long it = 0;
-                while (*gen == g && *verr == 0) {
-                    if (++it > TRD_SPIN_LIMIT) {
-                        atomicExch(err, 1);
-                        break;
-                    }
-                }
-            }
-            __threadfence();
-        }
+    const int t = threadIdx.x, cta = blockIdx.x;
+    volatile int *verr = a.err;
+    if (t == 0) {
+        __threadfence();
+        *(volatile unsigned *)(a.arrive + 8 * cta) = gen;
     }
+    if (cta == 0) {
+        if (t < (int)gridDim.x) {
+            long it = 0;
+            while (*(volatile unsigned *)(a.arrive + 8 * t) != gen && *verr == 0)
+                if (++it > TRD_SPIN_LIMIT) atomicExch(a.err, 1);
+        }
+        __syncthreads();
+        if (t == 0) {
+            __threadfence();
+            *(volatile unsigned *)(a.bar + 2) = 0u;
+            __threadfence();
+            *(volatile unsigned *)a.release = gen;
+        }
+    } else if (t == 0) {
+        long it = 0;
+        while (*(volatile unsigned *)a.release != gen && *verr == 0)
+            if (++it > TRD_SPIN_LIMIT) atomicExch(a.err, 1);
+    }
+    if (t == 0) __threadfence();
     __syncthreads();
-    return *(volatile int *)err == 0;
+    return *verr == 0;
+}
+
+// tiles per block edge for a trailing matrix of m rows: the largest that still
+// gives every CTA two work units (small m: 64 x 64 units, large m: 256 x 256)
+__host__ __device__ __forceinline__ int bb_for(int m, int ncta)
+{
+    for (int bb = TRD_BB; bb > 1; bb >>= 1) {
+        const int nb = (m + TRD_TT * bb - 1) / (TRD_TT * bb);
+        if (nb * (nb + 1) / 2 >= 2 * ncta) return bb;
+    }
+    return 1;
 }
 
 __device__ __forceinline__ double vval(const double *col, int r, int c, int n, double scale)
@@ -104,29 +121,35 @@ __device__ double block_sum(double v, double *sh)
 }
 
 // Row phase for row r (8 lanes; every lane of the warp calls it, act = row exists):
-// py = y_r of the product of column c-1, pc = its panel corrections (l < i-1),
-// pu = update of column c at row r by panel columns l < i, without W(r,i-1)*V(c,i-1).
+// py = y_r of the product of column c-1 (its blocks of bt rows), pc = the panel
+// corrections of that product (l < i-1), pu = the update of column c at row r by
+// panel columns l < i-1.  The l = i-1 terms need W(c, i-1), added by the caller.
 struct RowSums {
     double py, pc, pu;
 };
 
-__device__ __forceinline__ RowSums row_sums(const TrdArgs &a, int r, bool act, int c, int i, const double *sxw,
-                                            const double *sxv, const double *sWc, const double *sVc)
+__device__ __forceinline__ RowSums row_sums(const TrdArgs &a, int r, bool act, int c, int i, int bt,
+                                            const double *sxw, const double *sxv, const double *sWc,
+                                            const double *sVc)
 {
     const int lane = threadIdx.x & (TRD_G - 1);
     const int n = a.n, lda = a.lda;
     double py0 = 0.0, py1 = 0.0, pc = 0.0, pu = 0.0;
     if (act) {
         if (i > 0) {
-            const int IBr = r / TRD_BT;
-            const int JB0 = c / TRD_BT;               // blocks of the product of column c-1
+            const int IBr = r / bt;
+            const int JB0 = c / bt;                   // blocks of the product of column c-1
+            const int nblk = (n + bt - 1) / bt;
+#pragma unroll 4
             for (int JB = JB0 + lane; JB <= IBr; JB += TRD_G) py0 += a.P[(size_t)JB * n + r];
-            for (int IB = IBr + lane; IB < a.nblk; IB += TRD_G) py1 += a.Q[(size_t)IB * n + r];
+#pragma unroll 4
+            for (int IB = IBr + lane; IB < nblk; IB += TRD_G) py1 += a.Q[(size_t)IB * n + r];
         }
-        for (int l = lane; l < i; l += TRD_G) {
+#pragma unroll 4
+        for (int l = lane; l < i - 1; l += TRD_G) {
             const double v = a.A[r + (size_t)(a.p0 + l) * lda];
-            const double w = (l < i - 1) ? a.W[r + (size_t)l * n] : 0.0;
-            if (l < i - 1) pc += v * sxw[l] + w * sxv[l];
+            const double w = a.W[r + (size_t)l * n];
+            pc += v * sxw[l] + w * sxv[l];
             pu += v * sWc[l] + w * sVc[l];
         }
     }
@@ -140,25 +163,27 @@ __device__ __forceinline__ RowSums row_sums(const TrdArgs &a, int r, bool act, i
     return {py, pc, pu};
 }
 
-// one block (IB, JB) of y = A22 v, JB <= IB: its 64 x 64 tiles of the lower
-// triangle are staged through shared memory (double-buffered, two tiles of
-// loads in flight) and each is read once from HBM; row sums go to P(JB, rows),
-// transposed sums to Q(IB, cols); s1acc collects v^T (A22 v) of what it writes.
-__device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int JB, double *smem, double &s1acc)
+// one block (IB, JB) of bb x bb tiles of y = A22 v, JB <= IB: the 64 x 64
+// tiles of the lower triangle are staged through shared memory
+// (double-buffered, two tiles of loads in flight) and each is read once; row
+// sums go to P(JB, rows), transposed sums to Q(IB, cols); s1acc collects
+// v^T (A22 v) of what it writes.
+__device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int JB, int bb, double *smem,
+                             double &s1acc)
 {
     const int n = a.n, lda = a.lda, t = threadIdx.x;
     const int tr = t % TRD_TT, g = t / TRD_TT;
+    const int bt = bb * TRD_TT;
     const double *A = a.A;
     double *tile0 = smem, *tile1 = smem + TRD_TT * TRD_LDT;
     double *red = smem + 2 * TRD_TT * TRD_LDT;                 // TRD_CG x TRD_BT
     double *vI = red + TRD_CG * TRD_BT, *vJ = vI + TRD_BT;
     const bool diag = (IB == JB);
-    // tiles of the block in order (il, jl), skipping il < jl on the diagonal block
-    const int ntile = diag ? TRD_BB * (TRD_BB + 1) / 2 : TRD_BB * TRD_BB;
+    const int ntile = diag ? bb * (bb + 1) / 2 : bb * bb;
     auto tile_of = [&](int q, int &il, int &jl) {
         if (!diag) {
-            il = q / TRD_BB;
-            jl = q % TRD_BB;
+            il = q / bb;
+            jl = q % bb;
         } else {
             il = 0;
             while (q > il) {
@@ -171,7 +196,7 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
     auto load = [&](int q, double *dst) {
         int il, jl;
         tile_of(q, il, jl);
-        const int I = IB * TRD_BB + il, J = JB * TRD_BB + jl;
+        const int I = IB * bb + il, J = JB * bb + jl;
         const int r = I * TRD_TT + tr;
 #pragma unroll
         for (int k = 0; k < TRD_CPT; k++) {
@@ -180,16 +205,16 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
             dst[k] = ok ? A[r + (size_t)sc * lda] : 0.0;
         }
     };
-    if (t < TRD_BT) {
-        vI[t] = vval(a.col, IB * TRD_BT + t, c, n, scale);
-        vJ[t] = vval(a.col, JB * TRD_BT + t, c, n, scale);
+    double ra[TRD_CPT], rb[TRD_CPT];
+    load(0, ra);
+    if (ntile > 1) load(1, rb);
+    if (t < bt) {
+        vI[t] = vval(a.col, IB * bt + t, c, n, scale);
+        vJ[t] = vval(a.col, JB * bt + t, c, n, scale);
     }
     double rowacc[TRD_BB], zacc[TRD_BB];
 #pragma unroll
     for (int q = 0; q < TRD_BB; q++) rowacc[q] = zacc[q] = 0.0;
-    double ra[TRD_CPT], rb[TRD_CPT];
-    load(0, ra);
-    if (ntile > 1) load(1, rb);
     for (int q = 0; q < ntile; q++) {
         double *T = (q & 1) ? tile1 : tile0;
 #pragma unroll
@@ -201,7 +226,6 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
         int il, jl;
         tile_of(q, il, jl);
         const bool dtile = diag && il == jl;
-        // row part: row tr, columns g*8 .. g*8+7
         {
             double sacc = 0.0;
 #pragma unroll
@@ -213,7 +237,6 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
             for (int qq = 0; qq < TRD_BB; qq++)
                 if (qq == il) rowacc[qq] += sacc;
         }
-        // column part: column tr, rows g*8 .. g*8+7 (strictly below the diagonal)
         {
             double sacc = 0.0;
 #pragma unroll
@@ -227,15 +250,15 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
                 if (qq == jl) zacc[qq] += sacc;
         }
     }
-    // reduce over the 8 groups: rows -> P, columns -> Q
 #pragma unroll
-    for (int q = 0; q < TRD_BB; q++) red[g * TRD_BT + q * TRD_TT + tr] = rowacc[q];
+    for (int q = 0; q < TRD_BB; q++)
+        if (q < bb) red[g * TRD_BT + q * TRD_TT + tr] = rowacc[q];
     __syncthreads();
-    if (t < TRD_BT) {
+    if (t < bt) {
         double y = 0.0;
 #pragma unroll
         for (int gg = 0; gg < TRD_CG; gg++) y += red[gg * TRD_BT + t];
-        const int rr = IB * TRD_BT + t;
+        const int rr = IB * bt + t;
         if (rr < n) {
             a.P[(size_t)JB * n + rr] = y;
             s1acc += vI[t] * y;
@@ -243,13 +266,14 @@ __device__ void product_unit(const TrdArgs &a, int c, double scale, int IB, int 
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < TRD_BB; q++) red[g * TRD_BT + q * TRD_TT + tr] = zacc[q];
+    for (int q = 0; q < TRD_BB; q++)
+        if (q < bb) red[g * TRD_BT + q * TRD_TT + tr] = zacc[q];
     __syncthreads();
-    if (t < TRD_BT) {
+    if (t < bt) {
         double z = 0.0;
 #pragma unroll
         for (int gg = 0; gg < TRD_CG; gg++) z += red[gg * TRD_BT + t];
-        const int cc = JB * TRD_BT + t;
+        const int cc = JB * bt + t;
         if (cc < n) {
             a.Q[(size_t)IB * n + cc] = z;
             s1acc += vJ[t] * z;
@@ -304,6 +328,8 @@ __device__ void dot_chunk(const TrdArgs &a, int c, double scale, int i, int dq, 
     __syncthreads();
 }
 
+constexpr int TRD_MAXPASS = 4;              // row passes per CTA: n <= 4 * 64 * (number of CTAs)
+
 __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
 {
     extern __shared__ double dsm[];             // staged tiles and block reductions (TRD_SMEM bytes)
@@ -314,37 +340,49 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
     const int t = threadIdx.x, cta = blockIdx.x, ncta = gridDim.x;
     const int n = a.n, lda = a.lda;
     double *A = a.A;
+    unsigned gen = a.gen0;
     double tau_p = 0.0, alpha2_p = 0.0;          // of the previous column (same in every CTA)
+    int bt_p = TRD_TT;                          // block edge of the previous column's product
     for (int i = 0; i <= a.nbp; i++) {
         // column c = p0 + i; i == nbp only finishes w of the last panel column
         // (and the last diagonal element when c == n-1)
         const int c = a.p0 + i;
         const bool last = (i == a.nbp);
         // ---- row phase: finish w of column c-1 at rows >= c, update column c ----
-        if (t < i) {
-            sVc[t] = A[c + (size_t)(a.p0 + t) * lda];
-            sWc[t] = (t < i - 1) ? a.W[c + (size_t)t * n] : 0.0;
+        // sVc(0:i-1) and sWc(0:i-2) hold row c of V and W (loaded after the last barrier)
+        RowSums rs[TRD_MAXPASS];
+        double vr[TRD_MAXPASS], arc[TRD_MAXPASS];
+#pragma unroll
+        for (int q = 0; q < TRD_MAXPASS; q++) {
+            const int base = c + (cta + q * ncta) * TRD_RPC;     // the same in the whole CTA
+            rs[q] = {0.0, 0.0, 0.0};
+            vr[q] = arc[q] = 0.0;
+            if (base < n) {
+                const int r = base + t / TRD_G;
+                const bool act = r < n;
+                rs[q] = row_sums(a, r, act, c, i, bt_p, sxw, sxv, sWc, sVc);
+                vr[q] = (act && i > 0) ? A[r + (size_t)(c - 1) * lda] : 0.0;
+                arc[q] = act ? A[r + (size_t)c * lda] : 0.0;
+            }
         }
-        __syncthreads();
         if (i > 0 && t < 32) {
-            // W(c, i-1), needed by every row: computed by every CTA with the row code
-            const RowSums rc = row_sums(a, c, t < TRD_G, c, i, sxw, sxv, sWc, sVc);
+            // W(c, i-1), needed by every row: every CTA computes it with the row code
+            const RowSums rc = row_sums(a, c, t < TRD_G, c, i, bt_p, sxw, sxv, sWc, sVc);
             if (t == 0) sWc[i - 1] = tau_p * (rc.py - rc.pc) + alpha2_p * A[c + (size_t)(c - 1) * lda];
         }
         __syncthreads();
         double nrm = 0.0;
-        for (int base = c + cta * TRD_RPC; base < n; base += ncta * TRD_RPC) {
-            const int r = base + t / TRD_G;
-            const bool act = r < n;
-            const RowSums rs = row_sums(a, r, act, c, i, sxw, sxv, sWc, sVc);
-            if (act && (t & (TRD_G - 1)) == 0) {
-                double wr = 0.0;
+#pragma unroll
+        for (int q = 0; q < TRD_MAXPASS; q++) {
+            const int r = c + (cta + q * ncta) * TRD_RPC + t / TRD_G;
+            if (r < n && (t & (TRD_G - 1)) == 0) {
+                double wr = 0.0, ar = arc[q] - rs[q].pu;
                 if (i > 0) {
-                    wr = tau_p * (rs.py - rs.pc) + alpha2_p * A[r + (size_t)(c - 1) * lda];
+                    wr = tau_p * (rs[q].py - rs[q].pc) + alpha2_p * vr[q];
                     a.W[r + (size_t)(i - 1) * n] = wr;
+                    ar -= vr[q] * sWc[i - 1] + wr * sVc[i - 1];
                 }
                 if (!last || c == n - 1) {
-                    const double ar = A[r + (size_t)c * lda] - rs.pu - (i > 0 ? wr * sVc[i - 1] : 0.0);
                     a.col[r] = ar;
                     if (r == c) {
                         a.d[c] = ar;
@@ -357,22 +395,21 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
         if (last) break;
         nrm = block_sum(nrm, sh);
         if (t == 0) a.red_norm[cta] = nrm;
-        if (!grid_barrier(a.bar, a.err)) return;
+        if (!grid_barrier(a, ++gen)) return;
         // ---- reflector, product, dots ----
         const int m = n - c;
-        if (t < 32) {
-            double s = 0.0;
-            for (int q = t; q < ncta; q += 32) s += a.red_norm[q];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        {
+            double sq = (t < ncta) ? a.red_norm[t] : 0.0;
+            const double alpha = a.col[c + 1];
+            sq = block_sum(sq, sh);
             if (t == 0) {
-                const double alpha = a.col[c + 1];
                 double beta, tau, scale;
-                if (s == 0.0) {
+                if (sq == 0.0) {
                     beta = alpha;
                     tau = 0.0;
                     scale = 0.0;
                 } else {
-                    beta = -copysign(sqrt(alpha * alpha + s), alpha);
+                    beta = -copysign(sqrt(alpha * alpha + sq), alpha);
                     tau = (beta - alpha) / beta;
                     scale = 1.0 / (alpha - beta);
                 }
@@ -380,8 +417,8 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
                 sbc[2] = tau;
                 sbc[3] = scale;
             }
+            __syncthreads();
         }
-        __syncthreads();
         const double tau = sbc[2], scale = sbc[3];
         if (cta == 0 && t == 0) {
             a.e[c] = sbc[1];
@@ -391,8 +428,11 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
             const int r = c + 1 + q * TRD_NT + t;
             if (r < n) A[r + (size_t)c * lda] = vval(a.col, r, c, n, scale);
         }
-        const int jb0 = (c + 1) / TRD_BT;
-        const int nb = a.nblk - jb0;
+        const int bb = bb_for(m - 1, ncta);
+        const int bt = bb * TRD_TT;
+        const int nblk = (n + bt - 1) / bt;
+        const int jb0 = (c + 1) / bt;
+        const int nb = nblk - jb0;
         const int noff = nb * (nb - 1) / 2;        // off-diagonal blocks first (largest), then diagonal ones
         const int nunit = noff + nb;
         const int ndot = (i > 0) ? (m - 1 + TRD_DR - 1) / TRD_DR : 0;
@@ -402,14 +442,14 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
             if (t == 0) snext = (int)atomicAdd(a.bar + 2, 1u) + ncta;   // next unit, fetched ahead
             if (u < noff) {
                 int uu = u, JB = jb0;
-                while (uu >= a.nblk - JB - 1) {
-                    uu -= a.nblk - JB - 1;
+                while (uu >= nblk - JB - 1) {
+                    uu -= nblk - JB - 1;
                     JB++;
                 }
-                product_unit(a, c, scale, JB + 1 + uu, JB, dsm, s1acc);
+                product_unit(a, c, scale, JB + 1 + uu, JB, bb, dsm, s1acc);
             } else if (u < nunit) {
                 const int JB = jb0 + (u - noff);
-                product_unit(a, c, scale, JB, JB, dsm, s1acc);
+                product_unit(a, c, scale, JB, JB, bb, dsm, s1acc);
             } else {
                 dot_chunk(a, c, scale, i, u - nunit, sh);
             }
@@ -419,13 +459,18 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
         }
         s1acc = block_sum(s1acc, sh);
         if (t == 0) a.red_s1[cta] = s1acc;
-        if (!grid_barrier(a.bar, a.err)) return;
-        // ---- every CTA: sums of the dots and of v^T A22 v, alpha2 ----
+        if (!grid_barrier(a, ++gen)) return;
+        // ---- every CTA: sums of the dots and of v^T A22 v, alpha2; rows c+1 of V and W ----
         {
             const int l = t % (2 * TRD_NB), g = t / (2 * TRD_NB);
-            double s = 0.0;
-            for (int dq = g; dq < ndot; dq += TRD_NT / (2 * TRD_NB)) s += a.red_dot[(size_t)dq * 2 * TRD_NB + l];
-            sh[g * 2 * TRD_NB + l] = s;
+            double sd = 0.0;
+            for (int dq = g; dq < ndot; dq += TRD_NT / (2 * TRD_NB)) sd += a.red_dot[(size_t)dq * 2 * TRD_NB + l];
+            const double s1p = (t < ncta) ? a.red_s1[t] : 0.0;
+            // next column's row of V (l <= i) and W (l < i; W(c+1, i) comes from the row phase)
+            double vnext = 0.0, wnext = 0.0;
+            if (t <= i) vnext = A[c + 1 + (size_t)(a.p0 + t) * lda];
+            if (t < i) wnext = a.W[c + 1 + (size_t)t * n];
+            sh[g * 2 * TRD_NB + l] = sd;
             __syncthreads();
             if (t < 2 * TRD_NB) {
                 double tot = 0.0;
@@ -433,15 +478,16 @@ __global__ void __launch_bounds__(TRD_NT, 1) trd_panel_kernel(TrdArgs a)
                 if (t < TRD_NB) sxw[t] = (t < i) ? tot : 0.0;
                 else sxv[t - TRD_NB] = (t - TRD_NB < i) ? tot : 0.0;
             }
-            __syncthreads();
-            double s1p = 0.0;
-            for (int q = t; q < ncta; q += TRD_NT) s1p += a.red_s1[q];
-            const double s1 = block_sum(s1p, sh);
+            const double s1 = block_sum(s1p, sh);    // its leading barrier orders the sxw/sxv writes
             double xx = 0.0;
             for (int ll = 0; ll < i; ll++) xx += sxv[ll] * sxw[ll];
             const double wv = s1 - 2.0 * xx;
             tau_p = tau;
             alpha2_p = -0.5 * tau * tau * wv;
+            bt_p = bt;
+            if (t <= i) sVc[t] = vnext;
+            if (t < i) sWc[t] = wnext;
+            __syncthreads();
         }
     }
 }
@@ -454,22 +500,36 @@ __global__ void trd_restore_e_kernel(int n, double *A, int lda, const double *e)
 
 }  // namespace
 
-size_t trd_workspace_bytes(int n)
+// workspace layout of one reduction (the same carve for the launch and the error check)
+struct TrdLayout {
+    double *W, *P, *Q, *col, *red_norm, *red_dot, *red_s1;
+    unsigned *bar, *arrive, *release;
+    int *err;
+    size_t bytes;
+};
+
+static TrdLayout trd_layout(void *ws, int n)
 {
-    const size_t nblk = (n + TRD_BT - 1) / TRD_BT;
+    const size_t nt = (n + TRD_TT - 1) / TRD_TT;       // partial rows for the smallest blocks
     const size_t ndot = (n + TRD_DR - 1) / TRD_DR;
-    size_t b = 0;
-    auto add = [&](size_t bytes) { b += (bytes + 255) & ~(size_t)255; };
-    add(sizeof(double) * (size_t)n * TRD_NB);   // W
-    add(sizeof(double) * nblk * n);             // P
-    add(sizeof(double) * nblk * n);             // Q
-    add(sizeof(double) * n);                    // col
-    add(sizeof(double) * 1024);                 // per-CTA norms
-    add(sizeof(double) * ndot * 2 * TRD_NB);
-    add(sizeof(double) * 1024);                 // per-CTA v^T A v
-    add(64);                                    // barrier + error flag
-    return b + 256;
+    Arena ar{(char *)ws, 0, 0};
+    TrdLayout L{};
+    L.W = ar.take<double>((size_t)n * TRD_NB);
+    L.P = ar.take<double>(nt * n);
+    L.Q = ar.take<double>(nt * n);
+    L.col = ar.take<double>(n);
+    L.red_norm = ar.take<double>(TRD_NT);
+    L.red_dot = ar.take<double>(ndot * 2 * TRD_NB);
+    L.red_s1 = ar.take<double>(TRD_NT);
+    L.bar = ar.take<unsigned>(16);                      // [2] work counter, [8] error flag
+    L.err = (int *)(L.bar + 8);
+    L.arrive = ar.take<unsigned>(8 * TRD_NT);
+    L.release = ar.take<unsigned>(16);
+    L.bytes = ar.off + 256;
+    return L;
 }
+
+size_t trd_workspace_bytes(int n) { return trd_layout(nullptr, n).bytes; }
 
 // A (n x n, lower triangle) -> T (d, e) and reflectors; ws holds trd_workspace_bytes(n)
 int trd_reduce(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, double *tau, void *ws)
@@ -480,28 +540,29 @@ int trd_reduce(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, dou
         cudaError_t er = cudaMemcpyAsync(d, A, sizeof(double), cudaMemcpyDeviceToDevice, s);
         return er == cudaSuccess ? BSRG_OK : cuda_fail(er, "tridiagonal reduction");
     }
-    const size_t nblk = (n + TRD_BT - 1) / TRD_BT;
-    const size_t ndot = (n + TRD_DR - 1) / TRD_DR;
-    Arena ar{(char *)ws, 0, trd_workspace_bytes(n)};
+    const TrdLayout L = trd_layout(ws, n);
     TrdArgs a{};
     a.A = A;
     a.n = n;
     a.lda = lda;
-    a.W = ar.take<double>((size_t)n * TRD_NB);
-    a.P = ar.take<double>(nblk * n);
-    a.Q = ar.take<double>(nblk * n);
-    a.col = ar.take<double>(n);
-    a.red_norm = ar.take<double>(1024);
-    a.red_dot = ar.take<double>(ndot * 2 * TRD_NB);
-    a.red_s1 = ar.take<double>(1024);
-    a.bar = ar.take<unsigned>(16);
-    a.err = (int *)(a.bar + 8);
+    a.W = L.W;
+    a.P = L.P;
+    a.Q = L.Q;
+    a.col = L.col;
+    a.red_norm = L.red_norm;
+    a.red_dot = L.red_dot;
+    a.red_s1 = L.red_s1;
+    a.bar = L.bar;
+    a.err = L.err;
+    a.arrive = L.arrive;
+    a.release = L.release;
     a.d = d;
     a.e = e;
     a.tau = tau;
-    a.nblk = (int)nblk;
     cudaError_t er;
-    if ((er = cudaMemsetAsync(a.bar, 0, 64, s)) != cudaSuccess) return cuda_fail(er, "tridiagonal reduction");
+    // flags start at generation 0; every launch uses generations above its own gen0
+    const size_t flag_bytes = (char *)(L.release + 16) - (char *)L.bar;
+    if ((er = cudaMemsetAsync(L.bar, 0, flag_bytes, s)) != cudaSuccess) return cuda_fail(er, "tridiagonal reduction");
     int dev = c->device, nsm = 0, occ = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if ((er = cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TRD_SMEM)) !=
@@ -513,13 +574,22 @@ int trd_reduce(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, dou
         set_error("tridiagonal reduction: kernel cannot be resident");
         return BSRG_ERR_CUDA;
     }
-    const int grid = nsm < 1024 ? nsm : 1024;   // one CTA per SM: all resident (the cooperative launch checks it)
+    // one CTA per SM, all resident (the cooperative launch checks it); the
+    // per-CTA slots are read by one thread each, so at most TRD_NT CTAs
+    const int grid = nsm < TRD_NT ? nsm : TRD_NT;
+    if (n > TRD_MAXPASS * TRD_RPC * grid) {
+        set_error("tridiagonal reduction: n = %d above the limit %d of this device", n, TRD_MAXPASS * TRD_RPC * grid);
+        return BSRG_ERR_ARG;
+    }
     const double one = 1.0, mone = -1.0;
+    unsigned launch = 0;
     for (int p0 = 0; p0 < n - 1; p0 += TRD_NB) {
         a.p0 = p0;
         a.nbp = min(TRD_NB, n - 1 - p0);
+        a.gen0 = ++launch * 256u;            // at most 2 * TRD_NB barriers per launch
         void *args[] = {&a};
-        if ((er = cudaLaunchCooperativeKernel((const void *)trd_panel_kernel, grid, TRD_NT, args, TRD_SMEM, s)) != cudaSuccess)
+        if ((er = cudaLaunchCooperativeKernel((const void *)trd_panel_kernel, grid, TRD_NT, args, TRD_SMEM, s)) !=
+            cudaSuccess)
             return cuda_fail(er, "tridiagonal reduction panel");
         const int q0 = p0 + a.nbp;
         if (q0 < n - 1) {
@@ -541,19 +611,9 @@ int trd_reduce(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, dou
 // error flag of the last reduction (read after the stream is synchronised)
 int trd_check(void *ws, int n, cudaStream_t s)
 {
-    const size_t nblk = (n + TRD_BT - 1) / TRD_BT;
-    const size_t ndot = (n + TRD_DR - 1) / TRD_DR;
-    Arena ar{(char *)ws, 0, trd_workspace_bytes(n)};
-    ar.take<double>((size_t)n * TRD_NB);
-    ar.take<double>(nblk * n);
-    ar.take<double>(nblk * n);
-    ar.take<double>(n);
-    ar.take<double>(1024);
-    ar.take<double>(ndot * 2 * TRD_NB);
-    ar.take<double>(1024);
-    unsigned *bar = ar.take<unsigned>(16);
+    const TrdLayout L = trd_layout(ws, n);
     int herr = 0;
-    cudaError_t er = cudaMemcpyAsync(&herr, bar + 8, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaError_t er = cudaMemcpyAsync(&herr, L.err, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (er == cudaSuccess) er = cudaStreamSynchronize(s);
     if (er != cudaSuccess) return cuda_fail(er, "tridiagonal reduction");
     if (herr) {
