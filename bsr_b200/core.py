@@ -158,6 +158,25 @@ def mrk_cell(basis, k, ldp=None, out=None):
     return out
 
 
+def nk_moments(basis, k):
+    """Breit-Pauli N^k cell moments (rkd1 (ik,nv), rkd2 (ik,nv), rkd (ik,ik,nv)), k >= -1."""
+    ik = basis.ks * (basis.ks + 1) // 2
+    rkd1 = fortran_empty((ik, basis.nv))
+    rkd2 = fortran_empty((ik, basis.nv))
+    rkd = fortran_empty((ik, ik, basis.nv))
+    call("bsrg_nk_moments", basis.handle, k, _ptr(rkd1), _ptr(rkd2), _ptr(rkd), _stream())
+    return rkd1, rkd2, rkd
+
+
+def mnk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
+    """N^k table rkb(ns,ns,ldp,ldp) times fine (mnk_cell.f90); i, ip the r1 splines, r2 < r1."""
+    ldp = basis.ks if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mnk_cell", basis.handle, k, float(fine), _ptr(out), ldp, _stream())
+    return out
+
+
 # ---------------------------------------------------------------------------
 # density.f90, convol.f90, sum_amb.f90
 # ---------------------------------------------------------------------------

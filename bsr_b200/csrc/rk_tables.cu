@@ -400,6 +400,138 @@ rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rk
     rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc;
 }
 
+
+// ---------------------------------------------------------------------------
+// Breit-Pauli N^k tables.  nk_triang (nk_moments.f90:105): the diagonal cell of
+// r2 < r1 only (inner weight r2^k, k >= -1; outer r1^-(k+3) folded into the
+// inner integral), not symmetrised; nk_pdiag's scaling law divides by (1+h).
+// ---------------------------------------------------------------------------
+__device__ static double ipow_dev(double x, int k)
+{
+    if (k == 0) return 1.0;
+    double p = x;
+    const int a = k > 0 ? k : -k;
+    for (int q = 1; q < a; q++) p = p * x;
+    return k > 0 ? p : 1.0 / p;
+}
+
+__global__ void nk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+                                    const double *__restrict__ t, GaussRule g, const double *gr,
+                                    const double *grm, const double *grw, const double *bsp, double *rkd)
+{
+    extern __shared__ double sm[];
+    const int ik = ks * (ks + 1) / 2;
+    double *bt = sm;                          // [m][i][j] : B-spline values at the inner points
+    double *wx = bt + ks * ks * ks;           // [m][i]   : inner weights * x^k
+    double *INT = wx + ks * ks;               // [m][jj]
+    int iv_out = blockIdx.x;
+    int iv1 = iv_out + 1;
+    int s0 = ml + ks, s1 = ml + me - ks + 2;
+    int nscale = 0, iv = iv_out;
+    if (me != 0 && iv1 >= s0 && iv1 <= s1) { iv = s0 - 2; nscale = iv1 - s0 + 1; }
+    int left = iv + ks - 1;
+    double xbase = t[left];
+    size_t ld = (size_t)(nv + 1);
+    for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) {
+        int m = q / ks, i = q % ks;
+        double span = gr[iv + (size_t)nv * m] - xbase;
+        double x = span * g.x[i] + xbase;
+        double v[BSRG_MAXKS];
+        bspl_values(t, ks, x, left, v);
+        for (int j = 0; j < ks; j++) bt[(m * ks + i) * ks + j] = v[j];
+        wx[m * ks + i] = span * g.w[i] * ipow_dev(x, k);
+    }
+    __syncthreads();
+    // INT(j,jp,m) = (SUM_i (wx_i bt(i,j)) bt(i,jp)) * grw(m) grm(m)^(k+3)
+    for (int q = threadIdx.x; q < ks * ik; q += blockDim.x) {
+        int m = q / ik, jj = q % ik;
+        int j = 0, rem = jj;
+        while (rem >= ks - j) { rem -= ks - j; j++; }
+        int jp = j + rem;
+        double s = 0.0;
+        for (int i = 0; i < ks; i++) {
+            double tmp = wx[m * ks + i] * bt[(m * ks + i) * ks + j];
+            s = s + tmp * bt[(m * ks + i) * ks + jp];
+        }
+        const double c = grw[iv + (size_t)nv * m] * ipow_dev(grm[iv + (size_t)nv * m], k + 3);
+        INT[m * ik + jj] = s * c;
+    }
+    __syncthreads();
+    double *out = rkd + (size_t)ik * ik * iv_out;
+    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
+        int ii = q % ik, jj = q / ik;
+        int i = 0, rem = ii;
+        while (rem >= ks - i) { rem -= ks - i; i++; }
+        int ip = i + rem;
+        double s = 0.0;
+        for (int m = 0; m < ks; m++) {
+            double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * bsp[iv + ld * (m + (size_t)ks * ip)];
+            s = s + g3 * INT[m * ik + jj];
+        }
+        for (int n = 0; n < nscale; n++) s = s / hscale;
+        out[ii + (size_t)ik * jj] = s;
+    }
+}
+
+// mnk_cell (mnk_cell.f90:2): rkb(i,j,ip,jp) = fine * sum over cells iv (outer,
+// r1) and jv <= iv (r2), in the reference's order; off-diagonal cells
+// factorise as rkd2(ii,iv) rkd1(jj,jv).  Staging as in rkb_expand_kernel.
+__global__ void __launch_bounds__(EXP_TI * EXP_TJ)
+nkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__restrict__ rkd1,
+                  const double *__restrict__ rkd2, const double *__restrict__ rkd, double *__restrict__ rkb)
+{
+    extern __shared__ double sm[];
+    const int ip = blockIdx.z % ldp, jp = blockIdx.z / ldp;
+    const int i0 = blockIdx.x * EXP_TI, j0 = blockIdx.y * EXP_TJ;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const int ik = ks * (ks + 1) / 2;
+    const int LI = EXP_TI + ks - 1, LJ = EXP_TJ + ks - 1;
+    const int ivb = i0 - (ks - 1), jvb = j0 - (ks - 1);
+    double *u2 = sm, *w1 = u2 + ks * LI;      // rkd2 on the r1 side, rkd1 on the r2 side
+    const bool active = ip < ks && jp < ks;
+    if (active) {
+        const int tid = threadIdx.y * EXP_TI + threadIdx.x, nt = EXP_TI * EXP_TJ;
+        for (int q = tid; q < ks * LI; q += nt) {
+            int ih = q / LI, iv = ivb + q % LI;
+            double b = 0.0;
+            if (ih + ip < ks && iv >= 0 && iv < nv) b = rkd2[ih * ks - ih * (ih - 1) / 2 + ip + (size_t)ik * iv];
+            u2[q] = b;
+        }
+        for (int q = tid; q < ks * LJ; q += nt) {
+            int jh = q / LJ, jv = jvb + q % LJ;
+            double a = 0.0;
+            if (jh + jp < ks && jv >= 0 && jv < nv) a = rkd1[jh * ks - jh * (jh - 1) / 2 + jp + (size_t)ik * jv];
+            w1[q] = a;
+        }
+    }
+    __syncthreads();
+    if (i >= ns || j >= ns) return;
+    double acc = 0.0;
+    if (active && i + ip < ns && j + jp < ns) {
+        int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
+        int iv_hi = i < nv - 1 ? i : nv - 1;
+        int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = j < nv - 1 ? j : nv - 1;
+        for (int iv = iv_lo; iv <= iv_hi; iv++) {
+            const int ih = i - iv, il = ih * LI + (iv - ivb);
+            const double r2i = u2[il];
+            const int jmax = jv_hi < iv ? jv_hi : iv;
+            for (int jv = jv_lo; jv <= jmax; jv++) {
+                const int jh = j - jv;
+                double c;
+                if (jv < iv) c = r2i * w1[jh * LJ + (jv - jvb)];
+                else {
+                    int ii = ih * ks - ih * (ih - 1) / 2 + ip;
+                    int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                    c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                }
+                acc = acc + c;
+            }
+        }
+    }
+    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * fine;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -474,6 +606,40 @@ int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2,
     size_t shm = sizeof(double) * 2 * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
     rkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, rkd1, rkd2, rkd, rkb);
     return cuda_fail(cudaGetLastError(), "mrk_cell");
+}
+
+int launch_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s)
+{
+    int ks = b->ks, nv = b->nv, ik = ik_of(ks);
+    double q = 1.0 + b->h;
+    int n = ik * nv;
+    if (rkd1)
+        moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k) * q, k, b->gr,
+                                                       b->grm, b->grw, b->bsp, rkd1);
+    if (rkd2)
+        moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 3)) * q,
+                                                       -(k + 3), b->gr, b->grm, b->grw, b->bsp, rkd2);
+    if (rkd) {
+        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik);
+        if (shm > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(nk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)shm);
+            if (e != cudaSuccess) return cuda_fail(e, "nk diag_cell smem");
+        }
+        nk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
+                                                b->grm, b->grw, b->bsp, rkd);
+    }
+    return cuda_fail(cudaGetLastError(), "nk_moments");
+}
+
+int launch_mnk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd, double fine,
+                    double *rkb, int ldp, cudaStream_t s)
+{
+    dim3 blk(EXP_TI, EXP_TJ);
+    dim3 grd((b->ns + EXP_TI - 1) / EXP_TI, (b->ns + EXP_TJ - 1) / EXP_TJ, ldp * ldp);
+    size_t shm = sizeof(double) * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
+    nkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, fine, rkd1, rkd2, rkd, rkb);
+    return cuda_fail(cudaGetLastError(), "mnk_cell");
 }
 
 }  // namespace bsrg

@@ -75,6 +75,20 @@ int bsrg_mrk_cell(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream
 /* Same, from moments already computed by bsrg_rk_moments (no allocation). */
 int bsrg_mrk_cell_from_moments(const bsrg_basis *b, const double *rkd1, const double *rkd2,
                                const double *rkd, double *rkb, int ldp, void *stream);
+/* ---- Breit-Pauli N^k cell moments: src/libs/BS/nk_moments.f90:2 (moments
+ *      rkd1 = <B_i|r^k|B_j>, rkd2 = <B_i|r^-(k+3)|B_j>; nk_triang :105 for the
+ *      diagonal cells, the r2 < r1 triangle only).  k >= -1.  Layouts as for
+ *      bsrg_rk_moments.  Device. */
+int bsrg_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
+
+/* ---- N^k B-spline integral table: src/libs/BS/mnk_cell.f90:2.
+ *      rkb(i,j,ip,jp) = fine * N^k(B_i B_j; B_{i+ip-1} B_{j+jp-1}) over r2 < r1,
+ *      with i, ip the r1 splines (cells jv <= iv only, not symmetric);
+ *      layout as bsrg_mrk_cell.  fine is spline_atomic's `fine`
+ *      (0.25/137.036^2 in the reference; its TEST_BS harness sets 1).  The
+ *      moments go to scratch the call allocates and frees.  Device. */
+int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

@@ -1383,3 +1383,149 @@ void orc_rsol(int ns, int nch, const int *ipsol, const double *bb, int khm, cons
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Breit-Pauli N^k tables: nk_moments.f90:2-189 (moments k and -(k+3),       */
+/* nk_pdiag :56 with the scaling law rkd(iv) = rkd(iv-1)/(1+h), nk_triang    */
+/* :105 -- the one-sided diagonal cell r2 < r1, not symmetrised) and         */
+/* mnk_cell.f90:2-85 (cells jv <= iv only, times `fine`).                    */
+/* ------------------------------------------------------------------------ */
+static double ipow(double x, int k)
+{
+    if (k == 0) return 1.0;
+    double p = x;
+    for (int q = 1; q < (k > 0 ? k : -k); q++) p *= x;
+    return k > 0 ? p : 1.0 / p;
+}
+
+void orc_nk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
+{
+    int ks = b->ks;
+    int ik = ks * (ks + 1) / 2;
+    int left = iv + ks - 1;
+    double xbase = b->t[left];
+    double gx[MAXKS], gw[MAXKS], bt[MAXKS * MAXKS], db[MAXKS], g2[MAXKS];
+    double *INT = (double *)malloc(sizeof(double) * ks * ks * ks);
+    for (int m = 0; m < ks; m++) {
+        double span = GR(b, iv, m) - xbase;
+        for (int i = 0; i < ks; i++) gx[i] = span * b->gx[i] + xbase;
+        for (int i = 0; i < ks; i++) {
+            orc_bsplvd(b->t, ks, gx[i], left, 1, db);
+            for (int j = 0; j < ks; j++) bt[i + ks * j] = db[j];
+        }
+        for (int i = 0; i < ks; i++) gw[i] = span * b->gw[i] * ipow(gx[i], k);
+        double c = GRW(b, iv, m) * ipow(GRM(b, iv, m), k + 3);
+        for (int j = 0; j < ks; j++) {
+            for (int i = 0; i < ks; i++) g2[i] = gw[i] * bt[i + ks * j];
+            for (int jp = j; jp < ks; jp++) {
+                double s = 0.0;
+                for (int i = 0; i < ks; i++) s = s + g2[i] * bt[i + ks * jp];
+                INT[j + ks * (jp + ks * m)] = s * c;
+            }
+        }
+    }
+    int ii = 0;
+    for (int i = 0; i < ks; i++)
+        for (int ip = i; ip < ks; ip++) {
+            double g3[MAXKS];
+            for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, i) * BSP(b, iv, m, ip);
+            int jj = 0;
+            for (int j = 0; j < ks; j++)
+                for (int jp = j; jp < ks; jp++) {
+                    double s = 0.0;
+                    for (int m = 0; m < ks; m++) s = s + g3[m] * INT[j + ks * (jp + ks * m)];
+                    rkd_iv[ii + ik * jj] = s;
+                    jj++;
+                }
+            ii++;
+        }
+    free(INT);
+}
+
+void orc_nk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd)
+{
+    int ks = b->ks, nv = b->nv, ml = b->ml, me = b->me;
+    int ik = ks * (ks + 1) / 2;
+    orc_moments(b, k, rkd1, 's', 'b');
+    orc_moments(b, -(k + 3), rkd2, 's', 'b');
+    size_t cell = (size_t)ik * ik;
+    if (me == 0) {
+        for (int iv = 0; iv < nv; iv++) orc_nk_triang(b, k, iv, rkd + cell * iv);
+        return;
+    }
+    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) orc_nk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+    double hp = b->h + 1.0;
+    for (int iv = ml + ks; iv <= ml + me - ks + 2; iv++)
+        for (size_t q = 0; q < cell; q++) rkd[q + cell * (iv - 1)] = rkd[q + cell * (iv - 2)] / hp;
+    for (int iv = ml + me - ks + 3; iv <= nv; iv++)
+        if (iv >= 1) orc_nk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+}
+
+/* rkb(i,j,ip,jp): i, ip the r1 (outer) splines, j, jp the r2 < r1 ones */
+void orc_mnk_cell_from(const orc_basis *b, const double *rkd1, const double *rkd2, const double *rkd, double fine,
+                       double *rkb, int ldp)
+{
+    int ks = b->ks, ns = b->ns, nv = b->nv;
+    int ik = ks * (ks + 1) / 2;
+    size_t nn = (size_t)ns * ns;
+    memset(rkb, 0, sizeof(double) * nn * ldp * ldp);
+    for (int iv = 0; iv < nv; iv++) {
+        int ii = 0;
+        for (int ih = 0; ih < ks; ih++) {
+            int i = iv + ih;
+            for (int ihp = ih; ihp < ks; ihp++) {
+                int ip = ihp - ih;
+                for (int jv = 0; jv <= iv; jv++) {
+                    int jj = 0;
+                    for (int jh = 0; jh < ks; jh++) {
+                        int j = jv + jh;
+                        for (int jhp = jh; jhp < ks; jhp++) {
+                            int jp = jhp - jh;
+                            double c = (jv < iv) ? rkd2[ii + (size_t)ik * iv] * rkd1[jj + (size_t)ik * jv]
+                                                 : rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
+                            size_t o = i + (size_t)ns * j + nn * (ip + (size_t)ldp * jp);
+                            rkb[o] = rkb[o] + c;
+                            jj++;
+                        }
+                    }
+                }
+                ii++;
+            }
+        }
+    }
+    for (size_t q = 0; q < nn * ldp * ldp; q++) rkb[q] = rkb[q] * fine;
+}
+
+void orc_mnk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, nv = b->nv;
+    int ik = ks * (ks + 1) / 2;
+    double *rkd1 = (double *)malloc(sizeof(double) * ik * nv);
+    double *rkd2 = (double *)malloc(sizeof(double) * ik * nv);
+    double *rkd = (double *)malloc(sizeof(double) * ik * ik * nv);
+    orc_nk_moments(b, k, rkd1, rkd2, rkd);
+    orc_mnk_cell_from(b, rkd1, rkd2, rkd, fine, rkb, ldp);
+    free(rkd1); free(rkd2); free(rkd);
+}
+
+/* nk.f90:2-47 with meth 'c': sum a(i,ip) b(j,jp) rkb(i,j,ip,jp), a = p_i1 p_i2, b = p_j1 p_j2 */
+double orc_nk(int ns, int ks, const double *rkb, int ldp, const double *pi1, const double *pj1, const double *pi2,
+              const double *pj2)
+{
+    double *a = (double *)malloc(sizeof(double) * ns * ks), *bb = (double *)malloc(sizeof(double) * ns * ks);
+    size_t nn = (size_t)ns * ns;
+    orc_density(ns, ks, a, pi1, pi2, 's');
+    orc_density(ns, ks, bb, pj1, pj2, 's');
+    double nk = 0.0;
+    for (int ip = 1; ip <= ks; ip++)
+        for (int i = 1; i <= ns - ip + 1; i++) {
+            double nkj = 0.0;
+            for (int jp = 1; jp <= ks; jp++)
+                for (int j = 1; j <= ns - jp + 1; j++)
+                    nkj = nkj + bb[(j - 1) + (size_t)ns * (jp - 1)] *
+                                rkb[(i - 1) + (size_t)ns * (j - 1) + nn * ((ip - 1) + (size_t)ldp * (jp - 1))];
+            nk = nk + a[(i - 1) + (size_t)ns * (ip - 1)] * nkj;
+        }
+    free(a); free(bb);
+    return nk;
+}

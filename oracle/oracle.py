@@ -57,6 +57,10 @@ def lib():
         L.orc_assemble.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, _I, _D,
                                    ctypes.c_int, _D, ctypes.c_int, _D,
                                    ctypes.c_int, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D]
+        L.orc_nk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.orc_mnk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_nk.restype = ctypes.c_double
+        L.orc_nk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
         L.orc_rsol.argtypes = [ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int, _D, _D, _D]
         _LIB = L
@@ -161,6 +165,23 @@ class Basis:
         ldp = ldp or self.ks
         rkb = np.zeros(self.ns * self.ns * ldp * ldp)
         lib().orc_mrk_cell(self._h, k, _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
+
+    def nk_moments(self, k):
+        """nk_moments (nk_moments.f90:2): rkd1 (ik,nv) power k, rkd2 power -(k+3), rkd (ik,ik,nv)."""
+        ik = self.ks * (self.ks + 1) // 2
+        rkd1 = np.zeros(ik * self.nv)
+        rkd2 = np.zeros(ik * self.nv)
+        rkd = np.zeros(ik * ik * self.nv)
+        lib().orc_nk_moments(self._h, k, _p(rkd1), _p(rkd2), _p(rkd))
+        return (rkd1.reshape((ik, self.nv), order="F"), rkd2.reshape((ik, self.nv), order="F"),
+                rkd.reshape((ik, ik, self.nv), order="F"))
+
+    def mnk_cell(self, k, fine=1.0, ldp=None):
+        """mnk_cell (mnk_cell.f90:2): N^k table rkb (ns,ns,ldp,ldp), Fortran order, times fine."""
+        ldp = ldp or self.ks
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mnk_cell(self._h, k, float(fine), _p(rkb), ldp)
         return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def quadr(self, p1, p2, m):
@@ -348,3 +369,10 @@ def rsol(ns, nch, ipsol, bb, a, want_v=True):
     lib().orc_rsol(ns, nch, _pi(ipsol), bbf.ctypes.data_as(_D), khm, af.ctypes.data_as(_D),
                    v.ctypes.data_as(_D) if want_v else None, w.ctypes.data_as(_D))
     return v, w
+
+
+def nk(ns, ks, rkb, pi1, pj1, pi2, pj2):
+    """nk.f90 (meth 'c'): N^k(i1, j1; i2, j2) from an mnk_cell table."""
+    r = np.asfortranarray(rkb)
+    f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
+    return lib().orc_nk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f])

@@ -1,0 +1,91 @@
+"""Breit-Pauli N^k cell moments and tables on the GPU against the oracle: bit for bit.
+
+nk_moments (nk_moments.f90:2) and mnk_cell (mnk_cell.f90:2) run in the
+reference's summation order without fused multiply-adds, as the R^k tables do;
+the N^k integrals of the TEST_BS hydrogenic orbitals computed from the GPU table
+reproduce int_inp1's exact values."""
+import numpy as np
+import pytest
+
+from tests.gpu_helpers import grids, to_np
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = grids()
+
+
+@pytest.fixture(scope="module", params=GRIDS, ids=[g[0] for g in GRIDS])
+def pair(request):
+    import bsr_b200 as bsr
+    from oracle import oracle as O
+    name, ks, t, ml, me, h = request.param
+    return name, bsr.define_spline(t, ks, ml, me, h), O.Basis(ks, t, ml, me, h)
+
+
+@pytest.mark.parametrize("k", [-1, 0, 2])
+def test_nk_moments_bitwise(pair, k):
+    from bsr_b200 import core
+    name, gb, ob = pair
+    if name == "config2" and k != 2:
+        pytest.skip("one multipole suffices at ns=200")
+    got = [to_np(x) for x in core.nk_moments(gb, k)]
+    ref = ob.nk_moments(k)
+    for g, r in zip(got, ref):
+        assert np.array_equal(g, r), name
+
+
+@pytest.mark.parametrize("k,fine", [(-1, 1.0), (1, 1.0), (3, 0.25 / 137.036 ** 2)])
+def test_mnk_cell_bitwise(pair, k, fine):
+    from bsr_b200 import core
+    name, gb, ob = pair
+    if name == "config2" and k != 3:
+        pytest.skip("one multipole suffices at ns=200")
+    got = to_np(core.mnk_cell(gb, k, fine=fine))
+    ref = ob.mnk_cell(k, fine=fine)
+    assert got.shape == ref.shape
+    assert np.array_equal(got, ref), name
+
+
+def test_mnk_cell_wide_ldp_zero(pair):
+    from bsr_b200 import core
+    name, gb, ob = pair
+    if name != "config1":
+        pytest.skip("layout check on one grid")
+    ks = gb.ks
+    got = to_np(core.mnk_cell(gb, 1, fine=1.0, ldp=2 * ks - 1))
+    assert np.array_equal(got[:, :, :ks, :ks], ob.mnk_cell(1, fine=1.0))
+    assert not np.any(got[:, :, ks:, :]) and not np.any(got[:, :, :, ks:])
+
+
+def test_int_inp1_nk_on_gpu(golden, test_bs):
+    """N^k of the Z=2 hydrogenic orbitals from the GPU tables against int_inp1 (x Z^3)."""
+    import bsr_b200 as bsr
+    from bsr_b200 import core
+    from oracle import oracle as O
+    B = test_bs["basis"]
+    g = test_bs["grid"]
+    gb = bsr.define_spline(g["t"], B.ks, g["ml"], g["me"], g["h"])
+    z = test_bs["knot"]["z"]
+    orbs = {"%d%s" % (n, "spdfg"[l]): B.bhwf(n, l, z) for n in range(1, 6) for l in range(n)}
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "N":
+            continue
+        rkb = to_np(core.mnk_cell(gb, e["k"], fine=1.0))
+        got = O.nk(B.ns, B.ks, rkb, *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
+        n += 1
+    assert n == 10
+
+
+def test_bad_k_rejected():
+    import bsr_b200 as bsr
+    from bsr_b200 import core
+    from bsr_b200._lib import BsrgError
+    from bsr_b200 import workload as W
+    cfg = W.CONFIGS["config1"]
+    t, _ = W.knot_grid(cfg["ks"], cfg["ns"], cfg["rmin"], cfg["rmax"])
+    gb = bsr.define_spline(t, cfg["ks"])
+    with pytest.raises(BsrgError, match="out of range"):
+        core.mnk_cell(gb, -2)

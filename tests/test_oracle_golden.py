@@ -66,3 +66,39 @@ def test_orthogonality_matches_quadr_out(test_bs, golden):
             assert abs(v - e["err"]) <= half_ulp3 * (1 + 1e-9), (e, v)
         else:
             assert abs(v) < 1e-12, (e, v)
+
+
+def test_int_inp1_analytic_nk(test_bs, golden):
+    """Breit-Pauli N^k (nk_moments + mnk_cell + the nk.f90 route, fine = 1 as the TEST_BS
+    harness sets it) of Z=2 hydrogenic orbitals against int_inp1's exact values x Z^3
+    (test_bs.f90:326-328), including the k = -1 entries."""
+    B = test_bs["basis"]
+    z = test_bs["knot"]["z"]
+    orbs = {}
+    for n in range(1, 6):
+        for l in range(n):
+            orbs["%d%s" % (n, "spdfg"[l])] = B.bhwf(n, l, z)
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "N":
+            continue
+        rkb = B.mnk_cell(e["k"])
+        got = O.nk(B.ns, B.ks, rkb, *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
+        n += 1
+    assert n == 10
+
+
+def test_mnk_cell_fine_scales():
+    """mnk_cell multiplies the whole table by `fine` after the cell sums (mnk_cell.f90:78)."""
+    from bsr_b200 import workload as W
+    cfg = W.CONFIGS["config1"]
+    t, _ = W.knot_grid(cfg["ks"], cfg["ns"], cfg["rmin"], cfg["rmax"])
+    B = O.Basis(cfg["ks"], t)
+    a = B.mnk_cell(1, fine=1.0)
+    f = 0.25 / 137.036 ** 2
+    b = B.mnk_cell(1, fine=f)
+    assert np.array_equal(b, a * f)
+    # not symmetric under r1 <-> r2, unlike R^k
+    assert np.max(np.abs(a - a.transpose(1, 0, 3, 2))) > 1e-3 * np.max(np.abs(a))
