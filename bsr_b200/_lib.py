@@ -32,6 +32,8 @@ SIGNATURES = [
     ("bsrg_mrk_cell_from_moments", _c_int, [_P, _P, _P, _P, _P, _c_int, _P]),
     ("bsrg_nk_moments", _c_int, [_P, _c_int, _P, _P, _P, _P]),
     ("bsrg_mnk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),
+    ("bsrg_mk_moments", _c_int, [_P, _c_int, _P, _P, _P, _P]),
+    ("bsrg_mmk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),
     ("bsrg_mrk_cell_noalloc", _c_int, [_P, _c_int, _P, _c_int, _P]),
     ("bsrg_density", _c_int, [_c_int, _c_int, _P, _P, _P, _c_char, _P]),
     ("bsrg_convol", _c_int, [_c_int, _c_int, _P, _P, _P, _c_int, _c_int, _c_char, _c_char, _P]),

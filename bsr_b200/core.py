@@ -168,6 +168,25 @@ def nk_moments(basis, k):
     return rkd1, rkd2, rkd
 
 
+def mk_moments(basis, k):
+    """Breit-Pauli M^k cell moments (the N^k ones with symmetrised diagonal cells), k >= -1."""
+    ik = basis.ks * (basis.ks + 1) // 2
+    rkd1 = fortran_empty((ik, basis.nv))
+    rkd2 = fortran_empty((ik, basis.nv))
+    rkd = fortran_empty((ik, ik, basis.nv))
+    call("bsrg_mk_moments", basis.handle, k, _ptr(rkd1), _ptr(rkd2), _ptr(rkd), _stream())
+    return rkd1, rkd2, rkd
+
+
+def mmk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
+    """M^k table rkb(ns,ns,ldp,ldp) times fine (mmk_cell.f90)."""
+    ldp = basis.ks if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mmk_cell", basis.handle, k, float(fine), _ptr(out), ldp, _stream())
+    return out
+
+
 def mnk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     """N^k table rkb(ns,ns,ldp,ldp) times fine (mnk_cell.f90); i, ip the r1 splines, r2 < r1."""
     ldp = basis.ks if ldp is None else ldp

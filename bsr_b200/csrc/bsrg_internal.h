@@ -40,7 +40,10 @@ int launch_mrm(const bsrg_basis *b, int mm, double *rm, cudaStream_t s);
 int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s);
 int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
                     double *rkb, int ldp, cudaStream_t s);
-int launch_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s);
+int launch_nkmk_moments(const bsrg_basis *b, int k, int sym, double *rkd1, double *rkd2, double *rkd,
+                        cudaStream_t s);
+int launch_mrk_cell_scaled(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                           double fine, double *rkb, int ldp, cudaStream_t s);
 int launch_mnk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd, double fine,
                     double *rkb, int ldp, cudaStream_t s);
 int launch_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, cudaStream_t s);

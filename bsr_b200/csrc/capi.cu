@@ -280,7 +280,31 @@ int bsrg_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, doub
 {
     CHECK_ARG(b, "nk_moments: null basis");
     CHECK_ARG(k >= -1 && k <= 64, "nk_moments: k=%d out of range", k);
-    return launch_nk_moments(b, k, rkd1, rkd2, rkd, (cudaStream_t)stream);
+    return launch_nkmk_moments(b, k, 0, rkd1, rkd2, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_mk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream)
+{
+    CHECK_ARG(b, "mk_moments: null basis");
+    CHECK_ARG(k >= -1 && k <= 64, "mk_moments: k=%d out of range", k);
+    return launch_nkmk_moments(b, k, 1, rkd1, rkd2, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_mmk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkb, "mmk_cell: null argument");
+    CHECK_ARG(ldp >= b->ks, "mmk_cell: ldp=%d < ks=%d", ldp, b->ks);
+    CHECK_ARG(k >= -1 && k <= 64, "mmk_cell: k=%d out of range", k);
+    cudaStream_t s = (cudaStream_t)stream;
+    int ik = ik_of(b->ks);
+    size_t n1 = (size_t)ik * b->nv, n3 = (size_t)ik * ik * b->nv;
+    double *buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * n1 + n3) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "mmk_cell scratch");
+    int rc = launch_nkmk_moments(b, k, 1, buf, buf + n1, buf + 2 * n1, s);
+    if (rc == BSRG_OK) rc = launch_mrk_cell_scaled(b, buf, buf + n1, buf + 2 * n1, fine, rkb, ldp, s);
+    cudaFreeAsync(buf, s);
+    return rc;
 }
 
 int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
@@ -294,7 +318,7 @@ int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
     double *buf = nullptr;
     cudaError_t e = cudaMallocAsync((void **)&buf, (2 * n1 + n3) * sizeof(double), s);
     if (e != cudaSuccess) return cuda_fail(e, "mnk_cell scratch");
-    int rc = launch_nk_moments(b, k, buf, buf + n1, buf + 2 * n1, s);
+    int rc = launch_nkmk_moments(b, k, 0, buf, buf + n1, buf + 2 * n1, s);
     if (rc == BSRG_OK) rc = launch_mnk_cell(b, buf, buf + n1, buf + 2 * n1, fine, rkb, ldp, s);
     cudaFreeAsync(buf, s);
     return rc;

@@ -335,7 +335,7 @@ __global__ void diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, 
 constexpr int EXP_TI = 32, EXP_TJ = 8;
 
 __global__ void __launch_bounds__(EXP_TI * EXP_TJ)
-rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rkd1,
+rkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__restrict__ rkd1,
                   const double *__restrict__ rkd2, const double *__restrict__ rkd, double *__restrict__ rkb)
 {
     extern __shared__ double sm[];
@@ -397,7 +397,8 @@ rkb_expand_kernel(int ks, int ns, int nv, int ldp, const double *__restrict__ rk
             }
         }
     }
-    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc;
+    // fine = 1 for R^k (exact), spline_atomic's fine for M^k (mmk_cell.f90:79)
+    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * fine;
 }
 
 
@@ -415,7 +416,7 @@ __device__ static double ipow_dev(double x, int k)
     return k > 0 ? p : 1.0 / p;
 }
 
-__global__ void nk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+__global__ void nk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k, int sym,
                                     const double *__restrict__ t, GaussRule g, const double *gr,
                                     const double *grm, const double *grw, const double *bsp, double *rkd)
 {
@@ -424,6 +425,7 @@ __global__ void nk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscal
     double *bt = sm;                          // [m][i][j] : B-spline values at the inner points
     double *wx = bt + ks * ks * ks;           // [m][i]   : inner weights * x^k
     double *INT = wx + ks * ks;               // [m][jj]
+    double *a = INT + ks * ik;                // [jj][ii] (sym only): a(ii,jj) before a + a^T
     int iv_out = blockIdx.x;
     int iv1 = iv_out + 1;
     int s0 = ml + ks, s1 = ml + me - ks + 2;
@@ -468,8 +470,21 @@ __global__ void nk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscal
             double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * bsp[iv + ld * (m + (size_t)ks * ip)];
             s = s + g3 * INT[m * ik + jj];
         }
-        for (int n = 0; n < nscale; n++) s = s / hscale;
-        out[ii + (size_t)ik * jj] = s;
+        if (sym) {
+            a[ii + ik * jj] = s;
+        } else {
+            for (int n = 0; n < nscale; n++) s = s / hscale;
+            out[ii + (size_t)ik * jj] = s;
+        }
+    }
+    if (!sym) return;
+    // mk_triang (mk_moments.f90:96): the cell returned as a + transpose(a)
+    __syncthreads();
+    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
+        int r = q % ik, c = q / ik;
+        double v = a[r + ik * c] + a[c + ik * r];
+        for (int n = 0; n < nscale; n++) v = v / hscale;
+        out[r + (size_t)ik * c] = v;
     }
 }
 
@@ -598,17 +613,25 @@ int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
     return cuda_fail(cudaGetLastError(), "rk_moments");
 }
 
-int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
-                    double *rkb, int ldp, cudaStream_t s)
+int launch_mrk_cell_scaled(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                           double fine, double *rkb, int ldp, cudaStream_t s)
 {
     dim3 blk(EXP_TI, EXP_TJ);
     dim3 grd((b->ns + EXP_TI - 1) / EXP_TI, (b->ns + EXP_TJ - 1) / EXP_TJ, ldp * ldp);
     size_t shm = sizeof(double) * 2 * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
-    rkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, rkd1, rkd2, rkd, rkb);
+    rkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, fine, rkd1, rkd2, rkd, rkb);
     return cuda_fail(cudaGetLastError(), "mrk_cell");
 }
 
-int launch_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s)
+int launch_mrk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd,
+                    double *rkb, int ldp, cudaStream_t s)
+{
+    return launch_mrk_cell_scaled(b, rkd1, rkd2, rkd, 1.0, rkb, ldp, s);
+}
+
+// N^k (sym = 0) or M^k (sym = 1) moments: the same moments, M^k symmetrises the diagonal cells
+int launch_nkmk_moments(const bsrg_basis *b, int k, int sym, double *rkd1, double *rkd2, double *rkd,
+                        cudaStream_t s)
 {
     int ks = b->ks, nv = b->nv, ik = ik_of(ks);
     double q = 1.0 + b->h;
@@ -620,16 +643,16 @@ int launch_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
         moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 3)) * q,
                                                        -(k + 3), b->gr, b->grm, b->grw, b->bsp, rkd2);
     if (rkd) {
-        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik);
+        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik + (sym ? (size_t)ik * ik : 0));
         if (shm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(nk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)shm);
             if (e != cudaSuccess) return cuda_fail(e, "nk diag_cell smem");
         }
-        nk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
+        nk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, sym, b->t, rule_of(b), b->gr,
                                                 b->grm, b->grw, b->bsp, rkd);
     }
-    return cuda_fail(cudaGetLastError(), "nk_moments");
+    return cuda_fail(cudaGetLastError(), sym ? "mk_moments" : "nk_moments");
 }
 
 int launch_mnk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd, double fine,

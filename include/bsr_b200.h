@@ -89,6 +89,13 @@ int bsrg_nk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, doub
  *      moments go to scratch the call allocates and frees.  Device. */
 int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
 
+/* ---- Breit-Pauli M^k: src/libs/BS/mk_moments.f90:2 (the N^k moments, the
+ *      diagonal cells symmetrised a + a^T as mk_triang :96 does) and
+ *      mmk_cell.f90:2 (mrk_cell's symmetric cell sums, times fine).
+ *      Layouts and fine as for the N^k calls.  Device. */
+int bsrg_mk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
+int bsrg_mmk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

@@ -1398,7 +1398,9 @@ static double ipow(double x, int k)
     return k > 0 ? p : 1.0 / p;
 }
 
-void orc_nk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
+/* sym = 0: nk_triang (nk_moments.f90:105); sym = 1: mk_triang (mk_moments.f90:96),
+   the same cell integral returned as a + transpose(a) */
+static void nkmk_triang(const orc_basis *b, int k, int iv, double *rkd_iv, int sym)
 {
     int ks = b->ks;
     int ik = ks * (ks + 1) / 2;
@@ -1439,10 +1441,19 @@ void orc_nk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
                 }
             ii++;
         }
+    if (sym) {
+        double *a = (double *)malloc(sizeof(double) * ik * ik);
+        memcpy(a, rkd_iv, sizeof(double) * ik * ik);
+        for (int c = 0; c < ik; c++)
+            for (int r = 0; r < ik; r++) rkd_iv[r + ik * c] = a[r + ik * c] + a[c + ik * r];
+        free(a);
+    }
     free(INT);
 }
 
-void orc_nk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd)
+void orc_nk_triang(const orc_basis *b, int k, int iv, double *rkd_iv) { nkmk_triang(b, k, iv, rkd_iv, 0); }
+
+static void nkmk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd, int sym)
 {
     int ks = b->ks, nv = b->nv, ml = b->ml, me = b->me;
     int ik = ks * (ks + 1) / 2;
@@ -1450,15 +1461,41 @@ void orc_nk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, doubl
     orc_moments(b, -(k + 3), rkd2, 's', 'b');
     size_t cell = (size_t)ik * ik;
     if (me == 0) {
-        for (int iv = 0; iv < nv; iv++) orc_nk_triang(b, k, iv, rkd + cell * iv);
+        for (int iv = 0; iv < nv; iv++) nkmk_triang(b, k, iv, rkd + cell * iv, sym);
         return;
     }
-    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) orc_nk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) nkmk_triang(b, k, iv - 1, rkd + cell * (iv - 1), sym);
     double hp = b->h + 1.0;
     for (int iv = ml + ks; iv <= ml + me - ks + 2; iv++)
         for (size_t q = 0; q < cell; q++) rkd[q + cell * (iv - 1)] = rkd[q + cell * (iv - 2)] / hp;
     for (int iv = ml + me - ks + 3; iv <= nv; iv++)
-        if (iv >= 1) orc_nk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+        if (iv >= 1) nkmk_triang(b, k, iv - 1, rkd + cell * (iv - 1), sym);
+}
+
+void orc_nk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd)
+{
+    nkmk_moments(b, k, rkd1, rkd2, rkd, 0);
+}
+
+/* mk_moments.f90:2: moments k and -(k+3) as for N^k, symmetrised diagonal cells */
+void orc_mk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd)
+{
+    nkmk_moments(b, k, rkd1, rkd2, rkd, 1);
+}
+
+/* mmk_cell.f90:2-83: mrk_cell's symmetric cell sums of the M^k moments, times fine */
+void orc_mmk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, nv = b->nv, ns = b->ns;
+    int ik = ks * (ks + 1) / 2;
+    double *rkd1 = (double *)malloc(sizeof(double) * ik * nv);
+    double *rkd2 = (double *)malloc(sizeof(double) * ik * nv);
+    double *rkd = (double *)malloc(sizeof(double) * ik * ik * nv);
+    orc_mk_moments(b, k, rkd1, rkd2, rkd);
+    orc_mrk_cell_from(b, rkd1, rkd2, rkd, rkb, ldp);
+    size_t tot = (size_t)ns * ns * ldp * ldp;
+    for (size_t q = 0; q < tot; q++) rkb[q] = rkb[q] * fine;
+    free(rkd1); free(rkd2); free(rkd);
 }
 
 /* rkb(i,j,ip,jp): i, ip the r1 (outer) splines, j, jp the r2 < r1 ones */

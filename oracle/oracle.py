@@ -59,6 +59,8 @@ def lib():
                                    ctypes.c_int, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D]
         L.orc_nk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.orc_mnk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_mk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.orc_mmk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_nk.restype = ctypes.c_double
         L.orc_nk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
@@ -176,6 +178,23 @@ class Basis:
         lib().orc_nk_moments(self._h, k, _p(rkd1), _p(rkd2), _p(rkd))
         return (rkd1.reshape((ik, self.nv), order="F"), rkd2.reshape((ik, self.nv), order="F"),
                 rkd.reshape((ik, ik, self.nv), order="F"))
+
+    def mk_moments(self, k):
+        """mk_moments (mk_moments.f90:2): as nk_moments with symmetrised diagonal cells."""
+        ik = self.ks * (self.ks + 1) // 2
+        rkd1 = np.zeros(ik * self.nv)
+        rkd2 = np.zeros(ik * self.nv)
+        rkd = np.zeros(ik * ik * self.nv)
+        lib().orc_mk_moments(self._h, k, _p(rkd1), _p(rkd2), _p(rkd))
+        return (rkd1.reshape((ik, self.nv), order="F"), rkd2.reshape((ik, self.nv), order="F"),
+                rkd.reshape((ik, ik, self.nv), order="F"))
+
+    def mmk_cell(self, k, fine=1.0, ldp=None):
+        """mmk_cell (mmk_cell.f90:2): M^k table rkb (ns,ns,ldp,ldp), Fortran order, times fine."""
+        ldp = ldp or self.ks
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mmk_cell(self._h, k, float(fine), _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def mnk_cell(self, k, fine=1.0, ldp=None):
         """mnk_cell (mnk_cell.f90:2): N^k table rkb (ns,ns,ldp,ldp), Fortran order, times fine."""
@@ -376,3 +395,10 @@ def nk(ns, ks, rkb, pi1, pj1, pi2, pj2):
     r = np.asfortranarray(rkb)
     f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
     return lib().orc_nk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f])
+
+
+def mk(ns, ks, rkb, pi1, pj1, pi2, pj2):
+    """mk.f90 (meth 'c'): M^k(i1, j1; i2, j2), the rk.f90 sum over an mmk_cell table halved."""
+    r = np.asfortranarray(rkb)
+    f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
+    return lib().orc_rk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f]) / 2.0

@@ -102,3 +102,20 @@ def test_mnk_cell_fine_scales():
     assert np.array_equal(b, a * f)
     # not symmetric under r1 <-> r2, unlike R^k
     assert np.max(np.abs(a - a.transpose(1, 0, 3, 2))) > 1e-3 * np.max(np.abs(a))
+
+
+def test_int_inp1_analytic_mk(test_bs, golden):
+    """Breit-Pauli M^k (mk_moments + mmk_cell + the mk.f90 route, fine = 1) against
+    int_inp1's exact values x Z^3."""
+    B = test_bs["basis"]
+    z = test_bs["knot"]["z"]
+    orbs = {"%d%s" % (n, "spdfg"[l]): B.bhwf(n, l, z) for n in range(1, 6) for l in range(n)}
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "M":
+            continue
+        got = O.mk(B.ns, B.ks, B.mmk_cell(e["k"]), *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
+        n += 1
+    assert n == 7
