@@ -187,6 +187,25 @@ def mmk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     return out
 
 
+def tk_moments(basis, k):
+    """Breit-Pauli T^k cell moments: rkd1, rkd2 (ks*ks, nv) and rkd (ks*ks, ks*ks, nv)."""
+    jk = basis.ks * basis.ks
+    rkd1 = fortran_empty((jk, basis.nv))
+    rkd2 = fortran_empty((jk, basis.nv))
+    rkd = fortran_empty((jk, jk, basis.nv))
+    call("bsrg_tk_moments", basis.handle, k, _ptr(rkd1), _ptr(rkd2), _ptr(rkd), _stream())
+    return rkd1, rkd2, rkd
+
+
+def mtk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
+    """T^k table rkb(ns,ns,ldp,ldp), ldp >= 2ks-1 (default), times fine/(2k+1) (mtk_cell.f90)."""
+    ldp = 2 * basis.ks - 1 if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mtk_cell", basis.handle, k, float(fine), _ptr(out), ldp, _stream())
+    return out
+
+
 def mnk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     """N^k table rkb(ns,ns,ldp,ldp) times fine (mnk_cell.f90); i, ip the r1 splines, r2 < r1."""
     ldp = basis.ks if ldp is None else ldp

@@ -324,6 +324,29 @@ int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
     return rc;
 }
 
+int bsrg_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream)
+{
+    CHECK_ARG(b, "tk_moments: null basis");
+    CHECK_ARG(k >= 0 && k <= 64, "tk_moments: k=%d out of range", k);
+    return launch_tk_moments(b, k, rkd1, rkd2, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_mtk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkb, "mtk_cell: null argument");
+    CHECK_ARG(ldp >= 2 * b->ks - 1, "mtk_cell: ldp=%d < 2ks-1=%d", ldp, 2 * b->ks - 1);
+    CHECK_ARG(k >= 0 && k <= 64, "mtk_cell: k=%d out of range", k);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t jk = (size_t)b->ks * b->ks, n1 = jk * b->nv, n3 = jk * jk * b->nv;
+    double *buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * n1 + n3) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "mtk_cell scratch");
+    int rc = launch_tk_moments(b, k, buf, buf + n1, buf + 2 * n1, s);
+    if (rc == BSRG_OK) rc = launch_mtk_cell(b, k, buf, buf + n1, buf + 2 * n1, fine, rkb, ldp, s);
+    cudaFreeAsync(buf, s);
+    return rc;
+}
+
 int bsrg_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, void *stream)
 {
     CHECK_ARG(d && p1 && p2, "density: null argument");

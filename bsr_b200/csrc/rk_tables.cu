@@ -547,6 +547,176 @@ nkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__
     rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * fine;
 }
 
+
+// ---------------------------------------------------------------------------
+// Breit-Pauli T^k (tk_moments.f90, mtk_cell.f90).  moments 'n','d': all ks*ks
+// pairs ii = i*ks + j with the derivative operator bsq on the second spline.
+// ---------------------------------------------------------------------------
+__global__ void moments_nd_kernel(int ks, int nv, int ml, int me, double hp, int k, const double *gr,
+                                  const double *grm, const double *grw, const double *bsp, const double *bsq,
+                                  double *rkm)
+{
+    const int jk = ks * ks;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= jk * nv) return;
+    const int ii = tid % jk, iv_out = tid / jk;
+    const int i = ii / ks, j = ii % ks;
+    const int iv1 = iv_out + 1;
+    const int s0 = ml + ks, s1 = ml + me - ks + 2;
+    const bool scaled = me != 0 && iv1 >= s0 && iv1 <= s1;
+    const int iv = scaled ? s0 - 2 : iv_out;
+    const size_t ld = (size_t)(nv + 1);
+    double v = 0.0;
+    for (int m = 0; m < ks; m++) {
+        double gw = grw[iv + (size_t)nv * m];
+        if (k > 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(gr[iv + (size_t)nv * m], k);
+        if (k < 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], -k);
+        const double bj = bsq[iv + ld * (m + (size_t)ks * j)] * gw;
+        v = v + bsp[iv + ld * (m + (size_t)ks * i)] * bj;
+    }
+    if (scaled)
+        for (int q = s0; q <= iv1; q++) v = v * hp;
+    rkm[ii + (size_t)jk * iv_out] = v;
+}
+
+// tk_triang (tk_moments.f90:101): inner integral of B_j (dB_jp/dr - B_jp/r) r^k
+// up to each outer Gauss point, outer weights bsq grw grm^(k+1), a + a^T.
+__global__ void tk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+                                    const double *__restrict__ t, GaussRule g, const double *gr,
+                                    const double *grm, const double *grw, const double *bsp,
+                                    const double *bsq, double *rkd)
+{
+    extern __shared__ double sm[];
+    const int jk = ks * ks;
+    double *bt = sm;                          // [m][i][j] values
+    double *bd = bt + ks * ks * ks;           // [m][i][j] derivative - value/x
+    double *wx = bd + ks * ks * ks;           // [m][i]
+    double *INT = wx + ks * ks;               // [m][j][jp]
+    double *bq = INT + ks * ks * ks;          // [m][ip]
+    double *a = bq + ks * ks;                 // a(ii,jj), column-major jk x jk
+    const int iv_out = blockIdx.x, iv1 = iv_out + 1;
+    const int s0 = ml + ks, s1 = ml + me - ks + 2;
+    int nscale = 0, iv = iv_out;
+    if (me != 0 && iv1 >= s0 && iv1 <= s1) { iv = s0 - 2; nscale = iv1 - s0 + 1; }
+    const int left = iv + ks - 1;
+    const double xbase = t[left];
+    const size_t ld = (size_t)(nv + 1);
+    for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) {
+        const int m = q / ks, i = q % ks;
+        const double span = gr[iv + (size_t)nv * m] - xbase;
+        const double x = span * g.x[i] + xbase;
+        double db[2 * BSRG_MAXKS];
+        bsplvd_dev(t, ks, x, left, 2, db);
+        for (int j = 0; j < ks; j++) {
+            bt[(m * ks + i) * ks + j] = db[j];
+            bd[(m * ks + i) * ks + j] = db[j + ks] - db[j] / x;
+        }
+        wx[m * ks + i] = ipow_dev(x, k) * (span * g.w[i]);
+    }
+    for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) {
+        const int m = q / ks, ip = q % ks;
+        const double g2 = grw[iv + (size_t)nv * m] * ipow_dev(grm[iv + (size_t)nv * m], k + 1);
+        bq[m * ks + ip] = bsq[iv + ld * (m + (size_t)ks * ip)] * g2;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < ks * jk; q += blockDim.x) {
+        const int m = q / jk, j = (q % jk) / ks, jp = q % ks;
+        double s = 0.0;
+        for (int i = 0; i < ks; i++) {
+            const double tmp = wx[m * ks + i] * bt[(m * ks + i) * ks + j];
+            s = s + tmp * bd[(m * ks + i) * ks + jp];
+        }
+        INT[(m * ks + j) * ks + jp] = s;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < jk * jk; q += blockDim.x) {
+        const int ii = q % jk, jj = q / jk;
+        const int i = ii / ks, ip = ii % ks, j = jj / ks, jp = jj % ks;
+        double s = 0.0;
+        for (int m = 0; m < ks; m++) {
+            const double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * bq[m * ks + ip];
+            s = s + g3 * INT[(m * ks + j) * ks + jp];
+        }
+        a[ii + jk * jj] = s;
+    }
+    __syncthreads();
+    double *out = rkd + (size_t)jk * jk * iv_out;
+    for (int q = threadIdx.x; q < jk * jk; q += blockDim.x) {
+        const int r = q % jk, c = q / jk;
+        double v = a[r + jk * c] + a[c + jk * r];
+        for (int n = 0; n < nscale; n++) v = v / hscale;
+        out[r + (size_t)jk * c] = v;
+    }
+}
+
+// mtk_cell (mtk_cell.f90:2): rkb(i,j,ip,jp), ip = ihp - ih + ks - 1 (0-based, up
+// to 2ks-2), summed over cells jv outer, iv inner; times fine/(2k+1).
+__global__ void __launch_bounds__(EXP_TI * EXP_TJ)
+tkb_expand_kernel(int ks, int ns, int nv, int ldp, double cfine, const double *__restrict__ rkd1,
+                  const double *__restrict__ rkd2, const double *__restrict__ rkd, double *__restrict__ rkb)
+{
+    extern __shared__ double sm[];
+    const int ip = blockIdx.z % ldp, jp = blockIdx.z / ldp;
+    const int i0 = blockIdx.x * EXP_TI, j0 = blockIdx.y * EXP_TJ;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const int jk = ks * ks;
+    const int LI = EXP_TI + ks - 1, LJ = EXP_TJ + ks - 1;
+    const int ivb = i0 - (ks - 1), jvb = j0 - (ks - 1);
+    double *u1 = sm, *u2 = u1 + ks * LI, *w1 = u2 + ks * LI, *w2 = w1 + ks * LJ;
+    const bool active = ip < 2 * ks - 1 && jp < 2 * ks - 1;
+    if (active) {
+        const int tid = threadIdx.y * EXP_TI + threadIdx.x, nt = EXP_TI * EXP_TJ;
+        for (int q = tid; q < ks * LI; q += nt) {
+            const int ih = q / LI, iv = ivb + q % LI, ihp = ih + ip - (ks - 1);
+            double a = 0.0, b = 0.0;
+            if (ihp >= 0 && ihp < ks && iv >= 0 && iv < nv) {
+                a = rkd1[ih * ks + ihp + (size_t)jk * iv];
+                b = rkd2[ih * ks + ihp + (size_t)jk * iv];
+            }
+            u1[q] = a;
+            u2[q] = b;
+        }
+        for (int q = tid; q < ks * LJ; q += nt) {
+            const int jh = q / LJ, jv = jvb + q % LJ, jhp = jh + jp - (ks - 1);
+            double a = 0.0, b = 0.0;
+            if (jhp >= 0 && jhp < ks && jv >= 0 && jv < nv) {
+                a = rkd1[jh * ks + jhp + (size_t)jk * jv];
+                b = rkd2[jh * ks + jhp + (size_t)jk * jv];
+            }
+            w1[q] = a;
+            w2[q] = b;
+        }
+    }
+    __syncthreads();
+    if (i >= ns || j >= ns) return;
+    double acc = 0.0;
+    if (active) {
+        // ih = i - iv with 0 <= ih < ks and 0 <= ih + ip - (ks-1) < ks
+        const int ihmin = (ks - 1 - ip) > 0 ? ks - 1 - ip : 0, ihmax = (2 * ks - 2 - ip) < ks - 1 ? 2 * ks - 2 - ip : ks - 1;
+        const int jhmin = (ks - 1 - jp) > 0 ? ks - 1 - jp : 0, jhmax = (2 * ks - 2 - jp) < ks - 1 ? 2 * ks - 2 - jp : ks - 1;
+        int iv_lo = i - ihmax; if (iv_lo < 0) iv_lo = 0;
+        int iv_hi = i - ihmin; if (iv_hi > nv - 1) iv_hi = nv - 1;
+        int jv_lo = j - jhmax; if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = j - jhmin; if (jv_hi > nv - 1) jv_hi = nv - 1;
+        for (int jv = jv_lo; jv <= jv_hi; jv++) {
+            const int jh = j - jv, jl = jh * LJ + (jv - jvb);
+            const double r2j = w2[jl], r1j = w1[jl];
+            for (int iv = iv_lo; iv <= iv_hi; iv++) {
+                const int ih = i - iv, il = ih * LI + (iv - ivb);
+                double c;
+                if (iv < jv) c = u1[il] * r2j;
+                else if (iv > jv) c = r1j * u2[il];
+                else {
+                    const int ii = ih * ks + ih + ip - (ks - 1), jj = jh * ks + jh + jp - (ks - 1);
+                    c = rkd[ii + (size_t)jk * (jj + (size_t)jk * iv)];
+                }
+                acc = acc + c;
+            }
+        }
+    }
+    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * cfine;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -663,6 +833,47 @@ int launch_mnk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2,
     size_t shm = sizeof(double) * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
     nkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, fine, rkd1, rkd2, rkd, rkb);
     return cuda_fail(cudaGetLastError(), "mnk_cell");
+}
+
+int launch_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s)
+{
+    const int ks = b->ks, nv = b->nv, jk = ks * ks;
+    const double q = 1.0 + b->h;
+    const int n = jk * nv;
+    // dir 'd': the scaling law of the moments carries no extra (1+h) (moments.f90)
+    if (rkd1)
+        moments_nd_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr, b->grm,
+                                                          b->grw, b->bsp, b->bsq, rkd1);
+    if (rkd2)
+        moments_nd_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 1)), -(k + 1),
+                                                          b->gr, b->grm, b->grw, b->bsp, b->bsq, rkd2);
+    if (rkd) {
+        const size_t shm = sizeof(double) * (3 * (size_t)ks * ks * ks + 2 * (size_t)ks * ks + (size_t)jk * jk);
+        int dev = 0, optin = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (shm > (size_t)optin) {
+            set_error("tk_moments: a diagonal cell of ks=%d needs %zu bytes of shared memory (device limit %d)", ks,
+                      shm, optin);
+            return BSRG_ERR_ARG;
+        }
+        cudaError_t e = cudaFuncSetAttribute(tk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (e != cudaSuccess) return cuda_fail(e, "tk diag_cell smem");
+        tk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
+                                                b->grm, b->grw, b->bsp, b->bsq, rkd);
+    }
+    return cuda_fail(cudaGetLastError(), "tk_moments");
+}
+
+int launch_mtk_cell(const bsrg_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
+                    double fine, double *rkb, int ldp, cudaStream_t s)
+{
+    dim3 blk(EXP_TI, EXP_TJ);
+    dim3 grd((b->ns + EXP_TI - 1) / EXP_TI, (b->ns + EXP_TJ - 1) / EXP_TJ, ldp * ldp);
+    const size_t shm = sizeof(double) * 2 * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
+    const double cfine = fine / (k + k + 1);
+    tkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, cfine, rkd1, rkd2, rkd, rkb);
+    return cuda_fail(cudaGetLastError(), "mtk_cell");
 }
 
 }  // namespace bsrg

@@ -96,6 +96,15 @@ int bsrg_mnk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
 int bsrg_mk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
 int bsrg_mmk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
 
+/* ---- Breit-Pauli T^k: src/libs/BS/tk_moments.f90:2 (moments k and -(k+1)
+ *      of all ks*ks spline pairs with the derivative operator, 'n','d'; the
+ *      diagonal cells of tk_triang :101 symmetrised) and mtk_cell.f90:2
+ *      (rkb(i,j,ip,jp) with ip = ihp - ih + ks, i.e. (ns, ns, ldp, ldp),
+ *      ldp >= 2ks-1; times fine/(2k+1)).  rkd1, rkd2: (ks*ks, nv); rkd:
+ *      (ks*ks, ks*ks, nv).  k >= 0.  Device. */
+int bsrg_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
+int bsrg_mtk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

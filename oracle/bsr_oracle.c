@@ -1566,3 +1566,158 @@ double orc_nk(int ns, int ks, const double *rkb, int ldp, const double *pi1, con
     free(a); free(bb);
     return nk;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Breit-Pauli T^k: tk_moments.f90:2-216 (moments k and -(k+1) of 'n' pairs  */
+/* with the derivative operator, tk_triang :101 -- inner integral of         */
+/* B_j (dB_jp/dr - B_jp/r) r^k, outer bsq grm^(k+1), symmetrised; tk_pdiag   */
+/* divides by (1+h)) and mtk_cell.f90:2-86 (all (ih, ihp) pairs,             */
+/* ip = ihp - ih + ks, times fine/(2k+1)).  Tables (ns, ns, ldp, ldp), ldp   */
+/* >= 2ks-1; moments jk = ks*ks.                                             */
+/* ------------------------------------------------------------------------ */
+void orc_tk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
+{
+    int ks = b->ks, jk = ks * ks;
+    int left = iv + ks - 1;
+    double xbase = b->t[left];
+    double gx[MAXKS], gw[MAXKS], bt[MAXKS * MAXKS], bd[MAXKS * MAXKS], db[2 * MAXKS];
+    double *INT = (double *)malloc(sizeof(double) * ks * ks * ks);
+    for (int m = 0; m < ks; m++) {
+        double span = GR(b, iv, m) - xbase;
+        for (int i = 0; i < ks; i++) gx[i] = span * b->gx[i] + xbase;
+        for (int i = 0; i < ks; i++) {
+            orc_bsplvd(b->t, ks, gx[i], left, 2, db);
+            for (int j = 0; j < ks; j++) {
+                bt[i + ks * j] = db[j];
+                bd[i + ks * j] = db[j + ks] - bt[i + ks * j] / gx[i];
+            }
+        }
+        for (int i = 0; i < ks; i++) gw[i] = span * b->gw[i];
+        for (int i = 0; i < ks; i++) gx[i] = ipow(gx[i], k) * gw[i];
+        for (int j = 0; j < ks; j++) {
+            for (int i = 0; i < ks; i++) gw[i] = gx[i] * bt[i + ks * j];
+            for (int jp = 0; jp < ks; jp++) {
+                double s = 0.0;
+                for (int i = 0; i < ks; i++) s = s + gw[i] * bd[i + ks * jp];
+                INT[j + ks * (jp + ks * m)] = s;
+            }
+        }
+    }
+    double g2[MAXKS], bq[MAXKS * MAXKS];
+    for (int m = 0; m < ks; m++) g2[m] = GRW(b, iv, m) * ipow(GRM(b, iv, m), k + 1);
+    for (int ip = 0; ip < ks; ip++)
+        for (int m = 0; m < ks; m++) bq[m + ks * ip] = BSQ(b, iv, m, ip) * g2[m];
+    double *a = (double *)malloc(sizeof(double) * jk * jk);
+    int ii = 0;
+    for (int i = 0; i < ks; i++)
+        for (int ip = 0; ip < ks; ip++) {
+            double g3[MAXKS];
+            for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, i) * bq[m + ks * ip];
+            int jj = 0;
+            for (int j = 0; j < ks; j++)
+                for (int jp = 0; jp < ks; jp++) {
+                    double s = 0.0;
+                    for (int m = 0; m < ks; m++) s = s + g3[m] * INT[j + ks * (jp + ks * m)];
+                    a[ii + jk * jj] = s;
+                    jj++;
+                }
+            ii++;
+        }
+    for (int c = 0; c < jk; c++)
+        for (int r = 0; r < jk; r++) rkd_iv[r + jk * c] = a[r + jk * c] + a[c + jk * r];
+    free(a);
+    free(INT);
+}
+
+void orc_tk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd)
+{
+    int ks = b->ks, nv = b->nv, ml = b->ml, me = b->me;
+    int jk = ks * ks;
+    orc_moments(b, k, rkd1, 'n', 'd');
+    orc_moments(b, -(k + 1), rkd2, 'n', 'd');
+    size_t cell = (size_t)jk * jk;
+    if (me == 0) {
+        for (int iv = 0; iv < nv; iv++) orc_tk_triang(b, k, iv, rkd + cell * iv);
+        return;
+    }
+    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) orc_tk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+    double hp = b->h + 1.0;
+    for (int iv = ml + ks; iv <= ml + me - ks + 2; iv++)
+        for (size_t q = 0; q < cell; q++) rkd[q + cell * (iv - 1)] = rkd[q + cell * (iv - 2)] / hp;
+    for (int iv = ml + me - ks + 3; iv <= nv; iv++)
+        if (iv >= 1) orc_tk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+}
+
+void orc_mtk_cell_from(const orc_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
+                       double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, ns = b->ns, nv = b->nv, jk = ks * ks;
+    size_t nn = (size_t)ns * ns;
+    memset(rkb, 0, sizeof(double) * nn * ldp * ldp);
+    for (int jv = 0; jv < nv; jv++) {
+        int jj = 0;
+        for (int jh = 0; jh < ks; jh++) {
+            int j = jv + jh;
+            for (int jhp = 0; jhp < ks; jhp++) {
+                int jp = jhp - jh + ks - 1;
+                for (int iv = 0; iv < nv; iv++) {
+                    int ii = 0;
+                    for (int ih = 0; ih < ks; ih++) {
+                        int i = iv + ih;
+                        for (int ihp = 0; ihp < ks; ihp++) {
+                            int ip = ihp - ih + ks - 1;
+                            double c;
+                            if (iv < jv) c = rkd1[ii + (size_t)jk * iv] * rkd2[jj + (size_t)jk * jv];
+                            else if (iv > jv) c = rkd1[jj + (size_t)jk * jv] * rkd2[ii + (size_t)jk * iv];
+                            else c = rkd[ii + (size_t)jk * (jj + (size_t)jk * iv)];
+                            size_t o = i + (size_t)ns * j + nn * (ip + (size_t)ldp * jp);
+                            rkb[o] = rkb[o] + c;
+                            ii++;
+                        }
+                    }
+                }
+                jj++;
+            }
+        }
+    }
+    double c = fine / (k + k + 1);
+    for (size_t q = 0; q < nn * ldp * ldp; q++) rkb[q] = rkb[q] * c;
+}
+
+void orc_mtk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, nv = b->nv, jk = ks * ks;
+    double *rkd1 = (double *)malloc(sizeof(double) * jk * nv);
+    double *rkd2 = (double *)malloc(sizeof(double) * jk * nv);
+    double *rkd = (double *)malloc(sizeof(double) * jk * jk * nv);
+    orc_tk_moments(b, k, rkd1, rkd2, rkd);
+    orc_mtk_cell_from(b, k, rkd1, rkd2, rkd, fine, rkb, ldp);
+    free(rkd1); free(rkd2); free(rkd);
+}
+
+/* tk.f90:2-58 (meth 'c'): sum b(j,jp) a(i,ip) rkb(i,j,ip,jp), a, b 'n' densities (ns, 2ks-1) */
+double orc_tk(int ns, int ks, const double *rkb, int ldp, const double *pi1, const double *pj1, const double *pi2,
+              const double *pj2)
+{
+    int kk = ks + ks - 1;
+    double *a = (double *)malloc(sizeof(double) * ns * kk), *bb = (double *)malloc(sizeof(double) * ns * kk);
+    size_t nn = (size_t)ns * ns;
+    orc_density(ns, ks, a, pi1, pi2, 'n');
+    orc_density(ns, ks, bb, pj1, pj2, 'n');
+    double tk = 0.0;
+    for (int jp = 1; jp <= kk; jp++) {
+        int jmin = 1 + ks - jp > 1 ? 1 + ks - jp : 1, jmax = ns + ks - jp < ns ? ns + ks - jp : ns;
+        for (int j = jmin; j <= jmax; j++) {
+            double tki = 0.0;
+            for (int ip = 1; ip <= kk; ip++) {
+                int imin = 1 + ks - ip > 1 ? 1 + ks - ip : 1, imax = ns + ks - ip < ns ? ns + ks - ip : ns;
+                for (int i = imin; i <= imax; i++)
+                    tki = tki + a[(i - 1) + (size_t)ns * (ip - 1)] *
+                                rkb[(i - 1) + (size_t)ns * (j - 1) + nn * ((ip - 1) + (size_t)ldp * (jp - 1))];
+            }
+            tk = tk + bb[(j - 1) + (size_t)ns * (jp - 1)] * tki;
+        }
+    }
+    free(a); free(bb);
+    return tk;
+}

@@ -61,6 +61,10 @@ def lib():
         L.orc_mnk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_mk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
         L.orc_mmk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_tk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D]
+        L.orc_mtk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_tk.restype = ctypes.c_double
+        L.orc_tk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_nk.restype = ctypes.c_double
         L.orc_nk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
@@ -194,6 +198,23 @@ class Basis:
         ldp = ldp or self.ks
         rkb = np.zeros(self.ns * self.ns * ldp * ldp)
         lib().orc_mmk_cell(self._h, k, float(fine), _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
+
+    def tk_moments(self, k):
+        """tk_moments (tk_moments.f90:2): rkd1, rkd2 (ks*ks, nv) 'n','d' moments, rkd (ks*ks, ks*ks, nv)."""
+        jk = self.ks * self.ks
+        rkd1 = np.zeros(jk * self.nv)
+        rkd2 = np.zeros(jk * self.nv)
+        rkd = np.zeros(jk * jk * self.nv)
+        lib().orc_tk_moments(self._h, k, _p(rkd1), _p(rkd2), _p(rkd))
+        return (rkd1.reshape((jk, self.nv), order="F"), rkd2.reshape((jk, self.nv), order="F"),
+                rkd.reshape((jk, jk, self.nv), order="F"))
+
+    def mtk_cell(self, k, fine=1.0, ldp=None):
+        """mtk_cell (mtk_cell.f90:2): T^k table (ns,ns,ldp,ldp), ldp >= 2ks-1, times fine/(2k+1)."""
+        ldp = ldp or 2 * self.ks - 1
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mtk_cell(self._h, k, float(fine), _p(rkb), ldp)
         return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def mnk_cell(self, k, fine=1.0, ldp=None):
@@ -402,3 +423,10 @@ def mk(ns, ks, rkb, pi1, pj1, pi2, pj2):
     r = np.asfortranarray(rkb)
     f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
     return lib().orc_rk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f]) / 2.0
+
+
+def tk(ns, ks, rkb, pi1, pj1, pi2, pj2):
+    """tk.f90 (meth 'c'): T^k(i1, j1; i2, j2) from an mtk_cell table."""
+    r = np.asfortranarray(rkb)
+    f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
+    return lib().orc_tk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f])

@@ -119,3 +119,21 @@ def test_int_inp1_analytic_mk(test_bs, golden):
         assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
         n += 1
     assert n == 7
+
+
+def test_int_inp1_analytic_tk(test_bs, golden):
+    """Breit-Pauli T^k (tk_moments + mtk_cell + the tk.f90 route, fine = 1) against
+    int_inp1 x Z^3 to 1e-12 (measured: the exact rationals within 3.4e-14, the two
+    entries the file states as 16-digit decimals within 5.5e-13)."""
+    B = test_bs["basis"]
+    z = test_bs["knot"]["z"]
+    orbs = {"%d%s" % (n, "spdfg"[l]): B.bhwf(n, l, z) for n in range(1, 6) for l in range(n)}
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "T":
+            continue
+        got = O.tk(B.ns, B.ks, B.mtk_cell(e["k"]), *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        assert abs(got - sa) / abs(sa) < 1e-12, (e, got, sa)
+        n += 1
+    assert n == 12
