@@ -717,6 +717,154 @@ tkb_expand_kernel(int ks, int ns, int nv, int ldp, double cfine, const double *_
     rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * cfine;
 }
 
+
+// ---------------------------------------------------------------------------
+// Breit-Pauli V^k (vk_moments.f90, mvk_cell.f90).  vk_triang (:131): two inner
+// integrals, I1(i,ip) of B_i (dB_ip/dr - B_ip/r) r^k with outer grm^(k+2), and
+// I2(j,jp) of B_j B_jp r^(k+1) with outer grm^(k+3); rkd(ii = (i,ip) all pairs,
+// jj = (j <= jp)) = sum bsp_j bsp_jp I1 + sum bsp_i bsq_ip I2.
+// ---------------------------------------------------------------------------
+__global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+                                    const double *__restrict__ t, GaussRule g, const double *gr,
+                                    const double *grm, const double *grw, const double *bsp,
+                                    const double *bsq, double *rkd)
+{
+    extern __shared__ double sm[];
+    const int jk = ks * ks, ik = ks * (ks + 1) / 2;
+    double *bt = sm;                          // [m][q][j] values
+    double *bd = bt + ks * ks * ks;           // [m][q][j] derivative - value/x
+    double *w1 = bd + ks * ks * ks;           // [m][q] span w x^k
+    double *w2 = w1 + ks * ks;                // [m][q] span w x^(k+1)
+    double *I1 = w2 + ks * ks;                // [m][i][ip]
+    double *I2 = I1 + ks * ks * ks;           // [m][j][jp]
+    const int iv_out = blockIdx.x, iv1 = iv_out + 1;
+    const int s0 = ml + ks, s1 = ml + me - ks + 2;
+    int nscale = 0, iv = iv_out;
+    if (me != 0 && iv1 >= s0 && iv1 <= s1) { iv = s0 - 2; nscale = iv1 - s0 + 1; }
+    const int left = iv + ks - 1;
+    const double xbase = t[left];
+    const size_t ld = (size_t)(nv + 1);
+    for (int q = threadIdx.x; q < ks * ks; q += blockDim.x) {
+        const int m = q / ks, i = q % ks;
+        const double span = gr[iv + (size_t)nv * m] - xbase;
+        const double x = span * g.x[i] + xbase;
+        double db[2 * BSRG_MAXKS];
+        bsplvd_dev(t, ks, x, left, 2, db);
+        for (int j = 0; j < ks; j++) {
+            bt[(m * ks + i) * ks + j] = db[j];
+            bd[(m * ks + i) * ks + j] = db[j + ks] - db[j] / x;
+        }
+        const double w = span * g.w[i] * ipow_dev(x, k);
+        w1[m * ks + i] = w;
+        w2[m * ks + i] = w * x;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < ks * jk; q += blockDim.x) {
+        const int m = q / jk, a = (q % jk) / ks, b = q % ks;
+        const double gm = grm[iv + (size_t)nv * m], gwm = grw[iv + (size_t)nv * m];
+        double s = 0.0, u = 0.0;
+        for (int i = 0; i < ks; i++) {
+            const double x1 = w1[m * ks + i] * bt[(m * ks + i) * ks + a];
+            s = s + x1 * bd[(m * ks + i) * ks + b];
+            const double x2 = w2[m * ks + i] * bt[(m * ks + i) * ks + a];
+            u = u + x2 * bt[(m * ks + i) * ks + b];
+        }
+        I1[(m * ks + a) * ks + b] = s * (ipow_dev(gm, k + 2) * gwm);
+        I2[(m * ks + a) * ks + b] = u * (ipow_dev(gm, k + 3) * gwm);
+    }
+    __syncthreads();
+    double *out = rkd + (size_t)jk * ik * iv_out;
+    for (int q = threadIdx.x; q < jk * ik; q += blockDim.x) {
+        const int ii = q % jk, jj = q / jk;
+        const int i = ii / ks, ip = ii % ks;
+        int j = 0, rem = jj;
+        while (rem >= ks - j) { rem -= ks - j; j++; }
+        const int jp = j + rem;
+        double s1 = 0.0, s2 = 0.0;
+        for (int m = 0; m < ks; m++) {
+            const double g3 = bsp[iv + ld * (m + (size_t)ks * j)] * bsp[iv + ld * (m + (size_t)ks * jp)];
+            s1 = s1 + g3 * I1[(m * ks + i) * ks + ip];
+        }
+        for (int m = 0; m < ks; m++) {
+            const double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * bsq[iv + ld * (m + (size_t)ks * ip)];
+            s2 = s2 + g3 * I2[(m * ks + j) * ks + jp];
+        }
+        double v = s1 + s2;
+        for (int n = 0; n < nscale; n++) v = v / hscale;
+        out[ii + (size_t)jk * jj] = v;
+    }
+}
+
+// mvk_cell (mvk_cell.f90:2): rkb(i,j,ip,jp), ip = ihp - ih + ks - 1 (0-based, up
+// to 2ks-2) over all (ih, ihp), jp = jhp - jh over jh <= jhp; jv outer, iv
+// inner; off-diagonal cells rkd3 x rkd2 (iv < jv) or rkd1 x rkd4; times fine.
+__global__ void __launch_bounds__(EXP_TI * EXP_TJ)
+vkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__restrict__ rkd1,
+                  const double *__restrict__ rkd2, const double *__restrict__ rkd3,
+                  const double *__restrict__ rkd4, const double *__restrict__ rkd, double *__restrict__ rkb)
+{
+    extern __shared__ double sm[];
+    const int ip = blockIdx.z % ldp, jp = blockIdx.z / ldp;
+    const int i0 = blockIdx.x * EXP_TI, j0 = blockIdx.y * EXP_TJ;
+    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    const int jk = ks * ks, ik = ks * (ks + 1) / 2;
+    const int LI = EXP_TI + ks - 1, LJ = EXP_TJ + ks - 1;
+    const int ivb = i0 - (ks - 1), jvb = j0 - (ks - 1);
+    double *u3 = sm, *u4 = u3 + ks * LI, *w1 = u4 + ks * LI, *w2 = w1 + ks * LJ;
+    const bool active = ip < 2 * ks - 1 && jp < ks;
+    if (active) {
+        const int tid = threadIdx.y * EXP_TI + threadIdx.x, nt = EXP_TI * EXP_TJ;
+        for (int q = tid; q < ks * LI; q += nt) {
+            const int ih = q / LI, iv = ivb + q % LI, ihp = ih + ip - (ks - 1);
+            double a = 0.0, b = 0.0;
+            if (ihp >= 0 && ihp < ks && iv >= 0 && iv < nv) {
+                a = rkd3[ih * ks + ihp + (size_t)jk * iv];
+                b = rkd4[ih * ks + ihp + (size_t)jk * iv];
+            }
+            u3[q] = a;
+            u4[q] = b;
+        }
+        for (int q = tid; q < ks * LJ; q += nt) {
+            const int jh = q / LJ, jv = jvb + q % LJ;
+            double a = 0.0, b = 0.0;
+            if (jh + jp < ks && jv >= 0 && jv < nv) {
+                const int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                a = rkd1[jj + (size_t)ik * jv];
+                b = rkd2[jj + (size_t)ik * jv];
+            }
+            w1[q] = a;
+            w2[q] = b;
+        }
+    }
+    __syncthreads();
+    if (i >= ns || j >= ns) return;
+    double acc = 0.0;
+    if (active && j + jp < ns) {
+        const int ihmin = (ks - 1 - ip) > 0 ? ks - 1 - ip : 0, ihmax = (2 * ks - 2 - ip) < ks - 1 ? 2 * ks - 2 - ip : ks - 1;
+        int iv_lo = i - ihmax; if (iv_lo < 0) iv_lo = 0;
+        int iv_hi = i - ihmin; if (iv_hi > nv - 1) iv_hi = nv - 1;
+        int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = j < nv - 1 ? j : nv - 1;
+        for (int jv = jv_lo; jv <= jv_hi; jv++) {
+            const int jh = j - jv, jl = jh * LJ + (jv - jvb);
+            const double r1j = w1[jl], r2j = w2[jl];
+            for (int iv = iv_lo; iv <= iv_hi; iv++) {
+                const int ih = i - iv, il = ih * LI + (iv - ivb);
+                double c;
+                if (iv < jv) c = u3[il] * r2j;
+                else if (iv > jv) c = r1j * u4[il];
+                else {
+                    const int ii = ih * ks + ih + ip - (ks - 1);
+                    const int jj = jh * ks - jh * (jh - 1) / 2 + jp;
+                    c = rkd[ii + (size_t)jk * (jj + (size_t)ik * iv)];
+                }
+                acc = acc + c;
+            }
+        }
+    }
+    rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * fine;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -874,6 +1022,47 @@ int launch_mtk_cell(const bsrg_basis *b, int k, const double *rkd1, const double
     const double cfine = fine / (k + k + 1);
     tkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, cfine, rkd1, rkd2, rkd, rkb);
     return cuda_fail(cudaGetLastError(), "mtk_cell");
+}
+
+int launch_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
+                      double *rkd, cudaStream_t s)
+{
+    const int ks = b->ks, nv = b->nv, jk = ks * ks, ik = ik_of(ks);
+    const double q = 1.0 + b->h;
+    if (rkd1)
+        moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k + 1) * q, k + 1,
+                                                              b->gr, b->grm, b->grw, b->bsp, rkd1);
+    if (rkd2)
+        moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 2)) * q,
+                                                              -(k + 2), b->gr, b->grm, b->grw, b->bsp, rkd2);
+    if (rkd3)
+        moments_nd_kernel<<<(jk * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr,
+                                                                 b->grm, b->grw, b->bsp, b->bsq, rkd3);
+    if (rkd4)
+        moments_nd_kernel<<<(jk * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 3)),
+                                                                 -(k + 3), b->gr, b->grm, b->grw, b->bsp, b->bsq,
+                                                                 rkd4);
+    if (rkd) {
+        const size_t shm = sizeof(double) * (4 * (size_t)ks * ks * ks + 2 * (size_t)ks * ks);
+        if (shm > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(vk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)shm);
+            if (e != cudaSuccess) return cuda_fail(e, "vk diag_cell smem");
+        }
+        vk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
+                                                b->grm, b->grw, b->bsp, b->bsq, rkd);
+    }
+    return cuda_fail(cudaGetLastError(), "vk_moments");
+}
+
+int launch_mvk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,
+                    const double *rkd4, const double *rkd, double fine, double *rkb, int ldp, cudaStream_t s)
+{
+    dim3 blk(EXP_TI, EXP_TJ);
+    dim3 grd((b->ns + EXP_TI - 1) / EXP_TI, (b->ns + EXP_TJ - 1) / EXP_TJ, ldp * ldp);
+    const size_t shm = sizeof(double) * 2 * (size_t)b->ks * ((EXP_TI + b->ks - 1) + (EXP_TJ + b->ks - 1));
+    vkb_expand_kernel<<<grd, blk, shm, s>>>(b->ks, b->ns, b->nv, ldp, fine, rkd1, rkd2, rkd3, rkd4, rkd, rkb);
+    return cuda_fail(cudaGetLastError(), "mvk_cell");
 }
 
 }  // namespace bsrg

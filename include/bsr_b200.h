@@ -105,6 +105,17 @@ int bsrg_mmk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
 int bsrg_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, void *stream);
 int bsrg_mtk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
 
+/* ---- Breit-Pauli V^k: src/libs/BS/vk_moments.f90:2 (rkd1 = moments k+1 and
+ *      rkd2 = moments -(k+2) of the ik symmetric pairs; rkd3 = moments k and
+ *      rkd4 = moments -(k+3) of all ks*ks pairs with the derivative operator;
+ *      diagonal cells rkd (ks*ks, ik, nv) from vk_triang :131) and
+ *      mvk_cell.f90:2 (rkb(i,j,ip,jp) with ip = ihp - ih + ks over all pairs,
+ *      jp = jhp - jh + 1; (ns, ns, ldp, ldp), ldp >= 2ks-1; times fine).
+ *      k >= 0.  Device. */
+int bsrg_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
+                    void *stream);
+int bsrg_mvk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

@@ -1721,3 +1721,170 @@ double orc_tk(int ns, int ks, const double *rkb, int ldp, const double *pi1, con
     free(a); free(bb);
     return tk;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Breit-Pauli V^k: vk_moments.f90:2-218 -- rkd1 = moments(k+1,'s','b'),     */
+/* rkd2 = moments(-(k+2),'s','b'), rkd3 = moments(k,'n','d'), rkd4 =         */
+/* moments(-(k+3),'n','d'); diagonal cells rkd(ii in ks*ks, jj in ik) from   */
+/* two inner integrals (vk_triang :131); vk_pdiag divides by (1+h) -- and    */
+/* mvk_cell.f90:2-83 (jj over ik pairs with jp = jhp - jh + 1, ii over all   */
+/* ks*ks pairs with ip = ihp - ih + ks; times fine).                         */
+/* ------------------------------------------------------------------------ */
+void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
+{
+    int ks = b->ks, jk = ks * ks;
+    int left = iv + ks - 1;
+    double xbase = b->t[left];
+    double gx[MAXKS], gw[MAXKS], bt[MAXKS * MAXKS], bd[MAXKS * MAXKS], db[2 * MAXKS], bi[MAXKS];
+    double *I1 = (double *)malloc(sizeof(double) * ks * ks * ks);
+    double *I2 = (double *)malloc(sizeof(double) * ks * ks * ks);
+    for (int m = 0; m < ks; m++) {
+        double span = GR(b, iv, m) - xbase;
+        for (int i = 0; i < ks; i++) gx[i] = span * b->gx[i] + xbase;
+        for (int i = 0; i < ks; i++) {
+            orc_bsplvd(b->t, ks, gx[i], left, 2, db);
+            for (int j = 0; j < ks; j++) {
+                bt[i + ks * j] = db[j];
+                bd[i + ks * j] = db[j + ks] - bt[i + ks * j] / gx[i];
+            }
+        }
+        for (int i = 0; i < ks; i++) gw[i] = span * b->gw[i] * ipow(gx[i], k);
+        double c = ipow(GRM(b, iv, m), k + 2) * GRW(b, iv, m);
+        for (int i = 0; i < ks; i++) {
+            for (int q = 0; q < ks; q++) bi[q] = gw[q] * bt[q + ks * i];
+            for (int ip = 0; ip < ks; ip++) {
+                double s = 0.0;
+                for (int q = 0; q < ks; q++) s = s + bi[q] * bd[q + ks * ip];
+                I1[i + ks * (ip + ks * m)] = s * c;
+            }
+        }
+        for (int q = 0; q < ks; q++) gw[q] = gw[q] * gx[q];
+        c = ipow(GRM(b, iv, m), k + 3) * GRW(b, iv, m);
+        for (int j = 0; j < ks; j++) {
+            for (int q = 0; q < ks; q++) bi[q] = gw[q] * bt[q + ks * j];
+            for (int jp = 0; jp < ks; jp++) {
+                double s = 0.0;
+                for (int q = 0; q < ks; q++) s = s + bi[q] * bt[q + ks * jp];
+                I2[j + ks * (jp + ks * m)] = s * c;
+            }
+        }
+    }
+    int jj = 0;
+    for (int j = 0; j < ks; j++)
+        for (int jp = j; jp < ks; jp++) {
+            double g3[MAXKS];
+            for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, j) * BSP(b, iv, m, jp);
+            int ii = 0;
+            for (int i = 0; i < ks; i++)
+                for (int ip = 0; ip < ks; ip++) {
+                    double s = 0.0;
+                    for (int m = 0; m < ks; m++) s = s + g3[m] * I1[i + ks * (ip + ks * m)];
+                    rkd_iv[ii + jk * jj] = s;
+                    ii++;
+                }
+            jj++;
+        }
+    int ii = 0;
+    for (int i = 0; i < ks; i++)
+        for (int ip = 0; ip < ks; ip++) {
+            double g3[MAXKS];
+            for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, i) * BSQ(b, iv, m, ip);
+            jj = 0;
+            for (int j = 0; j < ks; j++)
+                for (int jp = j; jp < ks; jp++) {
+                    double s = 0.0;
+                    for (int m = 0; m < ks; m++) s = s + g3[m] * I2[j + ks * (jp + ks * m)];
+                    rkd_iv[ii + jk * jj] = rkd_iv[ii + jk * jj] + s;
+                    jj++;
+                }
+            ii++;
+        }
+    free(I1);
+    free(I2);
+}
+
+void orc_vk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
+{
+    int ks = b->ks, nv = b->nv, ml = b->ml, me = b->me;
+    int jk = ks * ks, ik = ks * (ks + 1) / 2;
+    orc_moments(b, k + 1, rkd1, 's', 'b');
+    orc_moments(b, -(k + 2), rkd2, 's', 'b');
+    orc_moments(b, k, rkd3, 'n', 'd');
+    orc_moments(b, -(k + 3), rkd4, 'n', 'd');
+    size_t cell = (size_t)jk * ik;
+    if (me == 0) {
+        for (int iv = 0; iv < nv; iv++) orc_vk_triang(b, k, iv, rkd + cell * iv);
+        return;
+    }
+    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) orc_vk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+    double hp = b->h + 1.0;
+    for (int iv = ml + ks; iv <= ml + me - ks + 2; iv++)
+        for (size_t q = 0; q < cell; q++) rkd[q + cell * (iv - 1)] = rkd[q + cell * (iv - 2)] / hp;
+    for (int iv = ml + me - ks + 3; iv <= nv; iv++)
+        if (iv >= 1) orc_vk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+}
+
+/* rkb (ns, ns, ldp, ldp): ip up to 2ks-1 wide, jp up to ks */
+void orc_mvk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, ns = b->ns, nv = b->nv, jk = ks * ks, ik = ks * (ks + 1) / 2;
+    double *rkd1 = (double *)malloc(sizeof(double) * ik * nv), *rkd2 = (double *)malloc(sizeof(double) * ik * nv);
+    double *rkd3 = (double *)malloc(sizeof(double) * jk * nv), *rkd4 = (double *)malloc(sizeof(double) * jk * nv);
+    double *rkd = (double *)malloc(sizeof(double) * jk * ik * nv);
+    orc_vk_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd);
+    size_t nn = (size_t)ns * ns;
+    memset(rkb, 0, sizeof(double) * nn * ldp * ldp);
+    for (int jv = 0; jv < nv; jv++) {
+        int jj = 0;
+        for (int jh = 0; jh < ks; jh++) {
+            int j = jv + jh;
+            for (int jhp = jh; jhp < ks; jhp++) {
+                int jp = jhp - jh;
+                for (int iv = 0; iv < nv; iv++) {
+                    int ii = 0;
+                    for (int ih = 0; ih < ks; ih++) {
+                        int i = iv + ih;
+                        for (int ihp = 0; ihp < ks; ihp++) {
+                            int ip = ihp - ih + ks - 1;
+                            double c;
+                            if (iv < jv) c = rkd3[ii + (size_t)jk * iv] * rkd2[jj + (size_t)ik * jv];
+                            else if (iv > jv) c = rkd1[jj + (size_t)ik * jv] * rkd4[ii + (size_t)jk * iv];
+                            else c = rkd[ii + (size_t)jk * (jj + (size_t)ik * iv)];
+                            size_t o = i + (size_t)ns * j + nn * (ip + (size_t)ldp * jp);
+                            rkb[o] = rkb[o] + c;
+                            ii++;
+                        }
+                    }
+                }
+                jj++;
+            }
+        }
+    }
+    for (size_t q = 0; q < nn * ldp * ldp; q++) rkb[q] = rkb[q] * fine;
+    free(rkd1); free(rkd2); free(rkd3); free(rkd4); free(rkd);
+}
+
+/* vk.f90 (meth 'c'): a = 'n' density of (i1,i2), b = 's' density of (j1,j2) */
+double orc_vk(int ns, int ks, const double *rkb, int ldp, const double *pi1, const double *pj1, const double *pi2,
+              const double *pj2)
+{
+    int kk = ks + ks - 1;
+    double *a = (double *)malloc(sizeof(double) * ns * kk), *bb = (double *)malloc(sizeof(double) * ns * ks);
+    size_t nn = (size_t)ns * ns;
+    orc_density(ns, ks, a, pi1, pi2, 'n');
+    orc_density(ns, ks, bb, pj1, pj2, 's');
+    double vk = 0.0;
+    for (int jp = 1; jp <= ks; jp++)
+        for (int j = 1; j <= ns - jp + 1; j++) {
+            double vki = 0.0;
+            for (int ip = 1; ip <= kk; ip++) {
+                int imin = 1 + ks - ip > 1 ? 1 + ks - ip : 1, imax = ns + ks - ip < ns ? ns + ks - ip : ns;
+                for (int i = imin; i <= imax; i++)
+                    vki = vki + a[(i - 1) + (size_t)ns * (ip - 1)] *
+                                rkb[(i - 1) + (size_t)ns * (j - 1) + nn * ((ip - 1) + (size_t)ldp * (jp - 1))];
+            }
+            vk = vk + bb[(j - 1) + (size_t)ns * (jp - 1)] * vki;
+        }
+    free(a); free(bb);
+    return vk;
+}

@@ -65,6 +65,10 @@ def lib():
         L.orc_mtk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_tk.restype = ctypes.c_double
         L.orc_tk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
+        L.orc_vk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D]
+        L.orc_mvk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_vk.restype = ctypes.c_double
+        L.orc_vk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_nk.restype = ctypes.c_double
         L.orc_nk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
@@ -215,6 +219,22 @@ class Basis:
         ldp = ldp or 2 * self.ks - 1
         rkb = np.zeros(self.ns * self.ns * ldp * ldp)
         lib().orc_mtk_cell(self._h, k, float(fine), _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
+
+    def vk_moments(self, k):
+        """vk_moments (vk_moments.f90:2): rkd1, rkd2 (ik, nv), rkd3, rkd4 (ks*ks, nv), rkd (ks*ks, ik, nv)."""
+        ik, jk, nv = self.ks * (self.ks + 1) // 2, self.ks * self.ks, self.nv
+        r1, r2, r3, r4 = np.zeros(ik * nv), np.zeros(ik * nv), np.zeros(jk * nv), np.zeros(jk * nv)
+        rd = np.zeros(jk * ik * nv)
+        lib().orc_vk_moments(self._h, k, _p(r1), _p(r2), _p(r3), _p(r4), _p(rd))
+        return (r1.reshape((ik, nv), order="F"), r2.reshape((ik, nv), order="F"), r3.reshape((jk, nv), order="F"),
+                r4.reshape((jk, nv), order="F"), rd.reshape((jk, ik, nv), order="F"))
+
+    def mvk_cell(self, k, fine=1.0, ldp=None):
+        """mvk_cell (mvk_cell.f90:2): V^k table (ns,ns,ldp,ldp), ldp >= 2ks-1, times fine."""
+        ldp = ldp or 2 * self.ks - 1
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mvk_cell(self._h, k, float(fine), _p(rkb), ldp)
         return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def mnk_cell(self, k, fine=1.0, ldp=None):
@@ -430,3 +450,10 @@ def tk(ns, ks, rkb, pi1, pj1, pi2, pj2):
     r = np.asfortranarray(rkb)
     f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
     return lib().orc_tk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f])
+
+
+def vk(ns, ks, rkb, pi1, pj1, pi2, pj2):
+    """vk.f90 (meth 'c'): V^k(i1, j1; i2, j2) from an mvk_cell table."""
+    r = np.asfortranarray(rkb)
+    f = [np.ascontiguousarray(x, dtype=np.float64) for x in (pi1, pj1, pi2, pj2)]
+    return lib().orc_vk(ns, ks, r.ctypes.data_as(_D), r.shape[2], *[_p(x) for x in f])

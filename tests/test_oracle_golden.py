@@ -137,3 +137,20 @@ def test_int_inp1_analytic_tk(test_bs, golden):
         assert abs(got - sa) / abs(sa) < 1e-12, (e, got, sa)
         n += 1
     assert n == 12
+
+
+def test_int_inp1_analytic_vk(test_bs, golden):
+    """Breit-Pauli V^k (vk_moments + mvk_cell + the vk.f90 route, fine = 1) against
+    int_inp1 x Z^3 (measured within 1.6e-15)."""
+    B = test_bs["basis"]
+    z = test_bs["knot"]["z"]
+    orbs = {"%d%s" % (n, "spdfg"[l]): B.bhwf(n, l, z) for n in range(1, 6) for l in range(n)}
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "V":
+            continue
+        got = O.vk(B.ns, B.ks, B.mvk_cell(e["k"]), *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
+        n += 1
+    assert n == 13
