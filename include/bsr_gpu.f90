@@ -8,6 +8,10 @@
 !       gpu_define_spline       after define_grid + define_spline
 !       gpu_mrk_cell(k)         mrk_cell (libs/BS/mrk_cell.f90:2): fills
 !                               module spline_integrals rkb from the GPU
+!       gpu_mnk_cell(k), gpu_mmk_cell(k), gpu_mtk_cell(k), gpu_mvk_cell(k)
+!                               the Breit-Pauli tables mnk_cell, mmk_cell,
+!                               mtk_cell, mvk_cell (libs/BS/m?k_cell.f90:2),
+!                               with spline_atomic's fine
 !       gpu_add_two_electron    the I_data Case(6..9) call for icase 5
 !                               (bsr/BSR_MAT3/I_data.f90:192-218)
 !       gpu_diag_hd             the eigen-solution of diag_hd for a
@@ -56,6 +60,38 @@
         Type(c_ptr), value :: b, rkb, stream
         Integer(c_int), value :: k, ldp
         Integer(c_int) :: bsrg_mrk_cell
+       End Function
+
+       Function bsrg_mnk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mnk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mnk_cell
+       End Function
+
+       Function bsrg_mmk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mmk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mmk_cell
+       End Function
+
+       Function bsrg_mtk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mtk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mtk_cell
+       End Function
+
+       Function bsrg_mvk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mvk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mvk_cell
        End Function
 
        Function bsrg_ctx_create(device, stream, out) bind(C, name="bsrg_ctx_create")
@@ -161,6 +197,56 @@
       itype = 'rk '
       krk = k
       End Subroutine gpu_mrk_cell
+
+!======================================================================
+      Subroutine gpu_breit_cell(which, k)
+!----------------------------------------------------------------------
+!     m?k_cell(k) for which = 'nk ', 'mk ', 'tk ', 'vk ': module rkb
+!     (ns,ns,2ks-1,2ks-1) filled from the GPU table, fine included
+!----------------------------------------------------------------------
+      Use spline_param
+      Use spline_integrals
+      Use spline_atomic, only: fine
+      Character(3), intent(in) :: which
+      Integer, intent(in) :: k
+      Integer(c_size_t) :: bytes
+      Integer(c_int) :: rc
+      if (itype == 'aaa') Call allocate_integrals
+      if (itype == which .and. krk == k) Return
+      bytes = int(ns, c_size_t) * ns * (2*ks-1) * (2*ks-1) * 8
+      if (.not. c_associated(d_rkb)) Call gpu_check(cudaMalloc(d_rkb, bytes), 'cudaMalloc rkb')
+      Select case (which)
+       case ('nk '); rc = bsrg_mnk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case ('mk '); rc = bsrg_mmk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case ('tk '); rc = bsrg_mtk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case ('vk '); rc = bsrg_mvk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case default; Stop 'gpu_breit_cell: unknown integral type'
+      End Select
+      Call gpu_check(rc, which // '_cell')
+      Call gpu_check(cudaMemcpy(c_loc(rkb), d_rkb, bytes, cudaMemcpyDeviceToHost), 'cudaMemcpy rkb')
+      itype = which
+      krk = k
+      End Subroutine gpu_breit_cell
+
+      Subroutine gpu_mnk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('nk ', k)
+      End Subroutine gpu_mnk_cell
+
+      Subroutine gpu_mmk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('mk ', k)
+      End Subroutine gpu_mmk_cell
+
+      Subroutine gpu_mtk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('tk ', k)
+      End Subroutine gpu_mtk_cell
+
+      Subroutine gpu_mvk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('vk ', k)
+      End Subroutine gpu_mvk_cell
 
 !======================================================================
       Subroutine gpu_add_two_electron(nch, norb, pbs, kmax, ncoef, ck, ctype, &
