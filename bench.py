@@ -394,6 +394,11 @@ def run_b200(args):
     x_exec_flops = (2.0 * ns * ns * ((2 * ks - 1) ** 2 * norb + (2 * ks - 1) * norb * norb) +
                     2.0 * ns * ns * nxterms / nk)
     x_ms, x_n = stages["exchange"]
+    # blocks that receive an exchange group in one multipole (the launch's read-modify-write)
+    xsel = c["type"] == 1
+    xblocks = [len(np.unique(c["ich"][xsel & (c["k"] == kk)].astype(np.int64) * 1000 + c["jch"][xsel & (c["k"] == kk)]))
+               for kk in range(nk)]
+    x_min_bytes = 2.0 * ns * ns * 8 * (sum(xblocks) / nk)
     x_launch_ms = x_ms / (nst * nk)
     d_flops = 2.0 * ngd * (ns * ks) ** 2 / nk
     d_ms, d_n = stages["direct"]
@@ -411,7 +416,11 @@ def run_b200(args):
                                     "flop per exchange group, %d groups over %d launches" % (ngx, nk),
                      "executed_tflops": x_exec_flops / (x_launch_ms * 1e-3) / 1e12,
                      "executed": "the factored kernel's own count: 2*ns^2*((2ks-1)^2 norb + (2ks-1) norb^2) + "
-                                 "2*ns^2 per coefficient, per launch"},
+                                 "2*ns^2 per coefficient, per launch",
+                     "hbm_view": {"bytes": x_min_bytes, "achieved_gbs": x_min_bytes / (x_launch_ms * 1e-3) / 1e9,
+                                  "frac": x_min_bytes / (x_launch_ms * 1e-3) / 1e9 / hbm_peak,
+                                  "what": "the update's minimum HBM traffic per launch: each channel block with an "
+                                          "exchange group read and written once (ns^2 x 8 B x 2 per block)"}},
         "direct": {"bound": "tensor", "achieved": d_flops / (d_launch_ms * 1e-3) / 1e12, "peak": fp64,
                    "unit": "TFLOP/s", "launch_ms": d_launch_ms,
                    "algorithmic": "2*(ns ks)^2 flop per direct group, %d groups" % ngd},

@@ -638,5 +638,10 @@ extern "C" int bsrg_dsytrd(bsrg_ctx *c, int n, double *A, int lda, double *d, do
     if (rc != BSRG_OK) return rc;
     rc = trd_reduce(c, n, A, lda, d, e, tau, c->ws);
     if (rc != BSRG_OK) return rc;
-    return trd_check(c->ws, n > 0 ? n : 1, c->stream);
+    // the error flag exists only once a reduction ran (n >= 2 clears and launches)
+    if (n < 2) {
+        cudaError_t er = cudaStreamSynchronize(c->stream);
+        return er == cudaSuccess ? BSRG_OK : cuda_fail(er, "tridiagonal reduction");
+    }
+    return trd_check(c->ws, n, c->stream);
 }
