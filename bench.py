@@ -402,7 +402,7 @@ def run_b200(args):
     x_launch_ms = x_ms / (nst * nk)
     d_flops = 2.0 * ngd * (ns * ks) ** 2 / nk
     d_ms, d_n = stages["direct"]
-    d_launch_ms = d_ms / max(nk, 1)
+    d_launch_ms = d_ms / (nst * nk)        # stage time summed over nst steps and nk multipoles
     eig_ms, _ = stages["dense_eig"]
     eig_ms /= nst
     eig_flops = (4.0 / 3.0 + 2.0 + 4.0) * khm ** 3     # tridiagonalisation + D&C + back-transform, rough
@@ -423,7 +423,8 @@ def run_b200(args):
                                           "exchange group read and written once (ns^2 x 8 B x 2 per block)"}},
         "direct": {"bound": "tensor", "achieved": d_flops / (d_launch_ms * 1e-3) / 1e12, "peak": fp64,
                    "unit": "TFLOP/s", "launch_ms": d_launch_ms,
-                   "algorithmic": "2*(ns ks)^2 flop per direct group, %d groups" % ngd},
+                   "algorithmic": "2*(ns ks)^2 flop per direct group, %d groups; the stage is the group "
+                                  "densities, the table reshape, cuBLAS DGEMM and the band update" % ngd},
         "dense_eig": {"bound": "tensor", "achieved": eig_flops / (eig_ms * 1e-3) / 1e12, "peak": fp64,
                       "unit": "TFLOP/s", "launch_ms": eig_ms, "library": "cuSOLVER Xsyevd",
                       "algorithmic": "~7.3 khm^3 flop (sytrd + stedc + ormtr)"},

@@ -248,6 +248,35 @@ direct_gemm_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd, con
     }
 }
 
+// The direct contraction as one library GEMM: the multipole's table reshaped to
+// the dense (ns ks) x (ns ks) matrix R3[(i,ip),(j,jp)] = rkb(i,j,ip,jp), then
+// C[(i,ip), g] = sum_(j,jp) R3[(i,ip),(j,jp)] Xd[(j,jp), g] by cuBLAS DGEMM, then
+// UPDATE_HX 's' of each group's band into its channel block.
+__global__ void direct_table_kernel(int ns, int ks, const double *__restrict__ rkbp, PadLayout L,
+                                    double *__restrict__ R3)
+{
+    const size_t nk = (size_t)ns * ks;
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (q >= nk * nk) return;
+    const int row = (int)(q % nk), colk = (int)(q / nk);
+    const int i = row % ns, ip = row / ns, j = colk % ns, jp = colk / ns;
+    R3[q] = rkbp[L.at(i, j, ip, jp, ks)];
+}
+
+__global__ void direct_update_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd,
+                                     const double *__restrict__ C, double *hcc)
+{
+    const int g = blockIdx.y;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ng || q >= ns * ks) return;
+    const int i = q % ns, ip = q / ns;
+    if (i + ip >= ns) return;
+    const double v = C[q + (size_t)ns * ks * g];
+    double *blk = hcc + (size_t)gd[g].blk * ns * ns;
+    blk[i + (size_t)ns * (i + ip)] += v;
+    if (ip > 0) blk[(i + ip) + (size_t)ns * i] += v;
+}
+
 // ---------------------------------------------------------------------------
 // The R^k table of the assembly pipeline, in a zero-margined layout:
 //   rkbp[(i+PL) + NP*((j+PL) + NP*(ip + ks*jp))],  PL = ks-1 low margin,
@@ -875,6 +904,13 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     if (!tabs) add(sizeof(double) * PL.slice * ks * ks);
     add(sizeof(double) * maxgd * ns * ks);
     add(sizeof(double) * (size_t)ns * ks * 3);
+    // direct contraction by DGEMM (unless BSRG_DIRECT_SIMT selects the register-tiled kernel)
+    const bool direct_blas = maxgd > 0 && !getenv("BSRG_DIRECT_SIMT");
+    const size_t nk = (size_t)ns * ks;
+    if (direct_blas) {
+        add(sizeof(double) * nk * nk);
+        add(sizeof(double) * nk * maxgd);
+    }
     add(sizeof(unsigned short) * (size_t)ncoef);
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) return rc;
@@ -895,6 +931,8 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     double *rmk = ar.take<double>((size_t)ns * ks);
     double *M1 = ar.take<double>((size_t)ns * ks), *M2 = ar.take<double>((size_t)ns * ks);
     unsigned short *d_zoff = ar.take<unsigned short>(std::max(ncoef, 1));
+    double *R3 = direct_blas ? ar.take<double>(nk * nk) : nullptr;
+    double *Cd = direct_blas ? ar.take<double>(nk * maxgd) : nullptr;
     // stage host metadata through pinned memory, one copy
     char *hp = (char *)c->pinned;
     size_t o = 0;
@@ -977,15 +1015,28 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             const GroupDesc *gdd = d_gd + doff[k];
             dim3 g1((ns * ks + 127) / 128, nd);
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
-            dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
-            direct_gemm_kernel<<<g2, DG_THREADS, 0, s>>>(ns, ks, nd, gdd, Xd, rkbk, PL, hcc);
+            if (direct_blas) {
+                direct_table_kernel<<<(unsigned)((nk * nk + 255) / 256), 256, 0, s>>>(ns, ks, rkbk, PL, R3);
+                const double one = 1.0, zero = 0.0;
+                cublasStatus_t bs = cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)nk, nd, (int)nk, &one, R3,
+                                                (int)nk, Xd, (int)nk, &zero, Cd, (int)nk);
+                if (bs != CUBLAS_STATUS_SUCCESS) {
+                    set_error("assemble: direct DGEMM failed (%d)", (int)bs);
+                    return BSRG_ERR_SOLVER;
+                }
+                dim3 g4((unsigned)((nk + 127) / 128), nd);
+                direct_update_kernel<<<g4, 128, 0, s>>>(ns, ks, nd, gdd, Cd, hcc);
+            } else {
+                dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
+                direct_gemm_kernel<<<g2, DG_THREADS, 0, s>>>(ns, ks, nd, gdd, Xd, rkbk, PL, hcc);
+            }
             if (acf) {
                 rc = launch_mrm(b, k, rmk, s);
                 if (rc != BSRG_OK) return rc;
                 acf_kernel<<<(nd * 32 + 127) / 128, 128, 0, s>>>(ns, ks, nch, k, nd, gdd, d_ca, d_cb, d_cv, P,
                                                                  rmk, acf);
             }
-            stage_end(c, 1, acf ? 4 : 2);
+            stage_end(c, 1, (direct_blas ? 3 : 2) + (acf ? 2 : 0));
         }
         if (nx > 0) {
             stage_begin(c, 2);

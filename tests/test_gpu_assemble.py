@@ -146,3 +146,17 @@ def test_exchange_paths_match_oracle(monkeypatch, gather):
     gb, ctx, out = gpu_assemble(pw, want=False)
     errs = block_errors(to_np(out["hcc"]), ref["hcc"])
     assert errs.max() < TOL_H, errs.max()
+
+
+@pytest.mark.parametrize("simt", [False, True])
+def test_direct_paths_match_oracle(monkeypatch, simt):
+    """Both direct contractions -- the reshaped table times the group densities by
+    cuBLAS DGEMM (default) and the register-tiled SIMT kernel (BSRG_DIRECT_SIMT) --
+    give the oracle's blocks to 1e-12, and agree with each other to 1e-13."""
+    pw = W.partial_wave("config1", seed=13)
+    ob, ref = oracle_assemble(pw, want_acf=False)
+    if simt:
+        monkeypatch.setenv("BSRG_DIRECT_SIMT", "1")
+    gb, ctx, out = gpu_assemble(pw, want=False)
+    errs = block_errors(to_np(out["hcc"]), ref["hcc"])
+    assert errs.max() < TOL_H, errs.max()
