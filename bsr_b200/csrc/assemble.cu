@@ -487,6 +487,9 @@ exchange_kernel(int ns, int ng, PadLayout L, const GroupDesc *__restrict__ gd, c
 constexpr int XCH = 4;                  // rows x per CTA
 constexpr int NORB_MAX = 32;            // orbitals the factored kernel handles
 constexpr int ZLD = NORB_MAX + 1;       // padded leading dimension of Z rows
+// stride of one row xi's Z block, odd so the XCH threads of a group (same term,
+// different xi) read different shared-memory banks in the term loop
+constexpr int ZXS = NORB_MAX * ZLD + 1;
 
 template <int KS>
 __global__ void __launch_bounds__(256)
@@ -553,7 +556,7 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
 #pragma unroll
         for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) Zs[(xi * NORB_MAX + a0 + i) * ZLD + b0 + j] = z[i][j];
+            for (int j = 0; j < 4; j++) Zs[xi * ZXS + (a0 + i) * ZLD + b0 + j] = z[i][j];
     }
     __syncthreads();
     // ---- a_g(x, y') = sum_t c_t Z[xi][a_t][b_t]; UPDATE_HX 'x' ----
@@ -563,7 +566,7 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
         int g = q / XCH, xi = q % XCH, x = x0 + xi;
         if (x >= ns) continue;
         GroupDesc G = gd[g];
-        const double *Z = Zs + xi * NORB_MAX * ZLD;
+        const double *Z = Zs + xi * ZXS;
         double acc = 0.0;
         for (int t = G.start; t < G.end; t++) acc = fma(cv[t], Z[zoff[t]], acc);
         hcc[(size_t)G.blk * nn + x + (size_t)ns * yp] += acc;
@@ -586,7 +589,7 @@ static size_t exchange_factored_smem(int ks)
 {
     int NE = 2 * ks - 1, PXR = XCH + 2 * (ks - 1);
     return sizeof(double) * ((size_t)NE * NORB_MAX + (size_t)PXR * NORB_MAX + (size_t)XCH * NE * NE +
-                             (size_t)XCH * NE * NORB_MAX + (size_t)XCH * NORB_MAX * ZLD);
+                             (size_t)XCH * NE * NORB_MAX + (size_t)XCH * ZXS);
 }
 
 static exchange_factored_fn exchange_factored_for(int ks)
