@@ -224,6 +224,24 @@ def mvk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     return out
 
 
+def wk_moments(basis, k):
+    """Breit-Pauli W^k moments, layouts as vk_moments."""
+    ik, jk, nv = basis.ks * (basis.ks + 1) // 2, basis.ks * basis.ks, basis.nv
+    out = [fortran_empty((ik, nv)), fortran_empty((ik, nv)), fortran_empty((jk, nv)), fortran_empty((jk, nv)),
+           fortran_empty((jk, ik, nv))]
+    call("bsrg_wk_moments", basis.handle, k, *[_ptr(x) for x in out], _stream())
+    return out
+
+
+def mwk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
+    """W^k table rkb(ns,ns,ldp,ldp), ldp >= 2ks-1 (default), times fine (mwk_cell.f90)."""
+    ldp = 2 * basis.ks - 1 if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mwk_cell", basis.handle, k, float(fine), _ptr(out), ldp, _stream())
+    return out
+
+
 def mnk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     """N^k table rkb(ns,ns,ldp,ldp) times fine (mnk_cell.f90); i, ip the r1 splines, r2 < r1."""
     ldp = basis.ks if ldp is None else ldp

@@ -49,8 +49,8 @@ int launch_mnk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2,
 int launch_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd, cudaStream_t s);
 int launch_mtk_cell(const bsrg_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
                     double fine, double *rkb, int ldp, cudaStream_t s);
-int launch_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
-                      double *rkd, cudaStream_t s);
+int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
+                      double *rkd, double *tmp, cudaStream_t s);
 int launch_mvk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,
                     const double *rkd4, const double *rkd, double fine, double *rkb, int ldp, cudaStream_t s);
 int launch_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, cudaStream_t s);

@@ -347,12 +347,49 @@ int bsrg_mtk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
     return rc;
 }
 
+// V^k (mode 0) and W^k (mode 1) share the layouts; W^k's moment combinations need a
+// ks*ks*nv scratch, which bsrg_wk_moments allocates and frees
+static int vw_moments_call(const bsrg_basis *b, int k, int mode, double *rkd1, double *rkd2, double *rkd3,
+                           double *rkd4, double *rkd, cudaStream_t s)
+{
+    double *tmp = nullptr;
+    if (mode && (rkd3 || rkd4)) {
+        cudaError_t e = cudaMallocAsync((void **)&tmp, sizeof(double) * (size_t)b->ks * b->ks * b->nv, s);
+        if (e != cudaSuccess) return cuda_fail(e, "wk_moments scratch");
+    }
+    int rc = launch_vw_moments(b, k, mode, rkd1, rkd2, rkd3, rkd4, rkd, tmp, s);
+    if (tmp) cudaFreeAsync(tmp, s);
+    return rc;
+}
+
 int bsrg_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
                     void *stream)
 {
     CHECK_ARG(b, "vk_moments: null basis");
     CHECK_ARG(k >= 0 && k <= 64, "vk_moments: k=%d out of range", k);
-    return launch_vk_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, (cudaStream_t)stream);
+    return vw_moments_call(b, k, 0, rkd1, rkd2, rkd3, rkd4, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_wk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
+                    void *stream)
+{
+    CHECK_ARG(b, "wk_moments: null basis");
+    CHECK_ARG(k >= 0 && k <= 64, "wk_moments: k=%d out of range", k);
+    return vw_moments_call(b, k, 1, rkd1, rkd2, rkd3, rkd4, rkd, (cudaStream_t)stream);
+}
+
+static int mvw_cell_call(const bsrg_basis *b, int k, int mode, double fine, double *rkb, int ldp, cudaStream_t s)
+{
+    const size_t ik = (size_t)ik_of(b->ks), jk = (size_t)b->ks * b->ks, nv = (size_t)b->nv;
+    double *buf = nullptr;
+    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * ik * nv + 3 * jk * nv + jk * ik * nv) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, mode ? "mwk_cell scratch" : "mvk_cell scratch");
+    double *r1 = buf, *r2 = r1 + ik * nv, *r3 = r2 + ik * nv, *r4 = r3 + jk * nv, *rd = r4 + jk * nv;
+    double *tmp = rd + jk * ik * nv;
+    int rc = launch_vw_moments(b, k, mode, r1, r2, r3, r4, rd, tmp, s);
+    if (rc == BSRG_OK) rc = launch_mvk_cell(b, r1, r2, r3, r4, rd, fine, rkb, ldp, s);
+    cudaFreeAsync(buf, s);
+    return rc;
 }
 
 int bsrg_mvk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
@@ -360,16 +397,15 @@ int bsrg_mvk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
     CHECK_ARG(b && rkb, "mvk_cell: null argument");
     CHECK_ARG(ldp >= 2 * b->ks - 1, "mvk_cell: ldp=%d < 2ks-1=%d", ldp, 2 * b->ks - 1);
     CHECK_ARG(k >= 0 && k <= 64, "mvk_cell: k=%d out of range", k);
-    cudaStream_t s = (cudaStream_t)stream;
-    const size_t ik = (size_t)ik_of(b->ks), jk = (size_t)b->ks * b->ks, nv = (size_t)b->nv;
-    double *buf = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * ik * nv + 2 * jk * nv + jk * ik * nv) * sizeof(double), s);
-    if (e != cudaSuccess) return cuda_fail(e, "mvk_cell scratch");
-    double *r1 = buf, *r2 = r1 + ik * nv, *r3 = r2 + ik * nv, *r4 = r3 + jk * nv, *rd = r4 + jk * nv;
-    int rc = launch_vk_moments(b, k, r1, r2, r3, r4, rd, s);
-    if (rc == BSRG_OK) rc = launch_mvk_cell(b, r1, r2, r3, r4, rd, fine, rkb, ldp, s);
-    cudaFreeAsync(buf, s);
-    return rc;
+    return mvw_cell_call(b, k, 0, fine, rkb, ldp, (cudaStream_t)stream);
+}
+
+int bsrg_mwk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkb, "mwk_cell: null argument");
+    CHECK_ARG(ldp >= 2 * b->ks - 1, "mwk_cell: ldp=%d < 2ks-1=%d", ldp, 2 * b->ks - 1);
+    CHECK_ARG(k >= 0 && k <= 64, "mwk_cell: k=%d out of range", k);
+    return mvw_cell_call(b, k, 1, fine, rkb, ldp, (cudaStream_t)stream);
 }
 
 int bsrg_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, void *stream)

@@ -554,7 +554,7 @@ nkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__
 // ---------------------------------------------------------------------------
 __global__ void moments_nd_kernel(int ks, int nv, int ml, int me, double hp, int k, const double *gr,
                                   const double *grm, const double *grw, const double *bsp, const double *bsq,
-                                  double *rkm)
+                                  double *rkm, int dir_b)
 {
     const int jk = ks * ks;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -571,12 +571,20 @@ __global__ void moments_nd_kernel(int ks, int nv, int ml, int me, double hp, int
         double gw = grw[iv + (size_t)nv * m];
         if (k > 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(gr[iv + (size_t)nv * m], k);
         if (k < 0) gw = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], -k);
-        const double bj = bsq[iv + ld * (m + (size_t)ks * j)] * gw;
+        const double bj = (dir_b ? bsp : bsq)[iv + ld * (m + (size_t)ks * j)] * gw;
         v = v + bsp[iv + ld * (m + (size_t)ks * i)] * bj;
     }
     if (scaled)
         for (int q = s0; q <= iv1; q++) v = v * hp;
     rkm[ii + (size_t)jk * iv_out] = v;
+}
+
+// wk_moments.f90:44-52: out = 2 out + c tmp (c = k+2) or 2 out - c tmp (c = k+1)
+__global__ void moments_combine_kernel(int n, double c, int minus, double *out, const double *tmp)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    out[q] = minus ? 2 * out[q] - c * tmp[q] : 2 * out[q] + c * tmp[q];
 }
 
 // tk_triang (tk_moments.f90:101): inner integral of B_j (dB_jp/dr - B_jp/r) r^k
@@ -724,10 +732,10 @@ tkb_expand_kernel(int ks, int ns, int nv, int ldp, double cfine, const double *_
 // I2(j,jp) of B_j B_jp r^(k+1) with outer grm^(k+3); rkd(ii = (i,ip) all pairs,
 // jj = (j <= jp)) = sum bsp_j bsp_jp I1 + sum bsp_i bsq_ip I2.
 // ---------------------------------------------------------------------------
-__global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k,
+__global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, int k, int mode,
                                     const double *__restrict__ t, GaussRule g, const double *gr,
                                     const double *grm, const double *grw, const double *bsp,
-                                    const double *bsq, double *rkd)
+                                    const double *bsq, const double *bspd, double *rkd)
 {
     extern __shared__ double sm[];
     const int jk = ks * ks, ik = ks * (ks + 1) / 2;
@@ -752,7 +760,8 @@ __global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscal
         bsplvd_dev(t, ks, x, left, 2, db);
         for (int j = 0; j < ks; j++) {
             bt[(m * ks + i) * ks + j] = db[j];
-            bd[(m * ks + i) * ks + j] = db[j + ks] - db[j] / x;
+            // V^k: dB/dr - B/r; W^k (wk_triang, wk_moments.f90:167): 2 dB/dr + k B/r
+            bd[(m * ks + i) * ks + j] = mode ? 2 * db[j + ks] + (double)k * db[j] / x : db[j + ks] - db[j] / x;
         }
         const double w = span * g.w[i] * ipow_dev(x, k);
         w1[m * ks + i] = w;
@@ -786,7 +795,11 @@ __global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscal
             s1 = s1 + g3 * I1[(m * ks + i) * ks + ip];
         }
         for (int m = 0; m < ks; m++) {
-            const double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * bsq[iv + ld * (m + (size_t)ks * ip)];
+            // V^k: bsq; W^k (wk_moments.f90:218): 2 dB/dr - (k+3) B/r from the basis tables
+            const double op = mode ? 2 * bspd[iv + ld * (m + (size_t)ks * ip)] -
+                                         (double)(k + 3) * grm[iv + (size_t)nv * m] * bsp[iv + ld * (m + (size_t)ks * ip)]
+                                   : bsq[iv + ld * (m + (size_t)ks * ip)];
+            const double g3 = bsp[iv + ld * (m + (size_t)ks * i)] * op;
             s2 = s2 + g3 * I2[(m * ks + j) * ks + jp];
         }
         double v = s1 + s2;
@@ -991,10 +1004,10 @@ int launch_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
     // dir 'd': the scaling law of the moments carries no extra (1+h) (moments.f90)
     if (rkd1)
         moments_nd_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr, b->grm,
-                                                          b->grw, b->bsp, b->bsq, rkd1);
+                                                          b->grw, b->bsp, b->bsq, rkd1, 0);
     if (rkd2)
         moments_nd_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 1)), -(k + 1),
-                                                          b->gr, b->grm, b->grw, b->bsp, b->bsq, rkd2);
+                                                          b->gr, b->grm, b->grw, b->bsp, b->bsq, rkd2, 0);
     if (rkd) {
         const size_t shm = sizeof(double) * (3 * (size_t)ks * ks * ks + 2 * (size_t)ks * ks + (size_t)jk * jk);
         int dev = 0, optin = 0;
@@ -1024,8 +1037,9 @@ int launch_mtk_cell(const bsrg_basis *b, int k, const double *rkd1, const double
     return cuda_fail(cudaGetLastError(), "mtk_cell");
 }
 
-int launch_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
-                      double *rkd, cudaStream_t s)
+// mode 0: V^k (vk_moments.f90); mode 1: W^k (wk_moments.f90), tmp (ks*ks*nv) needed for the combinations
+int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
+                      double *rkd, double *tmp, cudaStream_t s)
 {
     const int ks = b->ks, nv = b->nv, jk = ks * ks, ik = ik_of(ks);
     const double q = 1.0 + b->h;
@@ -1035,13 +1049,25 @@ int launch_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
     if (rkd2)
         moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 2)) * q,
                                                               -(k + 2), b->gr, b->grm, b->grw, b->bsp, rkd2);
-    if (rkd3)
-        moments_nd_kernel<<<(jk * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr,
-                                                                 b->grm, b->grw, b->bsp, b->bsq, rkd3);
-    if (rkd4)
-        moments_nd_kernel<<<(jk * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 3)),
-                                                                 -(k + 3), b->gr, b->grm, b->grw, b->bsp, b->bsq,
-                                                                 rkd4);
+    const int nj = jk * nv, gj = (nj + 127) / 128;
+    if (rkd3) {
+        moments_nd_kernel<<<gj, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr, b->grm, b->grw, b->bsp,
+                                             b->bsq, rkd3, 0);
+        if (mode) {
+            moments_nd_kernel<<<gj, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k - 1) * q, k - 1, b->gr, b->grm,
+                                                 b->grw, b->bsp, b->bsq, tmp, 1);
+            moments_combine_kernel<<<gj, 128, 0, s>>>(nj, (double)(k + 2), 0, rkd3, tmp);
+        }
+    }
+    if (rkd4) {
+        moments_nd_kernel<<<gj, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 3)), -(k + 3), b->gr, b->grm,
+                                             b->grw, b->bsp, b->bsq, rkd4, 0);
+        if (mode) {
+            moments_nd_kernel<<<gj, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 4)) * q, -(k + 4), b->gr,
+                                                 b->grm, b->grw, b->bsp, b->bsq, tmp, 1);
+            moments_combine_kernel<<<gj, 128, 0, s>>>(nj, (double)(k + 1), 1, rkd4, tmp);
+        }
+    }
     if (rkd) {
         const size_t shm = sizeof(double) * (4 * (size_t)ks * ks * ks + 2 * (size_t)ks * ks);
         if (shm > 48 * 1024) {
@@ -1049,10 +1075,10 @@ int launch_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
                                                  (int)shm);
             if (e != cudaSuccess) return cuda_fail(e, "vk diag_cell smem");
         }
-        vk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
-                                                b->grm, b->grw, b->bsp, b->bsq, rkd);
+        vk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, mode, b->t, rule_of(b), b->gr,
+                                                b->grm, b->grw, b->bsp, b->bsq, b->bspd, rkd);
     }
-    return cuda_fail(cudaGetLastError(), "vk_moments");
+    return cuda_fail(cudaGetLastError(), mode ? "wk_moments" : "vk_moments");
 }
 
 int launch_mvk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,

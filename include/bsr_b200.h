@@ -116,6 +116,15 @@ int bsrg_vk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, doub
                     void *stream);
 int bsrg_mvk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
 
+/* ---- Breit-Pauli W^k: src/libs/BS/wk_moments.f90:2 (the V^k layouts with
+ *      rkd3 = 2 m(k,'n','d') + (k+2) m(k-1,'n','b'), rkd4 = 2 m(-(k+3),'n','d')
+ *      - (k+1) m(-(k+4),'n','b'), and wk_triang's operators 2 dB/dr + k B/r and
+ *      2 dB/dr - (k+3) B/r) and mwk_cell.f90:2 (mvk_cell's sums, times fine).
+ *      Layouts as for V^k.  k >= 0.  Device. */
+int bsrg_wk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
+                    void *stream);
+int bsrg_mwk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

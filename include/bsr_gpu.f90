@@ -8,7 +8,8 @@
 !       gpu_define_spline       after define_grid + define_spline
 !       gpu_mrk_cell(k)         mrk_cell (libs/BS/mrk_cell.f90:2): fills
 !                               module spline_integrals rkb from the GPU
-!       gpu_mnk_cell(k), gpu_mmk_cell(k), gpu_mtk_cell(k), gpu_mvk_cell(k)
+!       gpu_mnk_cell(k), gpu_mmk_cell(k), gpu_mtk_cell(k), gpu_mvk_cell(k),
+!       gpu_mwk_cell(k)
 !                               the Breit-Pauli tables mnk_cell, mmk_cell,
 !                               mtk_cell, mvk_cell (libs/BS/m?k_cell.f90:2),
 !                               with spline_atomic's fine
@@ -92,6 +93,14 @@
         Integer(c_int), value :: k, ldp
         Real(c_double), value :: fine
         Integer(c_int) :: bsrg_mvk_cell
+       End Function
+
+       Function bsrg_mwk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mwk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mwk_cell
        End Function
 
        Function bsrg_ctx_create(device, stream, out) bind(C, name="bsrg_ctx_create")
@@ -220,6 +229,7 @@
        case ('mk '); rc = bsrg_mmk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case ('tk '); rc = bsrg_mtk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case ('vk '); rc = bsrg_mvk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case ('wk '); rc = bsrg_mwk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case default; Stop 'gpu_breit_cell: unknown integral type'
       End Select
       Call gpu_check(rc, which // '_cell')
@@ -247,6 +257,11 @@
       Integer, intent(in) :: k
       Call gpu_breit_cell('vk ', k)
       End Subroutine gpu_mvk_cell
+
+      Subroutine gpu_mwk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('wk ', k)
+      End Subroutine gpu_mwk_cell
 
 !======================================================================
       Subroutine gpu_add_two_electron(nch, norb, pbs, kmax, ncoef, ck, ctype, &

@@ -1730,7 +1730,10 @@ double orc_tk(int ns, int ks, const double *rkb, int ldp, const double *pi1, con
 /* mvk_cell.f90:2-83 (jj over ik pairs with jp = jhp - jh + 1, ii over all   */
 /* ks*ks pairs with ip = ihp - ih + ks; times fine).                         */
 /* ------------------------------------------------------------------------ */
-void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
+/* mode 0: vk_triang (vk_moments.f90:131); mode 1: wk_triang (wk_moments.f90:116) --
+   inner operator 2 dB/dr + k B/r instead of dB/dr - B/r, and the outer operator of the
+   second part 2 dB/dr - (k+3) B/r (bspd, grm) instead of bsq */
+static void vw_triang(const orc_basis *b, int k, int iv, double *rkd_iv, int mode)
 {
     int ks = b->ks, jk = ks * ks;
     int left = iv + ks - 1;
@@ -1745,7 +1748,8 @@ void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
             orc_bsplvd(b->t, ks, gx[i], left, 2, db);
             for (int j = 0; j < ks; j++) {
                 bt[i + ks * j] = db[j];
-                bd[i + ks * j] = db[j + ks] - bt[i + ks * j] / gx[i];
+                bd[i + ks * j] = mode ? 2 * db[j + ks] + k * bt[i + ks * j] / gx[i]
+                                      : db[j + ks] - bt[i + ks * j] / gx[i];
             }
         }
         for (int i = 0; i < ks; i++) gw[i] = span * b->gw[i] * ipow(gx[i], k);
@@ -1788,7 +1792,11 @@ void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
     for (int i = 0; i < ks; i++)
         for (int ip = 0; ip < ks; ip++) {
             double g3[MAXKS];
-            for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, i) * BSQ(b, iv, m, ip);
+            for (int m = 0; m < ks; m++) {
+                double op = mode ? 2 * BSPD(b, iv, m, ip, 0) - (k + 3) * GRM(b, iv, m) * BSP(b, iv, m, ip)
+                                 : BSQ(b, iv, m, ip);
+                g3[m] = BSP(b, iv, m, i) * op;
+            }
             jj = 0;
             for (int j = 0; j < ks; j++)
                 for (int jp = j; jp < ks; jp++) {
@@ -1803,35 +1811,64 @@ void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv)
     free(I2);
 }
 
-void orc_vk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
+void orc_vk_triang(const orc_basis *b, int k, int iv, double *rkd_iv) { vw_triang(b, k, iv, rkd_iv, 0); }
+
+static void vw_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4,
+                       double *rkd, int mode)
 {
     int ks = b->ks, nv = b->nv, ml = b->ml, me = b->me;
     int jk = ks * ks, ik = ks * (ks + 1) / 2;
-    orc_moments(b, k + 1, rkd1, 's', 'b');
-    orc_moments(b, -(k + 2), rkd2, 's', 'b');
-    orc_moments(b, k, rkd3, 'n', 'd');
-    orc_moments(b, -(k + 3), rkd4, 'n', 'd');
+    if (!mode) {
+        orc_moments(b, k + 1, rkd1, 's', 'b');
+        orc_moments(b, -(k + 2), rkd2, 's', 'b');
+        orc_moments(b, k, rkd3, 'n', 'd');
+        orc_moments(b, -(k + 3), rkd4, 'n', 'd');
+    } else {
+        /* wk_moments.f90:44-52: rkd3 = 2 m(k,'n','d') + (k+2) m(k-1,'n','b'),
+           rkd4 = 2 m(-(k+3),'n','d') - (k+1) m(-(k+4),'n','b') */
+        double *tmp = (double *)malloc(sizeof(double) * jk * nv);
+        orc_moments(b, k, rkd3, 'n', 'd');
+        orc_moments(b, k - 1, tmp, 'n', 'b');
+        for (size_t q = 0; q < (size_t)jk * nv; q++) rkd3[q] = 2 * rkd3[q] + (k + 2) * tmp[q];
+        orc_moments(b, -(k + 2), rkd2, 's', 'b');
+        orc_moments(b, -(k + 3), rkd4, 'n', 'd');
+        orc_moments(b, -(k + 4), tmp, 'n', 'b');
+        for (size_t q = 0; q < (size_t)jk * nv; q++) rkd4[q] = 2 * rkd4[q] - (k + 1) * tmp[q];
+        orc_moments(b, k + 1, rkd1, 's', 'b');
+        free(tmp);
+    }
     size_t cell = (size_t)jk * ik;
     if (me == 0) {
-        for (int iv = 0; iv < nv; iv++) orc_vk_triang(b, k, iv, rkd + cell * iv);
+        for (int iv = 0; iv < nv; iv++) vw_triang(b, k, iv, rkd + cell * iv, mode);
         return;
     }
-    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) orc_vk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+    for (int iv = 1; iv <= ml + ks - 1 && iv <= nv; iv++) vw_triang(b, k, iv - 1, rkd + cell * (iv - 1), mode);
     double hp = b->h + 1.0;
     for (int iv = ml + ks; iv <= ml + me - ks + 2; iv++)
         for (size_t q = 0; q < cell; q++) rkd[q + cell * (iv - 1)] = rkd[q + cell * (iv - 2)] / hp;
     for (int iv = ml + me - ks + 3; iv <= nv; iv++)
-        if (iv >= 1) orc_vk_triang(b, k, iv - 1, rkd + cell * (iv - 1));
+        if (iv >= 1) vw_triang(b, k, iv - 1, rkd + cell * (iv - 1), mode);
 }
 
-/* rkb (ns, ns, ldp, ldp): ip up to 2ks-1 wide, jp up to ks */
-void orc_mvk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+void orc_vk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
+{
+    vw_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, 0);
+}
+
+/* wk_moments.f90:2-241 */
+void orc_wk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
+{
+    vw_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, 1);
+}
+
+/* rkb (ns, ns, ldp, ldp): ip up to 2ks-1 wide, jp up to ks; mode 0 mvk_cell, 1 mwk_cell (same sums) */
+static void mvw_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp, int mode)
 {
     int ks = b->ks, ns = b->ns, nv = b->nv, jk = ks * ks, ik = ks * (ks + 1) / 2;
     double *rkd1 = (double *)malloc(sizeof(double) * ik * nv), *rkd2 = (double *)malloc(sizeof(double) * ik * nv);
     double *rkd3 = (double *)malloc(sizeof(double) * jk * nv), *rkd4 = (double *)malloc(sizeof(double) * jk * nv);
     double *rkd = (double *)malloc(sizeof(double) * jk * ik * nv);
-    orc_vk_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd);
+    vw_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, mode);
     size_t nn = (size_t)ns * ns;
     memset(rkb, 0, sizeof(double) * nn * ldp * ldp);
     for (int jv = 0; jv < nv; jv++) {
@@ -1863,6 +1900,11 @@ void orc_mvk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
     for (size_t q = 0; q < nn * ldp * ldp; q++) rkb[q] = rkb[q] * fine;
     free(rkd1); free(rkd2); free(rkd3); free(rkd4); free(rkd);
 }
+
+void orc_mvk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp) { mvw_cell(b, k, fine, rkb, ldp, 0); }
+
+/* mwk_cell.f90:2-83 */
+void orc_mwk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp) { mvw_cell(b, k, fine, rkb, ldp, 1); }
 
 /* vk.f90 (meth 'c'): a = 'n' density of (i1,i2), b = 's' density of (j1,j2) */
 double orc_vk(int ns, int ks, const double *rkb, int ldp, const double *pi1, const double *pj1, const double *pi2,

@@ -67,6 +67,8 @@ def lib():
         L.orc_tk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_vk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D]
         L.orc_mvk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_wk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D]
+        L.orc_mwk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_vk.restype = ctypes.c_double
         L.orc_vk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_nk.restype = ctypes.c_double
@@ -229,6 +231,22 @@ class Basis:
         lib().orc_vk_moments(self._h, k, _p(r1), _p(r2), _p(r3), _p(r4), _p(rd))
         return (r1.reshape((ik, nv), order="F"), r2.reshape((ik, nv), order="F"), r3.reshape((jk, nv), order="F"),
                 r4.reshape((jk, nv), order="F"), rd.reshape((jk, ik, nv), order="F"))
+
+    def wk_moments(self, k):
+        """wk_moments (wk_moments.f90:2): the V^k layouts with W^k's combined moments and operators."""
+        ik, jk, nv = self.ks * (self.ks + 1) // 2, self.ks * self.ks, self.nv
+        r1, r2, r3, r4 = np.zeros(ik * nv), np.zeros(ik * nv), np.zeros(jk * nv), np.zeros(jk * nv)
+        rd = np.zeros(jk * ik * nv)
+        lib().orc_wk_moments(self._h, k, _p(r1), _p(r2), _p(r3), _p(r4), _p(rd))
+        return (r1.reshape((ik, nv), order="F"), r2.reshape((ik, nv), order="F"), r3.reshape((jk, nv), order="F"),
+                r4.reshape((jk, nv), order="F"), rd.reshape((jk, ik, nv), order="F"))
+
+    def mwk_cell(self, k, fine=1.0, ldp=None):
+        """mwk_cell (mwk_cell.f90:2): W^k table (ns,ns,ldp,ldp), ldp >= 2ks-1, times fine."""
+        ldp = ldp or 2 * self.ks - 1
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mwk_cell(self._h, k, float(fine), _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def mvk_cell(self, k, fine=1.0, ldp=None):
         """mvk_cell (mvk_cell.f90:2): V^k table (ns,ns,ldp,ldp), ldp >= 2ks-1, times fine."""
