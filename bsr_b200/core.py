@@ -242,6 +242,23 @@ def mwk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     return out
 
 
+def qk_moments(basis, k):
+    """Breit-Pauli Q^k moments: rkd1..rkd4 (ks*ks, nv), rkd (ks*ks, ks*ks, nv)."""
+    jk, nv = basis.ks * basis.ks, basis.nv
+    out = [fortran_empty((jk, nv)) for _ in range(4)] + [fortran_empty((jk, jk, nv))]
+    call("bsrg_qk_moments", basis.handle, k, *[_ptr(x) for x in out], _stream())
+    return out
+
+
+def mqk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
+    """Q^k table rkb(ns,ns,ldp,ldp), ldp >= 2ks-1 (default), times fine (mqk_cell.f90)."""
+    ldp = 2 * basis.ks - 1 if ldp is None else ldp
+    if out is None:
+        out = fortran_empty((basis.ns, basis.ns, ldp, ldp))
+    call("bsrg_mqk_cell", basis.handle, k, float(fine), _ptr(out), ldp, _stream())
+    return out
+
+
 def mnk_cell(basis, k, fine=0.25 / 137.036 ** 2, ldp=None, out=None):
     """N^k table rkb(ns,ns,ldp,ldp) times fine (mnk_cell.f90); i, ip the r1 splines, r2 < r1."""
     ldp = basis.ks if ldp is None else ldp

@@ -53,6 +53,8 @@ int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double
                       double *rkd, double *tmp, cudaStream_t s);
 int launch_mvk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,
                     const double *rkd4, const double *rkd, double fine, double *rkb, int ldp, cudaStream_t s);
+int launch_mqk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,
+                    const double *rkd4, const double *rkd, double fine, double *rkb, int ldp, cudaStream_t s);
 int launch_density(int ns, int ks, double *d, const double *p1, const double *p2, char type, cudaStream_t s);
 int launch_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp, int icase,
                   char si, char sj, cudaStream_t s);

@@ -380,14 +380,17 @@ int bsrg_wk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, doub
 
 static int mvw_cell_call(const bsrg_basis *b, int k, int mode, double fine, double *rkb, int ldp, cudaStream_t s)
 {
-    const size_t ik = (size_t)ik_of(b->ks), jk = (size_t)b->ks * b->ks, nv = (size_t)b->nv;
+    const size_t jk = (size_t)b->ks * b->ks, nv = (size_t)b->nv;
+    const size_t nj = mode == 2 ? jk : (size_t)ik_of(b->ks);       // pairs on the r2 side
     double *buf = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * ik * nv + 3 * jk * nv + jk * ik * nv) * sizeof(double), s);
-    if (e != cudaSuccess) return cuda_fail(e, mode ? "mwk_cell scratch" : "mvk_cell scratch");
-    double *r1 = buf, *r2 = r1 + ik * nv, *r3 = r2 + ik * nv, *r4 = r3 + jk * nv, *rd = r4 + jk * nv;
-    double *tmp = rd + jk * ik * nv;
+    cudaError_t e = cudaMallocAsync((void **)&buf, (2 * nj * nv + 3 * jk * nv + jk * nj * nv) * sizeof(double), s);
+    if (e != cudaSuccess) return cuda_fail(e, "m?k_cell scratch");
+    double *r1 = buf, *r2 = r1 + nj * nv, *r3 = r2 + nj * nv, *r4 = r3 + jk * nv, *rd = r4 + jk * nv;
+    double *tmp = rd + jk * nj * nv;
     int rc = launch_vw_moments(b, k, mode, r1, r2, r3, r4, rd, tmp, s);
-    if (rc == BSRG_OK) rc = launch_mvk_cell(b, r1, r2, r3, r4, rd, fine, rkb, ldp, s);
+    if (rc == BSRG_OK)
+        rc = mode == 2 ? launch_mqk_cell(b, r1, r2, r3, r4, rd, fine, rkb, ldp, s)
+                       : launch_mvk_cell(b, r1, r2, r3, r4, rd, fine, rkb, ldp, s);
     cudaFreeAsync(buf, s);
     return rc;
 }
@@ -398,6 +401,22 @@ int bsrg_mvk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
     CHECK_ARG(ldp >= 2 * b->ks - 1, "mvk_cell: ldp=%d < 2ks-1=%d", ldp, 2 * b->ks - 1);
     CHECK_ARG(k >= 0 && k <= 64, "mvk_cell: k=%d out of range", k);
     return mvw_cell_call(b, k, 0, fine, rkb, ldp, (cudaStream_t)stream);
+}
+
+int bsrg_qk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
+                    void *stream)
+{
+    CHECK_ARG(b, "qk_moments: null basis");
+    CHECK_ARG(k >= 0 && k <= 64, "qk_moments: k=%d out of range", k);
+    return vw_moments_call(b, k, 2, rkd1, rkd2, rkd3, rkd4, rkd, (cudaStream_t)stream);
+}
+
+int bsrg_mqk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)
+{
+    CHECK_ARG(b && rkb, "mqk_cell: null argument");
+    CHECK_ARG(ldp >= 2 * b->ks - 1, "mqk_cell: ldp=%d < 2ks-1=%d", ldp, 2 * b->ks - 1);
+    CHECK_ARG(k >= 0 && k <= 64, "mqk_cell: k=%d out of range", k);
+    return mvw_cell_call(b, k, 2, fine, rkb, ldp, (cudaStream_t)stream);
 }
 
 int bsrg_mwk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream)

@@ -782,13 +782,22 @@ __global__ void vk_diag_cell_kernel(int ks, int nv, int ml, int me, double hscal
         I2[(m * ks + a) * ks + b] = u * (ipow_dev(gm, k + 3) * gwm);
     }
     __syncthreads();
-    double *out = rkd + (size_t)jk * ik * iv_out;
-    for (int q = threadIdx.x; q < jk * ik; q += blockDim.x) {
+    // V^k, W^k: jj over the ik pairs j <= jp; Q^k (mode 2, qk_triang): over all ks*ks pairs
+    const int njj = mode == 2 ? jk : ik;
+    double *out = rkd + (size_t)jk * njj * iv_out;
+    for (int q = threadIdx.x; q < jk * njj; q += blockDim.x) {
         const int ii = q % jk, jj = q / jk;
         const int i = ii / ks, ip = ii % ks;
-        int j = 0, rem = jj;
-        while (rem >= ks - j) { rem -= ks - j; j++; }
-        const int jp = j + rem;
+        int j, jp;
+        if (mode == 2) {
+            j = jj / ks;
+            jp = jj % ks;
+        } else {
+            j = 0;
+            int rem = jj;
+            while (rem >= ks - j) { rem -= ks - j; j++; }
+            jp = j + rem;
+        }
         double s1 = 0.0, s2 = 0.0;
         for (int m = 0; m < ks; m++) {
             const double g3 = bsp[iv + ld * (m + (size_t)ks * j)] * bsp[iv + ld * (m + (size_t)ks * jp)];
@@ -876,6 +885,73 @@ vkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__
         }
     }
     rkb[i + (size_t)ns * (j + (size_t)ns * (ip + (size_t)ldp * jp))] = acc * fine;
+}
+
+// mqk_cell (mqk_cell.f90:2): the reference adds every cell term c to rkb(i,j,ip,jp)
+// and subtracts it from rkb(j,i,jp,ip) within one loop (jv, jh, jhp outer; iv, ih,
+// ihp inner).  For one element and one jv, all its added terms share (jh, jhp) and
+// all its subtracted terms share another (jh, jhp), so per jv one block precedes the
+// other in the reference's order; a self-transposed element gets +c then -c in the
+// same iteration.  One thread per element replays that order, then times fine.
+__device__ __forceinline__ double qk_term(int ks, int jk, int jv, int jh, int jhp, int iv, int ih, int ihp,
+                                          const double *rkd1, const double *rkd2, const double *rkd3,
+                                          const double *rkd4, const double *rkd)
+{
+    const int ii = ih * ks + ihp, jj = jh * ks + jhp;
+    if (iv < jv) return rkd3[ii + (size_t)jk * iv] * rkd2[jj + (size_t)jk * jv];
+    if (iv > jv) return rkd1[jj + (size_t)jk * jv] * rkd4[ii + (size_t)jk * iv];
+    return rkd[ii + (size_t)jk * (jj + (size_t)jk * iv)];
+}
+
+__global__ void qkb_expand_kernel(int ks, int ns, int nv, int ldp, double fine, const double *__restrict__ rkd1,
+                                  const double *__restrict__ rkd2, const double *__restrict__ rkd3,
+                                  const double *__restrict__ rkd4, const double *__restrict__ rkd,
+                                  double *__restrict__ rkb)
+{
+    const size_t nn = (size_t)ns * ns;
+    const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (q >= nn * ldp * ldp) return;
+    const int I = (int)(q % ns), J = (int)((q / ns) % ns);
+    const int IP = (int)((q / nn) % ldp), JP = (int)(q / (nn * ldp));
+    const int jk = ks * ks, H = ks - 1;
+    double acc = 0.0;
+    if (IP < 2 * ks - 1 && JP < 2 * ks - 1) {
+        const bool self = (I == J && IP == JP);
+        int jv_lo = (I < J ? I : J) - H; if (jv_lo < 0) jv_lo = 0;
+        int jv_hi = I > J ? I : J; if (jv_hi > nv - 1) jv_hi = nv - 1;
+        for (int jv = jv_lo; jv <= jv_hi; jv++) {
+            // added terms: (i,j,ip,jp) = (I,J,IP,JP); subtracted: (i,j,ip,jp) = (J,I,JP,IP)
+            const int jhA = J - jv, jhpA = JP - H + jhA;
+            const int jhS = I - jv, jhpS = IP - H + jhS;
+            const bool vA = jhA >= 0 && jhA < ks && jhpA >= 0 && jhpA < ks;
+            const bool vS = jhS >= 0 && jhS < ks && jhpS >= 0 && jhpS < ks;
+            if (self) {
+                if (!vA) continue;
+                for (int iv = (I - H > 0 ? I - H : 0); iv <= I && iv < nv; iv++) {
+                    const int ih = I - iv, ihp = IP - H + ih;
+                    if (ihp < 0 || ihp >= ks) continue;
+                    const double c = qk_term(ks, jk, jv, jhA, jhpA, iv, ih, ihp, rkd1, rkd2, rkd3, rkd4, rkd);
+                    acc = acc + c;
+                    acc = acc - c;
+                }
+                continue;
+            }
+            const bool addFirst = (jhA < jhS) || (jhA == jhS && jhpA < jhpS);
+            for (int pass = 0; pass < 2; pass++) {
+                const bool add = (pass == 0) == addFirst;
+                if (add ? !vA : !vS) continue;
+                const int Ir = add ? I : J, IPr = add ? IP : JP;       // the iteration's i and ip
+                const int jh = add ? jhA : jhS, jhp = add ? jhpA : jhpS;
+                for (int iv = (Ir - H > 0 ? Ir - H : 0); iv <= Ir && iv < nv; iv++) {
+                    const int ih = Ir - iv, ihp = IPr - H + ih;
+                    if (ihp < 0 || ihp >= ks) continue;
+                    const double c = qk_term(ks, jk, jv, jh, jhp, iv, ih, ihp, rkd1, rkd2, rkd3, rkd4, rkd);
+                    acc = add ? acc + c : acc - c;
+                }
+            }
+        }
+    }
+    rkb[q] = acc * fine;
 }
 
 // ---------------------------------------------------------------------------
@@ -1043,12 +1119,22 @@ int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double
 {
     const int ks = b->ks, nv = b->nv, jk = ks * ks, ik = ik_of(ks);
     const double q = 1.0 + b->h;
-    if (rkd1)
-        moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k + 1) * q, k + 1,
-                                                              b->gr, b->grm, b->grw, b->bsp, rkd1);
-    if (rkd2)
-        moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 2)) * q,
-                                                              -(k + 2), b->gr, b->grm, b->grw, b->bsp, rkd2);
+    if (mode == 2) {        // qk_moments.f90: rkd1, rkd2 over all ks*ks pairs ('n','b')
+        const int gq = (jk * nv + 127) / 128;
+        if (rkd1)
+            moments_nd_kernel<<<gq, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k + 1) * q, k + 1, b->gr, b->grm,
+                                                 b->grw, b->bsp, b->bsq, rkd1, 1);
+        if (rkd2)
+            moments_nd_kernel<<<gq, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 2)) * q, -(k + 2), b->gr,
+                                                 b->grm, b->grw, b->bsp, b->bsq, rkd2, 1);
+    } else {
+        if (rkd1)
+            moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k + 1) * q, k + 1,
+                                                                  b->gr, b->grm, b->grw, b->bsp, rkd1);
+        if (rkd2)
+            moments_kernel<<<(ik * nv + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 2)) * q,
+                                                                  -(k + 2), b->gr, b->grm, b->grw, b->bsp, rkd2);
+    }
     const int nj = jk * nv, gj = (nj + 127) / 128;
     if (rkd3) {
         moments_nd_kernel<<<gj, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, k), k, b->gr, b->grm, b->grw, b->bsp,
@@ -1078,7 +1164,16 @@ int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double
         vk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, mode, b->t, rule_of(b), b->gr,
                                                 b->grm, b->grw, b->bsp, b->bsq, b->bspd, rkd);
     }
-    return cuda_fail(cudaGetLastError(), mode ? "wk_moments" : "vk_moments");
+    return cuda_fail(cudaGetLastError(), mode == 2 ? "qk_moments" : mode ? "wk_moments" : "vk_moments");
+}
+
+int launch_mqk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,
+                    const double *rkd4, const double *rkd, double fine, double *rkb, int ldp, cudaStream_t s)
+{
+    const size_t n = (size_t)b->ns * b->ns * ldp * ldp;
+    qkb_expand_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(b->ks, b->ns, b->nv, ldp, fine, rkd1, rkd2, rkd3,
+                                                                  rkd4, rkd, rkb);
+    return cuda_fail(cudaGetLastError(), "mqk_cell");
 }
 
 int launch_mvk_cell(const bsrg_basis *b, const double *rkd1, const double *rkd2, const double *rkd3,

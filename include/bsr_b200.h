@@ -125,6 +125,15 @@ int bsrg_wk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, doub
                     void *stream);
 int bsrg_mwk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
 
+/* ---- Breit-Pauli Q^k: src/libs/BS/qk_moments.f90:2 (W^k's moments with rkd1,
+ *      rkd2 over all ks*ks pairs; diagonal cells rkd (ks*ks, ks*ks, nv)) and
+ *      mqk_cell.f90:2 (every cell term added to rkb(i,j,ip,jp) and subtracted
+ *      from rkb(j,i,jp,ip), in the reference's order; times fine).  rkb
+ *      (ns, ns, ldp, ldp), ldp >= 2ks-1.  k >= 0.  Device. */
+int bsrg_qk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd,
+                    void *stream);
+int bsrg_mqk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp, void *stream);
+
 /* ---- No counterpart in the reference.  bsrg_mrk_cell for callers that must
  *      not allocate device memory while they run (a serving process that has
  *      split all of its HBM among its solves at start-up; loops that cannot

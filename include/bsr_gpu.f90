@@ -9,9 +9,10 @@
 !       gpu_mrk_cell(k)         mrk_cell (libs/BS/mrk_cell.f90:2): fills
 !                               module spline_integrals rkb from the GPU
 !       gpu_mnk_cell(k), gpu_mmk_cell(k), gpu_mtk_cell(k), gpu_mvk_cell(k),
-!       gpu_mwk_cell(k)
+!       gpu_mwk_cell(k), gpu_mqk_cell(k)
 !                               the Breit-Pauli tables mnk_cell, mmk_cell,
-!                               mtk_cell, mvk_cell (libs/BS/m?k_cell.f90:2),
+!                               mtk_cell, mvk_cell, mwk_cell, mqk_cell
+!                               (libs/BS/m?k_cell.f90:2),
 !                               with spline_atomic's fine
 !       gpu_add_two_electron    the I_data Case(6..9) call for icase 5
 !                               (bsr/BSR_MAT3/I_data.f90:192-218)
@@ -101,6 +102,14 @@
         Integer(c_int), value :: k, ldp
         Real(c_double), value :: fine
         Integer(c_int) :: bsrg_mwk_cell
+       End Function
+
+       Function bsrg_mqk_cell(b, k, fine, rkb, ldp, stream) bind(C, name="bsrg_mqk_cell")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: b, rkb, stream
+        Integer(c_int), value :: k, ldp
+        Real(c_double), value :: fine
+        Integer(c_int) :: bsrg_mqk_cell
        End Function
 
        Function bsrg_ctx_create(device, stream, out) bind(C, name="bsrg_ctx_create")
@@ -210,7 +219,7 @@
 !======================================================================
       Subroutine gpu_breit_cell(which, k)
 !----------------------------------------------------------------------
-!     m?k_cell(k) for which = 'nk ', 'mk ', 'tk ', 'vk ': module rkb
+!     m?k_cell(k) for which = 'nk ', 'mk ', 'tk ', 'vk ', 'wk ', 'qk ': module rkb
 !     (ns,ns,2ks-1,2ks-1) filled from the GPU table, fine included
 !----------------------------------------------------------------------
       Use spline_param
@@ -230,6 +239,7 @@
        case ('tk '); rc = bsrg_mtk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case ('vk '); rc = bsrg_mvk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case ('wk '); rc = bsrg_mwk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
+       case ('qk '); rc = bsrg_mqk_cell(gpu_basis, k, fine, d_rkb, 2*ks-1, c_null_ptr)
        case default; Stop 'gpu_breit_cell: unknown integral type'
       End Select
       Call gpu_check(rc, which // '_cell')
@@ -262,6 +272,11 @@
       Integer, intent(in) :: k
       Call gpu_breit_cell('wk ', k)
       End Subroutine gpu_mwk_cell
+
+      Subroutine gpu_mqk_cell(k)
+      Integer, intent(in) :: k
+      Call gpu_breit_cell('qk ', k)
+      End Subroutine gpu_mqk_cell
 
 !======================================================================
       Subroutine gpu_add_two_electron(nch, norb, pbs, kmax, ncoef, ck, ctype, &

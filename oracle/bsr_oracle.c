@@ -1736,6 +1736,7 @@ double orc_tk(int ns, int ks, const double *rkb, int ldp, const double *pi1, con
 static void vw_triang(const orc_basis *b, int k, int iv, double *rkd_iv, int mode)
 {
     int ks = b->ks, jk = ks * ks;
+    const int jall = (mode == 2);       /* qk_triang: (j, jp) over all ks*ks pairs */
     int left = iv + ks - 1;
     double xbase = b->t[left];
     double gx[MAXKS], gw[MAXKS], bt[MAXKS * MAXKS], bd[MAXKS * MAXKS], db[2 * MAXKS], bi[MAXKS];
@@ -1775,7 +1776,7 @@ static void vw_triang(const orc_basis *b, int k, int iv, double *rkd_iv, int mod
     }
     int jj = 0;
     for (int j = 0; j < ks; j++)
-        for (int jp = j; jp < ks; jp++) {
+        for (int jp = jall ? 0 : j; jp < ks; jp++) {
             double g3[MAXKS];
             for (int m = 0; m < ks; m++) g3[m] = BSP(b, iv, m, j) * BSP(b, iv, m, jp);
             int ii = 0;
@@ -1799,7 +1800,7 @@ static void vw_triang(const orc_basis *b, int k, int iv, double *rkd_iv, int mod
             }
             jj = 0;
             for (int j = 0; j < ks; j++)
-                for (int jp = j; jp < ks; jp++) {
+                for (int jp = jall ? 0 : j; jp < ks; jp++) {
                     double s = 0.0;
                     for (int m = 0; m < ks; m++) s = s + g3[m] * I2[j + ks * (jp + ks * m)];
                     rkd_iv[ii + jk * jj] = rkd_iv[ii + jk * jj] + s;
@@ -1824,20 +1825,22 @@ static void vw_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, do
         orc_moments(b, k, rkd3, 'n', 'd');
         orc_moments(b, -(k + 3), rkd4, 'n', 'd');
     } else {
-        /* wk_moments.f90:44-52: rkd3 = 2 m(k,'n','d') + (k+2) m(k-1,'n','b'),
+        /* wk_moments.f90:44-52 (qk_moments.f90:44-52 with 'n' for rkd1, rkd2):
+           rkd3 = 2 m(k,'n','d') + (k+2) m(k-1,'n','b'),
            rkd4 = 2 m(-(k+3),'n','d') - (k+1) m(-(k+4),'n','b') */
+        const char sj = mode == 2 ? 'n' : 's';
         double *tmp = (double *)malloc(sizeof(double) * jk * nv);
         orc_moments(b, k, rkd3, 'n', 'd');
         orc_moments(b, k - 1, tmp, 'n', 'b');
         for (size_t q = 0; q < (size_t)jk * nv; q++) rkd3[q] = 2 * rkd3[q] + (k + 2) * tmp[q];
-        orc_moments(b, -(k + 2), rkd2, 's', 'b');
+        orc_moments(b, -(k + 2), rkd2, sj, 'b');
         orc_moments(b, -(k + 3), rkd4, 'n', 'd');
         orc_moments(b, -(k + 4), tmp, 'n', 'b');
         for (size_t q = 0; q < (size_t)jk * nv; q++) rkd4[q] = 2 * rkd4[q] - (k + 1) * tmp[q];
-        orc_moments(b, k + 1, rkd1, 's', 'b');
+        orc_moments(b, k + 1, rkd1, sj, 'b');
         free(tmp);
     }
-    size_t cell = (size_t)jk * ik;
+    size_t cell = (size_t)jk * (mode == 2 ? jk : ik);
     if (me == 0) {
         for (int iv = 0; iv < nv; iv++) vw_triang(b, k, iv, rkd + cell * iv, mode);
         return;
@@ -1853,6 +1856,55 @@ static void vw_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, do
 void orc_vk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
 {
     vw_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, 0);
+}
+
+/* qk_moments.f90:2-239: rkd1, rkd2 (ks*ks, nv), rkd3, rkd4 (ks*ks, nv), rkd (ks*ks, ks*ks, nv) */
+void orc_qk_moments(const orc_basis *b, int k, double *rkd1, double *rkd2, double *rkd3, double *rkd4, double *rkd)
+{
+    vw_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd, 2);
+}
+
+/* mqk_cell.f90:2-86: all (jh, jhp) and (ih, ihp) pairs, ip = ihp - ih + ks, jp = jhp - jh + ks;
+   each term added to rkb(i,j,ip,jp) and subtracted from rkb(j,i,jp,ip) in loop order; times fine */
+void orc_mqk_cell(const orc_basis *b, int k, double fine, double *rkb, int ldp)
+{
+    int ks = b->ks, ns = b->ns, nv = b->nv, jk = ks * ks;
+    double *rkd1 = (double *)malloc(sizeof(double) * jk * nv), *rkd2 = (double *)malloc(sizeof(double) * jk * nv);
+    double *rkd3 = (double *)malloc(sizeof(double) * jk * nv), *rkd4 = (double *)malloc(sizeof(double) * jk * nv);
+    double *rkd = (double *)malloc(sizeof(double) * jk * jk * nv);
+    orc_qk_moments(b, k, rkd1, rkd2, rkd3, rkd4, rkd);
+    size_t nn = (size_t)ns * ns;
+    memset(rkb, 0, sizeof(double) * nn * ldp * ldp);
+    for (int jv = 0; jv < nv; jv++) {
+        int jj = 0;
+        for (int jh = 0; jh < ks; jh++) {
+            int j = jv + jh;
+            for (int jhp = 0; jhp < ks; jhp++) {
+                int jp = jhp - jh + ks - 1;
+                for (int iv = 0; iv < nv; iv++) {
+                    int ii = 0;
+                    for (int ih = 0; ih < ks; ih++) {
+                        int i = iv + ih;
+                        for (int ihp = 0; ihp < ks; ihp++) {
+                            int ip = ihp - ih + ks - 1;
+                            double c;
+                            if (iv < jv) c = rkd3[ii + (size_t)jk * iv] * rkd2[jj + (size_t)jk * jv];
+                            else if (iv > jv) c = rkd1[jj + (size_t)jk * jv] * rkd4[ii + (size_t)jk * iv];
+                            else c = rkd[ii + (size_t)jk * (jj + (size_t)jk * iv)];
+                            size_t o1 = i + (size_t)ns * j + nn * (ip + (size_t)ldp * jp);
+                            size_t o2 = j + (size_t)ns * i + nn * (jp + (size_t)ldp * ip);
+                            rkb[o1] = rkb[o1] + c;
+                            rkb[o2] = rkb[o2] - c;
+                            ii++;
+                        }
+                    }
+                }
+                jj++;
+            }
+        }
+    }
+    for (size_t q = 0; q < nn * ldp * ldp; q++) rkb[q] = rkb[q] * fine;
+    free(rkd1); free(rkd2); free(rkd3); free(rkd4); free(rkd);
 }
 
 /* wk_moments.f90:2-241 */

@@ -69,6 +69,8 @@ def lib():
         L.orc_mvk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_wk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D]
         L.orc_mwk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
+        L.orc_qk_moments.argtypes = [ctypes.c_void_p, ctypes.c_int, _D, _D, _D, _D, _D]
+        L.orc_mqk_cell.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _D, ctypes.c_int]
         L.orc_vk.restype = ctypes.c_double
         L.orc_vk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_nk.restype = ctypes.c_double
@@ -246,6 +248,21 @@ class Basis:
         ldp = ldp or 2 * self.ks - 1
         rkb = np.zeros(self.ns * self.ns * ldp * ldp)
         lib().orc_mwk_cell(self._h, k, float(fine), _p(rkb), ldp)
+        return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
+
+    def qk_moments(self, k):
+        """qk_moments (qk_moments.f90:2): rkd1..rkd4 (ks*ks, nv), rkd (ks*ks, ks*ks, nv)."""
+        jk, nv = self.ks * self.ks, self.nv
+        r = [np.zeros(jk * nv) for _ in range(4)]
+        rd = np.zeros(jk * jk * nv)
+        lib().orc_qk_moments(self._h, k, *[_p(x) for x in r], _p(rd))
+        return tuple(x.reshape((jk, nv), order="F") for x in r) + (rd.reshape((jk, jk, nv), order="F"),)
+
+    def mqk_cell(self, k, fine=1.0, ldp=None):
+        """mqk_cell (mqk_cell.f90:2): Q^k table (ns,ns,ldp,ldp), ldp >= 2ks-1, times fine."""
+        ldp = ldp or 2 * self.ks - 1
+        rkb = np.zeros(self.ns * self.ns * ldp * ldp)
+        lib().orc_mqk_cell(self._h, k, float(fine), _p(rkb), ldp)
         return rkb.reshape((self.ns, self.ns, ldp, ldp), order="F")
 
     def mvk_cell(self, k, fine=1.0, ldp=None):

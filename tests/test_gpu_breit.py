@@ -233,3 +233,45 @@ def test_int_inp1_wk_on_gpu(golden, test_bs):
             assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
         n += 1
     assert n == 13
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_qk_moments_and_mqk_cell_bitwise(pair, k):
+    """Q^k: the GPU moments and the expanded table equal the oracle's bit for bit; the
+    expansion replays the reference's interleaved add/subtract order per element."""
+    from bsr_b200 import core
+    name, gb, ob = pair
+    if name == "config2" and k != 1:
+        pytest.skip("one multipole suffices at ns=200")
+    got = [to_np(x) for x in core.qk_moments(gb, k)]
+    for g, r in zip(got, ob.qk_moments(k)):
+        assert np.array_equal(g, r), name
+    f = 0.25 / 137.036 ** 2
+    assert np.array_equal(to_np(core.mqk_cell(gb, k, fine=f)), ob.mqk_cell(k, fine=f)), name
+
+
+def test_int_inp1_qk_on_gpu(golden, test_bs):
+    """Q^k (qk.f90 route, the tk.f90 sum) from the GPU tables against int_inp1 (x Z^3);
+    the entries whose exact value is zero to 1e-15 absolute."""
+    import bsr_b200 as bsr
+    from bsr_b200 import core
+    from oracle import oracle as O
+    B = test_bs["basis"]
+    g = test_bs["grid"]
+    gb = bsr.define_spline(g["t"], B.ks, g["ml"], g["me"], g["h"])
+    z = test_bs["knot"]["z"]
+    orbs = {"%d%s" % (n, "spdfg"[l]): B.bhwf(n, l, z) for n in range(1, 6) for l in range(n)}
+    n = 0
+    for e in golden["int_inp1"]:
+        if e["int"] != "Q":
+            continue
+        rkb = to_np(core.mqk_cell(gb, e["k"], fine=1.0))
+        got = O.tk(B.ns, B.ks, rkb, *[orbs[o] for o in e["orbs"]])
+        sa = e["ratio"] * z ** 3
+        if sa == 0.0:
+            assert abs(got) < 1e-15, (e, got)
+        else:
+            assert abs(got - sa) / abs(sa) < 1e-13, (e, got, sa)
+        n += 1
+    assert n == 14
+
