@@ -39,6 +39,7 @@ SIGNATURES = [
     ("bsrg_wk_moments", _c_int, [_P, _c_int, _P, _P, _P, _P, _P, _P]),
     ("bsrg_mwk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),
     ("bsrg_qk_moments", _c_int, [_P, _c_int, _P, _P, _P, _P, _P, _P]),
+    ("bsrg_channel_weights", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _P, _P]),
     ("bsrg_mqk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),
     ("bsrg_mtk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),
     ("bsrg_mmk_cell", _c_int, [_P, _c_int, _c_double, _P, _c_int, _P]),

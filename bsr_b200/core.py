@@ -462,6 +462,20 @@ def rsol_out(ctx, ns, ipsol, bb, vectors, want_v=True):
     return v, w
 
 
+def channel_weights(ctx, ipsol, vectors, want_iprm=True):
+    """W_OUT's weights: wt (nch x khm), isol (khm,, 1-based dominant channel) and
+    iprm (nch x khm, SORTA order, 1-based) of the eigenvectors a (khm x khm)."""
+    ipsol = np.ascontiguousarray(ipsol, dtype=np.int32)
+    nch, khm = len(ipsol) - 1, int(ipsol[-1])
+    a = as_fortran(vectors)
+    wt = fortran_empty((nch, khm))
+    isol = torch.empty(khm, device="cuda", dtype=torch.int32)
+    iprm = fortran_empty((nch, khm), dtype=torch.int32) if want_iprm else None
+    call("bsrg_channel_weights", ctx.handle, nch, _iptr(ipsol), khm, _ptr(a), _ptr(wt), _ptr(isol),
+         _ptr(iprm) if want_iprm else None)
+    return wt, isol, iprm
+
+
 def dsytrd(ctx, A):
     """LAPACK DSYTRD (lower) on the device: returns (d, e, tau); A (n x n, Fortran
     layout, overwritten) keeps the reflectors below the subdiagonal."""

@@ -73,8 +73,102 @@ __global__ void last_rows_kernel(int ns, int nch, int khm, const double *__restr
     wmat[q] = v[(size_t)ich * ns + ns - 1 + (size_t)nch * ns * is];
 }
 
+// W_OUT (w_out.f90:58-76): per solution is, channel weights WT(ich) = sum over the
+// channel's rows j of a(j,is)^2, summed in row order as Fortran's SUM does; then
+// SORTA's exchange sort (sorting_routines.f90:79-97) of |WT| gives iprm, and isol is
+// the channel of largest weight.  One block per solution; the column passes through
+// shared memory in chunks so that the loads are coalesced while each channel's sum
+// keeps its sequential order.
+constexpr int CW_CHUNK = 2048;
+
+__global__ void channel_weights_kernel(int nch, const int *__restrict__ ipsol, int khm, const double *__restrict__ a,
+                                       double *__restrict__ wt, int *__restrict__ isol, int *__restrict__ iprm)
+{
+    extern __shared__ double cw_sm[];
+    double *col = cw_sm;                       // CW_CHUNK
+    double *w = col + CW_CHUNK;                // nch
+    int *ipt = (int *)(w + nch);               // nch
+    const int is = blockIdx.x;
+    const double *acol = a + (size_t)khm * is;
+    for (int i = threadIdx.x; i < nch; i += blockDim.x) w[i] = 0.0;
+    for (int c0 = 0; c0 < khm; c0 += CW_CHUNK) {
+        const int c1 = min(c0 + CW_CHUNK, khm);
+        __syncthreads();
+        for (int j = c0 + threadIdx.x; j < c1; j += blockDim.x) col[j - c0] = acol[j];
+        __syncthreads();
+        for (int i = threadIdx.x; i < nch; i += blockDim.x) {
+            const int j1 = max(ipsol[i], c0), j2 = min(ipsol[i + 1], c1);
+            double sum = w[i];
+            for (int j = j1; j < j2; j++) sum = __dadd_rn(sum, __dmul_rn(col[j - c0], col[j - c0]));
+            w[i] = sum;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nch; i += blockDim.x) wt[i + (size_t)nch * is] = w[i];
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < nch; i++) ipt[i] = i;
+        for (int i1 = 0; i1 < nch - 1; i1++) {
+            int j1 = ipt[i1];
+            for (int i2 = i1 + 1; i2 < nch; i2++) {
+                const int j2 = ipt[i2];
+                if (fabs(w[j1]) < fabs(w[j2])) {
+                    ipt[i2] = j1;
+                    j1 = j2;
+                }
+            }
+            ipt[i1] = j1;
+        }
+        isol[is] = ipt[0] + 1;
+    }
+    if (iprm) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < nch; i += blockDim.x) iprm[i + (size_t)nch * is] = ipt[i] + 1;
+    }
+}
+
 }  // namespace
 }  // namespace bsrg
+
+extern "C" int bsrg_channel_weights(bsrg_ctx *c, int nch, const int *ipsol, int khm, const double *a, double *wt,
+                                    int *isol, int *iprm)
+{
+    using namespace bsrg;
+    if (!c || !ipsol || !a || !wt || !isol || nch < 1 || khm < 1 || ipsol[0] != 0 || ipsol[nch] != khm) {
+        set_error("bsrg_channel_weights: bad arguments");
+        return BSRG_ERR_ARG;
+    }
+    for (int i = 0; i < nch; i++)
+        if (ipsol[i + 1] < ipsol[i]) {
+            set_error("bsrg_channel_weights: ipsol decreases at channel %d", i + 1);
+            return BSRG_ERR_ARG;
+        }
+    const size_t shm = sizeof(double) * (CW_CHUNK + (size_t)nch) + sizeof(int) * (size_t)nch;
+    int dev_max = 0;
+    cudaSetDevice(c->device);
+    cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    if (shm > (size_t)dev_max) {
+        set_error("bsrg_channel_weights: nch=%d needs %zu B of shared memory (limit %d)", nch, shm, dev_max);
+        return BSRG_ERR_ARG;
+    }
+    cudaStream_t s = c->stream;
+    cudaError_t e;
+    int rc = ctx_reserve(c, sizeof(int) * (nch + 1) + 256);
+    if (rc != BSRG_OK) return rc;
+    if ((rc = ctx_reserve_pinned(c, sizeof(int) * (nch + 1))) != BSRG_OK) return rc;
+    if ((e = cudaEventSynchronize(c->ev_stage)) != cudaSuccess) return cuda_fail(e, "channel_weights staging");
+    std::memcpy(c->pinned, ipsol, sizeof(int) * (nch + 1));
+    int *d_ip = (int *)c->ws;
+    if ((e = cudaMemcpyAsync(d_ip, c->pinned, sizeof(int) * (nch + 1), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return cuda_fail(e, "channel_weights upload");
+    cudaEventRecord(c->ev_stage, s);
+    if (shm > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(channel_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm)) !=
+            cudaSuccess)
+        return cuda_fail(e, "channel_weights smem");
+    channel_weights_kernel<<<khm, 128, shm, s>>>(nch, d_ip, khm, a, wt, isol, iprm);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "channel_weights");
+    return BSRG_OK;
+}
 
 extern "C" int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const double *P, const int *ort_ptr,
                             const int *ort_idx, double *hcc)

@@ -262,6 +262,17 @@ int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const doub
  *      channel i owns rows ipsol[i] .. ipsol[i+1]-1 of the eigenvectors. */
 int bsrg_diag_hd_ipsol(bsrg_ctx *c, int nch, int *ipsol);
 
+/* ---- src/bsr/BSR_HD3/w_out.f90:58-76 (W_OUT, the weights behind w.nnn and
+ *      b_out.f90's bound-state selection): for every solution is,
+ *      wt(ich, is) = sum_{j in channel ich} a(j, is)^2 in row order (device,
+ *      nch x khm), iprm(:, is) the channels ordered by SORTA
+ *      (libs/ZCOM/sorting_routines.f90:79-97; 1-based; device, nch x khm, may be
+ *      NULL) and isol(is) = iprm(1, is), the dominant channel (device, khm).
+ *      a and ipsol (host) as for bsrg_rsol_out.  Perturbers (kcp > 0) are
+ *      outside this path. */
+int bsrg_channel_weights(bsrg_ctx *c, int nch, const int *ipsol, int khm, const double *a, double *wt, int *isol,
+                         int *iprm);
+
 /* ---- src/bsr/BSR_HD3/rsol_out.f90:20-36: solutions in the B-spline basis
  *      v(:, is) = sum_j a(j, is) bb(:, j) channel by channel (device,
  *      (nch*ns) x khm, may be NULL) and the surface amplitudes

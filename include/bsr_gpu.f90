@@ -19,6 +19,8 @@
 !       gpu_diag_hd             the eigen-solution of diag_hd for a
 !                               block-diagonal overlap (bsr/BSR_HD3/
 !                               diag_hd.f90:82-312)
+!       gpu_w_out_weights       W_OUT's channel weights, dominant channel
+!                               and SORTA order (bsr/BSR_HD3/w_out.f90:58-76)
 !
 !     Device memory is obtained from the CUDA runtime through its C
 !     interface (cudaMalloc / cudaMemcpy / cudaFree) bound below.
@@ -139,6 +141,15 @@
         Real(c_double), value :: edmax, egap
         Integer(c_int), intent(out) :: khm
         Integer(c_int) :: bsrg_diag_hd
+       End Function
+
+       Function bsrg_channel_weights(c, nch, ipsol, khm, a, wt, isol, iprm) &
+                bind(C, name="bsrg_channel_weights")
+        Import :: c_int, c_ptr
+        Type(c_ptr), value :: c, a, wt, isol, iprm
+        Integer(c_int), value :: nch, khm
+        Integer(c_int), intent(in) :: ipsol(*)
+        Integer(c_int) :: bsrg_channel_weights
        End Function
 
        Function cudaMalloc(p, bytes) bind(C, name="cudaMalloc")
@@ -346,5 +357,35 @@
       Call gpu_check(cudaFree(dH), 'cudaFree'); Call gpu_check(cudaFree(dE), 'cudaFree')
       Call gpu_check(cudaFree(dV), 'cudaFree')
       End Subroutine gpu_diag_hd
+
+!======================================================================
+      Subroutine gpu_w_out_weights(nch, ipsol, khm, a, WT, isol, iprm)
+!----------------------------------------------------------------------
+!     w_out.f90:58-76 for every solution: WT(ich,is) = SUM(a(rows of
+!     ich,is)**2), iprm(:,is) from SORTA, isol(is) = iprm(1,is)
+!----------------------------------------------------------------------
+      Integer, intent(in) :: nch, khm
+      Integer(c_int), intent(in) :: ipsol(0:nch)
+      Real(8), intent(in), target :: a(khm, khm)
+      Real(8), intent(out), target :: WT(nch, khm)
+      Integer(c_int), intent(out), target :: isol(khm), iprm(nch, khm)
+      Type(c_ptr) :: dA, dW, dI, dP
+      Integer(c_size_t) :: ba, bw, bi, bp
+      ba = int(khm, c_size_t) * khm * 8
+      bw = int(nch, c_size_t) * khm * 8
+      bi = int(khm, c_size_t) * 4
+      bp = int(nch, c_size_t) * khm * 4
+      Call gpu_check(cudaMalloc(dA, ba), 'cudaMalloc a')
+      Call gpu_check(cudaMalloc(dW, bw), 'cudaMalloc WT')
+      Call gpu_check(cudaMalloc(dI, bi), 'cudaMalloc isol')
+      Call gpu_check(cudaMalloc(dP, bp), 'cudaMalloc iprm')
+      Call gpu_check(cudaMemcpy(dA, c_loc(a), ba, cudaMemcpyHostToDevice), 'upload a')
+      Call gpu_check(bsrg_channel_weights(gpu_ctx, nch, ipsol, khm, dA, dW, dI, dP), 'w_out weights')
+      Call gpu_check(cudaMemcpy(c_loc(WT), dW, bw, cudaMemcpyDeviceToHost), 'download WT')
+      Call gpu_check(cudaMemcpy(c_loc(isol), dI, bi, cudaMemcpyDeviceToHost), 'download isol')
+      Call gpu_check(cudaMemcpy(c_loc(iprm), dP, bp, cudaMemcpyDeviceToHost), 'download iprm')
+      Call gpu_check(cudaFree(dA), 'cudaFree'); Call gpu_check(cudaFree(dW), 'cudaFree')
+      Call gpu_check(cudaFree(dI), 'cudaFree'); Call gpu_check(cudaFree(dP), 'cudaFree')
+      End Subroutine gpu_w_out_weights
 
       End Module bsr_gpu

@@ -1385,6 +1385,44 @@ void orc_rsol(int ns, int nch, const int *ipsol, const double *bb, int khm, cons
 }
 
 /* ------------------------------------------------------------------------ */
+/* W_OUT weights (w_out.f90:58-76): cval = a(:,is)^2, WT(ich) = SUM(cval over  */
+/* the channel's rows), SORTA (ZCOM/sorting_routines.f90:79-97) of |WT| into */
+/* iprm, isol = iprm(1).  wt, iprm: (nch, khm); iprm/isol 1-based.           */
+/* ------------------------------------------------------------------------ */
+void orc_channel_weights(int nch, const int *ipsol, int khm, const double *a, double *wt, int *isol, int *iprm)
+{
+    int *ipt = (int *)malloc(sizeof(int) * (size_t)nch);
+    for (int is = 0; is < khm; is++) {
+        const double *col = a + (size_t)khm * is;
+        double *w = wt + (size_t)nch * is;
+        for (int ich = 0; ich < nch; ich++) {
+            double s = 0.0;
+            for (int j = ipsol[ich]; j < ipsol[ich + 1]; j++) {
+                double cv = col[j] * col[j];
+                s = s + cv;
+            }
+            w[ich] = s;
+        }
+        for (int i = 0; i < nch; i++) ipt[i] = i;
+        for (int i1 = 0; i1 < nch - 1; i1++) {
+            int j1 = ipt[i1];
+            for (int i2 = i1 + 1; i2 < nch; i2++) {
+                int j2 = ipt[i2];
+                if (fabs(w[j1]) < fabs(w[j2])) {
+                    ipt[i2] = j1;
+                    j1 = j2;
+                }
+            }
+            ipt[i1] = j1;
+        }
+        isol[is] = ipt[0] + 1;
+        if (iprm)
+            for (int i = 0; i < nch; i++) iprm[i + (size_t)nch * is] = ipt[i] + 1;
+    }
+    free(ipt);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Breit-Pauli N^k tables: nk_moments.f90:2-189 (moments k and -(k+3),       */
 /* nk_pdiag :56 with the scaling law rkd(iv) = rkd(iv-1)/(1+h), nk_triang    */
 /* :105 -- the one-sided diagonal cell r2 < r1, not symmetrised) and         */

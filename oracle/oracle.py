@@ -77,6 +77,7 @@ def lib():
         L.orc_nk.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _D, _D, _D]
         L.orc_bs_orth.argtypes = [ctypes.c_int, ctypes.c_int, _D, ctypes.c_int, _D, _I, _I, _D]
         L.orc_rsol.argtypes = [ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int, _D, _D, _D]
+        L.orc_channel_weights.argtypes = [ctypes.c_int, _I, ctypes.c_int, _D, _D, _I, _I]
         _LIB = L
     return _LIB
 
@@ -464,6 +465,19 @@ def rsol(ns, nch, ipsol, bb, a, want_v=True):
     lib().orc_rsol(ns, nch, _pi(ipsol), bbf.ctypes.data_as(_D), khm, af.ctypes.data_as(_D),
                    v.ctypes.data_as(_D) if want_v else None, w.ctypes.data_as(_D))
     return v, w
+
+
+def channel_weights(ipsol, a):
+    """W_OUT (w_out.f90:58-76): wt (nch, khm), isol (khm,), iprm (nch, khm), 1-based."""
+    ipsol = np.ascontiguousarray(ipsol, dtype=np.int32)
+    nch, khm = len(ipsol) - 1, int(ipsol[-1])
+    af = np.asfortranarray(a, dtype=np.float64)
+    wt = np.zeros((nch, khm), order="F")
+    isol = np.zeros(khm, dtype=np.int32)
+    iprm = np.zeros((nch, khm), dtype=np.int32, order="F")
+    lib().orc_channel_weights(nch, _pi(ipsol), khm, af.ctypes.data_as(_D), wt.ctypes.data_as(_D), _pi(isol),
+                              _pi(iprm))
+    return wt, isol, iprm
 
 
 def nk(ns, ks, rkb, pi1, pj1, pi2, pj2):

@@ -141,3 +141,79 @@ def test_h_and_rsol_files(solved, tmp_path):
     hout_io.write_rsol(q, ns, nch, ev, v)
     r = hout_io.read_rsol(q)
     assert r["nhm"] == nch * ns and np.array_equal(r["v"], v) and np.array_equal(r["eval"], ev)
+
+
+def test_channel_weights_matches_oracle(solved):
+    """W_OUT's weights, dominant channel and SORTA order from the device
+    eigenvectors equal the oracle's bit for bit."""
+    import bsr_b200 as bsr
+    pw, gb, ctx, H, res = solved
+    wt, isol, iprm = bsr.channel_weights(ctx, res["ipsol"], res["vectors"])
+    wr, ir, pr = O.channel_weights(res["ipsol"], to_np(res["vectors"]))
+    assert np.array_equal(to_np(wt), wr)
+    assert np.array_equal(to_np(isol), ir) and np.array_equal(to_np(iprm), pr)
+    # the weights of an S-orthonormal solution in the orthonormal channel basis sum to 1
+    assert np.max(np.abs(wr.sum(axis=0) - 1.0)) < 1e-12
+
+
+def test_channel_weights_chunks_and_many_channels():
+    """khm above one shared-memory chunk (2048 rows), more channels than threads
+    per block, empty channels: still the oracle's values bit for bit."""
+    import torch
+
+    import bsr_b200 as bsr
+    rng = np.random.default_rng(21)
+    nch = 150
+    sizes = rng.integers(0, 36, nch)
+    sizes[[3, 77, 149]] = 0
+    ipsol = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    khm = int(ipsol[-1])
+    assert khm > 2048
+    a = np.asfortranarray(rng.standard_normal((khm, khm)))
+    ctx = bsr.Context()
+    wt, isol, iprm = bsr.channel_weights(ctx, ipsol, torch.from_numpy(a).cuda().t().contiguous().t())
+    wr, ir, pr = O.channel_weights(ipsol, a)
+    assert np.array_equal(to_np(wt), wr)
+    assert np.array_equal(to_np(isol), ir) and np.array_equal(to_np(iprm), pr)
+    _, isol2, none = bsr.channel_weights(ctx, ipsol, torch.from_numpy(a).cuda().t().contiguous().t(),
+                                         want_iprm=False)
+    assert none is None and np.array_equal(to_np(isol2), ir)
+
+
+def test_channel_weights_rejects_bad_offsets():
+    import torch
+
+    import bsr_b200 as bsr
+    ctx = bsr.Context()
+    a = torch.zeros((6, 6), dtype=torch.float64, device="cuda")
+    with pytest.raises(bsr.BsrgError):
+        bsr.channel_weights(ctx, np.array([0, 4, 3, 6], np.int32), a)
+
+
+def test_bound_and_w_files_from_device(solved, tmp_path):
+    """b_out.f90's bound.nnn from the device solutions: the states below Emax,
+    their energies and B-spline vectors read back to the precision of the format."""
+    import bsr_b200 as bsr
+    from bsr_b200 import hout_io
+    pw, gb, ctx, H, res = solved
+    ns, nch = gb.ns, pw["nch"]
+    v, _ = bsr.rsol_out(ctx, ns, res["ipsol"], res["bb"], res["vectors"])
+    wt, isol, iprm = bsr.channel_weights(ctx, res["ipsol"], res["vectors"])
+    ev, v, isol, wt, iprm = to_np(res["eval"]), to_np(v), to_np(isol), to_np(wt), to_np(iprm)
+    iptar = [1 + (i % 2) for i in range(nch)]
+    etarg = [float(ev[0]) + 0.5, float(ev[0]) + 1.0]
+    emax = float(ev[len(ev) // 3])
+    pb, pu = tmp_path / "bound.001", tmp_path / "ubound.001"
+    nb = hout_io.write_bound(pb, pu, ns, ev, v, isol, iptar, etarg, nz=int(pw["z"]), nelc=int(pw["z"]) - 1, lpar=1,
+                             ispar=1, ipar=1, emax=emax, msol=0, iub=-1)
+    keep, eb, effn, _ = hout_io.bound_states(ev, isol, iptar, etarg, int(pw["z"]), int(pw["z"]) - 1, emax, 0)
+    r = hout_io.read_bound(pb)
+    assert nb == r["nbound"] == int(keep.sum()) == int(np.sum(ev <= emax))
+    for st, i in zip(r["states"], np.nonzero(keep)[0]):
+        assert abs(st["eval"] - ev[i]) <= 5e-10 * abs(ev[i])
+        scale = np.max(np.abs(v[:, i]))
+        assert np.max(np.abs(st["v"] - v[:, i])) <= 5e-8 * scale
+    pw_ = tmp_path / "w.001"
+    hout_io.write_w(pw_, wt, isol, ev, np.zeros_like(iprm), [""] * len(ev), iprm)
+    w = hout_io.read_w(pw_)
+    assert np.array_equal(w["wt"], wt) and np.array_equal(w["isol"], isol)

@@ -82,3 +82,25 @@ def test_rsol_amplitudes():
         blockv = bb[:, ich * ns: ich * ns + m] @ a[ipsol[ich]: ipsol[ich + 1], :]
         assert np.allclose(v[ich * ns:(ich + 1) * ns], blockv, rtol=0, atol=1e-12)
         assert np.allclose(w[ich], blockv[-1], rtol=0, atol=1e-12)
+
+
+def test_channel_weights_restatement():
+    """W_OUT's weights (w_out.f90:58-76): sums of squares per channel, SORTA's
+    descending order with ties kept in channel order, empty channels weigh 0."""
+    rng = np.random.default_rng(11)
+    ipsol = np.array([0, 5, 5, 9, 14, 20], np.int32)
+    a = rng.standard_normal((20, 20))
+    a[:, 3] = 0.1
+    a[0:4, 3] = 1.0
+    a[4, 3] = 0.0
+    a[5:9, 3] = 1.0                     # channels 1 and 3 tie for the largest weight in solution 4
+    wt, isol, iprm = O.channel_weights(ipsol, a)
+    for s in range(20):
+        ref = [sum(a[j, s] * a[j, s] for j in range(ipsol[i], ipsol[i + 1])) for i in range(5)]
+        assert list(wt[:, s]) == ref
+        order = sorted(range(5), key=lambda i: -ref[i])
+        assert ref[iprm[0, s] - 1] == max(ref) and isol[s] == iprm[0, s]
+        assert [ref[i - 1] for i in iprm[:, s]] == [ref[i] for i in order]
+    assert wt[1].max() == 0.0
+    assert wt[0, 3] == wt[2, 3] == max(wt[:, 3])
+    assert isol[3] == 1 and list(iprm[:2, 3]) == [1, 3]
