@@ -285,9 +285,9 @@ __global__ void direct_update_kernel(int ns, int ks, int ng, const GroupDesc *__
 // bounds tests.  Values equal mrk_cell's (mrk_cell.f90:2): the cells of two
 // disjoint interval ranges factorise, sum_iv sum_jv rkd1(iv) rkd2(jv) =
 // M1(i,ip) M2(j,jp) with the band moments M1 = <B_i|r^k|B_i'>, M2 =
-// <B_i|r^-(k+1)|B_i'>; only pairs whose interval ranges overlap (|i-j| < ks)
-// sum cell by cell.  All terms are positive, so the regrouping changes the
-// result by a few ulp at most.
+// <B_i|r^-(k+1)|B_i'>; pairs whose interval ranges overlap (|i-j| < ks) keep
+// the diagonal cells and factorise the rest with running sums over iv.  All
+// terms are positive, so the regrouping changes the result by a few ulp at most.
 // ---------------------------------------------------------------------------
 // M1(i,ip) = sum over cells of rkd1, M2 likewise (ascending interval order)
 __global__ void band_moment_kernel(int ks, int ns, int nv, const double *__restrict__ rkd1,
@@ -311,39 +311,98 @@ __global__ void band_moment_kernel(int ks, int ns, int nv, const double *__restr
     M2[tid] = b;
 }
 
+constexpr int PAD_TI = 32, PAD_TJ = 32, PAD_JT = PAD_TJ / 8;      // block tile, columns per thread
+
+template <int KS>
 __global__ void __launch_bounds__(256)
-rkb_pad_kernel(int ks, int ns, int nv, PadLayout L, const double *__restrict__ rkd1, const double *__restrict__ rkd2,
+rkb_pad_kernel(int ns, int nv, PadLayout L, const double *__restrict__ rkd1, const double *__restrict__ rkd2,
                const double *__restrict__ rkd, const double *__restrict__ M1, const double *__restrict__ M2,
                double *__restrict__ rkbp)
 {
+    constexpr int ks = KS;
+    // the block's band moments (A: M1(i,ip), M2(i,ip) of its rows; B: M1(j,jp), M2(j,jp) of
+    // its columns) and, near the diagonal, its cell moments [ih][r] / [jh][c], iv = i - ih
+    __shared__ double A1[PAD_TI], A2[PAD_TI], B1[PAD_TJ], B2[PAD_TJ];
+    __shared__ double S1[KS][PAD_TI], S2[KS][PAD_TI], T1[KS][PAD_TJ], T2[KS][PAD_TJ];
     const int ipjp = blockIdx.z, ip = ipjp % ks, jp = ipjp / ks;
-    const int pr = blockIdx.x * 32 + threadIdx.x, pc = blockIdx.y * 8 + threadIdx.y;
-    if (pr >= L.NP || pc >= L.NP) return;
-    const int i = pr - L.PL, j = pc - L.PL;
-    double v = 0.0;
-    if (i >= 0 && j >= 0 && i + ip < ns && j + jp < ns) {
-        int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
-        int iv_hi = i < nv - 1 ? i : nv - 1;
-        int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
-        int jv_hi = j < nv - 1 ? j : nv - 1;
-        if (iv_hi < jv_lo) v = M1[i + (size_t)ns * ip] * M2[j + (size_t)ns * jp];
-        else if (jv_hi < iv_lo) v = M1[j + (size_t)ns * jp] * M2[i + (size_t)ns * ip];
-        else {
-            const int ik = ks * (ks + 1) / 2;
-            for (int jv = jv_lo; jv <= jv_hi; jv++) {
-                int jh = j - jv, jj = jh * ks - jh * (jh - 1) / 2 + jp;
-                for (int iv = iv_lo; iv <= iv_hi; iv++) {
-                    int ih = i - iv, ii = ih * ks - ih * (ih - 1) / 2 + ip;
-                    double c;
-                    if (iv < jv) c = rkd1[ii + (size_t)ik * iv] * rkd2[jj + (size_t)ik * jv];
-                    else if (iv > jv) c = rkd1[jj + (size_t)ik * jv] * rkd2[ii + (size_t)ik * iv];
-                    else c = rkd[ii + (size_t)ik * (jj + (size_t)ik * iv)];
-                    v += c;
+    constexpr int ik = KS * (KS + 1) / 2;
+    const int i0 = (int)blockIdx.x * PAD_TI - L.PL, j0 = (int)blockIdx.y * PAD_TJ - L.PL;
+    const int t = threadIdx.x + 32 * threadIdx.y;
+    if (t < PAD_TI) {
+        const int i = i0 + t;
+        const bool ok = i >= 0 && i + ip < ns;
+        A1[t] = ok ? M1[i + (size_t)ns * ip] : 0.0;
+        A2[t] = ok ? M2[i + (size_t)ns * ip] : 0.0;
+    } else if (t < PAD_TI + PAD_TJ) {
+        const int j = j0 + t - PAD_TI;
+        const bool ok = j >= 0 && j + jp < ns;
+        B1[t - PAD_TI] = ok ? M1[j + (size_t)ns * jp] : 0.0;
+        B2[t - PAD_TI] = ok ? M2[j + (size_t)ns * jp] : 0.0;
+    }
+    // overlapping interval ranges need |i - j| < ks; a block with none skips the staging
+    const bool near = !(i0 > j0 + PAD_TJ - 1 + ks - 1 || j0 > i0 + PAD_TI - 1 + ks - 1);
+    if (near) {
+        for (int q = t; q < ks * PAD_TI; q += 256) {
+            const int ih = q / PAD_TI, r = q % PAD_TI, i = i0 + r, iv = i - ih;
+            const bool ok = i >= 0 && i < ns && iv >= 0 && iv < nv && ih + ip < ks;
+            const int idx = ih * ks - ih * (ih - 1) / 2 + ip + ik * iv;
+            S1[ih][r] = ok ? rkd1[idx] : 0.0;
+            S2[ih][r] = ok ? rkd2[idx] : 0.0;
+        }
+        for (int q = t; q < ks * PAD_TJ; q += 256) {
+            const int jh = q / PAD_TJ, c = q % PAD_TJ, j = j0 + c, jv = j - jh;
+            const bool ok = j >= 0 && j < ns && jv >= 0 && jv < nv && jh + jp < ks;
+            const int idx = jh * ks - jh * (jh - 1) / 2 + jp + ik * jv;
+            T1[jh][c] = ok ? rkd1[idx] : 0.0;
+            T2[jh][c] = ok ? rkd2[idx] : 0.0;
+        }
+    }
+    __syncthreads();
+    const int r = threadIdx.x, pr = blockIdx.x * PAD_TI + r, i = pr - L.PL;
+    if (pr >= L.NP) return;
+    const bool irow = i >= 0 && i + ip < ns;
+    int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
+    const int iv_hi = i < nv - 1 ? i : nv - 1;
+    double *out = rkbp + (size_t)pr + L.slice * ipjp;
+#pragma unroll
+    for (int u = 0; u < PAD_JT; u++) {
+        const int c = threadIdx.y + 8 * u, pc = blockIdx.y * PAD_TJ + c, j = pc - L.PL;
+        if (pc >= L.NP) break;
+        double v = 0.0;
+        if (irow && j >= 0 && j + jp < ns) {
+            int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+            const int jv_hi = j < nv - 1 ? j : nv - 1;
+            if (iv_hi < jv_lo) v = A1[r] * B2[c];
+            else if (jv_hi < iv_lo) v = B1[c] * A2[r];
+            else {
+                // overlapping interval ranges: sum over the cells jv both ranges share of
+                // rkd(ii,jj,jv), then sum_jv [ rkd2(jj,jv) sum_{iv<jv} rkd1(ii,iv) +
+                // rkd1(jj,jv) sum_{iv>jv} rkd2(ii,iv) ], the iv sums running (ascending for
+                // iv < jv, descending for iv > jv)
+                // the diagonal cells first: independent loads, unrolled so they overlap
+                const int ov_lo = iv_lo > jv_lo ? iv_lo : jv_lo, ov_hi = iv_hi < jv_hi ? iv_hi : jv_hi;
+#pragma unroll 4
+                for (int jv = ov_lo; jv <= ov_hi; jv++) {
+                    const int ih = i - jv, jh = j - jv;
+                    v += __ldg(rkd + ih * ks - ih * (ih - 1) / 2 + ip +
+                               (size_t)ik * (jh * ks - jh * (jh - 1) / 2 + jp + (size_t)ik * jv));
+                }
+                double lo_sum = 0.0;               // sum of rkd1(ii,iv) over iv < jv
+                int ivn = iv_lo;
+                for (int jv = jv_lo; jv <= jv_hi; jv++) {
+                    for (; ivn < jv && ivn <= iv_hi; ivn++) lo_sum += S1[i - ivn][r];
+                    v += lo_sum * T2[j - jv][c];
+                }
+                double hi_sum = 0.0;               // sum of rkd2(ii,iv) over iv > jv
+                ivn = iv_hi;
+                for (int jv = jv_hi; jv >= jv_lo; jv--) {
+                    for (; ivn > jv && ivn >= iv_lo; ivn--) hi_sum += S2[i - ivn][r];
+                    v += hi_sum * T1[j - jv][c];
                 }
             }
         }
+        out[(size_t)L.NP * pc] = v;
     }
-    rkbp[(size_t)pr + (size_t)L.NP * pc + L.slice * ipjp] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -566,10 +625,13 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
         int g = q / XCH, xi = q % XCH, x = x0 + xi;
         if (x >= ns) continue;
         GroupDesc G = gd[g];
+        double *dst = hcc + (size_t)G.blk * nn + x + (size_t)ns * yp;
+        const double old = *dst;            // issued before the term loop so its latency overlaps it
         const double *Z = Zs + xi * ZXS;
         double acc = 0.0;
+#pragma unroll 4
         for (int t = G.start; t < G.end; t++) acc = fma(cv[t], Z[zoff[t]], acc);
-        hcc[(size_t)G.blk * nn + x + (size_t)ns * yp] += acc;
+        *dst = old + acc;
     }
 }
 
@@ -610,6 +672,31 @@ static exchange_factored_fn exchange_factored_for(int ks)
     }
 }
 
+typedef void (*rkb_pad_fn)(int, int, PadLayout, const double *, const double *, const double *, const double *,
+                           const double *, double *);
+
+static rkb_pad_fn rkb_pad_for(int ks)
+{
+    switch (ks) {
+    case 2: return rkb_pad_kernel<2>;
+    case 3: return rkb_pad_kernel<3>;
+    case 4: return rkb_pad_kernel<4>;
+    case 5: return rkb_pad_kernel<5>;
+    case 6: return rkb_pad_kernel<6>;
+    case 7: return rkb_pad_kernel<7>;
+    case 8: return rkb_pad_kernel<8>;
+    case 9: return rkb_pad_kernel<9>;
+    case 10: return rkb_pad_kernel<10>;
+    case 11: return rkb_pad_kernel<11>;
+    case 12: return rkb_pad_kernel<12>;
+    case 13: return rkb_pad_kernel<13>;
+    case 14: return rkb_pad_kernel<14>;
+    case 15: return rkb_pad_kernel<15>;
+    case 16: return rkb_pad_kernel<16>;
+    default: return nullptr;
+    }
+}
+
 // band moments + zero-margined R^k table of multipole k (from its cell moments)
 static int build_padded_table(const bsrg_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
                               double *M1, double *M2, double *rkbp, cudaStream_t s)
@@ -617,8 +704,13 @@ static int build_padded_table(const bsrg_basis *b, int k, const double *rkd1, co
     const int ns = b->ns, ks = b->ks, nv = b->nv;
     const PadLayout PL = pad_layout(ns, ks);
     band_moment_kernel<<<(ns * ks + 127) / 128, 128, 0, s>>>(ks, ns, nv, rkd1, rkd2, M1, M2);
-    dim3 gp((PL.NP + 31) / 32, (PL.NP + 7) / 8, ks * ks);
-    rkb_pad_kernel<<<gp, dim3(32, 8), 0, s>>>(ks, ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
+    dim3 gp((PL.NP + PAD_TI - 1) / PAD_TI, (PL.NP + PAD_TJ - 1) / PAD_TJ, ks * ks);
+    rkb_pad_fn fn = rkb_pad_for(ks);
+    if (!fn) {
+        set_error("R^k table: ks=%d outside the compiled range 2..%d", ks, BSRG_MAXKS);
+        return BSRG_ERR_ARG;
+    }
+    fn<<<gp, dim3(32, 8), 0, s>>>(ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
     (void)k;
     return cuda_fail(cudaGetLastError(), "R^k table");
 }

@@ -257,6 +257,7 @@ __global__ void diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, 
     double *wx = bt + ks * ks * ks;           // [m][i]   : weights * x^k at inner points
     double *INT = wx + ks * ks;               // [m][jj]  : ks*ik
     double *a = INT + ks * ik;                // [jj][ii] : ik*ik  (column-major a(ii,jj))
+    double *BI = a + ik * ik;                 // [ii][m]  : ik*ks  bsp(i)*bsp(ip)*grw*grm^(k+1)
     int iv_out = blockIdx.x;
     int iv1 = iv_out + 1;
     int s0 = ml + ks, s1 = ml + me - ks + 2;
@@ -295,20 +296,24 @@ __global__ void diag_cell_kernel(int ks, int nv, int ml, int me, double hscale, 
         INT[m * ik + jj] = s;
     }
     __syncthreads();
-    // a(ii,jj) = SUM_m bi(m) * INT(jj,m), bi = bsp(i)*bsp(ip)*grw*grm^(k+1)
-    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
-        int ii = q % ik, jj = q / ik;
+    // bi(ii,m) = bsp(i)*bsp(ip)*grw*grm^(k+1), once per cell
+    for (int q = threadIdx.x; q < ik * ks; q += blockDim.x) {
+        int ii = q / ks, m = q % ks;
         int i = 0, rem = ii;
         while (rem >= ks - i) { rem -= ks - i; i++; }
         int ip = i + rem;
+        double g2;
+        if (k != 0) g2 = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], k + 1);
+        else g2 = grw[iv + (size_t)nv * m] * grm[iv + (size_t)nv * m];
+        BI[q] = bsp[iv + ld * (m + (size_t)ks * i)] * bsp[iv + ld * (m + (size_t)ks * ip)] * g2;
+    }
+    __syncthreads();
+    // a(ii,jj) = SUM_m bi(ii,m) * INT(jj,m)
+    for (int q = threadIdx.x; q < ik * ik; q += blockDim.x) {
+        int ii = q % ik, jj = q / ik;
+        const double *bi = BI + ii * ks;
         double s = 0.0;
-        for (int m = 0; m < ks; m++) {
-            double g2;
-            if (k != 0) g2 = grw[iv + (size_t)nv * m] * rpow_dev(grm[iv + (size_t)nv * m], k + 1);
-            else g2 = grw[iv + (size_t)nv * m] * grm[iv + (size_t)nv * m];
-            double bi = bsp[iv + ld * (m + (size_t)ks * i)] * bsp[iv + ld * (m + (size_t)ks * ip)] * g2;
-            s = s + bi * INT[m * ik + jj];
-        }
+        for (int m = 0; m < ks; m++) s = s + bi[m] * INT[m * ik + jj];
         a[ii + ik * jj] = s;
     }
     __syncthreads();
@@ -1008,7 +1013,7 @@ int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
         moments_kernel<<<(n + 127) / 128, 128, 0, s>>>(ks, nv, b->ml, b->me, ipow_host(q, -(k + 1)) * q,
                                                        -(k + 1), b->gr, b->grm, b->grw, b->bsp, rkd2);
     if (rkd) {
-        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik + (size_t)ik * ik);
+        size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + 2 * (size_t)ks * ik + (size_t)ik * ik);
         if (shm > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                  (int)shm);
