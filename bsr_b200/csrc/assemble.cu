@@ -566,6 +566,12 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
     const int yp = blockIdx.y;
     const int x0 = blockIdx.x * XCH;
     const int tid = threadIdx.x;
+    const size_t nn = (size_t)ns * ns;
+    // the XCH outputs of a group's block lie in one 32-byte sector when ns is a multiple
+    // of 4: pull them towards L2 now, so the update at the end finds them there
+    if (x0 < ns)
+        for (int g = tid; g < ng; g += 256)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(hcc + (size_t)gd[g].blk * nn + x0 + (size_t)ns * yp));
     // ---- stage p(y'+f), p(x0-HW+r) and the CTA's R values ----
     for (int q = tid; q < NE * NORB_MAX; q += 256) {
         int f = q / NORB_MAX - HW, b = q % NORB_MAX, y = yp + f;
@@ -620,7 +626,6 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
     __syncthreads();
     // ---- a_g(x, y') = sum_t c_t Z[xi][a_t][b_t]; UPDATE_HX 'x' ----
     // thread (g, xi): the XCH threads of a group read the same terms (broadcast)
-    const size_t nn = (size_t)ns * ns;
     for (int q = tid; q < ng * XCH; q += 256) {
         int g = q / XCH, xi = q % XCH, x = x0 + xi;
         if (x >= ns) continue;
@@ -905,6 +910,7 @@ int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
     c->events = new std::vector<bsrg_stage_event>();
     c->pool = new std::vector<cudaEvent_t>();
     c->last_ipsol = new std::vector<int>();
+    c->pw_knots = new std::vector<double>();
     *out = c;
     return BSRG_OK;
 }
@@ -922,6 +928,8 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
     delete c->pool;
     delete c->last_ipsol;
     if (c->pw_buf) cudaFree(c->pw_buf);
+    bsrg_basis_free(c->pw_basis);
+    delete c->pw_knots;
     cusolverDnDestroy(c->solver);
     cublasDestroy(c->blas);
     delete c;

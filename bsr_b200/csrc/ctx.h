@@ -41,6 +41,9 @@ struct bsrg_ctx {
     std::vector<int> *last_ipsol;            // channel solution offsets of the last diag_hd
     void *pw_buf;                            // device buffers of bsrg_partial_wave_solve (kept between calls)
     size_t pw_bytes;
+    bsrg_basis *pw_basis;                    // basis of the last bsrg_partial_wave_solve, reused while
+    std::vector<double> *pw_knots;           //   ks and the knots are unchanged
+    int pw_ks;
 };
 
 namespace bsrg {

@@ -605,9 +605,21 @@ extern "C" int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double
 {
     if (!c || !t || !P || !eval || !khm) { set_error("partial_wave_solve: null argument"); return BSRG_ERR_ARG; }
     cudaStream_t s = c->stream;
-    bsrg_basis *b = nullptr;
-    int rc = bsrg_define_spline(ks, ns, t, 0, 0, 0.0, s, &b);
-    if (rc != BSRG_OK) return rc;
+    // the basis is the module state of define_spline: partial waves on one knot grid share
+    // it, so it stays in the context until ks or a knot changes
+    int rc = BSRG_OK;
+    const bool same = c->pw_basis && c->pw_ks == ks && c->pw_knots->size() == (size_t)(ns + ks) &&
+                      std::memcmp(c->pw_knots->data(), t, sizeof(double) * (ns + ks)) == 0;
+    if (!same) {
+        cudaStreamSynchronize(s);
+        bsrg_basis_free(c->pw_basis);
+        c->pw_basis = nullptr;
+        c->pw_knots->clear();
+        if ((rc = bsrg_define_spline(ks, ns, t, 0, 0, 0.0, s, &c->pw_basis)) != BSRG_OK) return rc;
+        c->pw_knots->assign(t, t + ns + ks);
+        c->pw_ks = ks;
+    }
+    const bsrg_basis *b = c->pw_basis;
     size_t nn = (size_t)ns * ns, nblk = (size_t)nch * (nch + 1) / 2;
     const size_t nh = (size_t)nch * ns;
     // device buffers live in the context between calls (grown when a larger wave arrives)
@@ -627,10 +639,7 @@ extern "C" int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double
             rc = cuda_fail(e, "partial_wave_solve alloc");
         if (rc == BSRG_OK) c->pw_bytes = need;
     }
-    if (rc != BSRG_OK) {
-        bsrg_basis_free(b);
-        return rc;
-    }
+    if (rc != BSRG_OK) return rc;
     Arena ar{(char *)c->pw_buf, 0, c->pw_bytes};
     double *dP = ar.take<double>((size_t)ns * norb), *hcc = ar.take<double>(nn * nblk);
     double *dev_eval = ar.take<double>(nh);
@@ -647,6 +656,5 @@ extern "C" int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double
         rc = cuda_fail(e, "partial_wave_solve download");
     if (rc == BSRG_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "partial_wave_solve sync");
     cudaStreamSynchronize(s);
-    bsrg_basis_free(b);
     return rc;
 }

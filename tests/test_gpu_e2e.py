@@ -31,6 +31,28 @@ def test_repeatable():
     assert np.array_equal(a, b)
 
 
+def test_basis_kept_only_while_the_knots_match():
+    """The context keeps the last partial wave's basis; a wave on other knots (or
+    another ks) gets its own, and returning to the first grid gives the first result."""
+    import bsr_b200 as bsr
+    pw1 = W.partial_wave("config1", seed=7)
+    pw2 = dict(pw1)
+    t = np.array(pw1["t"], dtype=np.float64)
+    inner = slice(pw1["ks"], len(t) - pw1["ks"])
+    t[inner] = t[inner] * 0.97                   # same ns and ks, different interior knots
+    pw2["t"] = t
+    ctx = bsr.Context()
+    a = bsr.partial_wave_solve(ctx, pw1, want_vectors=False)
+    b = bsr.partial_wave_solve(ctx, pw2, want_vectors=False)
+    c = bsr.partial_wave_solve(ctx, pw1, want_vectors=False)
+    fresh = bsr.partial_wave_solve(bsr.Context(), pw2, want_vectors=False)
+    assert np.array_equal(a, c) and np.array_equal(b, fresh)
+    assert not np.array_equal(a, b)
+    pw3 = W.partial_wave("config4", seed=7, nch=5)    # ks 8, ns 150
+    d = bsr.partial_wave_solve(ctx, pw3, want_vectors=False)
+    assert np.array_equal(d, bsr.partial_wave_solve(bsr.Context(), pw3, want_vectors=False))
+
+
 def test_bsr_mat_file_round_trip(tmp_path):
     """GPU assembly -> bsr_mat.nnn (the reference's file) -> GPU diag_hd gives the same spectrum
     as solving the in-memory blocks: the file carries everything bsr_hd needs."""
