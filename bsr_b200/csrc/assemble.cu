@@ -263,18 +263,23 @@ __global__ void direct_table_kernel(int ns, int ks, const double *__restrict__ r
     R3[q] = rkbp[L.at(i, j, ip, jp, ks)];
 }
 
+// Thread (column c, offset o = row - c, |o| < ks): the band of column c is one
+// contiguous run of 2ks-1 doubles, so a warp's read-modify-writes share sectors.
+// Row c+o <= c holds the band element (i, i+ip) with i = c+o, ip = -o; row c+o > c
+// its mirror (i+ip, i) with i = c, ip = o (UPDATE_HX 's', both triangles).
 __global__ void direct_update_kernel(int ns, int ks, int ng, const GroupDesc *__restrict__ gd,
                                      const double *__restrict__ C, double *hcc)
 {
     const int g = blockIdx.y;
+    const int nb = 2 * ks - 1;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ng || q >= ns * ks) return;
-    const int i = q % ns, ip = q / ns;
-    if (i + ip >= ns) return;
-    const double v = C[q + (size_t)ns * ks * g];
+    if (g >= ng || q >= ns * nb) return;
+    const int c = q / nb, o = q % nb - (ks - 1), r = c + o;
+    if (r < 0 || r >= ns) return;
+    const int i = o <= 0 ? r : c, ip = o <= 0 ? -o : o;
+    const double v = C[i + (size_t)ns * ip + (size_t)ns * ks * g];
     double *blk = hcc + (size_t)gd[g].blk * ns * ns;
-    blk[i + (size_t)ns * (i + ip)] += v;
-    if (ip > 0) blk[(i + ip) + (size_t)ns * i] += v;
+    blk[r + (size_t)ns * c] += v;
 }
 
 // ---------------------------------------------------------------------------
@@ -550,11 +555,28 @@ constexpr int ZLD = NORB_MAX + 1;       // padded leading dimension of Z rows
 // different xi) read different shared-memory banks in the term loop
 constexpr int ZXS = NORB_MAX * ZLD + 1;
 
+// records (8-byte coefficient + 2-byte Z offset) that fit in the R and W tiles of a CTA
+__host__ __device__ constexpr int xf_term_cap(int ks)
+{
+    return (int)(sizeof(double) * ((size_t)XCH * (2 * ks - 1) * (2 * ks - 1) + (size_t)XCH * (2 * ks - 1) * NORB_MAX) /
+                 (sizeof(double) + sizeof(unsigned short)));
+}
+
+// The launch's groups in chunks whose records fit in the CTA's dead R/W area: a staged
+// chunk's coefficients and Z offsets are copied to shared memory once per CTA (one
+// coalesced pass) instead of every thread reading them through L1; a chunk holding one
+// group larger than the area is read from global memory.
+struct XChunk {
+    int g0, g1;       // groups [g0, g1) of the launch
+    int staged;
+};
+
 template <int KS>
 __global__ void __launch_bounds__(256)
 exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc *__restrict__ gd,
-                         const unsigned short *__restrict__ zoff, const double *__restrict__ cv,
-                         const double *__restrict__ P, const double *__restrict__ rkbp, double *hcc)
+                         const XChunk *__restrict__ chunks, int nchunk, const unsigned short *__restrict__ zoff,
+                         const double *__restrict__ cv, const double *__restrict__ P,
+                         const double *__restrict__ rkbp, double *hcc)
 {
     constexpr int HW = KS - 1, NE = 2 * KS - 1, PXR = XCH + 2 * HW;
     extern __shared__ double fsm[];
@@ -625,23 +647,44 @@ exchange_factored_kernel(int ns, int norb, int ng, PadLayout L, const GroupDesc 
     }
     __syncthreads();
     // ---- a_g(x, y') = sum_t c_t Z[xi][a_t][b_t]; UPDATE_HX 'x' ----
-    // thread (g, xi): the XCH threads of a group read the same terms (broadcast)
-    for (int q = tid; q < ng * XCH; q += 256) {
-        int g = q / XCH, xi = q % XCH, x = x0 + xi;
-        if (x >= ns) continue;
-        GroupDesc G = gd[g];
-        double *dst = hcc + (size_t)G.blk * nn + x + (size_t)ns * yp;
-        const double old = *dst;            // issued before the term loop so its latency overlaps it
-        const double *Z = Zs + xi * ZXS;
-        double acc = 0.0;
+    // thread (g, xi): the XCH threads of a group read the same terms (broadcast); the
+    // records of a staged chunk live in the R/W area, dead once Z is built
+    double *tcv = Rs;
+    unsigned short *tzo = (unsigned short *)(tcv + xf_term_cap(KS));
+    for (int ci = 0; ci < nchunk; ci++) {
+        const XChunk C = chunks[ci];
+        const int tb = gd[C.g0].start;
+        if (C.staged) {
+            const int te = gd[C.g1 - 1].end;
+            __syncthreads();                // the previous chunk's readers are done
+            for (int t = tb + tid; t < te; t += 256) {
+                tcv[t - tb] = cv[t];
+                tzo[t - tb] = zoff[t];
+            }
+            __syncthreads();
+        }
+        for (int q = tid; q < (C.g1 - C.g0) * XCH; q += 256) {
+            int g = C.g0 + q / XCH, xi = q % XCH, x = x0 + xi;
+            if (x >= ns) continue;
+            GroupDesc G = gd[g];
+            double *dst = hcc + (size_t)G.blk * nn + x + (size_t)ns * yp;
+            const double old = *dst;        // issued before the term loop so its latency overlaps it
+            const double *Z = Zs + xi * ZXS;
+            double acc = 0.0;
+            if (C.staged) {
 #pragma unroll 4
-        for (int t = G.start; t < G.end; t++) acc = fma(cv[t], Z[zoff[t]], acc);
-        *dst = old + acc;
+                for (int t = G.start - tb; t < G.end - tb; t++) acc = fma(tcv[t], Z[tzo[t]], acc);
+            } else {
+#pragma unroll 4
+                for (int t = G.start; t < G.end; t++) acc = fma(cv[t], Z[zoff[t]], acc);
+            }
+            *dst = old + acc;
+        }
     }
 }
 
-typedef void (*exchange_factored_fn)(int, int, int, PadLayout, const GroupDesc *, const unsigned short *,
-                                     const double *, const double *, const double *, double *);
+typedef void (*exchange_factored_fn)(int, int, int, PadLayout, const GroupDesc *, const XChunk *, int,
+                                     const unsigned short *, const double *, const double *, const double *, double *);
 
 // Z offset a*ZLD + b of every coefficient, so the term loop of the factored
 // kernel reads 10 bytes per term (all CTAs of a launch re-read the terms)
@@ -991,6 +1034,24 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         ngroups += dgroups[k].size() + xgroups[k].size();
         maxgd = std::max(maxgd, dgroups[k].size());
     }
+    // chunks of each multipole's exchange groups for the factored kernel's record staging
+    std::vector<std::vector<XChunk>> xchunks(kmax + 1);
+    size_t nchunks = 0;
+    {
+        const int cap = xf_term_cap(ks);
+        for (int k = 0; k <= kmax; k++) {
+            const std::vector<GroupDesc> &xg = xgroups[k];
+            int g = 0, nx = (int)xg.size();
+            while (g < nx) {
+                int g1 = g;
+                while (g1 < nx && xg[g1].end - xg[g].start <= cap) g1++;
+                if (g1 == g) xchunks[k].push_back(XChunk{g, g + 1, 0});
+                else xchunks[k].push_back(XChunk{g, g1, 1});
+                g = xchunks[k].back().g1;
+            }
+            nchunks += xchunks[k].size();
+        }
+    }
     // ---- workspace ----
     size_t nn = (size_t)ns * ns;
     size_t need = 0;
@@ -998,6 +1059,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     add(sizeof(int) * (size_t)ncoef * 2);
     add(sizeof(double) * (size_t)ncoef);
     add(sizeof(GroupDesc) * ngroups);
+    add(sizeof(XChunk) * std::max<size_t>(nchunks, 1));
     add(sizeof(int) * nch);
     add(sizeof(double) * nch);
     add(sizeof(double) * (size_t)ik * nv * 2);
@@ -1018,13 +1080,15 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) return rc;
     size_t host_bytes = sizeof(int) * (size_t)ncoef * 2 + sizeof(double) * (size_t)ncoef +
-                        sizeof(GroupDesc) * ngroups + sizeof(int) * nch + sizeof(double) * nch + 64;
+                        sizeof(GroupDesc) * ngroups + sizeof(XChunk) * nchunks + sizeof(int) * nch +
+                        sizeof(double) * nch + 64;
     rc = ctx_reserve_pinned(c, host_bytes);
     if (rc != BSRG_OK) return rc;
     Arena ar{(char *)c->ws, 0, c->ws_bytes};
     int *d_ca = ar.take<int>(ncoef), *d_cb = ar.take<int>(ncoef);
     double *d_cv = ar.take<double>(ncoef);
     GroupDesc *d_gd = ar.take<GroupDesc>(ngroups);
+    XChunk *d_xc = ar.take<XChunk>(std::max<size_t>(nchunks, 1));
     int *d_lch = ar.take<int>(nch);
     double *d_ech = ar.take<double>(nch);
     double *rkd1 = ar.take<double>((size_t)ik * nv), *rkd2 = ar.take<double>((size_t)ik * nv);
@@ -1050,6 +1114,12 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         xoff[k] = (o - o_gd) / sizeof(GroupDesc);
         stage(xgroups[k].data(), sizeof(GroupDesc) * xgroups[k].size());
     }
+    size_t o_xc = o;
+    std::vector<size_t> xcoff(kmax + 1);
+    for (int k = 0; k <= kmax; k++) {
+        xcoff[k] = (o - o_xc) / sizeof(XChunk);
+        stage(xchunks[k].data(), sizeof(XChunk) * xchunks[k].size());
+    }
     size_t o_lch = full ? stage(lch, sizeof(int) * nch) : 0, o_ech = full ? stage(ech, sizeof(double) * nch) : 0;
     cudaError_t e;
 #define CP(dst, off, bytes) \
@@ -1059,6 +1129,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     CP(d_cb, o_cb, sizeof(int) * ncoef);
     CP(d_cv, o_cv, sizeof(double) * ncoef);
     CP(d_gd, o_gd, sizeof(GroupDesc) * ngroups);
+    CP(d_xc, o_xc, sizeof(XChunk) * nchunks);
     if (full) {
         CP(d_lch, o_lch, sizeof(int) * nch);
         CP(d_ech, o_ech, sizeof(double) * nch);
@@ -1127,7 +1198,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
                     set_error("assemble: direct DGEMM failed (%d)", (int)bs);
                     return BSRG_ERR_SOLVER;
                 }
-                dim3 g4((unsigned)((nk + 127) / 128), nd);
+                dim3 g4((unsigned)(((size_t)ns * (2 * ks - 1) + 127) / 128), nd);
                 direct_update_kernel<<<g4, 128, 0, s>>>(ns, ks, nd, gdd, Cd, hcc);
             } else {
                 dim3 g2((ns + DG_TN - 1) / DG_TN, ks, (nd + DG_TM - 1) / DG_TM);
@@ -1145,7 +1216,8 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             stage_begin(c, 2);
             if (xf) {
                 dim3 g3((ns + XCH - 1) / XCH, ns);
-                xf<<<g3, 256, xfsm, s>>>(ns, norb, nx, PL, d_gd + xoff[k], d_zoff, d_cv, P, rkbk, hcc);
+                xf<<<g3, 256, xfsm, s>>>(ns, norb, nx, PL, d_gd + xoff[k], d_xc + xcoff[k], (int)xchunks[k].size(),
+                                         d_zoff, d_cv, P, rkbk, hcc);
             } else {
                 int tiles = ((ns + XTX - 1) / XTX) * ((ns + XTY - 1) / XTY);
                 dim3 g3(tiles, (nx + xg - 1) / xg);

@@ -293,7 +293,9 @@ int bsrg_dsytrd(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, do
 /* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
  *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.
  *      t (ns+ks), P (ns,norb), coefficient arrays as in bsrg_assemble, all
- *      host; eval (host) must hold nch*ns doubles. */
+ *      host; eval (host) must hold nch*ns doubles.  The context keeps the
+ *      basis built from t (define_spline's module state) and its device
+ *      buffers between calls; a call with the same ks and knots reuses them. */
 int bsrg_partial_wave_solve(bsrg_ctx *c, int ks, int ns, const double *t, double z, int nch,
                             const int *lch, const double *ech, int norb, const double *P, int kmax,
                             int ncoef, const int *ck, const int *ctype, const int *cich, const int *cjch,
