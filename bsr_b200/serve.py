@@ -220,26 +220,30 @@ def run_stream(server, symmetries, arrivals, want_vectors=True):
     return reqs
 
 
-def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=None):
+def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=None, margin=0.05):
     """Pick the worker-stream count with the highest solves/s on a sample batch.
 
-    make_server(n_streams) -> PartialWaveServer; sample: list of symmetries.
-    The choice is kept in `cache` (a dict, e.g. loaded from JSON) under `key`."""
+    make_server(n_streams) -> PartialWaveServer; sample: list of symmetries.  Each
+    candidate server first gets one request per worker, so every worker's context has
+    met the problem sizes before the timed run.  Extra streams gain little while the
+    dense eigensolve fills the GPU and a short sample's rates are noisy, so the fewest
+    streams whose rate is within `margin` of the best is chosen.  The choice is kept in
+    `cache` (a dict, e.g. loaded from JSON) under `key`."""
     if cache is not None and key in cache:
         return cache[key]["n_streams"]
-    best, best_rate, rates = None, -1.0, {}
+    rates = {}
     for n in candidates:
         srv = make_server(n)
         try:
-            run_stream(srv, sample[:1], [0.0], want_vectors=True)        # warm-up
+            warm = list(sample[:n]) or list(sample[:1])
+            run_stream(srv, warm, [0.0] * len(warm), want_vectors=True)
             srv.done.clear()
             reqs = run_stream(srv, sample, [0.0] * len(sample), want_vectors=True)
-            rate = srv.stats(reqs)["solves_per_s"]
+            rates[n] = srv.stats(reqs)["solves_per_s"]
         finally:
             srv.close()
-        rates[n] = rate
-        if rate > best_rate:
-            best, best_rate = n, rate
+    top = max(rates.values())
+    best = min(n for n in candidates if rates[n] >= top / (1.0 + margin))
     if cache is not None:
         cache[key] = {"n_streams": best, "solves_per_s": rates}
     return best

@@ -76,3 +76,42 @@ def test_request_bytes_numpy_ints():
     lch = np.arange(80, dtype=np.int32) % 7
     nb = serve.request_bytes(np.int32(80), np.int32(150), lch, 8)
     assert isinstance(nb, int) and nb > 3 * 11000 ** 2 * 8
+
+
+class _FakeServer:
+    def __init__(self, n, rate):
+        self.n, self.rate, self.done, self.warm, self.closed = n, rate, [], [], False
+
+    def stats(self, reqs):
+        return {"solves_per_s": self.rate}
+
+    def close(self):
+        self.closed = True
+
+
+def test_autotune_prefers_fewer_streams_within_margin(monkeypatch):
+    """The fewest streams within 5 % of the best rate win; every worker is warmed first;
+    the choice and the measured rates go to the cache."""
+    made = []
+
+    def fake_run(srv, syms, arrivals, want_vectors=True):
+        if not srv.warm:
+            srv.warm.append(len(syms))
+        return list(syms)
+
+    monkeypatch.setattr(serve, "run_stream", fake_run)
+    sample = list(range(8))
+    for rates, want in (({1: 10.0, 2: 10.3, 4: 9.0}, 1), ({1: 10.0, 2: 12.0, 4: 12.2}, 2),
+                        ({1: 10.0, 2: 10.0, 4: 13.0}, 4)):
+        made.clear()
+
+        def make(n, rates=rates):
+            made.append(_FakeServer(n, rates[n]))
+            return made[-1]
+
+        cache = {}
+        assert serve.autotune_streams(make, sample, candidates=(1, 2, 4), cache=cache, key="k") == want
+        assert [s.warm[0] for s in made] == [1, 2, 4] and all(s.closed for s in made)
+        assert cache["k"] == {"n_streams": want, "solves_per_s": rates}
+        assert serve.autotune_streams(make, sample, candidates=(1, 2, 4), cache=cache, key="k") == want
+        assert len(made) == 3                   # the cached choice runs nothing
