@@ -225,10 +225,11 @@ def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=
 
     make_server(n_streams) -> PartialWaveServer; sample: list of symmetries.  Each
     candidate server first gets one request per worker, so every worker's context has
-    met the problem sizes before the timed run.  Extra streams gain little while the
-    dense eigensolve fills the GPU and a short sample's rates are noisy, so the fewest
-    streams whose rate is within `margin` of the best is chosen.  The choice is kept in
-    `cache` (a dict, e.g. loaded from JSON) under `key`."""
+    met the problem sizes before the timed run.  A short sample's rates are noisy and
+    close together, while on a full batch more workers also overlap each other's host
+    work (record grouping, uploads, result reads), so the most streams whose rate is
+    within `margin` of the best is chosen.  The choice is kept in `cache` (a dict, e.g.
+    loaded from JSON) under `key`."""
     if cache is not None and key in cache:
         return cache[key]["n_streams"]
     rates = {}
@@ -243,7 +244,7 @@ def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=
         finally:
             srv.close()
     top = max(rates.values())
-    best = min(n for n in candidates if rates[n] >= top / (1.0 + margin))
+    best = max(n for n in candidates if rates[n] >= top / (1.0 + margin))
     if cache is not None:
         cache[key] = {"n_streams": best, "solves_per_s": rates}
     return best

@@ -89,8 +89,8 @@ class _FakeServer:
         self.closed = True
 
 
-def test_autotune_prefers_fewer_streams_within_margin(monkeypatch):
-    """The fewest streams within 5 % of the best rate win; every worker is warmed first;
+def test_autotune_prefers_more_streams_within_margin(monkeypatch):
+    """The most streams within 5 % of the best rate win; every worker is warmed first;
     the choice and the measured rates go to the cache."""
     made = []
 
@@ -101,8 +101,8 @@ def test_autotune_prefers_fewer_streams_within_margin(monkeypatch):
 
     monkeypatch.setattr(serve, "run_stream", fake_run)
     sample = list(range(8))
-    for rates, want in (({1: 10.0, 2: 10.3, 4: 9.0}, 1), ({1: 10.0, 2: 12.0, 4: 12.2}, 2),
-                        ({1: 10.0, 2: 10.0, 4: 13.0}, 4)):
+    for rates, want in (({1: 10.0, 2: 10.3, 4: 9.0}, 2), ({1: 12.5, 2: 11.0, 4: 9.0}, 1),
+                        ({1: 10.0, 2: 10.0, 4: 13.0}, 4), ({1: 9.7, 2: 9.9, 4: 9.95}, 4)):
         made.clear()
 
         def make(n, rates=rates):
