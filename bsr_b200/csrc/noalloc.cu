@@ -20,6 +20,12 @@
 // different host threads) race on it and must be serialised by the caller.
 // Nothing in the array has to start at zero: every moment the expansion reads
 // is written earlier in the same call.
+//
+// The call runs on the basis's device: if another device is current it is
+// switched to b->device for the call and switched back afterwards.  The
+// cached address belongs to the device's primary context; calls after a
+// cudaDeviceReset of that device (which tears the context down) are not
+// supported.
 #include <mutex>
 
 #include "bsrg_internal.h"
@@ -32,12 +38,11 @@ static const int kMaxDevices = 64;
 static double *g_scratch_ptr[kMaxDevices];
 static std::mutex g_scratch_mu;
 
-// device address of g_noalloc_scratch on the current device (set up once per device)
-static int scratch_address(double **out)
+// device address of g_noalloc_scratch on device `dev`, which must be current
+// (set up once per device)
+static int scratch_address(int dev, double **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return cuda_fail(e, "mrk_cell_noalloc: cudaGetDevice");
+    cudaError_t e;
     if (dev < 0 || dev >= kMaxDevices) {
         set_error("mrk_cell_noalloc: device %d beyond %d", dev, kMaxDevices);
         return BSRG_ERR_ARG;
@@ -71,11 +76,16 @@ extern "C" int bsrg_mrk_cell_noalloc(const bsrg_basis *b, int k, double *rkb, in
                   need, ik, b->nv, BSRG_NOALLOC_SCRATCH_DOUBLES);
         return BSRG_ERR_ARG;
     }
+    int cur = 0;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return cuda_fail(e, "mrk_cell_noalloc: cudaGetDevice");
+    if (cur != b->device && (e = cudaSetDevice(b->device)) != cudaSuccess)
+        return cuda_fail(e, "mrk_cell_noalloc: cudaSetDevice");
     double *scratch = nullptr;
-    int rc = scratch_address(&scratch);
-    if (rc != BSRG_OK) return rc;
+    int rc = scratch_address(b->device, &scratch);
     cudaStream_t s = (cudaStream_t)stream;
-    rc = launch_rk_moments(b, k, scratch, scratch + n1, scratch + 2 * n1, s);
-    if (rc != BSRG_OK) return rc;
-    return launch_mrk_cell(b, scratch, scratch + n1, scratch + 2 * n1, rkb, ldp, s);
+    if (rc == BSRG_OK) rc = launch_rk_moments(b, k, scratch, scratch + n1, scratch + 2 * n1, s);
+    if (rc == BSRG_OK) rc = launch_mrk_cell(b, scratch, scratch + n1, scratch + 2 * n1, rkb, ldp, s);
+    if (cur != b->device) cudaSetDevice(cur);
+    return rc;
 }

@@ -94,7 +94,9 @@ def run_sharded(symmetries, solve_fn, plan, group=None):
     if world == 1:
         return [mine[q] for q in range(len(symmetries))]
     gathered = [None] * world if rank == 0 else None
-    dist.gather_object(mine, gathered, dst=0, group=group)
+    # dst is a global rank: the group's rank 0 may not be global rank 0
+    dst = dist.get_global_rank(group, 0) if group is not None else 0
+    dist.gather_object(mine, gathered, dst=dst, group=group)
     if rank != 0:
         return None
     out = [None] * len(symmetries)

@@ -142,10 +142,13 @@ int bsrg_mqk_cell(const bsrg_basis *b, int k, double fine, double *rkb, int ldp,
  *      (BSRG_NOALLOC_SCRATCH_DOUBLES doubles = 6 MiB, held by every GPU that
  *      loads the library until exit), so the call allocates nothing.  Limit:
  *      (2*ik + ik*ik)*nv <= BSRG_NOALLOC_SCRATCH_DOUBLES with ik = ks(ks+1)/2
- *      (ks = 10: nv <= 250; ks = 8: nv <= 546); larger bases get BSRG_ERR_ARG.
+ *      (ks = 10: nv <= 250; ks = 8: nv <= 574); larger bases get BSRG_ERR_ARG.
  *      The first call on a device looks up the array's device address and
- *      should come before any stream capture on that device.  Calls share the
- *      array: calls that overlap on the GPU race and must be serialised. */
+ *      should come before any stream capture on that device; the call runs on
+ *      the basis's device (switched to and back if another is current), and
+ *      calls after a cudaDeviceReset of that device are not supported.  Calls
+ *      share the array: calls that overlap on the GPU race and must be
+ *      serialised. */
 #define BSRG_NOALLOC_SCRATCH_DOUBLES 786432
 int bsrg_mrk_cell_noalloc(const bsrg_basis *b, int k, double *rkb, int ldp, void *stream);
 

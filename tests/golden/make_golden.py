@@ -5,7 +5,8 @@ Reads, as text, the reference's B-spline known-answer harness
 Gauss-Legendre table of src/libs/BS/gauss.f90, and writes
 tests/golden/test_bs_golden.json.  Run from the repository root:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/jagot-bsr
+    BSR_REFERENCE=/path/to/jagot-bsr python tests/golden/make_golden.py
 
 The output is committed; tests never read the reference tree at run time.
 """
@@ -86,7 +87,9 @@ def parse_gauss_table(text, k):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BSR_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <jagot/bsr source tree> (or set BSR_REFERENCE)")
     tb = os.path.join(ref, "src/libs/BS/TEST_BS")
     read = lambda p: open(p).read()
     golden = {

@@ -40,6 +40,29 @@ def test_noalloc_matches_mrk_cell_twice():
         assert np.array_equal(a, b), k
 
 
+def test_noalloc_smaller_basis_after_larger():
+    """A smaller basis after a larger one: the shared array keeps the larger
+    call's moments in its tail, and none of them may leak into the result."""
+    import torch
+
+    import bsr_b200 as bsr
+    big = W.CONFIGS["config2"]
+    t, _ = W.knot_grid(big["ks"], big["ns"], big["rmin"], big["rmax"])
+    b1 = bsr.define_spline(t, big["ks"])
+    o1 = bsr.fortran_empty((b1.ns, b1.ns, b1.ks, b1.ks))
+    _call_noalloc(b1, 3, o1)
+    small = W.CONFIGS["config1"]
+    t2, _ = W.knot_grid(small["ks"], small["ns"], small["rmin"], small["rmax"])
+    b2 = bsr.define_spline(t2, small["ks"])
+    o2 = bsr.fortran_empty((b2.ns, b2.ns, b2.ks, b2.ks))
+    for k in (3, 1):
+        o2.fill_(float("nan"))
+        _call_noalloc(b2, k, o2)
+        ref = bsr.mrk_cell(b2, k)
+        torch.cuda.synchronize()
+        assert np.array_equal(o2.cpu().numpy(), ref.cpu().numpy()), k
+
+
 def test_noalloc_rejects_bases_beyond_the_scratch():
     import bsr_b200 as bsr
     t, _ = W.knot_grid(10, 320, 1e-3, 60.0)          # nv = 311 > 250 for ks = 10
