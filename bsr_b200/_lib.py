@@ -9,6 +9,7 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libbsrgpu.so")
 
+_c_long = ctypes.c_long
 _c_int, _c_double, _c_char, _c_void_p, _c_size_t = (ctypes.c_int, ctypes.c_double, ctypes.c_char,
                                                      ctypes.c_void_p, ctypes.c_size_t)
 _P = ctypes.c_void_p                      # device or host pointer
@@ -64,8 +65,13 @@ SIGNATURES = [
                               _c_int, _P, _IP, _P, _P]),
     ("bsrg_bs_orth", _c_int, [_P, _P, _c_int, _c_int, _P, _IP, _IP, _P]),
     ("bsrg_diag_hd_ipsol", _c_int, [_P, _c_int, _IP]),
+    ("bsrg_ctx_set_refine", _c_int, [_P, _c_int]),
+    ("bsrg_diag_hd_refine_stats", _c_int, [_P, _c_int, _P, _P]),
+    ("bsrg_dgemm", _c_int, [_c_char, _c_char, _c_int, _c_int, _c_int, _c_double, _P, _c_long, _c_long, _P,
+                            _c_long, _c_long, _c_double, _P, _c_long, _c_long, _c_int, _P]),
     ("bsrg_rsol_out", _c_int, [_P, _c_int, _c_int, _IP, _P, _c_int, _P, _P, _P]),
     ("bsrg_dsytrd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _P]),
+    ("bsrg_dstedc", _c_int, [_P, _c_int, _P, _P, _P, _P, _c_int]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),
 ]

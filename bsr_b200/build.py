@@ -25,6 +25,9 @@ UNITS = {
     "noalloc.cu": [],
     "eigen.cu": [],
     "post.cu": [],
+    "dgemm.cu": [],
+    "refine.cu": [],
+    "tridiag_dc.cu": [],
 }
 
 

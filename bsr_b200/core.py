@@ -324,7 +324,18 @@ class Context:
         self._tables = tables
 
     STAGES = ("rk_moments", "direct", "exchange", "one_electron", "channel_eig", "transform", "dense_eig",
-              "rk_expand")
+              "rk_expand", "refine")
+
+    def set_refine(self, on=True):
+        """FP64 Rayleigh-quotient refinement of diag_hd's eigenpairs (on by default)."""
+        call("bsrg_ctx_set_refine", self.handle, 1 if on else 0)
+
+    def refine_stats(self, n):
+        """(correction, residual norm) per eigenpair of the last refined diag_hd, as CUDA tensors."""
+        corr = torch.empty(n, device="cuda", dtype=torch.float64)
+        res = torch.empty(n, device="cuda", dtype=torch.float64)
+        call("bsrg_diag_hd_refine_stats", self.handle, n, _ptr(corr), _ptr(res))
+        return corr, res
 
     def set_timing(self, on=True):
         call("bsrg_ctx_set_timing", self.handle, 1 if on else 0)
@@ -434,6 +445,19 @@ def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0
     if want_bb:
         out["bb"] = bb
     return out
+
+
+def dgemm(A, B, transa="N", transb="N", alpha=1.0, beta=0.0, C=None):
+    """C = alpha op(A) op(B) + beta C on the FP64 tensor pipe (column-major CUDA tensors)."""
+    A, B = as_fortran(A), as_fortran(B)
+    m = A.shape[1] if transa == "T" else A.shape[0]
+    k = A.shape[0] if transa == "T" else A.shape[1]
+    n = B.shape[0] if transb == "T" else B.shape[1]
+    if C is None:
+        C = fortran_zeros((m, n))
+    call("bsrg_dgemm", transa.encode(), transb.encode(), m, n, k, float(alpha), _ptr(A), max(1, A.stride(1)), 0,
+         _ptr(B), max(1, B.stride(1)), 0, float(beta), _ptr(C), max(1, C.stride(1)), 0, 1, _stream())
+    return C
 
 
 def bs_orth(ctx, basis, P, ort_lists, hcc):

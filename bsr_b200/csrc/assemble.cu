@@ -954,6 +954,7 @@ int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
     c->pool = new std::vector<cudaEvent_t>();
     c->last_ipsol = new std::vector<int>();
     c->pw_knots = new std::vector<double>();
+    c->refine = 1;
     *out = c;
     return BSRG_OK;
 }
@@ -971,6 +972,7 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
     delete c->pool;
     delete c->last_ipsol;
     if (c->pw_buf) cudaFree(c->pw_buf);
+    if (c->rf_buf) cudaFree(c->rf_buf);
     bsrg_basis_free(c->pw_basis);
     delete c->pw_knots;
     cusolverDnDestroy(c->solver);

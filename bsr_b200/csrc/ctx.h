@@ -44,6 +44,10 @@ struct bsrg_ctx {
     bsrg_basis *pw_basis;                    // basis of the last bsrg_partial_wave_solve, reused while
     std::vector<double> *pw_knots;           //   ks and the knots are unchanged
     int pw_ks;
+    int refine;                              // FP64 refinement of the eigenpairs in diag_hd (default on)
+    double *rf_buf;                          // per-pair correction | residual of the last refined diag_hd
+    size_t rf_cap;                           //   (doubles held)
+    int rf_n;                                //   (pairs recorded)
 };
 
 namespace bsrg {
@@ -70,5 +74,17 @@ int ctx_reserve_pinned(bsrg_ctx *c, size_t bytes);
 void stage_begin(bsrg_ctx *c, int stage);
 void stage_end(bsrg_ctx *c, int stage, int launches = 1);
 int stage_collect(bsrg_ctx *c);   // waits for recorded events and accumulates
+
+// tridiagonal divide and conquer (tridiag_dc.cu)
+size_t dc_workspace_bytes(int n);
+size_t dc_pinned_bytes(int n);
+int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, double *Z, long ldz, void *ws_base,
+               size_t ws_bytes, void *pinned, size_t pinned_bytes);
+
+// eigenpair refinement (refine.cu)
+size_t refine_workspace_doubles(int n);
+int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s);
+int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *P, double *corr, double *resid,
+                 int *flag, cudaStream_t s);
 
 }  // namespace bsrg

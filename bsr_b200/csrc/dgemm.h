@@ -1,0 +1,24 @@
+// Host interface of the FP64 DMMA GEMM (dgemm.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace bsrg {
+
+// A uniform batch: item b multiplies A + b*sA (or Ap[b]) by B + b*sB (or Bp[b])
+// into C + b*sC (or Cp[b]); column-major, sizes of op(A) m x k, op(B) k x n.
+struct DgemmBatch {
+    int m, n, k;
+    const double *A; long lda, sA;
+    const double *B; long ldb, sB;
+    double *C; long ldc, sC;
+    const double *const *Ap;
+    const double *const *Bp;
+    double *const *Cp;
+    double alpha, beta;
+};
+
+int dgemm_batched(bool ta, bool tb, const DgemmBatch &p, int batch, cudaStream_t s);
+int dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, long lda, const double *B, long ldb,
+          double beta, double *C, long ldc, cudaStream_t s);
+
+}  // namespace bsrg

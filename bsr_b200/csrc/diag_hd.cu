@@ -9,14 +9,17 @@
 //   2. A = diag(bval) + bb_i^T H_ij bb_j for every stored off-diagonal block
 //      (:188-219);
 //   3. DSYEV('V','L') of A (:312, LAPACK_calls.f90:54).
-// Step 1 runs cuSOLVER's sygvd per channel, the filter and compaction run on
+// Step 1 runs batched cuSOLVER channel solves, the filter and compaction run on
 // the device (one small host read of the per-channel counts fixes khm), step 2
-// is two batched FP64 GEMMs over all blocks, step 3 is cuSOLVER's syevd.
+// is two batched FP64 tensor-core GEMMs over all blocks (dgemm.cu), step 3 is
+// cuSOLVER's syevd, followed by the FP64 Rayleigh-quotient refinement of every
+// eigenpair (refine.cu) when eigenvectors are computed.
 #include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include "ctx.h"
+#include "dgemm.h"
 
 namespace bsrg {
 
@@ -382,11 +385,18 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         nsolv[ich] = i2 - i1 + 1;
         if (nsolv[ich] < 1) { set_error("diag_hd: channel %d has no solutions", ich + 1); return BSRG_ERR_ARG; }
     }
-    int nb = nch * (nch - 1) / 2;
+    // The refined form (default with eigenvectors) also transforms the diagonal
+    // blocks, bb_i^T H_ii bb_i, instead of taking diag(bval): the two are equal in
+    // exact arithmetic (diag_hd.f90:188-219 stores diag(bval)), but explicitly
+    // formed blocks keep the channel solver's rounding (~eps ||H_ii||) out of
+    // the eigenvalues, which the Rayleigh quotients below then resolve.
+    const bool refine = want_vectors && c->refine;
     std::vector<BlockMap> bmap;
-    bmap.reserve(nb);
     for (int ic = 1; ic < nch; ic++)
         for (int jc = 0; jc < ic; jc++) bmap.push_back({ic, jc});
+    if (refine)
+        for (int ic = 0; ic < nch; ic++) bmap.push_back({ic, ic});
+    const int nb = (int)bmap.size();
     // ---- workspace: phase 1 ----
     size_t nn = (size_t)ns * ns;
     int lwork1 = 0;
@@ -424,6 +434,10 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     add(sizeof(double) * nn * std::max(nb, 1) * 2);   // Wt, T
     if (!vecs) add(sizeof(double) * (size_t)khm_max * khm_max);
     add(dws + 16);
+    if (refine) {
+        add(sizeof(double) * refine_workspace_doubles(khm_max));   // mirrored A, then the tile partial sums
+        add(sizeof(int) * 4);
+    }
     size_t batched_bytes = chan_batched_bytes(c, params, ns, s0v, nsolv);
     add(batched_bytes);
     int rc = ctx_reserve(c, need);
@@ -446,6 +460,8 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     double *Wt = ar.take<double>(nn * std::max(nb, 1)), *T = ar.take<double>(nn * std::max(nb, 1));
     double *Abuf = vecs ? nullptr : ar.take<double>((size_t)khm_max * khm_max);
     void *dwork = ar.take<char>(dws + 16);
+    double *Fsym = refine ? ar.take<double>(refine_workspace_doubles(khm_max)) : nullptr;
+    int *d_rflag = refine ? ar.take<int>(4) : nullptr;
     int *hi = (int *)c->pinned;
     std::memcpy(hi + o_s0, s0v.data(), sizeof(int) * nch);
     std::memcpy(hi + o_nsol, nsolv.data(), sizeof(int) * nch);
@@ -527,7 +543,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     double **h_ptrs = (double **)((char *)c->pinned + o_ptr_bytes);
     for (int q = 0; q < nb; q++) {
         const BlockMap &m = bmap[q];
-        h_ptrs[q] = (double *)(hcc + ((size_t)(m.ic + 1) * m.ic / 2 + m.jc) * nn);   // H_ij, i = ic+1 (1-based)
+        h_ptrs[q] = (double *)(hcc + ((size_t)(m.ic + 1) * m.ic / 2 + m.jc) * nn);   // H_ij, i = ic+1 (1-based), j <= i
         h_ptrs[nb + q] = BB + nn * m.jc;
         h_ptrs[2 * nb + q] = Wt + nn * q;
         h_ptrs[3 * nb + q] = BB + nn * m.ic;
@@ -552,26 +568,32 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         cusolverDnDestroyParams(params);
         return cuda_fail(e, "memset A");
     }
-    set_diag_kernel<<<(khm + 255) / 256, 256, 0, s>>>(khm, bval, A);
+    if (!refine) set_diag_kernel<<<(khm + 255) / 256, 256, 0, s>>>(khm, bval, A);
     if (nb > 0) {
-        const double one = 1.0, zero = 0.0;
         double **pH = d_ptrs, **pBj = d_ptrs + nb, **pW = d_ptrs + 2 * nb, **pBi = d_ptrs + 3 * nb,
                **pT = d_ptrs + 4 * nb;
-        cublasStatus_t bs1 = cublasDgemmBatched(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, ns, ns, ns, &one,
-                                                (const double *const *)pH, ns, (const double *const *)pBj, ns,
-                                                &zero, pW, ns, nb);
-        cublasStatus_t bs2 = cublasDgemmBatched(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, ns, ns, ns, &one,
-                                                (const double *const *)pBi, ns, (const double *const *)pW, ns,
-                                                &zero, pT, ns, nb);
-        if (bs1 != CUBLAS_STATUS_SUCCESS || bs2 != CUBLAS_STATUS_SUCCESS) {
-            cusolverDnDestroyParams(params);
-            set_error("diag_hd: block transform GEMM failed (%d, %d)", (int)bs1, (int)bs2);
-            return BSRG_ERR_SOLVER;
-        }
+        // W = H_ij bb_j, then T = bb_i^T W: two batched FP64 tensor-core GEMMs
+        DgemmBatch g1{};
+        g1.m = ns; g1.n = ns; g1.k = ns;
+        g1.lda = ns; g1.ldb = ns; g1.ldc = ns;
+        g1.Ap = (const double *const *)pH; g1.Bp = (const double *const *)pBj; g1.Cp = pW;
+        g1.alpha = 1.0; g1.beta = 0.0;
+        DgemmBatch g2 = g1;
+        g2.Ap = (const double *const *)pBi; g2.Bp = (const double *const *)pW; g2.Cp = pT;
+        int rg = dgemm_batched(false, false, g1, nb, s);
+        if (rg == BSRG_OK) rg = dgemm_batched(true, false, g2, nb, s);
+        if (rg != BSRG_OK) { cusolverDnDestroyParams(params); return rg; }
         dim3 g((unsigned)((nn + 127) / 128), nb);
         scatter_blocks_kernel<<<g, 128, 0, s>>>(ns, khm, d_bm, d_ipsol, T, A);
     }
-    stage_end(c, 5, nb > 0 ? 3 : 2);   // compact, set_diag, scatter (GEMMs are cuBLAS's)
+    stage_end(c, 5, (nb > 0 ? 4 : 1) + (refine ? 0 : 1));   // compact, [set_diag], 2 GEMMs, scatter
+    if (refine) {
+        // keep the full symmetric A for the residuals: the eigensolver overwrites A
+        stage_begin(c, 8);
+        int rr = refine_prepare(khm, A, khm, Fsym, s);
+        stage_end(c, 8, 1);
+        if (rr != BSRG_OK) { cusolverDnDestroyParams(params); return rr; }
+    }
     // ---- 3. eigensolve ----
     stage_begin(c, 6);
     cusolverStatus_t st = cusolverDnXsyevd(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm, CUDA_R_64F, A, khm,
@@ -582,6 +604,24 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     if (st != CUSOLVER_STATUS_SUCCESS) {
         set_error("diag_hd: syevd failed to launch (status %d)", (int)st);
         return BSRG_ERR_SOLVER;
+    }
+    if (refine) {
+        // ---- FP64 refinement of the eigenpairs (Rayleigh quotients) ----
+        if (c->rf_cap < 2 * (size_t)khm) {
+            if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diag_hd refine sync");
+            if (c->rf_buf) cudaFree(c->rf_buf);
+            c->rf_buf = nullptr;
+            c->rf_cap = 0;
+            if ((e = cudaMalloc(&c->rf_buf, sizeof(double) * 2 * (size_t)khm)) != cudaSuccess)
+                return cuda_fail(e, "diag_hd refine buffer");
+            c->rf_cap = 2 * (size_t)khm;
+        }
+        stage_begin(c, 8);
+        int rr = refine_apply(khm, Fsym, A, khm, eval, Fsym + (size_t)khm * khm, c->rf_buf, c->rf_buf + khm,
+                              d_rflag, s);
+        stage_end(c, 8, 3);
+        if (rr != BSRG_OK) return rr;
+        c->rf_n = khm;
     }
     if (bbout && (e = cudaMemcpyAsync(bbout, BB, sizeof(double) * nn * nch, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
         return cuda_fail(e, "diag_hd bb copy");
@@ -594,6 +634,31 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         return BSRG_ERR_INFO;
     }
     return stage_collect(c);
+}
+
+extern "C" int bsrg_ctx_set_refine(bsrg_ctx *c, int on)
+{
+    if (!c) { set_error("ctx_set_refine: null context"); return BSRG_ERR_ARG; }
+    c->refine = on ? 1 : 0;
+    return BSRG_OK;
+}
+
+extern "C" int bsrg_diag_hd_refine_stats(bsrg_ctx *c, int n, double *corr, double *resid)
+{
+    if (!c) { set_error("diag_hd_refine_stats: null context"); return BSRG_ERR_ARG; }
+    if (n < 0 || n > c->rf_n) {
+        set_error("diag_hd_refine_stats: n=%d but the last refined diag_hd had %d pairs", n, c->rf_n);
+        return BSRG_ERR_ARG;
+    }
+    cudaError_t e;
+    if (corr && n > 0 &&
+        (e = cudaMemcpyAsync(corr, c->rf_buf, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd_refine_stats");
+    if (resid && n > 0 &&
+        (e = cudaMemcpyAsync(resid, c->rf_buf + c->rf_n, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->stream)) !=
+            cudaSuccess)
+        return cuda_fail(e, "diag_hd_refine_stats");
+    return BSRG_OK;
 }
 
 // whole path with host buffers: bsr_mat SUB1 followed by bsr_hd's diag_hd

@@ -53,13 +53,14 @@ class Request:
 
 def request_bytes(nch, ns, lch, ks, want_vectors=True):
     """Device bytes one solve needs beyond the shared state (H blocks, the dense
-    problem with vectors and its eigensolver workspace, block-transform buffers)."""
+    problem with vectors and its eigensolver workspace, block-transform buffers;
+    with vectors also the eigenvectors and the refinement's copy of A)."""
     khm, hb, db = shard.symmetry_dims(nch, ns, lch, ks)
     nch, ns = int(nch), int(ns)
-    nb = nch * (nch - 1) // 2
+    nb = nch * (nch + 1) // 2
     transform = 2 * nb * ns * ns * 8
     channel = 4 * nch * ns * ns * 8
-    return hb + db + transform + channel + (khm * khm * 8 if want_vectors else 0)
+    return hb + db + transform + channel + (2 * khm * khm * 8 if want_vectors else 0)
 
 
 class AdmissionQueue:

@@ -180,8 +180,9 @@ size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c);
  * (library calls such as cuSOLVER's are timed but not counted), then resets
  * them.  Stages: 0 R^k cell moments, 1 direct groups, 2 exchange groups,
  * 3 one-electron / overlap / symmetrisation, 4 channel eigenproblems,
- * 5 block transforms, 6 dense eigensolve, 7 rkb expansion (mrk_cell). */
-#define BSRG_NSTAGE 8
+ * 5 block transforms, 6 dense eigensolve, 7 rkb expansion (mrk_cell),
+ * 8 eigenpair refinement. */
+#define BSRG_NSTAGE 9
 int bsrg_ctx_set_timing(bsrg_ctx *c, int on);
 int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n);
 
@@ -244,7 +245,15 @@ int bsrg_add_two_electron(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, c
  *      the dimension.  vecs (device, khm*khm, may be NULL): eigenvectors in the
  *      channel eigenbasis (the reference's a(:,:) after DSYEV); bb (device,
  *      (ns, nch*ns), may be NULL): the channel eigenbasis, columns packed.
- *      want_vectors = 0 computes eigenvalues only. */
+ *      want_vectors = 0 computes eigenvalues only.
+ *      With eigenvectors, and unless bsrg_ctx_set_refine turned it off, every
+ *      eigenvalue is then refined in FP64 by its Rayleigh quotient,
+ *      lambda + v^T (A v - lambda v) / v^T v (no counterpart in the reference:
+ *      DSYEV's eigenvalues carry errors ~eps ||A||, ~1e-9 absolute when the
+ *      kinetic entries reach 1e7; the quotient's error scales with
+ *      |v|^T |A| |v|, which makes the eigenvalues agree per eigenvalue).  The
+ *      eigenvalues stay ascending (pairs closer than the correction swap with
+ *      their vectors). */
 int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
                  int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
                  double *eval, int *khm, double *vecs, double *bb);
@@ -259,6 +268,24 @@ int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, cons
  *      Perturber blocks (kcp > 0) are outside this path. */
 int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const double *P, const int *ort_ptr,
                  const int *ort_idx, double *hcc);
+
+/* ---- No counterpart in the reference: switch the FP64 eigenpair refinement
+ *      of bsrg_diag_hd on (default) or off for this context, and read the
+ *      per-pair correction (refined minus raw eigenvalue) and residual norm
+ *      ||A v - lambda v|| / ||v|| of the last refined bsrg_diag_hd into corr
+ *      and resid (device, n <= khm doubles each, either may be NULL) on the
+ *      context's stream. */
+int bsrg_ctx_set_refine(bsrg_ctx *c, int on);
+int bsrg_diag_hd_refine_stats(bsrg_ctx *c, int n, double *corr, double *resid);
+
+/* ---- No counterpart in the reference (it links BLAS but calls no DGEMM on
+ *      this path; diag_hd.f90:188-219 transforms the blocks with hand loops):
+ *      the library's FP64 tensor-core GEMM, C = alpha op(A) op(B) + beta C,
+ *      column-major, for `batch` items spaced by the strides (elements).
+ *      transa/transb 'N' or 'T'.  Device. */
+int bsrg_dgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A, long lda, long strideA,
+               const double *B, long ldb, long strideB, double beta, double *C, long ldc, long strideC, int batch,
+               void *stream);
 
 /* ---- the channel solution offsets ipsol(0:nch) of the last bsrg_diag_hd on
  *      this context (module bsr_hd's ipsol, set in diag_hd.f90:100-111):
@@ -292,6 +319,14 @@ int bsrg_rsol_out(bsrg_ctx *c, int ns, int nch, const int *ipsol, const double *
  *      below the subdiagonal (LAPACK layout, so DORMTR applies Q).  Uses the
  *      context's stream and workspace. */
 int bsrg_dsytrd(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, double *tau);
+
+/* ---- the tridiagonal stage of DSYEV (LAP_DSYEV, src/libs/ZCOM/LAPACK_calls.f90:54-76,
+ *      from diag_hd.f90:312; DSYEV diagonalises T by DSTEQR): all eigenvalues
+ *      (ascending, w) and eigenvectors (Z, ldz >= n) of the symmetric tridiagonal
+ *      T = tridiag(e, d, e) by divide and conquer (LAPACK DSTEDC's algorithm).
+ *      d (n), e (n-1) device, unchanged.  n <= 10240.  Uses the context's stream
+ *      and workspace; reads small per-level counts back to the host. */
+int bsrg_dstedc(bsrg_ctx *c, int n, const double *d, const double *e, double *w, double *Z, int ldz);
 
 /* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
  *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.

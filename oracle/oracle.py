@@ -371,8 +371,20 @@ def assemble(basis, z, lch, ech, P, kmax, rkb_all, coefs, want_s=True, want_acf=
 # ---------------------------------------------------------------------------
 # diag_hd restatement (src/bsr/BSR_HD3/diag_hd.f90:2-340) with scipy LAPACK
 # ---------------------------------------------------------------------------
+def rayleigh_refine(A, ev, V, dtype=np.longdouble):
+    """Rayleigh quotients lambda + v^T (A v - lambda v) / v^T v of the eigenpairs
+    (ev, V) of the symmetric A, evaluated in `dtype` (long double: ~1e-19 relative
+    rounding, so the result is the exact quotient of the FP64 pair to working
+    precision).  Returns (refined eigenvalues, residual norms ||A v - lambda v|| / ||v||)."""
+    Al, Vl, el = A.astype(dtype), V.astype(dtype), ev.astype(dtype)
+    R = Al @ Vl - Vl * el[None, :]
+    vv = np.sum(Vl * Vl, axis=0)
+    ref = el + np.sum(Vl * R, axis=0) / vv
+    return np.asarray(ref, dtype=np.float64), np.sqrt(np.asarray(np.sum(R * R, axis=0) / vv, dtype=np.float64))
+
+
 def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001,
-            want_vectors=False):
+            want_vectors=False, refine=False, lowest=None, refine_dtype=np.longdouble):
     """Solve H c = E S c the way bsr_hd does for one partial wave.
 
     hcc, scc: (nch(nch+1)/2, ns, ns) lower-triangle channel blocks [row, col]
@@ -380,6 +392,14 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
     diagonal here (diag_ovl /= 0): the reference then solves a standard
     problem after the per-channel pre-diagonalisation (diag_hd.f90:68-71).
     Returns dict(eval, khm, bval, ipsol, [a_vectors]).
+
+    refine=True restates the library's refined form: the diagonal blocks of A
+    are bb_i^T H_ii bb_i (diag(bval) in exact arithmetic, diag_hd.f90:188-219)
+    and every eigenvalue is replaced by its Rayleigh quotient in refine_dtype
+    (rayleigh_refine); the eigenvectors come from LAPACK DSYEV as in the
+    reference (:312), or, with lowest=m, from DSYEVR for the m lowest pairs
+    only (the quotient makes the result independent of the driver).  Also
+    returns "a" (the symmetric A) and "resid".
     """
     from scipy.linalg import lapack
 
@@ -418,21 +438,35 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
         ipsol.append(ipsol[-1] + int(keep.sum()))
     khm = ipsol[-1]
     a = np.zeros((khm, khm), order="F")
-    a[np.arange(khm), np.arange(khm)] = bval
+    if not refine:
+        a[np.arange(khm), np.arange(khm)] = bval
     for ic in range(nch):
-        for jc in range(ic):
+        for jc in range(ic + 1 if refine else ic):
             h = blk(ic, jc)
             if not np.any(h != 0):
                 continue
             w = bb[ic].T @ h          # rows: solutions of ic, cols: B-splines
             a[ipsol[ic]: ipsol[ic + 1], ipsol[jc]: ipsol[jc + 1]] = w @ bb[jc]
+    out = {"khm": khm, "bval": np.array(bval), "ipsol": np.array(ipsol), "bb": bb}
+    if refine:
+        full = np.tril(a) + np.tril(a, -1).T
+        if lowest is not None:
+            from scipy.linalg import eigh
+            ev, vec = eigh(full, subset_by_index=[0, min(lowest, khm) - 1], driver="evr")
+        else:
+            ev, vec, info = lapack.dsyev(a, compute_v=1, lower=1)[:3]
+            if info != 0:
+                raise RuntimeError("DSYEV info %d" % info)
+        ev, resid = rayleigh_refine(full, ev, vec, refine_dtype)
+        o = np.argsort(ev, kind="stable")
+        out.update({"eval": ev[o], "resid": resid[o], "vectors": vec[:, o], "a": full})
+        return out
     ev, vec, info = lapack.dsyev(a, compute_v=1 if want_vectors else 0, lower=1)[:3]
     if info != 0:
         raise RuntimeError("DSYEV info %d" % info)
-    out = {"eval": ev, "khm": khm, "bval": np.array(bval), "ipsol": np.array(ipsol)}
+    out["eval"] = ev
     if want_vectors:
         out["vectors"] = vec
-        out["bb"] = bb
     return out
 
 

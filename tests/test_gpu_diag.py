@@ -1,11 +1,16 @@
 """bsr_hd's diag_hd on the GPU against the oracle's restatement (scipy LAPACK
 DSYGV / DSYEV standing in for the reference's LAPACK).
 
-Eigenvalue tolerance: 1e-11 relative to the spectral radius, |dE| / max|E|.
-H spans about 7 orders of magnitude here (kinetic energies ~1/h_min^2 of the
-1e-3 a.u. first interval), so two backward-stable FP64 eigensolvers -- LAPACK
-DSYEV and cuSOLVER syevd alike -- may differ by ~eps*||A|| in every
-eigenvalue; the bound part is checked against that scale (|dE| <= 64 eps ||A||)."""
+Eigenvalues are compared PER EIGENVALUE: |E_gpu - E_ref| / max(|E_ref|, 1e-3)
+<= 1e-11 (the floor 1e-3 is diag_hd's Egap: channel states closer to zero are
+dropped by the reference).  Both sides use the refined form: A's diagonal
+blocks formed as bb^T H bb and every eigenvalue replaced by its FP64 Rayleigh
+quotient (long double on the oracle side at config 1).  A raw FP64 eigensolver
+-- LAPACK DSYEV included -- leaves errors of ~eps ||A|| per eigenvalue, and
+||A|| ~ 4e7 here (kinetic energies of the 1e-3 a.u. first knot interval), so
+raw eigenvalues agree only to ~1e-7 relative at |E| ~ 0.01; the refined ones
+agree to ~1e-14.  The reference's unrefined form is checked separately,
+normwise."""
 import numpy as np
 import pytest
 
@@ -14,13 +19,19 @@ from oracle import oracle as O
 from tests.gpu_helpers import to_np
 
 pytestmark = pytest.mark.gpu
-TOL_E = 1e-11
+TOL_E = 1e-11          # per eigenvalue, relative (floor 1e-3)
+TOL_NORMWISE = 1e-11   # unrefined reference form, relative to max |E|
 
 
-def _solve(pw, want_vectors=True):
+def per_eig_rel(ev, er):
+    return np.abs(ev - er) / np.maximum(np.abs(er), 1e-3)
+
+
+def _solve(pw, want_vectors=True, refine=True):
     import bsr_b200 as bsr
     gb = bsr.define_spline(pw["t"], pw["ks"])
     ctx = bsr.Context()
+    ctx.set_refine(refine)
     H = bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], pw["coefs"], want_s=True)
     res = bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=want_vectors, want_bb=True)
     return gb, ctx, H, res
@@ -32,82 +43,99 @@ def config1():
     gb, ctx, H, res = _solve(pw)
     hcc = to_np(H["hcc"]).transpose(2, 0, 1)
     scc = to_np(H["scc"]).transpose(2, 0, 1)
-    ref = O.diag_hd(hcc, scc, pw["lch"], gb.ns, gb.ks, want_vectors=True)
-    return pw, gb, H, res, ref, hcc
+    ref = O.diag_hd(hcc, scc, pw["lch"], gb.ns, gb.ks, refine=True)
+    return pw, gb, ctx, H, res, ref, hcc, scc
 
 
 def test_khm_and_channel_eigenvalues(config1):
-    pw, gb, H, res, ref, hcc = config1
+    pw, gb, ctx, H, res, ref, hcc, scc = config1
     assert res["khm"] == ref["khm"]
     ev = to_np(res["eval"])
     assert ev.shape == (ref["khm"],)
+    assert np.all(np.diff(ev) >= 0)
 
 
-def test_eigenvalues_config1(config1):
-    pw, gb, H, res, ref, hcc = config1
+def test_eigenvalues_per_eigenvalue_config1(config1):
+    pw, gb, ctx, H, res, ref, hcc, scc = config1
     ev = to_np(res["eval"])
-    er = ref["eval"]
-    assert np.max(np.abs(ev - er)) / np.max(np.abs(er)) < TOL_E
-    bound = er < 0.0
-    anorm = np.max(np.abs(er))
-    assert np.max(np.abs(ev[bound] - er[bound])) <= 64 * np.finfo(float).eps * anorm
+    rel = per_eig_rel(ev, ref["eval"])
+    print("config1 per-eigenvalue relative error: max %.2e p99 %.2e median %.2e" %
+          (rel.max(), np.percentile(rel, 99), np.median(rel)))
+    assert np.max(rel) <= TOL_E
+
+
+def test_refine_stats_config1(config1):
+    """The per-pair residuals the library reports are the oracle's, to rounding; the
+    corrections are of the size of the raw eigensolver's error, ~eps ||A||."""
+    pw, gb, ctx, H, res, ref, hcc, scc = config1
+    n = res["khm"]
+    corr, resid = (to_np(x) for x in ctx.refine_stats(n))
+    anorm = np.max(np.abs(ref["a"]))
+    assert np.all(np.isfinite(corr)) and np.all(np.isfinite(resid))
+    assert np.max(resid) < 1e-13 * anorm
+    assert np.max(np.abs(corr)) < 1e3 * np.finfo(float).eps * anorm
+
+
+def test_reference_form_config1():
+    """Refinement off: the reference's own form (diag(bval), raw DSYEV-class solve),
+    normwise against the oracle's unrefined restatement."""
+    pw = W.partial_wave("config1")
+    gb, ctx, H, res = _solve(pw, refine=False)
+    hcc = to_np(H["hcc"]).transpose(2, 0, 1)
+    scc = to_np(H["scc"]).transpose(2, 0, 1)
+    er = O.diag_hd(hcc, scc, pw["lch"], gb.ns, gb.ks)["eval"]
+    ev = to_np(res["eval"])
+    assert np.max(np.abs(ev - er)) / np.max(np.abs(er)) < TOL_NORMWISE
 
 
 def test_eigenvectors_residual_config1(config1):
-    """||A v - E v|| / ||A|| for the GPU eigenvectors, with A rebuilt by the oracle."""
-    pw, gb, H, res, ref, hcc = config1
+    """||A v - E v|| / ||A|| for the GPU eigenvectors, with A rebuilt by the oracle in
+    the GPU's channel basis signs (bases agree up to the sign of each vector)."""
+    pw, gb, ctx, H, res, ref, hcc, scc = config1
     V = to_np(res["vectors"])
     ev = to_np(res["eval"])
-    # rebuild A = diag(bval) + bb^T H bb from the oracle's channel basis
-    nch, khm = pw["nch"], ref["khm"]
-    ip = ref["ipsol"]
-    A = np.zeros((khm, khm))
-    A[np.arange(khm), np.arange(khm)] = ref["bval"]
-    for ic in range(nch):
-        for jc in range(ic):
-            A[ip[ic]:ip[ic + 1], ip[jc]:ip[jc + 1]] = ref["bb"][ic].T @ hcc[ic * (ic + 1) // 2 + jc] @ ref["bb"][jc]
-    A = np.tril(A) + np.tril(A, -1).T
-    # eigenvectors are defined up to sign within the channel basis of the GPU; the
-    # residual is basis-independent only if the channel bases agree up to sign.
+    nch, ip, ns = pw["nch"], ref["ipsol"], gb.ns
+    A = ref["a"]
     bb_gpu = to_np(res["bb"])
-    ns = gb.ns
     for ic in range(nch):
-        n = ip[ic + 1] - ip[ic]
-        for q in range(n):
-            g = bb_gpu[:, ic * ns + q]
-            r = ref["bb"][ic][:, q]
-            sgn = np.sign(g @ r)
+        for q in range(ip[ic + 1] - ip[ic]):
+            sgn = np.sign(bb_gpu[:, ic * ns + q] @ ref["bb"][ic][:, q])
             V[ip[ic] + q, :] *= sgn
     R = A @ V - V * ev[None, :]
     assert np.max(np.abs(R)) / np.max(np.abs(A)) < 1e-12
 
 
-def test_trace_invariance_config2():
-    """Full size: sum of eigenvalues = trace(A) = sum of channel eigenvalues."""
+def test_config2_lowest_200_per_eigenvalue():
+    """Full size (khm 7810): the 200 lowest eigenvalues per eigenvalue against the oracle
+    (DSYEVR for the 200 lowest pairs of the oracle's A, FP64 Rayleigh quotients), and
+    sum of eigenvalues = trace(A)."""
     pw = W.partial_wave("config2")
-    gb, ctx, H, res = _solve(pw, want_vectors=False)
+    gb, ctx, H, res = _solve(pw)
     ev = to_np(res["eval"])
     assert res["khm"] > 7000
     assert np.all(np.diff(ev) >= 0)
-    import bsr_b200 as bsr
     hcc = to_np(H["hcc"]).transpose(2, 0, 1)
-    ref = O.diag_hd(hcc, to_np(H["scc"]).transpose(2, 0, 1), pw["lch"], gb.ns, gb.ks)
+    scc = to_np(H["scc"]).transpose(2, 0, 1)
+    del H
+    ref = O.diag_hd(hcc, scc, pw["lch"], gb.ns, gb.ks, refine=True, lowest=200, refine_dtype=np.float64)
     assert res["khm"] == ref["khm"]
-    er = ref["eval"]
-    assert abs(ev.sum() - ref["bval"].sum()) <= 1e-12 * np.abs(ref["bval"]).sum()
-    assert np.max(np.abs(ev - er)) / np.max(np.abs(er)) < TOL_E
+    rel = per_eig_rel(ev[:200], ref["eval"])
+    print("config2 lowest 200 per-eigenvalue relative error: max %.2e p99 %.2e" % (rel.max(), np.percentile(rel, 99)))
+    assert np.max(rel) <= TOL_E
+    tr = np.trace(ref["a"])
+    assert abs(ev.sum() - tr) <= 1e-12 * np.abs(np.diag(ref["a"])).sum()
 
 
 def test_batched_channel_solves_match_sygvd(monkeypatch):
     """The batched channel eigensolves (potrf + batched trsm + syevBatched) and the
-    per-channel sygvd path give the same spectrum."""
+    per-channel sygvd path give the same refined spectrum, per eigenvalue."""
     import bsr_b200 as bsr
     pw = W.partial_wave("config1", seed=8)
     gb = bsr.define_spline(pw["t"], pw["ks"])
     ctx = bsr.Context()
     H = bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], pw["coefs"])
-    a = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=False)["eval"])
+    a = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=True)["eval"])
     monkeypatch.setenv("BSRG_CHANNEL_SYGVD", "1")
-    b = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=False)["eval"])
+    b = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=True)["eval"])
     assert a.shape == b.shape
-    assert np.max(np.abs(a - b)) / np.max(np.abs(b)) < TOL_E
+    assert np.max(per_eig_rel(a, b)) < 1e-12
