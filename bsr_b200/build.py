@@ -28,6 +28,7 @@ UNITS = {
     "dgemm.cu": [],
     "refine.cu": [],
     "tridiag_dc.cu": [],
+    "syevd2.cu": [],
 }
 
 

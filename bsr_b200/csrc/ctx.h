@@ -81,6 +81,11 @@ size_t dc_pinned_bytes(int n);
 int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, double *Z, long ldz, void *ws_base,
                size_t ws_bytes, void *pinned, size_t pinned_bytes);
 
+// two-stage dense symmetric eigensolver (syevd2.cu)
+size_t syevd2_workspace_doubles(int n);
+int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
+                size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches);
+
 // eigenpair refinement (refine.cu)
 size_t refine_workspace_doubles(int n);
 int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s);

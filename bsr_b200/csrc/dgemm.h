@@ -18,7 +18,9 @@ struct DgemmBatch {
 };
 
 int dgemm_batched(bool ta, bool tb, const DgemmBatch &p, int batch, cudaStream_t s);
+// with a workspace (work_doubles doubles), a single product with few tiles is split along K
+int dgemm_ws(bool ta, bool tb, const DgemmBatch &p, int batch, cudaStream_t s, double *work, size_t work_doubles);
 int dgemm(bool ta, bool tb, int m, int n, int k, double alpha, const double *A, long lda, const double *B, long ldb,
-          double beta, double *C, long ldc, cudaStream_t s);
+          double beta, double *C, long ldc, cudaStream_t s, double *work = nullptr, size_t work_doubles = 0);
 
 }  // namespace bsrg

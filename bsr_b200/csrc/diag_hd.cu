@@ -391,6 +391,9 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     // formed blocks keep the channel solver's rounding (~eps ||H_ii||) out of
     // the eigenvalues, which the Rayleigh quotients below then resolve.
     const bool refine = want_vectors && c->refine;
+    const char *eig_env = getenv("BSRG_EIG");
+    // the library's two-stage eigensolver (syevd2.cu) or cuSOLVER's syevd
+    const bool own_eig = want_vectors && eig_env && strcmp(eig_env, "own") == 0;
     std::vector<BlockMap> bmap;
     for (int ic = 1; ic < nch; ic++)
         for (int jc = 0; jc < ic; jc++) bmap.push_back({ic, jc});
@@ -438,6 +441,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         add(sizeof(double) * refine_workspace_doubles(khm_max));   // mirrored A, then the tile partial sums
         add(sizeof(int) * 4);
     }
+    if (own_eig) add(sizeof(double) * syevd2_workspace_doubles(khm_max));
     size_t batched_bytes = chan_batched_bytes(c, params, ns, s0v, nsolv);
     add(batched_bytes);
     int rc = ctx_reserve(c, need);
@@ -447,7 +451,8 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
                  o_fin = 5 * (size_t)nch + 1;
     size_t o_bm_bytes = ((o_fin + 1) * sizeof(int) + 15) & ~(size_t)15;
     size_t o_ptr_bytes = (o_bm_bytes + sizeof(BlockMap) * nb + 15) & ~(size_t)15;
-    rc = ctx_reserve_pinned(c, o_ptr_bytes + sizeof(double *) * nb * 5 + 64);
+    const size_t o_dc_bytes = (o_ptr_bytes + sizeof(double *) * nb * 5 + 64 + 255) & ~(size_t)255;
+    rc = ctx_reserve_pinned(c, o_dc_bytes + (own_eig ? dc_pinned_bytes(khm_max) : 0) + 64);
     if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
     Arena ar{(char *)c->ws, 0, c->ws_bytes};
     int *d_s0 = ar.take<int>(nch), *d_nsol = ar.take<int>(nch), *d_cnt = ar.take<int>(nch);
@@ -462,6 +467,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     void *dwork = ar.take<char>(dws + 16);
     double *Fsym = refine ? ar.take<double>(refine_workspace_doubles(khm_max)) : nullptr;
     int *d_rflag = refine ? ar.take<int>(4) : nullptr;
+    double *eig_ws = own_eig ? ar.take<double>(syevd2_workspace_doubles(khm_max)) : nullptr;
     int *hi = (int *)c->pinned;
     std::memcpy(hi + o_s0, s0v.data(), sizeof(int) * nch);
     std::memcpy(hi + o_nsol, nsolv.data(), sizeof(int) * nch);
@@ -596,14 +602,24 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     }
     // ---- 3. eigensolve ----
     stage_begin(c, 6);
-    cusolverStatus_t st = cusolverDnXsyevd(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm, CUDA_R_64F, A, khm,
-                                           CUDA_R_64F, eval, CUDA_R_64F, dwork, dws, hwork.data(), hws,
-                                           d_info + nch);
-    cusolverDnDestroyParams(params);
-    stage_end(c, 6, 0);
-    if (st != CUSOLVER_STATUS_SUCCESS) {
-        set_error("diag_hd: syevd failed to launch (status %d)", (int)st);
-        return BSRG_ERR_SOLVER;
+    if (own_eig) {
+        cusolverDnDestroyParams(params);
+        int nlaunch = 0;
+        int re = dense_syevd(c, khm, A, khm, eval, A, khm, eig_ws, syevd2_workspace_doubles(khm_max),
+                             (char *)c->pinned + o_dc_bytes, c->pinned_bytes - o_dc_bytes, &nlaunch);
+        stage_end(c, 6, nlaunch);
+        if (re != BSRG_OK) return re;
+        if ((e = cudaMemsetAsync(d_info + nch, 0, sizeof(int), s)) != cudaSuccess) return cuda_fail(e, "diag_hd info");
+    } else {
+        cusolverStatus_t st = cusolverDnXsyevd(c->solver, params, jobz, CUBLAS_FILL_MODE_LOWER, khm, CUDA_R_64F, A,
+                                               khm, CUDA_R_64F, eval, CUDA_R_64F, dwork, dws, hwork.data(), hws,
+                                               d_info + nch);
+        cusolverDnDestroyParams(params);
+        stage_end(c, 6, 0);
+        if (st != CUSOLVER_STATUS_SUCCESS) {
+            set_error("diag_hd: syevd failed to launch (status %d)", (int)st);
+            return BSRG_ERR_SOLVER;
+        }
     }
     if (refine) {
         // ---- FP64 refinement of the eigenpairs (Rayleigh quotients) ----

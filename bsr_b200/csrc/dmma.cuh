@@ -1,13 +1,14 @@
 // FP64 tensor-core GEMM core for sm_100a: mma.sync.aligned.m8n8k4 f64 (DMMA).
 //
 // FP64 has no tcgen05 kind, so the FP64 tensor pipe is reached through the
-// warp-level m8n8k4 f64 MMA.  One CTA computes a 128 x 128 tile of
-// C = op(A) op(B) with 8 warps (2 along M x 4 along N, 64 x 32 per warp:
-// 8 x 4 MMA tiles, 64 accumulators per thread).  K advances in steps of 16
-// through a 3-stage cp.async pipeline; every operand tile is staged in shared
-// memory in the orientation its global layout gives (no transposes), with a
-// padding of 4 doubles so that the fragment loads of each half-warp hit 16
-// distinct 8-byte bank slots.
+// warp-level m8n8k4 f64 MMA.  A CTA computes a BM x BN tile of
+// C = op(A) op(B) with WM x WN warps, each warp a (BM/WM) x (BN/WN) sub-tile of
+// 8 x 8 MMA tiles.  K advances in steps of 16 through a 3-stage cp.async
+// pipeline; every operand tile is staged in shared memory in the orientation
+// its global layout gives (no transposes), with a padding of 4 doubles so that
+// the fragment loads of each half-warp hit 16 distinct 8-byte bank slots.
+// Shapes: 128 x 128 (8 warps, 64 x 32 each) for square work, 128 x 32 and
+// 32 x 128 (4 warps, 32 x 32 each) for the panel products of the eigensolver.
 //
 // Fragment layouts of m8n8k4 f64 (row.col): A 8x4 -- lane holds A[lane>>2][lane&3];
 // B 4x8 -- lane holds B[lane&3][lane>>2]; C 8x8 -- lane holds C[lane>>2][2(lane&3)+{0,1}].
@@ -20,20 +21,30 @@
 namespace bsrg {
 namespace dmma {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, NT = 256;
-constexpr int PAD = 4;
+constexpr int BK = 16, STAGES = 3, PAD = 4;
 
-template <bool TA> struct ALayout {
+template <int BM_, int BN_, int WM_, int WN_> struct Cfg {
+    static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_;
+    static constexpr int NT = 32 * WM * WN;
+    static constexpr int TM = BM / WM, TN = BN / WN;     // warp tile
+    static constexpr int FM = TM / 8, FN = TN / 8;       // MMA tiles per warp
+    static_assert(TM % 8 == 0 && TN % 8 == 0, "warp tile of whole 8x8 MMA tiles");
+    static_assert((BM * BK) % NT == 0 && (BN * BK) % NT == 0, "whole loads per thread");
+};
+using Sq = Cfg<128, 128, 2, 4>;   // 256 threads
+using Tall = Cfg<128, 32, 4, 1>;  // 128 threads
+using Wide = Cfg<32, 128, 1, 4>;  // 128 threads
+
+template <class C, bool TA> struct ALayout {
     // !TA: As[k][m] (m contiguous), TA: As[m][k] (k contiguous)
-    static constexpr int ELEMS = TA ? BM * (BK + PAD) : BK * (BM + PAD);
+    static constexpr int ELEMS = TA ? C::BM * (BK + PAD) : BK * (C::BM + PAD);
 };
-template <bool TB> struct BLayout {
+template <class C, bool TB> struct BLayout {
     // !TB: Bs[n][k] (k contiguous), TB: Bs[k][n] (n contiguous)
-    static constexpr int ELEMS = TB ? BK * (BN + PAD) : BN * (BK + PAD);
+    static constexpr int ELEMS = TB ? BK * (C::BN + PAD) : C::BN * (BK + PAD);
 };
-
-template <bool TA, bool TB> struct Smem {
-    static constexpr int STAGE = ALayout<TA>::ELEMS + BLayout<TB>::ELEMS;
+template <class C, bool TA, bool TB> struct Smem {
+    static constexpr int STAGE = ALayout<C, TA>::ELEMS + BLayout<C, TB>::ELEMS;
     static constexpr int BYTES = STAGES * STAGE * 8;
 };
 
@@ -53,56 +64,59 @@ __device__ __forceinline__ void mma884(double &d0, double &d1, double a, double 
                  : "d"(a), "d"(b));
 }
 
-// stage one BK slice of the A and B tiles (zero-filled outside the matrices)
-template <bool TA, bool TB>
+// stage one BK slice of the A and B tiles (zero-filled outside the matrices and
+// outside the K range [k0, kend))
+template <class C, bool TA, bool TB>
 __device__ __forceinline__ void load_stage(double *sA, double *sB, const double *A, long lda, const double *B,
-                                           long ldb, int M, int N, int K, int m0, int n0, int k0)
+                                           long ldb, int M, int N, int kend, int m0, int n0, int k0)
 {
     const int tid = threadIdx.x;
 #pragma unroll
-    for (int i = 0; i < (BM * BK) / NT; i++) {
-        const int idx = tid + i * NT;
+    for (int i = 0; i < (C::BM * BK) / C::NT; i++) {
+        const int idx = tid + i * C::NT;
         int ml, kl;
-        if (!TA) { ml = idx % BM; kl = idx / BM; }
+        if (!TA) { ml = idx % C::BM; kl = idx / C::BM; }
         else { kl = idx % BK; ml = idx / BK; }
         const int gm = m0 + ml, gk = k0 + kl;
-        const bool v = gm < M && gk < K;
+        const bool v = gm < M && gk < kend;
         const double *src = v ? (TA ? A + gk + (long)gm * lda : A + gm + (long)gk * lda) : A;
-        double *dst = TA ? sA + ml * (BK + PAD) + kl : sA + kl * (BM + PAD) + ml;
+        double *dst = TA ? sA + ml * (BK + PAD) + kl : sA + kl * (C::BM + PAD) + ml;
         cp_async8(dst, src, v);
     }
 #pragma unroll
-    for (int i = 0; i < (BN * BK) / NT; i++) {
-        const int idx = tid + i * NT;
+    for (int i = 0; i < (C::BN * BK) / C::NT; i++) {
+        const int idx = tid + i * C::NT;
         int nl, kl;
         if (!TB) { kl = idx % BK; nl = idx / BK; }
-        else { nl = idx % BN; kl = idx / BN; }
+        else { nl = idx % C::BN; kl = idx / C::BN; }
         const int gn = n0 + nl, gk = k0 + kl;
-        const bool v = gn < N && gk < K;
+        const bool v = gn < N && gk < kend;
         const double *src = v ? (TB ? B + gn + (long)gk * ldb : B + gk + (long)gn * ldb) : B;
-        double *dst = TB ? sB + kl * (BN + PAD) + nl : sB + nl * (BK + PAD) + kl;
+        double *dst = TB ? sB + kl * (C::BN + PAD) + nl : sB + nl * (BK + PAD) + kl;
         cp_async8(dst, src, v);
     }
 }
 
-// acc[s][t][j]: row m0 + wm*64 + s*8 + (lane>>2), column n0 + wn*32 + t*8 + 2*(lane&3) + j
-template <bool TA, bool TB>
-__device__ __forceinline__ void tile_mma(double acc[8][4][2], double *smem, const double *A, long lda,
-                                         const double *B, long ldb, int M, int N, int K, int m0, int n0)
+// acc[s][t][j]: row m0 + wm*TM + s*8 + (lane>>2), column n0 + wn*TN + t*8 + 2*(lane&3) + j,
+// summed over k in [kbeg, kend)
+template <class C, bool TA, bool TB>
+__device__ __forceinline__ void tile_mma(double (&acc)[C::FM][C::FN][2], double *smem, const double *A, long lda,
+                                         const double *B, long ldb, int M, int N, int kbeg, int kend, int m0, int n0)
 {
-    constexpr int SA = ALayout<TA>::ELEMS, STG = Smem<TA, TB>::STAGE;
+    constexpr int SA = ALayout<C, TA>::ELEMS, STG = Smem<C, TA, TB>::STAGE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wm = warp & 1, wn = warp >> 1;
+    const int wm = warp % C::WM, wn = warp / C::WM;
     const int r = lane >> 2, c = lane & 3;
 #pragma unroll
-    for (int s = 0; s < 8; s++)
+    for (int s = 0; s < C::FM; s++)
 #pragma unroll
-        for (int t = 0; t < 4; t++) acc[s][t][0] = acc[s][t][1] = 0.0;
-    const int ktiles = (K + BK - 1) / BK;
+        for (int t = 0; t < C::FN; t++) acc[s][t][0] = acc[s][t][1] = 0.0;
+    const int ktiles = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
 #pragma unroll
     for (int st = 0; st < STAGES - 1; st++) {
         if (st < ktiles)
-            load_stage<TA, TB>(smem + st * STG, smem + st * STG + SA, A, lda, B, ldb, M, N, K, m0, n0, st * BK);
+            load_stage<C, TA, TB>(smem + st * STG, smem + st * STG + SA, A, lda, B, ldb, M, N, kend, m0, n0,
+                                  kbeg + st * BK);
         cp_async_commit();
     }
     for (int kt = 0; kt < ktiles; kt++) {
@@ -111,27 +125,27 @@ __device__ __forceinline__ void tile_mma(double acc[8][4][2], double *smem, cons
         const int nk = kt + STAGES - 1;
         if (nk < ktiles) {
             double *base = smem + (nk % STAGES) * STG;
-            load_stage<TA, TB>(base, base + SA, A, lda, B, ldb, M, N, K, m0, n0, nk * BK);
+            load_stage<C, TA, TB>(base, base + SA, A, lda, B, ldb, M, N, kend, m0, n0, kbeg + nk * BK);
         }
         cp_async_commit();
         const double *sA = smem + (kt % STAGES) * STG, *sB = sA + SA;
 #pragma unroll
         for (int kk = 0; kk < BK / 4; kk++) {
-            double af[8], bf[4];
+            double af[C::FM], bf[C::FN];
 #pragma unroll
-            for (int s = 0; s < 8; s++) {
-                const int ml = wm * 64 + s * 8 + r, kl = kk * 4 + c;
-                af[s] = TA ? sA[ml * (BK + PAD) + kl] : sA[kl * (BM + PAD) + ml];
+            for (int s = 0; s < C::FM; s++) {
+                const int ml = wm * C::TM + s * 8 + r, kl = kk * 4 + c;
+                af[s] = TA ? sA[ml * (BK + PAD) + kl] : sA[kl * (C::BM + PAD) + ml];
             }
 #pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const int nl = wn * 32 + t * 8 + r, kl = kk * 4 + c;
-                bf[t] = TB ? sB[kl * (BN + PAD) + nl] : sB[nl * (BK + PAD) + kl];
+            for (int t = 0; t < C::FN; t++) {
+                const int nl = wn * C::TN + t * 8 + r, kl = kk * 4 + c;
+                bf[t] = TB ? sB[kl * (C::BN + PAD) + nl] : sB[nl * (BK + PAD) + kl];
             }
 #pragma unroll
-            for (int s = 0; s < 8; s++)
+            for (int s = 0; s < C::FM; s++)
 #pragma unroll
-                for (int t = 0; t < 4; t++) mma884(acc[s][t][0], acc[s][t][1], af[s], bf[t]);
+                for (int t = 0; t < C::FN; t++) mma884(acc[s][t][0], acc[s][t][1], af[s], bf[t]);
         }
     }
     cp_async_wait<0>();

@@ -48,14 +48,15 @@ __global__ void symmetrize_lower_kernel(int n, const double *__restrict__ A, lon
 
 // partial sums of the Rayleigh correction: P[(tm*3 + w)*n + j], w = 0: sum v r,
 // 1: sum r^2, 2: sum v^2 over rows of M tile tm (r = (F V)(i,j) - lambda_j V(i,j))
-__global__ void __launch_bounds__(dmma::NT) refine_gemm_kernel(int n, const double *__restrict__ F, long ldf,
+__global__ void __launch_bounds__(dmma::Sq::NT) refine_gemm_kernel(int n, const double *__restrict__ F, long ldf,
                                                                const double *__restrict__ V, long ldv,
                                                                const double *__restrict__ lam, double *__restrict__ P)
 {
     extern __shared__ __align__(16) double smem[];
-    const int m0 = blockIdx.x * dmma::BM, n0 = blockIdx.y * dmma::BN;
-    double acc[8][4][2];
-    dmma::tile_mma<false, false>(acc, smem, F, ldf, V, ldv, n, n, n, m0, n0);
+    using C = dmma::Sq;
+    const int m0 = blockIdx.x * C::BM, n0 = blockIdx.y * C::BN;
+    double acc[C::FM][C::FN][2];
+    dmma::tile_mma<C, false, false>(acc, smem, F, ldf, V, ldv, n, n, 0, n, m0, n0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = warp & 1, wn = warp >> 1, r = lane >> 2, q = lane & 3;
     double *red = smem;   // [2 wm][128 columns][3] after the pipeline has drained
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(dmma::NT) refine_gemm_kernel(int n, const doub
             }
         }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < 128 * 3; idx += dmma::NT) {
+    for (int idx = threadIdx.x; idx < 128 * 3; idx += C::NT) {
         const int cl = idx / 3, w = idx % 3, col = n0 + cl;
         if (col < n) P[((long)blockIdx.x * 3 + w) * n + col] = red[cl * 3 + w] + red[(128 + cl) * 3 + w];
     }
@@ -165,8 +166,15 @@ __global__ void refine_order_kernel(int n, double *lam, double *V, long ldv, dou
 
 size_t refine_workspace_doubles(int n)
 {
-    const size_t ntm = (size_t)(n + dmma::BM - 1) / dmma::BM;
+    const size_t ntm = (size_t)(n + dmma::Sq::BM - 1) / dmma::Sq::BM;
     return (size_t)n * n + ntm * 3 * n + 64;
+}
+
+int symmetrize_lower(int n, const double *A, long lda, double *F, long ldf, cudaStream_t s)
+{
+    dim3 g((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32)), blk(32, 8);
+    symmetrize_lower_kernel<<<g, blk, 0, s>>>(n, A, lda, F, ldf);
+    return cuda_fail(cudaGetLastError(), "symmetrize");
 }
 
 // F (n*n doubles of workspace) <- the lower triangle of A mirrored: call before
@@ -183,13 +191,13 @@ int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s)
 int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *P, double *corr, double *resid,
                  int *flag, cudaStream_t s)
 {
-    constexpr int bytes = dmma::Smem<false, false>::BYTES;
+    constexpr int bytes = dmma::Smem<dmma::Sq, false, false>::BYTES;
     static_assert(bytes >= 2 * 128 * 3 * 8, "epilogue reduction fits the pipeline's shared memory");
     cudaError_t e = cudaFuncSetAttribute(refine_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_fail(e, "refine: shared memory attribute");
-    const int ntm = (n + dmma::BM - 1) / dmma::BM;
-    dim3 g((unsigned)ntm, (unsigned)((n + dmma::BN - 1) / dmma::BN));
-    refine_gemm_kernel<<<g, dmma::NT, bytes, s>>>(n, F, n, V, ldv, lam, P);
+    const int ntm = (n + dmma::Sq::BM - 1) / dmma::Sq::BM;
+    dim3 g((unsigned)ntm, (unsigned)((n + dmma::Sq::BN - 1) / dmma::Sq::BN));
+    refine_gemm_kernel<<<g, dmma::Sq::NT, bytes, s>>>(n, F, n, V, ldv, lam, P);
     refine_finalize_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, ntm, P, lam, corr, resid);
     refine_order_kernel<<<1, 1024, 0, s>>>(n, lam, V, ldv, corr, resid, 64, flag);
     return cuda_fail(cudaGetLastError(), "refine launch");

@@ -1,0 +1,758 @@
+// Dense symmetric eigensolver for sm_100a: two-stage reduction to tridiagonal
+// form, divide and conquer, back-transformation.
+//
+// The reference's DSYEV (LAP_DSYEV, src/libs/ZCOM/LAPACK_calls.f90:54-76,
+// called from diag_hd.f90:312) reduces A = Q T Q^T one column at a time
+// (DSYTRD: every column reads the whole trailing matrix, a latency-bound
+// matrix-vector product per column on a GPU) and diagonalises T.  Here the
+// reduction goes through a band matrix, as in LAPACK's two-stage DSYTRD_2STAGE:
+//
+//   1. dense -> band (bandwidth NB): per panel of NB columns a Householder QR
+//      (one cooperative kernel, the panel in shared memory of a few CTAs, one
+//      grid barrier per column), then the two-sided update of the trailing
+//      matrix A22 <- (I - V T V^T)^T A22 (I - V T V^T) as FP64 tensor-core
+//      GEMMs: X = A22 V, Y = X T - 1/2 V (T^T V^T X T), A22 -= V Y^T + Y V^T
+//      (one GEMM of inner size 2 NB over the [V | Y | V] buffer);
+//   2. band -> tridiagonal: bulge chasing (sweeps of Householder reflectors of
+//      length NB, each annihilating one column and chasing the bulge down the
+//      band), one persistent cooperative kernel (syevd2 stage 2 below);
+//   3. tridiagonal eigenpairs by divide and conquer (tridiag_dc.cu);
+//   4. back-transformation: the stage-2 reflectors (in blocks of NB sweeps) and
+//      the stage-1 panels (compact WY, GEMMs), applied to the eigenvectors.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "ctx.h"
+#include "dgemm.h"
+
+namespace bsrg {
+namespace {
+
+constexpr int NB = 32;              // bandwidth of the intermediate band matrix
+constexpr int PQ_ROWS = 512;        // panel rows held in shared memory per CTA
+constexpr int PQ_NT = 256;
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // bound of every device-side wait (2 s)
+
+__device__ __forceinline__ unsigned long long gtime()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier (all CTAs co-resident: cooperative launch).  bar[0] arrivals,
+// bar[1] generation.  A wait longer than WAIT_NS sets *err and every CTA leaves.
+__device__ bool grid_sync(unsigned *bar, int *err, unsigned nblocks)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = bar + 1;
+        const unsigned my = *vgen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == nblocks - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const unsigned long long t0 = gtime();
+            while (*vgen == my) {
+                if (*(volatile int *)err) break;
+                if (gtime() - t0 > WAIT_NS) { atomicExch(err, 1); break; }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile int *)err == 0;
+}
+
+// ---------------------------------------------------------------------------
+// stage 1: panel QR
+// ---------------------------------------------------------------------------
+struct PanelArgs {
+    double *P;          // panel (m x NB), leading dimension ldp: rows j+NB.., columns j..j+NB-1 of A
+    long ldp;
+    int m, rpc;         // rows, rows per CTA
+    double *V;          // [V | Y | V] buffer (ld m): V written to columns 0..NB-1 and 2NB..3NB-1
+    double *Vs;         // the saved V of this panel for the back-transformation (ld m)
+    double *T;          // NB x NB (ld NB), upper triangular
+    double *Ts;         // saved copy of T
+    double *part;       // per CTA, per column parity: NB dots + NB pivot-row values
+    double *gram;       // per CTA: NB x NB Gram partial
+    unsigned *bar;
+    int *err;
+};
+
+// Householder QR of the panel, LAPACK's dgeqrf/dlarfg conventions:
+// H_c = I - tau_c v_c v_c^T, v_c(c) = 1, P = H_0 ... H_{NB-1} [R; 0].
+__global__ void __launch_bounds__(PQ_NT) panel_qr_kernel(PanelArgs a)
+{
+    extern __shared__ __align__(16) double ps[];       // rpc x (NB + 1)
+    __shared__ double tot[NB], piv[NB], wv[NB], tau_s[NB];
+    __shared__ double sc_tau, sc_scale, sc_beta;
+    const int cta = blockIdx.x, G = gridDim.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int m = a.m, r0 = cta * a.rpc, nr = max(0, min(a.rpc, m - r0));
+    constexpr int LD = NB + 1;
+    for (int q = tid; q < nr * NB; q += PQ_NT) {
+        const int r = q % nr, c = q / nr;
+        ps[r * LD + c] = a.P[(r0 + r) + a.ldp * (long)c];
+    }
+    const int kb = min(m, NB);
+    __syncthreads();
+    for (int c = 0; c < kb; c++) {
+        double *buf = a.part + ((long)cta * 2 + (c & 1)) * 2 * NB;
+        // partial dots over my rows below the pivot: g_k = sum P(r, c) P(r, k), k >= c
+        for (int k = c + warp; k < NB; k += PQ_NT / 32) {
+            double s = 0.0;
+            for (int r = lane; r < nr; r += 32)
+                if (r0 + r > c) s += ps[r * LD + c] * ps[r * LD + k];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) buf[k] = s;
+        }
+        if (cta == 0)
+            for (int k = c + tid; k < NB; k += PQ_NT) buf[NB + k] = ps[c * LD + k];
+        __threadfence();
+        if (!grid_sync(a.bar, a.err, G)) return;
+        for (int k = c + tid; k < NB; k += PQ_NT) {
+            double s = 0.0;
+            for (int q = 0; q < G; q++) s += __ldcg(a.part + ((long)q * 2 + (c & 1)) * 2 * NB + k);
+            tot[k] = s;
+            piv[k] = __ldcg(a.part + (c & 1) * 2 * NB + NB + k);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const double alpha = piv[c], sigma = tot[c];
+            if (sigma == 0.0) { sc_tau = 0.0; sc_scale = 0.0; sc_beta = alpha; }
+            else {
+                const double beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+                sc_tau = (beta - alpha) / beta;
+                sc_scale = 1.0 / (alpha - beta);
+                sc_beta = beta;
+            }
+            tau_s[c] = sc_tau;
+        }
+        __syncthreads();
+        const double tau = sc_tau, scale = sc_scale;
+        for (int k = c + 1 + tid; k < NB; k += PQ_NT) wv[k] = piv[k] + scale * tot[k];   // v^T P(:, k)
+        __syncthreads();
+        // P(:, k) -= tau v w_k, k > c: rows below the pivot, then the pivot row (CTA 0)
+        for (int q = tid; q < nr * (NB - c - 1); q += PQ_NT) {
+            const int r = q % nr, k = c + 1 + q / nr;
+            if (r0 + r > c) ps[r * LD + k] -= tau * scale * ps[r * LD + c] * wv[k];
+        }
+        if (cta == 0)
+            for (int k = c + 1 + tid; k < NB; k += PQ_NT) ps[c * LD + k] -= tau * wv[k];
+        __syncthreads();
+        for (int r = tid; r < nr; r += PQ_NT)
+            if (r0 + r > c) ps[r * LD + c] *= scale;        // v below the pivot
+        if (cta == 0 && tid == 0) ps[c * LD + c] = sc_beta;
+        __syncthreads();
+    }
+    // Gram of V (unit diagonal, zero above), partial over my rows
+    double *gp = a.gram + (long)cta * NB * NB;
+    for (int q = tid; q < NB * NB; q += PQ_NT) {
+        const int i = q % NB, j = q / NB;
+        double s = 0.0;
+        if (i <= j && j < kb)
+            for (int r = 0; r < nr; r++) {
+                const int gr = r0 + r;
+                const double vi = gr > i ? ps[r * LD + i] : (gr == i ? 1.0 : 0.0);
+                const double vj = gr > j ? ps[r * LD + j] : (gr == j ? 1.0 : 0.0);
+                s += vi * vj;
+            }
+        gp[q] = s;
+    }
+    // V out (unit diagonal, zeros above; columns beyond kb are zero) and the band form of the panel
+    for (int q = tid; q < nr * NB; q += PQ_NT) {
+        const int r = q % nr, c = q / nr, gr = r0 + r;
+        const double v = c < kb ? (gr > c ? ps[r * LD + c] : (gr == c ? 1.0 : 0.0)) : 0.0;
+        a.V[gr + (long)m * c] = v;
+        a.V[gr + (long)m * (2 * NB + c)] = v;
+        a.Vs[gr + (long)m * c] = v;
+        a.P[gr + a.ldp * (long)c] = gr <= c ? ps[r * LD + c] : 0.0;
+    }
+    __threadfence();
+    if (!grid_sync(a.bar, a.err, G)) return;
+    if (cta != 0) return;
+    // T from the Gram matrix: T(c,c) = tau_c, T(0:c, c) = -tau_c T(0:c, 0:c) G(0:c, c)
+    double *Gs = ps;                      // reuse: NB x NB
+    for (int q = tid; q < NB * NB; q += PQ_NT) {
+        double s = 0.0;
+        for (int g = 0; g < G; g++) s += __ldcg(a.gram + (long)g * NB * NB + q);
+        Gs[q] = s;
+    }
+    __shared__ double Tt[NB][NB + 1];
+    for (int q = tid; q < NB * NB; q += PQ_NT) Tt[q % NB][q / NB] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < kb; c++) {
+        if (tid < c) {
+            double s = 0.0;
+            for (int l = tid; l < c; l++) s += Tt[tid][l] * Gs[l + NB * c];
+            wv[tid] = s;
+        }
+        __syncthreads();
+        if (tid < c) Tt[tid][c] = -tau_s[c] * wv[tid];
+        if (tid == 0) Tt[c][c] = tau_s[c];
+        __syncthreads();
+    }
+    for (int q = tid; q < NB * NB; q += PQ_NT) {
+        a.T[q] = Tt[q % NB][q / NB];
+        a.Ts[q] = Tt[q % NB][q / NB];
+    }
+}
+
+// Y = X T (rows), partial M = V^T Y per chunk of 128 rows.  X, V, Y: ld m.
+__global__ void __launch_bounds__(128) ypass1_kernel(int m, const double *__restrict__ X, const double *__restrict__ V,
+                                                     const double *__restrict__ T, double *Y, double *Mp)
+{
+    __shared__ double Ts[NB][NB + 1];
+    extern __shared__ __align__(16) double ysm[];        // Vs, Ys: 128 x (NB + 1) each
+    double (*Vs)[NB + 1] = (double (*)[NB + 1])ysm;
+    double (*Ys)[NB + 1] = (double (*)[NB + 1])(ysm + 128 * (NB + 1));
+    const int tid = threadIdx.x, r0 = blockIdx.x * 128, r = r0 + tid;
+    for (int q = tid; q < NB * NB; q += 128) Ts[q % NB][q / NB] = T[q];
+    __syncthreads();
+    double x[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) x[k] = r < m ? X[r + (long)m * k] : 0.0;
+#pragma unroll
+    for (int c = 0; c < NB; c++) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; k++) s += x[k] * Ts[k][c];
+        Ys[tid][c] = s;
+        Vs[tid][c] = r < m ? V[r + (long)m * c] : 0.0;
+        if (r < m) Y[r + (long)m * c] = s;
+    }
+    __syncthreads();
+    for (int q = tid; q < NB * NB; q += 128) {
+        const int i = q % NB, j = q / NB;
+        double s = 0.0;
+        for (int rr = 0; rr < 128; rr++) s += Vs[rr][i] * Ys[rr][j];
+        Mp[(long)blockIdx.x * NB * NB + q] = s;
+    }
+}
+
+// M = sum of the chunk partials, M2 = 1/2 T^T M, Y -= V M2 (rows)
+__global__ void __launch_bounds__(128) ypass2_kernel(int m, int nchunk, const double *__restrict__ V,
+                                                     const double *__restrict__ T, const double *__restrict__ Mp,
+                                                     double *Y)
+{
+    __shared__ double Ms[NB][NB + 1], M2[NB][NB + 1], Ts[NB][NB + 1];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < NB * NB; q += 128) {
+        double s = 0.0;
+        for (int ch = 0; ch < nchunk; ch++) s += Mp[(long)ch * NB * NB + q];
+        Ms[q % NB][q / NB] = s;
+        Ts[q % NB][q / NB] = T[q];
+    }
+    __syncthreads();
+    for (int q = tid; q < NB * NB; q += 128) {
+        const int i = q % NB, j = q / NB;
+        double s = 0.0;
+        for (int l = 0; l <= i; l++) s += Ts[l][i] * Ms[l][j];     // T upper: T^T(i,l) = T(l,i), l <= i
+        M2[i][j] = 0.5 * s;
+    }
+    __syncthreads();
+    const int r = blockIdx.x * 128 + tid;
+    if (r >= m) return;
+    double v[NB];
+#pragma unroll
+    for (int k = 0; k < NB; k++) v[k] = V[r + (long)m * k];
+#pragma unroll
+    for (int c = 0; c < NB; c++) {
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < NB; k++) s += v[k] * M2[k][c];
+        Y[r + (long)m * c] -= s;
+    }
+}
+
+constexpr int YP1_SMEM = 2 * 128 * (NB + 1) * (int)sizeof(double);
+
+// AB[d + 2NB c] = A(c + d, c), d < 2NB (rows beyond the band zero: room for the bulges)
+__global__ void band_extract_kernel(int n, const double *__restrict__ A, long lda, double *AB)
+{
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)n * 2 * NB) return;
+    const int d = (int)(idx % (2 * NB)), c = (int)(idx / (2 * NB));
+    AB[idx] = (d <= NB && c + d < n) ? A[(c + d) + lda * (long)c] : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// stage 2: band -> tridiagonal (bulge chasing)
+// ---------------------------------------------------------------------------
+// Band storage: A(r, c), r >= c, r - c < 2NB, at AB[(r - c) + 2NB c] (the NB rows
+// below the band hold the bulges).  Sweep j annihilates column j below the
+// subdiagonal and chases the bulge: task (j, i) has the window rows
+// r0 = j + 1 + i NB .. r1 = min(r0 + NB, n) - 1 and reduces column col (= j for
+// i = 0, the previous window's first column otherwise) with one reflector H,
+// applied from the left to the rest of the previous bulge (columns col+1..r0-1),
+// from both sides to the diagonal block, and from the right to the NB rows
+// below the window (creating the next bulge).  Task (j, i) may run once sweep
+// j-1 has completed step i+2 (their footprints are disjoint from then on).
+constexpr int LDAB = 2 * NB;
+
+__host__ __device__ __forceinline__ int sweep_steps(int n, int j) { return j <= n - 3 ? (n - 3 - j) / NB + 1 : 0; }
+
+struct Sb2stArgs {
+    double *AB;
+    int n;
+    double *V2;        // reflectors: V2[((long)j * S + i) * NB + t]
+    double *tau2;      // tau2[(long)j * S + i]
+    int S;
+    int *progress;     // completed steps per sweep (zero on entry)
+    int *err;
+};
+
+// one warp per worker CTA; workers take sweeps j = blockIdx.x, + gridDim.x, ...
+__global__ void __launch_bounds__(32) sb2st_kernel(Sb2stArgs a)
+{
+    __shared__ double Lb[NB][NB + 1], Ds[NB][NB + 1], Bs[NB][NB + 1];
+    __shared__ double vs[NB], ws_[NB];
+    const int t = threadIdx.x, n = a.n;
+    double *AB = a.AB;
+    auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
+    for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
+        const int nst = sweep_steps(n, j);
+        const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
+        for (int i = 0; i < nst; i++) {
+            if (j > 0) {
+                const int need = min(i + 3, nprev);
+                if (t == 0) {
+                    volatile int *pg = a.progress + (j - 1);
+                    const unsigned long long t0 = gtime();
+                    while (*pg < need) {
+                        if (*(volatile int *)a.err) break;
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                    }
+                    __threadfence();
+                }
+                __syncwarp();
+                if (*(volatile int *)a.err) return;
+            }
+            const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+            const int col = i == 0 ? j : r0 - NB;
+            const int nl = r0 - col - 1;                        // left columns col+1 .. r0-1
+            const int r2 = min(r1 + NB, n), nb2 = r2 - r1;      // rows below the window
+            // ---- loads (through L2: other workers write the band) ----
+            const double x = t < L ? __ldcg(at(r0 + t, col)) : 0.0;
+            for (int c = 0; c < nl; c++) Lb[t][c] = t < L ? __ldcg(at(r0 + t, col + 1 + c)) : 0.0;
+            for (int a2 = 0; a2 < L; a2++) Ds[a2][t] = (t < L && a2 >= t) ? __ldcg(at(r0 + a2, r0 + t)) : 0.0;
+            for (int q = 0; q < nb2; q++) Bs[q][t] = t < L ? __ldcg(at(r1 + q, r0 + t)) : 0.0;
+            // ---- the reflector ----
+            double sig = (t >= 1 && t < L) ? x * x : 0.0;
+            for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+            const double alpha = __shfl_sync(0xffffffffu, x, 0);
+            double tau = 0.0, scale = 0.0, beta = alpha;
+            if (sig != 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+                tau = (beta - alpha) / beta;
+                scale = 1.0 / (alpha - beta);
+            }
+            const double v = t == 0 ? 1.0 : (t < L ? x * scale : 0.0);
+            vs[t] = v;
+            a.V2[((long)j * a.S + i) * NB + t] = v;
+            if (t == 0) a.tau2[(long)j * a.S + i] = tau;
+            if (t < L) *at(r0 + t, col) = t == 0 ? beta : 0.0;
+            __syncwarp();
+            if (tau != 0.0) {
+                // left: columns col+1 .. r0-1 of the window rows (lane = column)
+                if (t < nl) {
+                    double w = 0.0;
+                    for (int q = 0; q < L; q++) w += vs[q] * Lb[q][t];
+                    for (int q = 0; q < L; q++) Lb[q][t] -= tau * vs[q] * w;
+                }
+                // two-sided on the diagonal block: p = tau D v, w = p - tau/2 (v^T p) v
+                double p = 0.0;
+                if (t < L)
+                    for (int b = 0; b < L; b++) p += (t >= b ? Ds[t][b] : Ds[b][t]) * vs[b];
+                p *= tau;
+                double vp = v * p;
+                for (int o = 16; o > 0; o >>= 1) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+                ws_[t] = p - 0.5 * tau * vp * v;
+                __syncwarp();
+                if (t < L)
+                    for (int a2 = t; a2 < L; a2++) Ds[a2][t] -= vs[a2] * ws_[t] + ws_[a2] * vs[t];
+                // right: rows below the window (lane = row)
+                if (t < nb2) {
+                    double sr = 0.0;
+                    for (int c = 0; c < L; c++) sr += Bs[t][c] * vs[c];
+                    for (int c = 0; c < L; c++) Bs[t][c] -= tau * sr * vs[c];
+                }
+                __syncwarp();
+                // ---- stores ----
+                for (int c = 0; c < nl; c++)
+                    if (t < L) *at(r0 + t, col + 1 + c) = Lb[t][c];
+                for (int a2 = 0; a2 < L; a2++)
+                    if (t < L && a2 >= t) *at(r0 + a2, r0 + t) = Ds[a2][t];
+                for (int q = 0; q < nb2; q++)
+                    if (t < L) *at(r1 + q, r0 + t) = Bs[q][t];
+            }
+            __threadfence();
+            __syncwarp();
+            if (t == 0) *(volatile int *)(a.progress + j) = i + 1;
+        }
+    }
+}
+
+// d(c) = A(c, c), e(c) = A(c+1, c)
+__global__ void tridiag_extract_kernel(int n, const double *__restrict__ AB, double *d, double *e)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    d[c] = AB[(long)LDAB * c];
+    if (c + 1 < n) e[c] = AB[1 + (long)LDAB * c];
+}
+
+// ---------------------------------------------------------------------------
+// back-transformation of the stage-2 reflectors
+// ---------------------------------------------------------------------------
+// Block (g, i): the step-i reflectors of sweeps j = g NB + q, q < NB, as one
+// compact WY factor I - V T V^T = H_{gNB} H_{gNB+1} ... (V column q occupies rows
+// q .. q + NB - 1 of the block's window, which starts at row g NB + 1 + i NB).
+// Applied to Z: groups g descending, within a group blocks i ascending, each
+// block's reflectors in the product order above -- the order of creation
+// reversed up to commuting (disjoint) pairs.
+__device__ __forceinline__ int q2_nvalid(int n, int g, int i)
+{
+    int nv = 0;
+    for (int q = 0; q < NB; q++) {
+        const int j = g * NB + q;
+        if (j < n - 2 && i < sweep_steps(n, j)) nv = q + 1;
+    }
+    return nv;
+}
+
+// T factor of every block (one CTA of 32 threads per block)
+__global__ void __launch_bounds__(32) q2_tfactor_kernel(int n, int S, const double *__restrict__ V2,
+                                                        const double *__restrict__ tau2, double *Tq)
+{
+    const int g = blockIdx.y, i = blockIdx.x, t = threadIdx.x;
+    double *T = Tq + ((long)g * S + i) * NB * NB;
+    __shared__ double Vb[2 * NB][NB + 1], Gs[NB][NB + 1], Tt[NB][NB + 1], tau[NB], tmp[NB];
+    const int nv = q2_nvalid(n, g, i);
+    for (int r = 0; r < 2 * NB; r++) Vb[r][t] = 0.0;
+    __syncwarp();
+    if (t < nv) {
+        const int j = g * NB + t;
+        for (int q = 0; q < NB; q++) Vb[t + q][t] = V2[((long)j * S + i) * NB + q];
+        tau[t] = tau2[(long)j * S + i];
+    } else tau[t] = 0.0;
+    __syncwarp();
+    for (int b = 0; b < NB; b++) {       // Gs[t][b] = V(:, t) . V(:, b)
+        double s = 0.0;
+        for (int r = 0; r < 2 * NB; r++) s += Vb[r][t] * Vb[r][b];
+        Gs[t][b] = s;
+        Tt[t][b] = 0.0;
+    }
+    __syncwarp();
+    for (int c = 0; c < nv; c++) {
+        if (t < c) {
+            double s = 0.0;
+            for (int l = t; l < c; l++) s += Tt[t][l] * Gs[l][c];
+            tmp[t] = s;
+        }
+        __syncwarp();
+        if (t < c) Tt[t][c] = -tau[c] * tmp[t];
+        if (t == 0) Tt[c][c] = tau[c];
+        __syncwarp();
+    }
+    for (int c = 0; c < NB; c++) T[t + NB * c] = Tt[t][c];
+}
+
+constexpr int Q2_COLS = 32;
+constexpr int Q2_NT = 256;
+constexpr int Q2_SMEM = (2 * (2 * NB) * (Q2_COLS + 1) + 2 * NB * (NB + 1)) * (int)sizeof(double);
+
+// Z (n x ncol, ldz) <- Q2 Z; one CTA per strip of Q2_COLS columns
+__global__ void __launch_bounds__(Q2_NT) q2_apply_kernel(int n, int S, int ncol, const double *__restrict__ V2,
+                                                         const double *__restrict__ Tq, double *Z, long ldz)
+{
+    extern __shared__ __align__(16) double qsm[];
+    double (*Zw)[Q2_COLS + 1] = (double (*)[Q2_COLS + 1])qsm;                    // 2NB rows of the window
+    double (*Vb)[Q2_COLS + 1] = (double (*)[Q2_COLS + 1])(qsm + 2 * NB * (Q2_COLS + 1));   // V (2NB x NB)
+    double (*Ts)[NB + 1] = (double (*)[NB + 1])(qsm + 4 * NB * (Q2_COLS + 1));
+    double (*W)[NB + 1] = (double (*)[NB + 1])(qsm + 4 * NB * (Q2_COLS + 1) + NB * (NB + 1));
+    const int tid = threadIdx.x, c0 = blockIdx.x * Q2_COLS;
+    const int cl = tid % Q2_COLS, rg = tid / Q2_COLS;        // column, row group (8)
+    const int ng = (n - 2 + NB - 1) / NB;
+    for (int g = ng - 1; g >= 0; g--) {
+        const int imax = sweep_steps(n, g * NB);
+        for (int i = 0; i < imax; i++) {
+            const int nv = q2_nvalid(n, g, i);
+            if (nv == 0) continue;
+            const int top = g * NB + 1 + i * NB;
+            const int nrow = min(2 * NB - 1, n - top);
+            __syncthreads();
+            for (int q = tid; q < 2 * NB * NB; q += Q2_NT) {
+                const int r = q % (2 * NB), c = q / (2 * NB);
+                double v = 0.0;
+                if (c < nv && r >= c && r < c + NB) {
+                    const int j = g * NB + c;
+                    v = V2[((long)j * S + i) * NB + (r - c)];
+                }
+                Vb[r][c] = v;
+            }
+            for (int q = tid; q < NB * NB; q += Q2_NT) Ts[q % NB][q / NB] = Tq[((long)g * S + i) * NB * NB + q];
+            for (int q = tid; q < 2 * NB * Q2_COLS; q += Q2_NT) {
+                const int r = q % (2 * NB), c = q / (2 * NB);
+                Zw[r][c] = (r < nrow && c0 + c < ncol) ? Z[(top + r) + ldz * (long)(c0 + c)] : 0.0;
+            }
+            __syncthreads();
+            // W = V^T Zw (NB x cols): thread (cl, rg) computes rows q = rg, rg + 8, ...
+            for (int q = rg; q < NB; q += Q2_NT / Q2_COLS) {
+                double sacc = 0.0;
+                for (int r = q; r < q + NB && r < 2 * NB; r++) sacc += Vb[r][q] * Zw[r][cl];
+                W[q][cl] = sacc;
+            }
+            __syncthreads();
+            // W2 = T W (T upper), kept in registers then written back to W
+            double w2[NB / (Q2_NT / Q2_COLS)];
+#pragma unroll
+            for (int k = 0; k < NB / (Q2_NT / Q2_COLS); k++) {
+                const int q = rg + k * (Q2_NT / Q2_COLS);
+                double sacc = 0.0;
+                for (int l = q; l < NB; l++) sacc += Ts[q][l] * W[l][cl];
+                w2[k] = sacc;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < NB / (Q2_NT / Q2_COLS); k++) W[rg + k * (Q2_NT / Q2_COLS)][cl] = w2[k];
+            __syncthreads();
+            // Zw -= V W2
+            for (int r = rg; r < nrow; r += Q2_NT / Q2_COLS) {
+                double sacc = 0.0;
+                const int qlo = max(0, r - NB + 1), qhi = min(NB - 1, r);
+                for (int q = qlo; q <= qhi; q++) sacc += Vb[r][q] * W[q][cl];
+                if (c0 + cl < ncol) Z[(top + r) + ldz * (long)(c0 + cl)] = Zw[r][cl] - sacc;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// ---- stage 1 driver ----
+struct Sy2sbWork {
+    double *VYV;       // m x 3NB
+    double *X;         // m x NB
+    double *T;         // NB x NB
+    double *Mp;        // chunks x NB x NB
+    double *part;      // PQ CTAs x 4NB
+    double *gram;      // PQ CTAs x NB x NB
+    unsigned *bar;     // 2
+    int *err;
+    double *gemm_ws;   // split-K workspace
+    size_t gemm_ws_doubles;
+};
+
+int sy2sb_panels(int n) { return n > NB ? (n - 1) / NB : 0; }   // panels j = 0, NB, ... with j + NB < n
+
+// Saved panels for the back-transformation: V of panel p (m_p x NB, ld m_p) at Vsave + voff(p),
+// T of panel p at Tsave + p NB^2.
+size_t sy2sb_vsave_doubles(int n)
+{
+    size_t t = 0;
+    for (int j = 0; j + NB < n; j += NB) t += (size_t)(n - j - NB) * NB;
+    return t + 64;
+}
+
+int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Tsave, const Sy2sbWork &w)
+{
+    cudaError_t e;
+    const int smem = PQ_ROWS * (NB + 1) * (int)sizeof(double);
+    if ((e = cudaFuncSetAttribute(panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(ypass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, YP1_SMEM)) != cudaSuccess)
+        return cuda_fail(e, "sy2sb smem");
+    size_t voff = 0;
+    int p = 0;
+    for (int j = 0; j + NB < n; j += NB, p++) {
+        const int m = n - j - NB;
+        int G = (m + PQ_ROWS - 1) / PQ_ROWS;
+        G = std::max(1, std::min(G, std::max(1, m / NB)));      // CTA 0 holds the NB pivot rows
+        const int rpc = (m + G - 1) / G;
+        if (rpc > PQ_ROWS) { set_error("sy2sb: panel of %d rows does not fit", m); return BSRG_ERR_ARG; }
+        PanelArgs a;
+        a.P = A + (j + NB) + lda * (long)j;
+        a.ldp = lda;
+        a.m = m;
+        a.rpc = rpc;
+        a.V = w.VYV;
+        a.Vs = Vsave + voff;
+        a.T = w.T;
+        a.Ts = Tsave + (size_t)p * NB * NB;
+        a.part = w.part;
+        a.gram = w.gram;
+        a.bar = w.bar;
+        a.err = w.err;
+        void *args[] = {&a};
+        if ((e = cudaLaunchCooperativeKernel((const void *)panel_qr_kernel, G, PQ_NT, args, smem, st)) != cudaSuccess)
+            return cuda_fail(e, "sy2sb panel");
+        voff += (size_t)m * NB;
+        // trailing update of A22 = A(j+NB:, j+NB:) (m x m, full symmetric storage)
+        double *A22 = A + (j + NB) + lda * (long)(j + NB);
+        double *Vp = w.VYV, *Yp = w.VYV + (long)m * NB;
+        int rc = dgemm(false, false, m, NB, m, 1.0, A22, lda, Vp, m, 0.0, w.X, m, st, w.gemm_ws, w.gemm_ws_doubles);
+        if (rc != BSRG_OK) return rc;
+        const int nch = (m + 127) / 128;
+        ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp);
+        ypass2_kernel<<<nch, 128, 0, st>>>(m, nch, Vp, w.T, w.Mp, Yp);
+        // A22 -= [V Y] [Y V]^T
+        rc = dgemm(false, true, m, m, 2 * NB, -1.0, w.VYV, m, Yp, m, 1.0, A22, lda, st);
+        if (rc != BSRG_OK) return rc;
+    }
+    return cuda_fail(cudaGetLastError(), "sy2sb");
+}
+
+}  // namespace bsrg
+
+namespace bsrg {
+
+int symmetrize_lower(int n, const double *A, long lda, double *F, long ldf, cudaStream_t s);   // refine.cu
+
+// Workspace of dense_syevd in doubles (everything but the output Z)
+size_t syevd2_workspace_doubles(int n)
+{
+    const size_t nn = (size_t)n * n;
+    const size_t S = (size_t)sweep_steps(n, 0) + 1, ng = (size_t)(n + NB - 1) / NB + 1;
+    size_t t = 0;
+    t += nn + 64;                                  // working copy of A
+    t += (size_t)LDAB * n + 64;                    // band
+    t += sy2sb_vsave_doubles(n) + 64;              // stage-1 V
+    t += (size_t)(sy2sb_panels(n) + 1) * NB * NB + 64;   // stage-1 T
+    t += (size_t)n * S * NB + 64;                  // stage-2 V
+    t += (size_t)n * S + 64;                       // stage-2 tau
+    t += ng * S * NB * NB + 64;                    // stage-2 block T
+    t += 3 * (size_t)n + 256;                      // d, e, progress (ints fit in doubles)
+    t += (size_t)n * 3 * NB + (size_t)n * NB + 4 * NB * NB + 64;   // VYV, X, T, Mp chunk partials (below)
+    t += ((size_t)n / 128 + 2) * NB * NB + 64;
+    t += (size_t)(n / NB + 8) * 6 * NB + 64;       // panel partials + Gram
+    t += 2 * (size_t)NB * n + 64;                  // Q1 W1, W2
+    t += 8 * (size_t)NB * n + 64;                  // split-K slices
+    t += dc_workspace_bytes(n) / 8 + 64;           // divide and conquer
+    return t + 4096;
+}
+
+// Eigenvalues (ascending, w) and eigenvectors (Z, ldz) of the symmetric A (lower
+// triangle referenced).  Z may be A itself.  ws: syevd2_workspace_doubles(n).
+int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
+                size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches)
+{
+    int nl = 0;
+    if (n < 1) return BSRG_OK;
+    cudaStream_t st = c->stream;
+    cudaError_t e;
+    if (ws_doubles < syevd2_workspace_doubles(n)) { set_error("dsyevd: workspace too small"); return BSRG_ERR_NOMEM; }
+    if (n > 10240) { set_error("dsyevd: n=%d above 10240", n); return BSRG_ERR_ARG; }
+    const size_t nn = (size_t)n * n;
+    const int S = sweep_steps(n, 0) + 1, ng = (n + NB - 1) / NB + 1;
+    size_t off = 0;
+    auto take = [&](size_t cnt) { off = (off + 31) & ~(size_t)31; double *p = ws + off; off += cnt; return p; };
+    double *Wk = take(nn), *AB = take((size_t)LDAB * n);
+    double *V1 = take(sy2sb_vsave_doubles(n)), *T1 = take((size_t)(sy2sb_panels(n) + 1) * NB * NB);
+    double *V2 = take((size_t)n * S * NB), *tau2 = take((size_t)n * S), *Tq = take((size_t)ng * S * NB * NB);
+    double *dv = take(n), *ev = take(n + 1);
+    int *progress = (int *)take(n / 2 + 8);
+    Sy2sbWork sw;
+    sw.VYV = take((size_t)n * 3 * NB);
+    sw.X = take((size_t)n * NB);
+    sw.T = take(NB * NB);
+    sw.Mp = take(((size_t)n / 128 + 2) * NB * NB);
+    sw.part = take((size_t)(n / NB + 8) * 4 * NB);
+    sw.gram = take((size_t)(n / NB + 8) * NB * NB);
+    int *flags = (int *)take(8);                   // bar[2], err, err2
+    sw.bar = (unsigned *)flags;
+    sw.err = flags + 2;
+    double *W1 = take((size_t)NB * n), *W2 = take((size_t)NB * n);
+    sw.gemm_ws_doubles = 8 * (size_t)NB * n;
+    sw.gemm_ws = take(sw.gemm_ws_doubles);
+    double *dcw = take(dc_workspace_bytes(n) / 8 + 8);
+    if (off > ws_doubles) { set_error("dsyevd: workspace layout"); return BSRG_ERR_NOMEM; }
+    if ((e = cudaMemsetAsync(flags, 0, 8 * sizeof(int), st)) != cudaSuccess ||
+        (e = cudaMemsetAsync(progress, 0, sizeof(int) * n, st)) != cudaSuccess)
+        return cuda_fail(e, "dsyevd init");
+    // 1. full symmetric working copy, dense -> band
+    int rc = symmetrize_lower(n, A, lda, Wk, n, st);
+    if (rc == BSRG_OK) rc = sy2sb(st, n, Wk, n, V1, T1, sw);
+    if (rc != BSRG_OK) return rc;
+    band_extract_kernel<<<(unsigned)(((long)n * LDAB + 255) / 256), 256, 0, st>>>(n, Wk, n, AB);
+    // 2. band -> tridiagonal
+    if (n > 2) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+        int per = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st_kernel, 32, 0);
+        const int workers = std::max(1, std::min(n - 2, std::min(nsm * std::max(per, 1), 2 * nsm)));
+        Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
+        void *args[] = {&a2};
+        if ((e = cudaLaunchCooperativeKernel((const void *)sb2st_kernel, workers, 32, args, 0, st)) != cudaSuccess)
+            return cuda_fail(e, "dsyevd bulge chasing");
+    }
+    tridiag_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, AB, dv, ev);
+    // 3. tridiagonal eigenpairs into Z
+    rc = tridiag_dc(st, n, dv, ev, w, Z, ldz, dcw, dc_workspace_bytes(n), pinned, pinned_bytes);
+    if (rc != BSRG_OK) return rc;
+    // 4. back-transformation: Q2 then Q1
+    if (n > 2) {
+        dim3 gt((unsigned)S, (unsigned)((n - 2 + NB - 1) / NB));
+        q2_tfactor_kernel<<<gt, 32, 0, st>>>(n, S, V2, tau2, Tq);
+        if ((e = cudaFuncSetAttribute(q2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2_SMEM)) !=
+            cudaSuccess)
+            return cuda_fail(e, "dsyevd Q2 smem");
+        q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
+    }
+    {
+        std::vector<size_t> voff;
+        size_t vo = 0;
+        for (int j = 0; j + NB < n; j += NB) { voff.push_back(vo); vo += (size_t)(n - j - NB) * NB; }
+        for (int p = (int)voff.size() - 1; p >= 0; p--) {
+            const int j = p * NB, m = n - j - NB;
+            const double *Vp = V1 + voff[p], *Tp = T1 + (size_t)p * NB * NB;
+            double *Zs = Z + (j + NB);
+            rc = dgemm(true, false, NB, n, m, 1.0, Vp, m, Zs, ldz, 0.0, W1, NB, st, sw.gemm_ws, sw.gemm_ws_doubles);
+            if (rc == BSRG_OK) rc = dgemm(false, false, NB, n, NB, 1.0, Tp, NB, W1, NB, 0.0, W2, NB, st);
+            if (rc == BSRG_OK) rc = dgemm(false, false, m, n, NB, -1.0, Vp, m, W2, NB, 1.0, Zs, ldz, st);
+            if (rc != BSRG_OK) return rc;
+        }
+    }
+    // device-side waits report through the flags
+    int hflag[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(hflag, flags + 2, sizeof(int) * 2, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e, "dsyevd");
+    if (hflag[0] != 0) {
+        set_error("dsyevd: a device-side wait timed out (%s)", hflag[0] == 2 ? "bulge chasing" : "panel barrier");
+        return BSRG_ERR_CUDA;
+    }
+    // kernels of this library per call: symmetrize, per panel (QR, 2 passes, 2 GEMMs + split-K reduce),
+    // band, bulge chasing, extraction, D&C (counted approximately), Q2 (2), Q1 (3 per panel)
+    const int np = sy2sb_panels(n);
+    nl = 1 + np * 6 + 3 + 2 + (int)(3.5 * std::log2((double)std::max(n, 2))) * 8 + 3 * np + np;
+    if (launches) *launches = nl;
+    return BSRG_OK;
+}
+
+}  // namespace bsrg
+
+using namespace bsrg;
+
+extern "C" int bsrg_dsyevd(bsrg_ctx *c, int n, const double *A, int lda, double *w, double *Z, int ldz)
+{
+    if (!c || (n > 0 && (!A || !w || !Z))) { set_error("dsyevd: null argument"); return BSRG_ERR_ARG; }
+    if (n < 0 || lda < (n > 0 ? n : 1) || ldz < (n > 0 ? n : 1)) {
+        set_error("dsyevd: n=%d lda=%d ldz=%d", n, lda, ldz);
+        return BSRG_ERR_ARG;
+    }
+    if (n == 0) return BSRG_OK;
+    cudaSetDevice(c->device);
+    int rc = ctx_reserve(c, syevd2_workspace_doubles(n) * sizeof(double) + 1024);
+    if (rc == BSRG_OK) rc = ctx_reserve_pinned(c, dc_pinned_bytes(n));
+    if (rc != BSRG_OK) return rc;
+    rc = dense_syevd(c, n, A, lda, w, Z, ldz, (double *)c->ws, c->ws_bytes / sizeof(double), c->pinned,
+                     c->pinned_bytes, nullptr);
+    cudaEventRecord(c->ev_stage, c->stream);
+    return rc;
+}

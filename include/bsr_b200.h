@@ -328,6 +328,14 @@ int bsrg_dsytrd(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, do
  *      and workspace; reads small per-level counts back to the host. */
 int bsrg_dstedc(bsrg_ctx *c, int n, const double *d, const double *e, double *w, double *Z, int ldz);
 
+/* ---- DSYEV('V','L') as called by LAP_DSYEV (src/libs/ZCOM/LAPACK_calls.f90:54-76,
+ *      from diag_hd.f90:312): all eigenvalues (w, ascending) and eigenvectors
+ *      (Z, ldz) of the symmetric A (lower triangle read, lda; Z may be A).
+ *      Two-stage reduction (dense -> band of width 32 -> tridiagonal), divide
+ *      and conquer, back-transformation.  n <= 10240.  Device; uses the
+ *      context's stream and workspace. */
+int bsrg_dsyevd(bsrg_ctx *c, int n, const double *A, int lda, double *w, double *Z, int ldz);
+
 /* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
  *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.
  *      t (ns+ks), P (ns,norb), coefficient arrays as in bsrg_assemble, all
