@@ -120,7 +120,8 @@ class Clocks:
 # ---------------------------------------------------------------------------
 def _assemble_groups_worker(args):
     """One process of the CPU assembly sample: the I_data groups of one multipole
-    for a slice of channel pairs (the block distribution of bsr_mat3_mpi)."""
+    for a slice of channel pairs (the block distribution of bsr_mat3_mpi).
+    Returns (seconds, records assembled)."""
     pw, k, chans_slice = args
     from oracle import oracle as O
     ob = O.Basis(pw["ks"], pw["t"])
@@ -134,84 +135,131 @@ def _assemble_groups_worker(args):
     t0 = time.perf_counter()
     O.assemble(ob, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], rkb_all, sub, want_s=False,
                want_acf=True)
-    return time.perf_counter() - t0
+    return time.perf_counter() - t0, int(sel.sum())
 
 
-def cpu_reference_step(pw, threads):
-    """Time a bounded sample of one config-2 solve on the CPU, extrapolated per stage.
+class CpuReference:
+    """The reference's CPU path for one partial wave (the oracle restating its
+    routines, LAPACK from scipy's OpenBLAS), timed on a bounded sample and
+    scaled stage by stage to one solve.  Every scale factor is reported.
 
-    Sample (about 20-40 s of CPU work):
-      R^k tables   mrk_cell for 2 of the kmax+1 multipoles            -> x (kmax+1)/2
-      assembly     every I_data group of one multipole (k = kmax/2),
-                   channel pairs dealt over `threads` processes     -> x (kmax+1)
-      channel eig  DSYGV for 4 channels                              -> x nch/4
-      transforms   bb^T H_ij bb for nch-1 off-diagonal blocks        -> x nb/(nch-1)
-      DSYEV('V')   the leading khm/4 principal submatrix             -> x 64 (n^3)
-    Returns (seconds per solve, stage seconds, description)."""
-    from concurrent.futures import ProcessPoolExecutor
-    import multiprocessing as mp
+    Sample (one step): mrk_cell for one multipole (x nk); every I_data group of
+    the middle multipole for `frac_ch` of the channels, channel pairs dealt over
+    `procs` processes as bsr_mat3_mpi deals blocks (x records_total /
+    records_sampled); DSYGV for `nchan` channels (x nch / nchan); `nblk` block
+    transforms (x nblocks / nblk); DSYEV('V') at n = khm / `div` (x div^3, its
+    n^3 cost)."""
 
+    def __init__(self, pw, procs, threads, frac_ch=0.25, nchan=4, nblk=39, div=8):
+        from oracle import oracle as O
+        self.pw, self.procs, self.threads = pw, max(1, procs), threads
+        self.frac_ch, self.nchan, self.nblk, self.div = frac_ch, nchan, nblk, div
+        ks, ns = pw["ks"], pw["ns"]
+        self.ob = O.Basis(ks, pw["t"])
+        sb = self.ob.band("sb")
+        S = np.zeros((ns, ns))
+        for jc in range(ks):
+            for i in range(ks - 1 - jc, ns):
+                j = i + jc - ks + 1
+                S[i, j] = S[j, i] = sb[i, jc]
+        self.S = S
+        self.hl = [self.ob.hl_full(l, pw["z"]) for l in range(int(pw["lch"].max()) + 1)]
+        self.khm = pw["nch"] * ns - int(np.sum(np.minimum(pw["lch"], ks - 2) + 1))
+        rng = np.random.default_rng(0)
+        n = self.khm // div
+        A = rng.standard_normal((n, n))
+        self.A = np.tril(A + A.T)
+        self.Hx = rng.standard_normal((ns, ns))
+        self.pool = None
+        if self.procs > 1:
+            from concurrent.futures import ProcessPoolExecutor
+            import multiprocessing as mp
+            self.pool = ProcessPoolExecutor(max_workers=self.procs, mp_context=mp.get_context("spawn"))
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.shutdown()
+
+    def sample(self):
+        """Run the sample once; returns (wall seconds of the sample, extrapolated seconds per solve, stages)."""
+        from scipy.linalg import lapack
+        from threadpoolctl import threadpool_limits
+        pw, ks, ns, kmax, nch = self.pw, self.pw["ks"], self.pw["ns"], self.pw["kmax"], self.pw["nch"]
+        st, scale = {}, {}
+        w0 = time.perf_counter()
+        with threadpool_limits(self.threads):
+            t0 = time.perf_counter()
+            self.ob.mrk_cell(kmax // 2)
+            st["rk_tables"], scale["rk_tables"] = time.perf_counter() - t0, float(kmax + 1)
+            kmid = kmax // 2
+            chans = np.arange(1, nch + 1)
+            pick = chans[: max(1, int(round(self.frac_ch * nch)))]
+            slices = [pick[q::self.procs] for q in range(self.procs)]
+            if self.pool is None:
+                res = [_assemble_groups_worker((pw, kmid, slices[0]))]
+            else:
+                res = list(self.pool.map(_assemble_groups_worker, [(pw, kmid, sl) for sl in slices]))
+            nrec = sum(r[1] for r in res)
+            st["assembly"] = max(r[0] for r in res)
+            scale["assembly"] = float(len(pw["coefs"]["c"])) / max(nrec, 1)
+            t0 = time.perf_counter()
+            bbs = []
+            for ich in range(self.nchan):
+                l = min(pw["lch"][ich], ks - 2)
+                i1 = l + 1
+                Hd = -0.5 * self.hl[pw["lch"][ich]] + pw["ech"][ich] * self.S
+                w, v, info = lapack.dsygv(Hd[i1:, i1:].copy(), self.S[i1:, i1:].copy(), itype=1, jobz="V",
+                                          uplo="U")[:3]
+                bb = np.zeros((ns, len(w)))
+                bb[i1:, :] = v
+                bbs.append(bb)
+            st["channel_eig"], scale["channel_eig"] = time.perf_counter() - t0, nch / self.nchan
+            t0 = time.perf_counter()
+            for q in range(self.nblk):
+                _ = bbs[q % self.nchan].T @ self.Hx @ bbs[(q + 1) % self.nchan]
+            st["transform"] = time.perf_counter() - t0
+            scale["transform"] = (nch * (nch + 1) // 2) / self.nblk
+            t0 = time.perf_counter()
+            lapack.dsyev(self.A, compute_v=1, lower=1)
+            st["dense_eig"], scale["dense_eig"] = time.perf_counter() - t0, float(self.div) ** 3
+        wall = time.perf_counter() - w0
+        total = sum(st[k] * scale[k] for k in st)
+        return wall, total, st, scale
+
+    def describe(self):
+        pw = self.pw
+        return ("%s, one solve extrapolated from a bounded sample per step: mrk_cell for 1/%d multipoles; every "
+                "I_data group of multipole %d for %d/%d channels over %d processes; DSYGV for %d/%d channels; "
+                "%d/%d block transforms; DSYEV('V') at n=%d scaled by %d^3 to khm=%d; %d OpenBLAS threads"
+                % (pw["name"], pw["kmax"] + 1, pw["kmax"] // 2, max(1, int(round(self.frac_ch * pw["nch"]))),
+                   pw["nch"], self.procs, self.nchan, pw["nch"], self.nblk, pw["nch"] * (pw["nch"] + 1) // 2,
+                   self.khm // self.div, self.div, self.khm, self.threads or (os.cpu_count() or 1)))
+
+
+def cpu_full_solve(pw, threads):
+    """One complete partial-wave solve on the CPU, nothing extrapolated: mrk_cell for
+    every multipole, the I_data assembly, diag_hd (DSYGV per channel, transform,
+    DSYEV('V')).  Returns seconds."""
+    from threadpoolctl import threadpool_limits
     from oracle import oracle as O
-    from scipy.linalg import lapack
+    with threadpool_limits(threads):
+        t0 = time.perf_counter()
+        ob = O.Basis(pw["ks"], pw["t"])
+        rkb_all = np.stack([ob.mrk_cell(k) for k in range(pw["kmax"] + 1)], axis=-1)
+        H = O.assemble(ob, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], np.asfortranarray(rkb_all),
+                       pw["coefs"], want_s=True, want_acf=False)
+        O.diag_hd(H["hcc"], H["scc"], pw["lch"], ob.ns, ob.ks, want_vectors=True)
+        return time.perf_counter() - t0
 
-    ks, ns, kmax, nch = pw["ks"], pw["ns"], pw["kmax"], pw["nch"]
-    ob = O.Basis(ks, pw["t"])
-    st = {}
-    t0 = time.perf_counter()
-    for k in (0, kmax):
-        ob.mrk_cell(k)
-    st["rk_tables"] = (time.perf_counter() - t0) * (kmax + 1) / 2
-    kmid = kmax // 2
-    chans = np.arange(1, nch + 1)
-    nproc = max(1, threads)
-    slices = [chans[q::nproc] for q in range(nproc)]
-    # the parallel assembly time is the slowest process's own compute time
-    # (process start-up and table set-up are not charged to the reference)
-    if nproc == 1:
-        wt = [_assemble_groups_worker((pw, kmid, slices[0]))]
-    else:
-        with ProcessPoolExecutor(max_workers=nproc, mp_context=mp.get_context("spawn")) as ex:
-            wt = list(ex.map(_assemble_groups_worker, [(pw, kmid, s) for s in slices]))
-    st["assembly"] = max(wt) * (kmax + 1)
-    # diag_hd pieces on the oracle's restatement, H built blockwise on the CPU for 4 channels
-    rng = np.random.default_rng(0)
-    sb = ob.band("sb")
-    S = np.zeros((ns, ns))
-    for jc in range(ks):
-        for i in range(ks - 1 - jc, ns):
-            j = i + jc - ks + 1
-            S[i, j] = S[j, i] = sb[i, jc]
-    hl = [ob.hl_full(l, pw["z"]) for l in range(pw["lch"].max() + 1)]
-    t0 = time.perf_counter()
-    bbs = []
-    for ich in range(4):
-        l = min(pw["lch"][ich], ks - 2)
-        i1 = l + 1
-        Hd = -0.5 * hl[pw["lch"][ich]] + pw["ech"][ich] * S
-        w, v, info = lapack.dsygv(Hd[i1:, i1:].copy(), S[i1:, i1:].copy(), itype=1, jobz="V", uplo="U")[:3]
-        bb = np.zeros((ns, len(w)))
-        bb[i1:, :] = v
-        bbs.append(bb)
-    st["channel_eig"] = (time.perf_counter() - t0) * nch / 4
-    Hx = rng.standard_normal((ns, ns))
-    t0 = time.perf_counter()
-    for q in range(nch - 1):
-        _ = bbs[q % 4].T @ Hx @ bbs[(q + 1) % 4]
-    nb = nch * (nch - 1) // 2
-    st["transform"] = (time.perf_counter() - t0) * nb / (nch - 1)
-    khm = nch * ns - int(np.sum(np.minimum(pw["lch"], ks - 2) + 1))
-    n4 = khm // 4
-    A = rng.standard_normal((n4, n4))
-    A = np.tril(A + A.T)
-    t0 = time.perf_counter()
-    lapack.dsyev(A, compute_v=1, lower=1)
-    st["dense_eig"] = (time.perf_counter() - t0) * (khm / n4) ** 3
-    total = sum(st.values())
-    desc = ("bounded sample of one %s solve, extrapolated per stage: mrk_cell for 2/%d multipoles; all I_data "
-            "groups of multipole %d over %d processes; DSYGV for 4/%d channels; %d/%d block transforms; "
-            "DSYEV('V') at n=%d scaled by (khm/n)^3 to khm=%d" % (pw["name"], kmax + 1, kmid, nproc, nch,
-                                                                 nch - 1, nb, n4, khm))
-    return total, st, desc
+
+def config1_cpu(reps=3):
+    """config1 solved completely on the CPU: single thread and all cores (seconds per solve)."""
+    from bsr_b200 import workload as W
+    pw = W.partial_wave("config1")
+    cpu_full_solve(pw, 1)
+    one = min(cpu_full_solve(pw, 1) for _ in range(reps))
+    allc = min(cpu_full_solve(pw, None) for _ in range(reps))
+    return pw, one, allc
 
 
 def run_reference(args):
@@ -220,27 +268,46 @@ def run_reference(args):
         return
     from bsr_b200 import workload as W
     pw = W.partial_wave(args.workload)
-    threads = os.cpu_count() or 1
-    for _ in range(max(0, min(args.warmup, 1))):
-        pass        # the CPU path has no warm-up state; a sample is timed directly
-    secs = []
-    stages = None
-    desc = ""
-    for _ in range(args.steps):
-        total, stages, desc = cpu_reference_step(pw, threads)
-        secs.append(total)
-    spp = statistics.mean(secs)
+    cores = os.cpu_count() or 1
+    ref = CpuReference(pw, procs=cores, threads=None)
+    try:
+        for _ in range(args.warmup):
+            ref.sample()
+        walls, totals, stages, scales = [], [], None, None
+        for _ in range(args.steps):
+            wall, total, stages, scales = ref.sample()
+            walls.append(wall)
+            totals.append(total)
+    finally:
+        ref.close()
+    one = CpuReference(pw, procs=1, threads=1)
+    try:
+        w1, t1, st1, _ = one.sample()
+    finally:
+        one.close()
+    pw1, c1_one, c1_all = config1_cpu()
+    spp = statistics.mean(totals)
     value = 1.0 / spp
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": spp * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(walls) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_desc(pw),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port", "sample": desc,
-                         "stage_seconds": {k: round(v, 3) for k, v in stages.items()}},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": ref.describe(),
+                         "extrapolated_seconds_per_solve": spp,
+                         "sample_seconds_per_step": statistics.mean(walls),
+                         "stage_seconds_sampled": {k: round(v, 4) for k, v in stages.items()},
+                         "stage_scale_to_one_solve": {k: round(v, 3) for k, v in scales.items()},
+                         "single_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1,
+                                           "extrapolated_seconds_per_solve": t1, "sample_seconds": w1}},
+        "config1_full_solve": {"workload": "config1 (%dx%d), nothing extrapolated" % (pw1["nch"] * pw1["ns"],
+                                                                                     pw1["nch"] * pw1["ns"]),
+                               "single_thread_s": c1_one, "all_cores_s": c1_all, "cores": cores},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference is Fortran with no compiler in this image; its routines are timed through the "
-                "C restatement (oracle/) with LAPACK from scipy's OpenBLAS on all host cores",
+                "C restatement (oracle/) with LAPACK from scipy's OpenBLAS; each timed step runs the bounded "
+                "sample (ms_per_step) and value is one solve extrapolated from it stage by stage",
     }
     print(json.dumps(line), flush=True)
 
@@ -327,14 +394,30 @@ def run_b200(args):
     # ---- stage breakdown (separate pass with stage events on) ----
     ctx.set_timing(True)
     ctx.stage_times()
+    ctx.stage_flops()
     nst = max(1, min(args.steps, 2))
     for _ in range(nst):
         flush.fill_(1.0)
-        step()
+        res = step()
     torch.cuda.synchronize()
     stages = ctx.stage_times()
+    stage_flops = ctx.stage_flops()
     ctx.set_timing(False)
-    own_launches = sum(n for _, n in stages.values()) / nst
+    top = ("rk_moments", "direct", "exchange", "one_electron", "channel_eig", "transform", "dense_eig", "rk_expand",
+           "refine")
+    own_launches = sum(stages[k][1] for k in top) / nst
+    # refinement statistics of the last solve: correction (raw - refined eigenvalue) and residual per pair
+    corr, resid = ctx.refine_stats(khm)
+    ev = res["eval"].double()
+    den = torch.clamp(ev.abs(), min=1e-3)
+    rc = (corr.abs() / den).cpu().numpy()
+    accuracy = {"refined": True,
+                "raw_solver_error_vs_refined": {"max_rel": float(rc.max()), "p99_rel": float(np.percentile(rc, 99)),
+                                                "what": "|raw eigenvalue - Rayleigh quotient| / max(|E|, 1e-3)"},
+                "residual_norm": {"max": float(resid.max().item()), "median": float(resid.median().item()),
+                                  "what": "||A v - E v|| per eigenpair, A the khm x khm matrix in the channel basis"},
+                "vs_oracle": "per-eigenvalue relative error against the oracle's refined form: "
+                             "tests/test_gpu_diag.py (config 1 all pairs, config 2 lowest 200), <= 1e-11"}
     # ---- e2e: host buffers through the C ABI (bsrg_partial_wave_solve) ----
     e2e_ms = 0.0
     ne2e = max(1, min(args.steps, 3))
@@ -358,7 +441,7 @@ def run_b200(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    # ---- roofline figures (algorithmic work per launch / measured launch time) ----
+    # ---- roofline figures: EXECUTED work of each stage / its measured time ----
     import json as _json
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -385,64 +468,75 @@ def run_b200(args):
     s1.synchronize()
     dropin_ms = s0.elapsed_time(s1) / 5
     del rkb_buf
-    # exchange: per group ns^2 outputs x (2ks-1)^2 multiply-adds
     ngx = int(np.sum(_group_counts(c, 1)))
     ngd = int(np.sum(_group_counts(c, 0)))
-    x_flops = 2.0 * ngx * ns * ns * (2 * ks - 1) ** 2 / nk          # per launch (one launch per k)
     norb = pw["norb"]
     nxterms = int(np.sum(c["type"] == 1))
+    # the factored exchange kernel's own arithmetic per launch (one launch per multipole)
     x_exec_flops = (2.0 * ns * ns * ((2 * ks - 1) ** 2 * norb + (2 * ks - 1) * norb * norb) +
                     2.0 * ns * ns * nxterms / nk)
+    x_ref_flops = 2.0 * ngx * ns * ns * (2 * ks - 1) ** 2 / nk       # the reference's convol count (not executed)
     x_ms, x_n = stages["exchange"]
-    # blocks that receive an exchange group in one multipole (the launch's read-modify-write)
     xsel = c["type"] == 1
     xblocks = [len(np.unique(c["ich"][xsel & (c["k"] == kk)].astype(np.int64) * 1000 + c["jch"][xsel & (c["k"] == kk)]))
                for kk in range(nk)]
     x_min_bytes = 2.0 * ns * ns * 8 * (sum(xblocks) / nk)
     x_launch_ms = x_ms / (nst * nk)
-    d_flops = 2.0 * ngd * (ns * ks) ** 2 / nk
+    d_flops = 2.0 * ngd * (ns * ks) ** 2 / nk      # the DGEMM's own arithmetic per multipole
     d_ms, d_n = stages["direct"]
-    d_launch_ms = d_ms / (nst * nk)        # stage time summed over nst steps and nk multipoles
-    eig_ms, _ = stages["dense_eig"]
-    eig_ms /= nst
-    eig_flops = (4.0 / 3.0 + 2.0 + 4.0) * khm ** 3     # tridiagonalisation + D&C + back-transform, rough
+    d_launch_ms = d_ms / (nst * nk)
+    per_step_ms = {k: v[0] / nst for k, v in stages.items()}
+    per_step_flops = {k: v / nst for k, v in stage_flops.items()}
+    own_eig = per_step_flops.get("dense_eig", 0.0) > 0.0
     by_stage = {
-        "rk_expand": {"bound": "hbm", "achieved": rk_gbs, "peak": hbm_peak, "unit": "GB/s",
-                      "frac": rk_gbs / hbm_peak, "launch_ms": exp_launch_ms,
-                      "algorithmic": "%d bytes written per launch (rkb ns^2 ks^2 doubles, one multipole)" % rkb_bytes},
-        "exchange": {"bound": "tensor", "achieved": x_flops / (x_launch_ms * 1e-3) / 1e12, "peak": fp64,
+        "rk_expand": {"bound": "hbm", "achieved": rk_gbs, "peak": hbm_peak, "unit": "GB/s", "launch_ms": exp_launch_ms,
+                      "work": "%d bytes written per launch (rkb ns^2 ks^2 doubles, one multipole)" % rkb_bytes},
+        "exchange": {"bound": "tensor", "achieved": x_exec_flops / (x_launch_ms * 1e-3) / 1e12, "peak": fp64,
                      "unit": "TFLOP/s", "launch_ms": x_launch_ms,
-                     "algorithmic": "the reference algorithm's count, convol icase 3 per group: 2*ns^2*(2ks-1)^2 "
-                                    "flop per exchange group, %d groups over %d launches" % (ngx, nk),
-                     "executed_tflops": x_exec_flops / (x_launch_ms * 1e-3) / 1e12,
-                     "executed": "the factored kernel's own count: 2*ns^2*((2ks-1)^2 norb + (2ks-1) norb^2) + "
-                                 "2*ns^2 per coefficient, per launch",
+                     "work": "executed by the factored kernel per launch: 2 ns^2 ((2ks-1)^2 norb + (2ks-1) norb^2) "
+                             "+ 2 ns^2 per coefficient record",
+                     "reference_count_tflops_not_executed": x_ref_flops / (x_launch_ms * 1e-3) / 1e12,
                      "hbm_view": {"bytes": x_min_bytes, "achieved_gbs": x_min_bytes / (x_launch_ms * 1e-3) / 1e9,
                                   "frac": x_min_bytes / (x_launch_ms * 1e-3) / 1e9 / hbm_peak,
-                                  "what": "the update's minimum HBM traffic per launch: each channel block with an "
-                                          "exchange group read and written once (ns^2 x 8 B x 2 per block)"}},
+                                  "what": "minimum traffic of the launch: each channel block with an exchange "
+                                          "group read and written once"}},
         "direct": {"bound": "tensor", "achieved": d_flops / (d_launch_ms * 1e-3) / 1e12, "peak": fp64,
-                   "unit": "TFLOP/s", "launch_ms": d_launch_ms,
-                   "algorithmic": "2*(ns ks)^2 flop per direct group, %d groups; the stage is the group "
-                                  "densities, the table reshape, cuBLAS DGEMM and the band update" % ngd},
-        "dense_eig": {"bound": "tensor", "achieved": eig_flops / (eig_ms * 1e-3) / 1e12, "peak": fp64,
-                      "unit": "TFLOP/s", "launch_ms": eig_ms, "library": "cuSOLVER Xsyevd",
-                      "algorithmic": "~7.3 khm^3 flop (sytrd + stedc + ormtr)"},
+                   "unit": "TFLOP/s", "launch_ms": d_launch_ms, "library": "cuBLAS DGEMM inside the stage",
+                   "work": "2 (ns ks)^2 flop per direct group (%d groups), the GEMM's own arithmetic" % ngd},
     }
+    for name in ("transform", "refine", "eig_band", "eig_chase", "eig_dc", "eig_q2", "eig_q1"):
+        f, t = per_step_flops.get(name, 0.0), per_step_ms.get(name, 0.0)
+        if f > 0.0 and t > 0.0:
+            by_stage[name] = {"bound": "tensor", "achieved": f / (t * 1e-3) / 1e12, "peak": fp64, "unit": "TFLOP/s",
+                              "launch_ms": t, "work": "%.4g flop executed per step (counted by the library)" % f}
+    eig_t = per_step_ms.get("dense_eig", 0.0)
+    if own_eig:
+        by_stage["dense_eig"] = {"bound": "tensor", "achieved": per_step_flops["dense_eig"] / (eig_t * 1e-3) / 1e12,
+                                 "peak": fp64, "unit": "TFLOP/s", "launch_ms": eig_t,
+                                 "work": "%.4g flop executed per step: two-stage reduction, divide and conquer, "
+                                         "both back-transformations" % per_step_flops["dense_eig"]}
+    else:
+        lapack_count = (4.0 / 3.0 + 2.0 + 4.0 / 3.0) * khm ** 3
+        by_stage["dense_eig"] = {"bound": "tensor", "achieved": lapack_count / (eig_t * 1e-3) / 1e12, "peak": fp64,
+                                 "unit": "TFLOP/s", "launch_ms": eig_t, "library": "cuSOLVER Xsyevd",
+                                 "work": "LAPACK's operation count for dsyevd with vectors (4/3 + 2 + 4/3) khm^3"}
     for v in by_stage.values():
         v["frac"] = v["achieved"] / v["peak"]
-    own = {k: v for k, v in by_stage.items() if "library" not in v}
-    per_step_ms = {k: v[0] / nst for k, v in stages.items()}
-    dom_own = max(own, key=lambda k: per_step_ms[k])
+    # the dominant kernel of the library's own: the longest own stage made of one kernel per launch
+    single = ("rk_expand", "exchange", "eig_chase", "eig_q2", "refine")
+    cand = {k: per_step_ms[k] for k in single if k in by_stage and k in per_step_ms}
+    dom_own = max(cand, key=lambda k: cand[k])
     r = dict(by_stage[dom_own])
-    r["kernel"] = dom_own
-    # DRAM traffic per launch from the committed ncu capture of this kernel (profiles/traffic.json)
+    r["kernel"] = {"rk_expand": "rkb_pad_kernel", "exchange": "exchange_factored_kernel",
+                   "eig_chase": "sb2st_kernel", "eig_q2": "q2_apply_kernel",
+                   "refine": "refine_gemm_kernel"}[dom_own]
+    r["stage"] = dom_own
     r["traffic"] = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         tj = _json.load(open(tp))
-        if dom_own in tj:
-            r["traffic"] = tj[dom_own]["dram_bytes_per_launch"]
+        if r["kernel"] in tj:
+            r["traffic"] = tj[r["kernel"]]["dram_bytes_per_launch"]
             r["traffic_unit"] = "bytes per launch (ncu dram read + write)"
     r["peak_source"] = (hbm_src + " (MEASURED_PEAKS.json hbm_gbs)") if r["unit"] == "GB/s" else \
         "measured in this run: cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json has no FP64 figure)"
@@ -450,7 +544,8 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; see config)",
-        "config": dict(workload_desc(pw, khm), parallelism="one partial wave per GPU, no collective"),
+        "config": dict(workload_desc(pw, khm), parallelism="one partial wave per GPU, no collective",
+                       eigensolver="library two-stage (syevd2)" if own_eig else "cuSOLVER Xsyevd"),
         "rk_gbs": {"value": rk_gbs, "unit": "GB/s", "frac_of_hbm": rk_gbs / hbm_peak,
                    "what": "R^k table of the assembly pipeline: ns^2 ks^2 doubles per multipole over the time of "
                            "its build (band moments + zero-margined rkb)",
@@ -461,6 +556,7 @@ def run_b200(args):
         "roofline": r,
         "roofline_by_stage": by_stage,
         "fp64_gemm_tflops_measured": fp64,
+        "accuracy": accuracy,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                 "api": "bsrg_partial_wave_solve (host buffers: knots, orbitals, coefficient records in; "
                        "eigenvalues out)"},
@@ -471,14 +567,61 @@ def run_b200(args):
         del ctx, basis, P, res
         torch.cuda.empty_cache()
         line["batched"], line["serving"] = bench_batched_serving(torch, bsr)
+    if world == 1:
+        line["config1"] = bench_config1(torch, bsr, with_cpu=not args.no_cpu_baseline)
     if world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        total, st, desc = cpu_reference_step(pw, threads)
-        line["cpu_baseline"] = {"value": 1.0 / total, "unit": "solves/s", "cores": threads, "kind": "port",
-                                "sample": desc, "stage_seconds": {k: round(v, 3) for k, v in st.items()}}
+        cores = os.cpu_count() or 1
+        ref = CpuReference(pw, procs=cores, threads=None)
+        try:
+            ref.sample()
+            wall, total, st, sc = ref.sample()
+        finally:
+            ref.close()
+        line["cpu_baseline"] = {"value": 1.0 / total, "unit": "solves/s", "cores": cores, "kind": "port",
+                                "sample": ref.describe(), "extrapolated_seconds_per_solve": total,
+                                "sample_seconds": wall,
+                                "stage_seconds_sampled": {k: round(v, 4) for k, v in st.items()},
+                                "stage_scale_to_one_solve": {k: round(v, 3) for k, v in sc.items()}}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def bench_config1(torch, bsr, with_cpu=True, reps=10):
+    """config1 (the reference's CPU-runnable size) solved completely by both arms,
+    nothing extrapolated: the GPU path (mrk_cell tables, assembly, diag_hd with
+    vectors and refinement) by CUDA events, the CPU reference (oracle + LAPACK)
+    single-threaded and on all cores by wall clock."""
+    from bsr_b200 import workload as W
+    pw = W.partial_wave("config1")
+    ctx = bsr.Context()
+    basis = bsr.define_spline(pw["t"], pw["ks"])
+    P = bsr.as_fortran(pw["P"])
+
+    def step():
+        H = bsr.assemble(ctx, basis, pw["z"], pw["lch"], pw["ech"], P, pw["kmax"], pw["coefs"])
+        return bsr.diag_hd(ctx, basis, pw["lch"], H["hcc"], want_vectors=True)
+
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(reps):
+        step()
+    s1.record()
+    s1.synchronize()
+    gpu_s = s0.elapsed_time(s1) / reps * 1e-3
+    out = {"workload": "config1: ks=8 ns=60 Rmax=20 k=0..4, 10 orbitals, 8 channels (H 480x480), whole solve, "
+                       "nothing extrapolated",
+           "gpu_solves_per_s": 1.0 / gpu_s, "gpu_ms_per_solve": gpu_s * 1e3}
+    ctx.close()
+    if with_cpu:
+        _, one, allc = config1_cpu()
+        out.update({"cpu_single_thread_solves_per_s": 1.0 / one, "cpu_all_cores_solves_per_s": 1.0 / allc,
+                    "cpu_cores": os.cpu_count() or 1,
+                    "gpu_vs_cpu_single_thread": one / gpu_s, "gpu_vs_cpu_all_cores": allc / gpu_s})
+    return out
 
 
 def bench_batched_serving(torch, bsr):

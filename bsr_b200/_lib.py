@@ -48,11 +48,15 @@ SIGNATURES = [
     ("bsrg_density", _c_int, [_c_int, _c_int, _P, _P, _P, _c_char, _P]),
     ("bsrg_convol", _c_int, [_c_int, _c_int, _P, _P, _P, _c_int, _c_int, _c_char, _c_char, _P]),
     ("bsrg_sum_amb", _c_int, [_c_int, _c_int, _P, _P, _c_char, _P, _P]),
+    ("bsrg_bav", _c_int, [_c_int, _c_int, _P, _P, _P, _c_char, _c_char, _P]),
+    ("bsrg_bvmv", _c_int, [_c_int, _c_int, _P, _c_char, _P, _P, _P, _P]),
+    ("bsrg_quadr", _c_int, [_P, _P, _P, _c_int, _P, _P]),
     ("bsrg_ctx_create", _c_int, [_c_int, _P, ctypes.POINTER(_c_void_p)]),
     ("bsrg_ctx_destroy", _c_int, [_P]),
     ("bsrg_ctx_workspace_bytes", _c_size_t, [_P]),
     ("bsrg_ctx_set_timing", _c_int, [_P, _c_int]),
     ("bsrg_ctx_stage_times", _c_int, [_P, _DP, _IP, _c_int]),
+    ("bsrg_ctx_stage_flops", _c_int, [_P, _DP, _c_int]),
     ("bsrg_tables_create", _c_int, [_P, _P, _c_int, ctypes.POINTER(_c_void_p)]),
     ("bsrg_tables_free", _c_int, [_P]),
     ("bsrg_tables_bytes", _c_size_t, [_P]),

@@ -90,7 +90,7 @@ class Basis:
     """define_spline's module state, resident on the GPU (spline_grid + spline_galerkin)."""
 
     _WHICH = {"gr": 0, "grm": 1, "grw": 2, "bsp": 3, "bsq": 4, "bspd": 5, "sb": 6, "r1": 7, "rm1": 8, "rm2": 9,
-              "rm3": 10, "db1": 11, "db2": 12, "t": 13}
+              "rm3": 10, "db1": 11, "db2": 12, "t": 13, "bb": 14, "bs": 15}
 
     def __init__(self, t, ks, ml=0, me=0, h=0.0):
         t = np.ascontiguousarray(t, dtype=np.float64)
@@ -120,7 +120,8 @@ class Basis:
         """Module array `name` as a Fortran-layout CUDA tensor (gr, bsp, sb, db2, ...)."""
         ks, ns, nv = self.ks, self.ns, self.nv
         shapes = {"gr": (nv, ks), "grm": (nv, ks), "grw": (nv, ks), "bsp": (nv + 1, ks, ks),
-                  "bsq": (nv + 1, ks, ks), "bspd": (nv + 1, ks, ks, 2), "t": (ns + ks,)}
+                  "bsq": (nv + 1, ks, ks), "bspd": (nv + 1, ks, ks, 2), "t": (ns + ks,), "bb": (ns, ns),
+                  "bs": (ks, ns)}
         out = fortran_empty(shapes.get(name, (ns, ks)))
         call("bsrg_basis_get", self.handle, self._WHICH[name], _ptr(out), _stream())
         return out
@@ -302,6 +303,30 @@ def sum_amb(ns, ks, a, b, sym):
     return out
 
 
+def bav(ns, ks, b, v, type, side="r"):
+    """bav.f90: y = B v ('s', or 'n' with side 'r') or v B ('n', side 'l') for a band matrix."""
+    b, v = as_fortran(b), as_fortran(v)
+    y = torch.empty(ns, device="cuda", dtype=torch.float64)
+    call("bsrg_bav", ns, ks, _ptr(b), _ptr(v), _ptr(y), type.encode(), side.encode(), _stream())
+    return y
+
+
+def bvmv(n, k, ar, type, x, y):
+    """bvmv.f90: <x, A y> for a band array."""
+    ar, x, y = as_fortran(ar), as_fortran(x), as_fortran(y)
+    out = torch.empty(1, device="cuda", dtype=torch.float64)
+    call("bsrg_bvmv", n, k, _ptr(ar), type.encode(), _ptr(x), _ptr(y), _ptr(out), _stream())
+    return out
+
+
+def quadr(basis, p1, p2, m):
+    """quadr.f90: <p1 | r^m | p2>."""
+    p1, p2 = as_fortran(p1), as_fortran(p2)
+    out = torch.empty(1, device="cuda", dtype=torch.float64)
+    call("bsrg_quadr", basis.handle, _ptr(p1), _ptr(p2), m, _ptr(out), _stream())
+    return out
+
+
 # ---------------------------------------------------------------------------
 # bsr_mat assembly and bsr_hd diagonalisation
 # ---------------------------------------------------------------------------
@@ -324,7 +349,13 @@ class Context:
         self._tables = tables
 
     STAGES = ("rk_moments", "direct", "exchange", "one_electron", "channel_eig", "transform", "dense_eig",
-              "rk_expand", "refine")
+              "rk_expand", "refine", "eig_band", "eig_chase", "eig_dc", "eig_q2", "eig_q1")
+
+    def stage_flops(self):
+        """Executed floating-point operations per stage since the last read (then reset)."""
+        f = np.zeros(len(self.STAGES))
+        call("bsrg_ctx_stage_flops", self.handle, _dptr(f), len(self.STAGES))
+        return {s: float(f[i]) for i, s in enumerate(self.STAGES)}
 
     def set_refine(self, on=True):
         """FP64 Rayleigh-quotient refinement of diag_hd's eigenpairs (on by default)."""

@@ -926,6 +926,14 @@ int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n)
     return rc;
 }
 
+int bsrg_ctx_stage_flops(bsrg_ctx *c, double *flops, int n)
+{
+    if (!c || !flops) { set_error("ctx_stage_flops: null argument"); return BSRG_ERR_ARG; }
+    for (int q = 0; q < n && q < BSRG_NSTAGE; q++) flops[q] = c->stage_flops[q];
+    for (int q = 0; q < BSRG_NSTAGE; q++) c->stage_flops[q] = 0.0;
+    return BSRG_OK;
+}
+
 int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
 {
     if (!out) { set_error("ctx_create: null output"); return BSRG_ERR_ARG; }

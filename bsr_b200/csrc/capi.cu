@@ -210,8 +210,70 @@ int bsrg_basis_dims(const bsrg_basis *b, int *dims)
     return BSRG_OK;
 }
 
+}  // extern "C"
+
+namespace bsrg {
+// Full_mat_sym(ns, ks, sb, bb, 'l') (full_mat.f90): the full symmetric ns x ns matrix of the band
+__global__ void full_from_band_sym_kernel(int ns, int ks, const double *__restrict__ sb, double *bb)
+{
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)ns * ns) return;
+    const int i = (int)(idx % ns), j = (int)(idx / ns);
+    const int hi = i > j ? i : j, lo = i > j ? j : i;
+    bb[idx] = hi - lo < ks ? sb[hi + (size_t)ns * (lo - hi + ks - 1)] : 0.0;
+}
+
+// facsb (facsb.f90:2-36): bs = sb^T in upper band storage (ks, ns) with the r = 0 boundary
+// condition (first row and column replaced by e_1), then its banded Cholesky factor U
+// (DPBTRF('U', ns, ks-1, bs, ks): bs(ks+i-j, j) = U(i, j)), left-looking, one thread.
+__global__ void facsb_kernel(int ns, int ks, const double *__restrict__ sb, double *bs, int *info)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int kd = ks - 1;
+    for (int j = 0; j < ns; j++)
+        for (int m = 0; m < ks; m++) bs[m + (size_t)ks * j] = sb[j + (size_t)ns * m];
+    for (int m = 0; m < ks - 1; m++) bs[m + (size_t)ks * (ks - 1 - m)] = 0.0;
+    bs[(ks - 1)] = 1.0;
+    auto U = [&](int i, int j) -> double & { return bs[(kd + i - j) + (size_t)ks * j]; };   // 0-based i <= j
+    *info = 0;
+    for (int j = 0; j < ns; j++) {
+        const int k0 = j - kd > 0 ? j - kd : 0;
+        for (int i = k0; i < j; i++) {
+            double s = U(i, j);
+            for (int k = k0; k < i; k++) s -= U(k, i) * U(k, j);
+            U(i, j) = s / U(i, i);
+        }
+        double d = U(j, j);
+        for (int k = k0; k < j; k++) d -= U(k, j) * U(k, j);
+        if (!(d > 0.0)) { *info = j + 1; return; }
+        U(j, j) = sqrt(d);
+    }
+}
+}  // namespace bsrg
+
+extern "C" {
+
 int bsrg_basis_get(const bsrg_basis *b, int which, double *dst, void *stream)
 {
+    if (b && dst && (which == 14 || which == 15)) {
+        cudaStream_t s = (cudaStream_t)stream;
+        if (which == 14) {
+            const long nn = (long)b->ns * b->ns;
+            full_from_band_sym_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(b->ns, b->ks, b->sb, dst);
+            return cuda_fail(cudaGetLastError(), "basis_get bb");
+        }
+        int *dinfo = nullptr;
+        cudaError_t e = cudaMallocAsync((void **)&dinfo, sizeof(int), s);
+        if (e != cudaSuccess) return cuda_fail(e, "basis_get bs");
+        facsb_kernel<<<1, 32, 0, s>>>(b->ns, b->ks, b->sb, dst, dinfo);
+        int hinfo = 0;
+        e = cudaMemcpyAsync(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFreeAsync(dinfo, s);
+        if (e != cudaSuccess) return cuda_fail(e, "basis_get bs");
+        if (hinfo != 0) { set_error("facsb: dpbtrf (LAPACK) failed (column %d)", hinfo); return BSRG_ERR_INFO; }
+        return BSRG_OK;
+    }
     CHECK_ARG(b && dst, "basis_get: null argument");
     size_t nvk = (size_t)b->nv * b->ks, nb = (size_t)(b->nv + 1) * b->ks * b->ks,
            nband = (size_t)b->ns * b->ks;
@@ -447,6 +509,39 @@ int bsrg_convol(int ns, int ks, double *a, const double *d, const double *rkb, i
     int need = (sym_i == 'n' || sym_j == 'n') ? 2 * ks - 1 : ks;
     CHECK_ARG(ldp >= need, "convol: ldp=%d < %d", ldp, need);
     return launch_convol(ns, ks, a, d, rkb, ldp, icase, sym_i, sym_j, (cudaStream_t)stream);
+}
+
+int bsrg_bav(int ns, int ks, const double *b, const double *v, double *y, char type, char side, void *stream)
+{
+    CHECK_ARG(b && v && y, "bav: null argument");
+    CHECK_ARG(type == 's' || (type == 'n' && (side == 'r' || side == 'l')), "bav: type '%c' side '%c'", type, side);
+    return launch_bav(ns, ks, b, v, y, type, side, (cudaStream_t)stream);
+}
+
+int bsrg_bvmv(int n, int k, const double *ar, char type, const double *x, const double *y, double *out,
+              void *stream)
+{
+    CHECK_ARG(ar && x && y && out, "bvmv: null argument");
+    CHECK_ARG(n >= 2 && k >= 2, "bvmv: n=%d k=%d", n, k);
+    return launch_bvmv(n, k, ar, type, x, y, out, (cudaStream_t)stream);
+}
+
+int bsrg_quadr(const bsrg_basis *b, const double *p1, const double *p2, int m, double *out, void *stream)
+{
+    CHECK_ARG(b && p1 && p2 && out, "quadr: null argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double *rm = m == 1 ? b->r1 : m == 0 ? b->sb : m == -1 ? b->rm1 : m == -2 ? b->rm2 : nullptr;
+    double *tmp = nullptr;
+    if (!rm) {
+        cudaError_t e = cudaMallocAsync((void **)&tmp, sizeof(double) * (size_t)b->ns * b->ks, s);
+        if (e != cudaSuccess) return cuda_fail(e, "quadr");
+        int rc = launch_mrm(b, m, tmp, s);
+        if (rc != BSRG_OK) { cudaFreeAsync(tmp, s); return rc; }
+        rm = tmp;
+    }
+    int rc = launch_bvmv(b->ns, b->ks, rm, 's', p1, p2, out, s);
+    if (tmp) cudaFreeAsync(tmp, s);
+    return rc;
 }
 
 int bsrg_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, void *stream)

@@ -172,4 +172,79 @@ int launch_sum_amb(int ns, int ks, const double *a, const double *b, char sym, d
     return cuda_fail(cudaGetLastError(), "sum_amb");
 }
 
+// bav (bav.f90:2): y = B v ('s'; 'n' with side 'r') or y = v B ('n', side 'l').  One thread
+// per output, the terms added in the order the reference's scatter loops reach that output
+// (for 's': within each diagonal ip the transposed term b(x-ip+1, ip) v(x-ip+1) comes first).
+__global__ void bav_kernel(int ns, int ks, const double *__restrict__ b, const double *__restrict__ v, double *y,
+                           char type, char side)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;   // 0-based output index
+    if (x >= ns) return;
+    double acc;
+    if (type == 's') {
+        acc = b[x] * v[x];
+        for (int ip = 2; ip <= ks; ip++) {
+            const int i1 = x - ip + 1;            // row i whose j = i + ip - 1 is x
+            if (i1 >= 0) acc = acc + b[i1 + (size_t)ns * (ip - 1)] * v[i1];
+            if (x <= ns - ip) acc = acc + b[x + (size_t)ns * (ip - 1)] * v[x + ip - 1];
+        }
+    } else {
+        acc = 0.0;
+        for (int ip = 1; ip <= ks + ks - 1; ip++) {
+            const int imin = max(1, 1 + ks - ip), imax = min(ns, ns + ks - ip);
+            if (side == 'r') {
+                const int i = x + 1, j = i + ip - ks;
+                if (i >= imin && i <= imax) acc = acc + b[(i - 1) + (size_t)ns * (ip - 1)] * v[j - 1];
+            } else {
+                const int i = x + 1 - ip + ks;     // j = i + ip - ks = x + 1
+                if (i >= imin && i <= imax) acc = acc + b[(i - 1) + (size_t)ns * (ip - 1)] * v[i - 1];
+            }
+        }
+    }
+    y[x] = acc;
+}
+
+// bvmv (bvmv.f90:2): <x, A y> for a band array, in the reference's summation order
+// (one thread: the sum is a single ordered accumulation of O(n k) terms)
+__device__ double bvmv_dev(int n, int k, const double *ar, char type, const double *x, const double *y)
+{
+    double s = 0.0;
+    if (type != 'g') {
+        for (int jp = 1; jp <= k - 1; jp++)
+            for (int i = k + 1 - jp; i <= n; i++) {
+                const int j = i + jp - k;
+                s = s + ar[(i - 1) + (size_t)n * (jp - 1)] * (x[i - 1] * y[j - 1] + x[j - 1] * y[i - 1]);
+            }
+        if (type == 'a') s = s + x[n - 2] * y[n - 1] * (ar[0] - ar[(n - 1) + (size_t)n * (k - 2)]);
+    } else {
+        for (int jp = 1; jp <= k - 1; jp++)
+            for (int i = k - jp + 1; i <= n; i++) {
+                const int j = i + jp - k, kp = 2 * k - jp;
+                s = s + ar[(i - 1) + (size_t)n * (jp - 1)] * x[i - 1] * y[j - 1];
+                s = s + ar[(j - 1) + (size_t)n * (kp - 1)] * x[j - 1] * y[i - 1];
+            }
+    }
+    double c = 0.0;
+    for (int i = 1; i <= n; i++) c = c + ar[(i - 1) + (size_t)n * (k - 1)] * x[i - 1] * y[i - 1];
+    return s + c;
+}
+
+__global__ void bvmv_kernel(int n, int k, const double *ar, char type, const double *x, const double *y, double *out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) *out = bvmv_dev(n, k, ar, type, x, y);
+}
+
+int launch_bav(int ns, int ks, const double *b, const double *v, double *y, char type, char side, cudaStream_t s)
+{
+    bav_kernel<<<(ns + 127) / 128, 128, 0, s>>>(ns, ks, b, v, y, type, side);
+    return cuda_fail(cudaGetLastError(), "bav");
+}
+
+int launch_bvmv(int n, int k, const double *ar, char type, const double *x, const double *y, double *out,
+                cudaStream_t s)
+{
+    bvmv_kernel<<<1, 32, 0, s>>>(n, k, ar, type, x, y, out);
+    return cuda_fail(cudaGetLastError(), "bvmv");
+}
+
 }  // namespace bsrg

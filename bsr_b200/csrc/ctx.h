@@ -37,6 +37,7 @@ struct bsrg_ctx {
     std::vector<cudaEvent_t> *pool;          // free events
     double stage_ms[BSRG_NSTAGE];
     int stage_launches[BSRG_NSTAGE];
+    double stage_flops[BSRG_NSTAGE];        // executed flops (counted where the library knows them)
     const bsrg_tables *tables;               // resident tables to use, or NULL
     std::vector<int> *last_ipsol;            // channel solution offsets of the last diag_hd
     void *pw_buf;                            // device buffers of bsrg_partial_wave_solve (kept between calls)
@@ -79,7 +80,7 @@ int stage_collect(bsrg_ctx *c);   // waits for recorded events and accumulates
 size_t dc_workspace_bytes(int n);
 size_t dc_pinned_bytes(int n);
 int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, double *Z, long ldz, void *ws_base,
-               size_t ws_bytes, void *pinned, size_t pinned_bytes);
+               size_t ws_bytes, void *pinned, size_t pinned_bytes, double *gemm_flops, int *launches);
 
 // two-stage dense symmetric eigensolver (syevd2.cu)
 size_t syevd2_workspace_doubles(int n);

@@ -593,6 +593,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         scatter_blocks_kernel<<<g, 128, 0, s>>>(ns, khm, d_bm, d_ipsol, T, A);
     }
     stage_end(c, 5, (nb > 0 ? 4 : 1) + (refine ? 0 : 1));   // compact, [set_diag], 2 GEMMs, scatter
+    c->stage_flops[5] += 4.0 * (double)ns * ns * ns * nb;
     if (refine) {
         // keep the full symmetric A for the residuals: the eigensolver overwrites A
         stage_begin(c, 8);
@@ -636,6 +637,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         int rr = refine_apply(khm, Fsym, A, khm, eval, Fsym + (size_t)khm * khm, c->rf_buf, c->rf_buf + khm,
                               d_rflag, s);
         stage_end(c, 8, 3);
+        c->stage_flops[8] += 2.0 * (double)khm * khm * khm + 6.0 * (double)khm * khm;
         if (rr != BSRG_OK) return rr;
         c->rf_n = khm;
     }

@@ -674,11 +674,22 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
     if ((e = cudaMemsetAsync(flags, 0, 8 * sizeof(int), st)) != cudaSuccess ||
         (e = cudaMemsetAsync(progress, 0, sizeof(int) * n, st)) != cudaSuccess)
         return cuda_fail(e, "dsyevd init");
+    const int np = sy2sb_panels(n);
+    double fl_band = 0.0, fl_chase = 0.0, fl_q2 = 0.0, fl_q1 = 0.0, fl_dc = 0.0;
+    for (int j = 0; j + NB < n; j += NB) {
+        const double m = n - j - NB;
+        fl_band += 6.0 * m * m * NB + 6.0 * m * NB * NB + 4.0 * m * NB * NB;   // X, rank-2NB update; QR; Y passes
+        fl_q1 += 4.0 * m * n * NB + 2.0 * NB * NB * n;
+    }
     // 1. full symmetric working copy, dense -> band
+    stage_begin(c, 9);
     int rc = symmetrize_lower(n, A, lda, Wk, n, st);
     if (rc == BSRG_OK) rc = sy2sb(st, n, Wk, n, V1, T1, sw);
     if (rc != BSRG_OK) return rc;
     band_extract_kernel<<<(unsigned)(((long)n * LDAB + 255) / 256), 256, 0, st>>>(n, Wk, n, AB);
+    stage_end(c, 9, 2 + np * 6);
+    c->stage_flops[9] += fl_band;
+    stage_begin(c, 10);
     // 2. band -> tridiagonal
     if (n > 2) {
         int nsm = 148;
@@ -692,10 +703,23 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
             return cuda_fail(e, "dsyevd bulge chasing");
     }
     tridiag_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, AB, dv, ev);
+    for (int j = 0; j < n - 2; j++)
+        for (int i = 0; i < sweep_steps(n, j); i++) {
+            const double L = std::min(NB, n - (j + 1 + i * NB)), nlf = i == 0 ? 0 : NB - 1;
+            const double nb2 = std::max(0, std::min(NB, n - (j + 1 + i * NB) - (int)L));
+            fl_chase += 4.0 * L * (nlf + L + nb2);
+        }
+    stage_end(c, 10, 2);
+    c->stage_flops[10] += fl_chase;
     // 3. tridiagonal eigenpairs into Z
-    rc = tridiag_dc(st, n, dv, ev, w, Z, ldz, dcw, dc_workspace_bytes(n), pinned, pinned_bytes);
+    stage_begin(c, 11);
+    int ndc = 0;
+    rc = tridiag_dc(st, n, dv, ev, w, Z, ldz, dcw, dc_workspace_bytes(n), pinned, pinned_bytes, &fl_dc, &ndc);
     if (rc != BSRG_OK) return rc;
+    stage_end(c, 11, ndc);
+    c->stage_flops[11] += fl_dc;
     // 4. back-transformation: Q2 then Q1
+    stage_begin(c, 12);
     if (n > 2) {
         dim3 gt((unsigned)S, (unsigned)((n - 2 + NB - 1) / NB));
         q2_tfactor_kernel<<<gt, 32, 0, st>>>(n, S, V2, tau2, Tq);
@@ -703,7 +727,14 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
             cudaSuccess)
             return cuda_fail(e, "dsyevd Q2 smem");
         q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
+        // per block and column: W = V^T Z (2 NB nv), T W (~NB nv), Z -= V W (2 NB nv)
+        double nvsum = 0.0;
+        for (int j = 0; j < n - 2; j++) nvsum += sweep_steps(n, j);
+        fl_q2 = 5.0 * NB * nvsum * n;
     }
+    stage_end(c, 12, n > 2 ? 2 : 0);
+    c->stage_flops[12] += fl_q2;
+    stage_begin(c, 13);
     {
         std::vector<size_t> voff;
         size_t vo = 0;
@@ -718,6 +749,9 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
             if (rc != BSRG_OK) return rc;
         }
     }
+    stage_end(c, 13, 3 * np);
+    c->stage_flops[13] += fl_q1;
+    c->stage_flops[6] += fl_band + fl_chase + fl_dc + fl_q2 + fl_q1;
     // device-side waits report through the flags
     int hflag[2] = {0, 0};
     if ((e = cudaMemcpyAsync(hflag, flags + 2, sizeof(int) * 2, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -727,10 +761,8 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
         set_error("dsyevd: a device-side wait timed out (%s)", hflag[0] == 2 ? "bulge chasing" : "panel barrier");
         return BSRG_ERR_CUDA;
     }
-    // kernels of this library per call: symmetrize, per panel (QR, 2 passes, 2 GEMMs + split-K reduce),
-    // band, bulge chasing, extraction, D&C (counted approximately), Q2 (2), Q1 (3 per panel)
-    const int np = sy2sb_panels(n);
-    nl = 1 + np * 6 + 3 + 2 + (int)(3.5 * std::log2((double)std::max(n, 2))) * 8 + 3 * np + np;
+    // kernels of this library per call
+    nl = 2 + np * 6 + 2 + ndc + (n > 2 ? 2 : 0) + 3 * np;
     if (launches) *launches = nl;
     return BSRG_OK;
 }

@@ -555,9 +555,12 @@ size_t dc_pinned_bytes(int n)
 }
 
 int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, double *Z, long ldz, void *ws_base,
-               size_t ws_bytes, void *pinned, size_t pinned_bytes)
+               size_t ws_bytes, void *pinned, size_t pinned_bytes, double *gemm_flops, int *launches)
 {
+    if (gemm_flops) *gemm_flops = 0.0;
+    if (launches) *launches = 0;
     if (n < 1) return BSRG_OK;
+    int nlaunch = 0;
     if (n > DC_MAXK) { set_error("dstedc: n=%d above %d", n, DC_MAXK); return BSRG_ERR_ARG; }
     if (ws_bytes < dc_workspace_bytes(n) || pinned_bytes < dc_pinned_bytes(n)) {
         set_error("dstedc: workspace too small");
@@ -671,6 +674,8 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
                 const double *Qg = wsd + M.off_g, *U = wsd + M.off_u;
                 double *Qt = wsd + M.off_t;
                 // upper rows: Q1 columns (types 1, 2); lower rows: types 2, 3
+                if (gemm_flops) *gemm_flops += 2.0 * K * ((double)M.k1 * (n1 + n2) + (double)M.k2 * (K - n1));
+                nlaunch += 2;
                 int rc = dgemm(false, false, M.k1, K, n1 + n2, 1.0, Qg, k, U, K, 0.0, Qt, k, st);
                 if (rc == BSRG_OK)
                     rc = dgemm(false, false, M.k2, K, K - n1, 1.0, Qg + M.k1 + (long)k * n1, k, U + n1, K, 0.0,
@@ -678,11 +683,13 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
                 if (rc != BSRG_OK) return rc;
             }
         }
+        nlaunch += 3 + (Kmax > 0 ? 3 : 0) + 2;
         dc_rank_kernel<<<nm, 256, 0, st>>>(d_mg, d_scal, wsd, wsi, w);
         dim3 gc((unsigned)std::min(kmax, 2048), nm);
         dc_copy_kernel<<<gc, 128, 0, st>>>(d_mg, d_scal, wsd, wsi, Z, ldz);
         if ((err = cudaGetLastError()) != cudaSuccess) return cuda_fail(err, "dstedc merge");
     }
+    if (launches) *launches = nlaunch + 2;
     return BSRG_OK;
 }
 
@@ -707,7 +714,7 @@ extern "C" int bsrg_dstedc(bsrg_ctx *c, int n, const double *d, const double *e,
     if (e1 != cudaSuccess) return cuda_fail(e1, "dstedc copy");
     static const double zero = 0.0;
     rc = tridiag_dc(s, n, dt, n > 1 ? e : &zero, w, Z, ldz, rest, c->ws_bytes - (rest - (char *)c->ws), c->pinned,
-                    c->pinned_bytes);
+                    c->pinned_bytes, nullptr, nullptr);
     if (rc != BSRG_OK) return rc;
     cudaEventRecord(c->ev_stage, s);
     return cuda_fail(cudaGetLastError(), "dstedc");

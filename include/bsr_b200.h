@@ -55,7 +55,11 @@ int bsrg_basis_free(bsrg_basis *b);
 int bsrg_basis_dims(const bsrg_basis *b, int *dims);
 /* Copy one module array to dst (device).  which: 0 gr, 1 grm, 2 grw (nv,ks);
  * 3 bsp, 4 bsq (nv+1,ks,ks); 5 bspd (nv+1,ks,ks,2); 6 sb, 7 r1, 8 rm1, 9 rm2,
- * 10 rm3, 11 db1, 12 db2 (ns,ks); 13 t (ns+ks). */
+ * 10 rm3, 11 db1, 12 db2 (ns,ks); 13 t (ns+ks); 14 bb (ns,ns), the full
+ * overlap matrix of initas (define_spline.f90:171, Full_mat_sym); 15 bs
+ * (ks,ns), facsb's banded Cholesky factor of the overlap with the r = 0
+ * boundary condition (facsb.f90:2-36, DPBTRF('U') layout; BSRG_ERR_INFO with
+ * the reference's message if it is not positive definite). */
 int bsrg_basis_get(const bsrg_basis *b, int which, double *dst, void *stream);
 /* src/libs/BS/mrm.f90:2: <B_i|r^mm|B_j> band (ns,ks) into rm (device). */
 int bsrg_mrm(const bsrg_basis *b, int mm, double *rm, void *stream);
@@ -163,6 +167,21 @@ int bsrg_density(int ns, int ks, double *d, const double *p1, const double *p2, 
 int bsrg_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp,
                 int icase, char sym_i, char sym_j, void *stream);
 
+/* ---- src/libs/BS/bav.f90:2: y = B v (type 's', or 'n' with side 'r') or
+ *      y = v B ('n', side 'l') for a band matrix b (ns, ks) ('s') or
+ *      (ns, 2ks-1) ('n'), in the reference's summation order.  Device. */
+int bsrg_bav(int ns, int ks, const double *b, const double *v, double *y, char type, char side, void *stream);
+
+/* ---- src/libs/BS/bvmv.f90:2: *out = <x, A y> for the band array ar (n, k)
+ *      ('s', 'a') or (n, 2k-1) ('g'), in the reference's summation order.
+ *      Device (out: one double). */
+int bsrg_bvmv(int n, int k, const double *ar, char type, const double *x, const double *y, double *out,
+              void *stream);
+
+/* ---- src/libs/BS/quadr.f90:2: *out = <p1 | r^m | p2> (bvmv with sb, r1,
+ *      rm1, rm2 or mrm(m)).  p1, p2 (ns) and out (one double) device. */
+int bsrg_quadr(const bsrg_basis *b, const double *p1, const double *p2, int m, double *out, void *stream);
+
 /* ---- src/libs/BS/sum_amb.f90:2.  *out (device, one double) = SUM(a*b) over
  *      the storage mode sym in {'s','l','n','x'}. */
 int bsrg_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, void *stream);
@@ -181,10 +200,16 @@ size_t bsrg_ctx_workspace_bytes(const bsrg_ctx *c);
  * them.  Stages: 0 R^k cell moments, 1 direct groups, 2 exchange groups,
  * 3 one-electron / overlap / symmetrisation, 4 channel eigenproblems,
  * 5 block transforms, 6 dense eigensolve, 7 rkb expansion (mrk_cell),
- * 8 eigenpair refinement. */
-#define BSRG_NSTAGE 9
+ * 8 eigenpair refinement, and inside stage 6 when the library's own
+ * eigensolver runs: 9 dense -> band, 10 band -> tridiagonal, 11 divide and
+ * conquer, 12 stage-2 back-transformation, 13 stage-1 back-transformation.
+ * bsrg_ctx_stage_flops copies (then resets) the floating-point operations the
+ * library's kernels executed per stage where it counts them (block transforms,
+ * the own eigensolver's stages, the refinement; 0 elsewhere). */
+#define BSRG_NSTAGE 14
 int bsrg_ctx_set_timing(bsrg_ctx *c, int on);
 int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n);
+int bsrg_ctx_stage_flops(bsrg_ctx *c, double *flops, int n);
 
 /* ---- resident R^k tables (the reference keeps one multipole's rkb in module
  *      memory, mrk_cell.f90:34-35; a serving process keeps all of them): the

@@ -313,6 +313,36 @@ def convol(ns, ks, d, rkb, icase, sym_i, sym_j):
     return a
 
 
+def bav(ns, ks, b, v, typ, side="r"):
+    """bav.f90:2 (y = B v or v B for a band matrix)."""
+    b = np.asfortranarray(b, dtype=np.float64)
+    v = np.ascontiguousarray(v, dtype=np.float64)
+    y = np.zeros(ns)
+    lib().orc_bav(ns, ks, _p(b), _p(v), _p(y), typ.encode(), side.encode())
+    return y
+
+
+def bvmv(n, k, ar, typ, x, y):
+    """bvmv.f90:2 (<x, A y> for a band array)."""
+    ar = np.asfortranarray(ar, dtype=np.float64)
+    return lib().orc_bvmv(n, k, _p(ar), typ.encode(), _p(np.ascontiguousarray(x, dtype=np.float64)),
+                          _p(np.ascontiguousarray(y, dtype=np.float64)))
+
+
+def facsb(sb, ns, ks):
+    """facsb.f90:2-36: bs = sb^T (upper band storage (ks, ns)) with the r = 0 boundary
+    condition, factorised by LAPACK DPBTRF('U') (scipy's, standing in for the reference's)."""
+    from scipy.linalg import lapack
+    bs = np.asfortranarray(np.asarray(sb).T.copy())
+    for m in range(ks - 1):
+        bs[m, ks - 1 - m] = 0.0
+    bs[ks - 1, 0] = 1.0
+    c, info = lapack.dpbtrf(bs, lower=0)
+    if info != 0:
+        raise RuntimeError("facsb: dpbtrf (LAPACK) failed")
+    return np.asfortranarray(c)
+
+
 def sum_amb(ns, ks, a, b, sym):
     cols = ns
     aa = np.zeros((ns, cols), order="F")
