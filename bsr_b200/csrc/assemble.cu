@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "dgemm.h"
 
 namespace bsrg {
 
@@ -1079,7 +1080,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     if (!tabs) add(sizeof(double) * PL.slice * ks * ks);
     add(sizeof(double) * maxgd * ns * ks);
     add(sizeof(double) * (size_t)ns * ks * 3);
-    // direct contraction by DGEMM (unless BSRG_DIRECT_SIMT selects the register-tiled kernel)
+    // direct contraction by the FP64 tensor-core GEMM (unless BSRG_DIRECT_SIMT selects the register-tiled kernel)
     const bool direct_blas = maxgd > 0 && !getenv("BSRG_DIRECT_SIMT");
     const size_t nk = (size_t)ns * ks;
     if (direct_blas) {
@@ -1201,13 +1202,9 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
             if (direct_blas) {
                 direct_table_kernel<<<(unsigned)((nk * nk + 255) / 256), 256, 0, s>>>(ns, ks, rkbk, PL, R3);
-                const double one = 1.0, zero = 0.0;
-                cublasStatus_t bs = cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)nk, nd, (int)nk, &one, R3,
-                                                (int)nk, Xd, (int)nk, &zero, Cd, (int)nk);
-                if (bs != CUBLAS_STATUS_SUCCESS) {
-                    set_error("assemble: direct DGEMM failed (%d)", (int)bs);
-                    return BSRG_ERR_SOLVER;
-                }
+                // C = R Xd on the FP64 tensor pipe (dgemm.cu)
+                rc = dgemm(false, false, (int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd, (long)nk, s);
+                if (rc != BSRG_OK) return rc;
                 dim3 g4((unsigned)(((size_t)ns * (2 * ks - 1) + 127) / 128), nd);
                 direct_update_kernel<<<g4, 128, 0, s>>>(ns, ks, nd, gdd, Cd, hcc);
             } else {

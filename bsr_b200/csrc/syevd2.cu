@@ -533,6 +533,89 @@ __global__ void __launch_bounds__(Q2_NT) q2_apply_kernel(int n, int S, int ncol,
     }
 }
 
+// Wavefront form of the same application: one CTA per strip of 32 columns, Q2W_WARPS
+// warps; warp w applies groups q = w, w + Q2W_WARPS, ... in the order g = ng-1-q, each
+// group's blocks ascending.  Block (g, i) overlaps only blocks i-2 .. i of group g+1, so
+// it may run once group g+1 has finished block i (or all its blocks): warps wait on the
+// previous group's progress in shared memory (bounded), lane = column, each warp keeps its
+// block's window in shared memory.
+constexpr int Q2W_WARPS = 8;
+constexpr int Q2W_SMEM = Q2W_WARPS * (2 * NB) * 33 * (int)sizeof(double);
+
+__global__ void __launch_bounds__(Q2W_WARPS * 32) q2w_apply_kernel(int n, int S, int ncol,
+                                                                   const double *__restrict__ V2,
+                                                                   const double *__restrict__ Tq, double *Z, long ldz,
+                                                                   int *err)
+{
+    extern __shared__ __align__(16) double q2w_sm[];
+    __shared__ volatile int prog[1024];          // blocks done per group (q order), up to 1024 groups
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + lane;
+    const bool cok = c < ncol;
+    double (*Zw)[33] = (double (*)[33])(q2w_sm + wid * (2 * NB) * 33);   // window rows x 32 columns (+pad)
+    const int ng = (n - 2 + NB - 1) / NB;
+    for (int q = threadIdx.x; q < ng && q < 1024; q += blockDim.x) prog[q] = 0;
+    __syncthreads();
+    for (int q = wid; q < ng; q += Q2W_WARPS) {
+        const int g = ng - 1 - q;
+        const int imax = sweep_steps(n, g * NB);
+        const int iprev = q > 0 ? sweep_steps(n, (g + 1) * NB) : 0;
+        for (int i = 0; i < imax; i++) {
+            if (q > 0) {
+                const int need = min(i + 1, iprev);
+                const unsigned long long t0 = gtime();
+                while (prog[q - 1] < need) {
+                    if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
+                }
+                __threadfence_block();
+            }
+            const int nv = q2_nvalid(n, g, i);
+            const int top = g * NB + 1 + i * NB;
+            const int nrow = min(2 * NB - 1, n - top);
+            for (int r = 0; r < nrow; r++) Zw[r][lane] = cok ? Z[(top + r) + ldz * (long)c] : 0.0;
+            for (int r = nrow; r < 2 * NB; r++) Zw[r][lane] = 0.0;
+            __syncwarp();
+            // W = V^T Zw, then W2 = T W, then Zw -= V W2 (lane = column)
+            const double *Vb = V2 + ((long)(g * NB) * S + i) * NB;     // sweep j = g NB + qq: + qq * S * NB
+            const double *T = Tq + ((long)g * S + i) * NB * NB;
+            double w[NB];
+#pragma unroll
+            for (int qq = 0; qq < NB; qq++) {
+                double sacc = 0.0;
+                if (qq < nv) {
+                    const double *v = Vb + (long)qq * S * NB;
+#pragma unroll 8
+                    for (int t = 0; t < NB; t++) sacc += __ldg(v + t) * Zw[qq + t][lane];
+                }
+                w[qq] = sacc;
+            }
+            double w2[NB];
+#pragma unroll
+            for (int qq = 0; qq < NB; qq++) {
+                double sacc = 0.0;
+#pragma unroll
+                for (int l = qq; l < NB; l++) sacc += __ldg(T + qq + NB * l) * w[l];
+                w2[qq] = sacc;
+            }
+#pragma unroll
+            for (int qq = 0; qq < NB; qq++) {
+                if (qq < nv) {
+                    const double *v = Vb + (long)qq * S * NB;
+#pragma unroll 8
+                    for (int t = 0; t < NB; t++) Zw[qq + t][lane] -= __ldg(v + t) * w2[qq];
+                }
+            }
+            __syncwarp();
+            if (cok)
+                for (int r = 0; r < nrow; r++) Z[(top + r) + ldz * (long)c] = Zw[r][lane];
+            __threadfence_block();
+            __syncwarp();
+            if (lane == 0) prog[q] = i + 1;
+        }
+        if (imax == 0 && lane == 0) prog[q] = 0;
+    }
+}
+
 }  // namespace
 
 // ---- stage 1 driver ----
@@ -726,7 +809,15 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
         if ((e = cudaFuncSetAttribute(q2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2_SMEM)) !=
             cudaSuccess)
             return cuda_fail(e, "dsyevd Q2 smem");
-        q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
+        if (getenv("BSRG_Q2_SIMPLE")) {
+            q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
+        } else {
+            if ((e = cudaFuncSetAttribute(q2w_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2W_SMEM)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd Q2 smem");
+            q2w_apply_kernel<<<(unsigned)((n + 31) / 32), Q2W_WARPS * 32, Q2W_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz,
+                                                                                          sw.err);
+        }
         // per block and column: W = V^T Z (2 NB nv), T W (~NB nv), Z -= V W (2 NB nv)
         double nvsum = 0.0;
         for (int j = 0; j < n - 2; j++) nvsum += sweep_steps(n, j);
@@ -758,7 +849,8 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return cuda_fail(e, "dsyevd");
     if (hflag[0] != 0) {
-        set_error("dsyevd: a device-side wait timed out (%s)", hflag[0] == 2 ? "bulge chasing" : "panel barrier");
+        set_error("dsyevd: a device-side wait timed out (%s)",
+                  hflag[0] == 2 ? "bulge chasing" : hflag[0] == 3 ? "back-transformation wavefront" : "panel barrier");
         return BSRG_ERR_CUDA;
     }
     // kernels of this library per call
