@@ -77,6 +77,7 @@ SIGNATURES = [
     ("bsrg_dsytrd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _P]),
     ("bsrg_dstedc", _c_int, [_P, _c_int, _P, _P, _P, _P, _c_int]),
     ("bsrg_dsyevd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _c_int]),
+    ("bsrg_dsytrd_2stage", _c_int, [_P, _c_int, _P, _c_int, _P, _P]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),
 ]

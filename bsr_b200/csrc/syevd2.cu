@@ -721,8 +721,10 @@ size_t syevd2_workspace_doubles(int n)
 
 // Eigenvalues (ascending, w) and eigenvectors (Z, ldz) of the symmetric A (lower
 // triangle referenced).  Z may be A itself.  ws: syevd2_workspace_doubles(n).
-int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
-                size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches)
+// tri_d / tri_e non-null: stop after the reduction and copy the tridiagonal (d: n, e: n-1) there
+static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
+                       size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches, double *tri_d,
+                       double *tri_e)
 {
     int nl = 0;
     if (n < 1) return BSRG_OK;
@@ -794,6 +796,20 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
         }
     stage_end(c, 10, 2);
     c->stage_flops[10] += fl_chase;
+    if (tri_d) {
+        int hf = 0;
+        if ((e = cudaMemcpyAsync(tri_d, dv, sizeof(double) * n, cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+            (n > 1 && (e = cudaMemcpyAsync(tri_e, ev, sizeof(double) * (n - 1), cudaMemcpyDeviceToDevice, st)) !=
+                          cudaSuccess) ||
+            (e = cudaMemcpyAsync(&hf, flags + 2, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return cuda_fail(e, "dsytrd_2stage");
+        if (hf != 0) {
+            set_error("dsytrd_2stage: a device-side wait timed out (%s)", hf == 2 ? "bulge chasing" : "panel barrier");
+            return BSRG_ERR_CUDA;
+        }
+        return BSRG_OK;
+    }
     // 3. tridiagonal eigenpairs into Z
     stage_begin(c, 11);
     int ndc = 0;
@@ -859,9 +875,29 @@ int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double
     return BSRG_OK;
 }
 
+int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
+                size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches)
+{
+    return syevd2_impl(c, n, A, lda, w, Z, ldz, ws, ws_doubles, pinned, pinned_bytes, launches, nullptr, nullptr);
+}
+
 }  // namespace bsrg
 
 using namespace bsrg;
+
+extern "C" int bsrg_dsytrd_2stage(bsrg_ctx *c, int n, const double *A, int lda, double *d, double *e)
+{
+    if (!c || (n > 0 && (!A || !d || (n > 1 && !e)))) { set_error("dsytrd_2stage: null argument"); return BSRG_ERR_ARG; }
+    if (n < 0 || lda < (n > 0 ? n : 1)) { set_error("dsytrd_2stage: n=%d lda=%d", n, lda); return BSRG_ERR_ARG; }
+    if (n == 0) return BSRG_OK;
+    cudaSetDevice(c->device);
+    int rc = ctx_reserve(c, syevd2_workspace_doubles(n) * sizeof(double) + 1024);
+    if (rc != BSRG_OK) return rc;
+    rc = syevd2_impl(c, n, A, lda, nullptr, nullptr, n, (double *)c->ws, c->ws_bytes / sizeof(double), nullptr, 0,
+                     nullptr, d, e);
+    cudaEventRecord(c->ev_stage, c->stream);
+    return rc;
+}
 
 extern "C" int bsrg_dsyevd(bsrg_ctx *c, int n, const double *A, int lda, double *w, double *Z, int ldz)
 {

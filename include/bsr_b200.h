@@ -361,6 +361,13 @@ int bsrg_dstedc(bsrg_ctx *c, int n, const double *d, const double *e, double *w,
  *      context's stream and workspace. */
 int bsrg_dsyevd(bsrg_ctx *c, int n, const double *A, int lda, double *w, double *Z, int ldz);
 
+/* ---- the reduction alone, as LAPACK's DSYTRD_2STAGE with vect = 'N' (the
+ *      first half of DSYEV, LAPACK_calls.f90:54-76): the symmetric A (lower
+ *      triangle, lda) is reduced through a band of width 32 to the tridiagonal
+ *      T = tridiag(e, d, e) with the same eigenvalues; d (n), e (n-1) device.
+ *      n <= 10240. */
+int bsrg_dsytrd_2stage(bsrg_ctx *c, int n, const double *A, int lda, double *d, double *e);
+
 /* ---- whole path for one partial wave with HOST buffers (bsr_mat SUB1 then
  *      bsr_hd SUB1_HD): knots, orbitals, coefficients in; eigenvalues out.
  *      t (ns+ks), P (ns,norb), coefficient arrays as in bsrg_assemble, all

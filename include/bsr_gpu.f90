@@ -152,6 +152,13 @@
         Integer(c_int) :: bsrg_channel_weights
        End Function
 
+       Function bsrg_dsyevd(c, n, A, lda, w, Z, ldz) bind(C, name="bsrg_dsyevd")
+        Import :: c_int, c_ptr
+        Type(c_ptr), value :: c, A, w, Z
+        Integer(c_int), value :: n, lda, ldz
+        Integer(c_int) :: bsrg_dsyevd
+       End Function
+
        Function cudaMalloc(p, bytes) bind(C, name="cudaMalloc")
         Import :: c_int, c_ptr, c_size_t
         Type(c_ptr) :: p
@@ -357,6 +364,35 @@
       Call gpu_check(cudaFree(dH), 'cudaFree'); Call gpu_check(cudaFree(dE), 'cudaFree')
       Call gpu_check(cudaFree(dV), 'cudaFree')
       End Subroutine gpu_diag_hd
+
+!======================================================================
+      Subroutine gpu_lap_dsyev(job, uplo, n, m, A, eval, info)
+!----------------------------------------------------------------------
+!     LAP_DSYEV (ZCOM/LAPACK_calls.f90:54-76) for job = 'V', uplo = 'L':
+!     all eigenvalues and eigenvectors of A(1:n,1:n) (leading dimension
+!     m) by the library's dense eigensolver; A is overwritten by the
+!     eigenvectors as DSYEV leaves it.  info = 0, or the library's status.
+!----------------------------------------------------------------------
+      Character(1), intent(in) :: job, uplo
+      Integer, intent(in) :: n, m
+      Real(8), intent(inout), target :: A(m, n)
+      Real(8), intent(out), target :: eval(n)
+      Integer, intent(out) :: info
+      Type(c_ptr) :: dA, dE
+      Integer(c_size_t) :: ba, be
+      if (job /= 'V' .or. uplo /= 'L') Stop 'gpu_lap_dsyev: only job = V, uplo = L'
+      ba = int(m, c_size_t) * n * 8
+      be = int(n, c_size_t) * 8
+      Call gpu_check(cudaMalloc(dA, ba), 'cudaMalloc A')
+      Call gpu_check(cudaMalloc(dE, be), 'cudaMalloc eval')
+      Call gpu_check(cudaMemcpy(dA, c_loc(A), ba, cudaMemcpyHostToDevice), 'upload A')
+      info = bsrg_dsyevd(gpu_ctx, n, dA, m, dE, dA, m)
+      if (info == 0) then
+        Call gpu_check(cudaMemcpy(c_loc(A), dA, ba, cudaMemcpyDeviceToHost), 'download vectors')
+        Call gpu_check(cudaMemcpy(c_loc(eval), dE, be, cudaMemcpyDeviceToHost), 'download eval')
+      end if
+      Call gpu_check(cudaFree(dA), 'cudaFree'); Call gpu_check(cudaFree(dE), 'cudaFree')
+      End Subroutine gpu_lap_dsyev
 
 !======================================================================
       Subroutine gpu_w_out_weights(nch, ipsol, khm, a, WT, isol, iprm)

@@ -56,3 +56,27 @@ def test_dsyevd(case):
     assert np.max(np.abs(R)) <= tol * an, (name, np.max(np.abs(R)) / an)
     assert np.max(np.abs(V.T @ V - np.eye(n))) <= tol, (name, np.max(np.abs(V.T @ V - np.eye(n))))
     ctx.close()
+
+
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("random33", "random300", "random2047", "graded",
+                                                                    "block-diagonal")], ids=lambda c: c[0])
+def test_dsytrd_2stage(case):
+    """The reduction alone (dense -> band -> tridiagonal): T has A's eigenvalues."""
+    import torch
+    import bsr_b200 as bsr
+    from bsr_b200._lib import call
+    from bsr_b200.core import _ptr
+    name, A = case
+    n = len(A)
+    ctx = bsr.Context()
+    dA = torch.from_numpy(np.tril(A).T.copy()).cuda()
+    d = torch.empty(n, dtype=torch.float64, device="cuda")
+    e = torch.empty(max(n - 1, 1), dtype=torch.float64, device="cuda")
+    call("bsrg_dsytrd_2stage", ctx.handle, n, _ptr(dA), n, _ptr(d), _ptr(e))
+    torch.cuda.synchronize()
+    dd, ee = d.cpu().numpy(), e.cpu().numpy()[: n - 1]
+    T = np.diag(dd) + np.diag(ee, 1) + np.diag(ee, -1)
+    wr = np.linalg.eigvalsh(A)
+    an = np.max(np.abs(wr))
+    assert np.max(np.abs(np.linalg.eigvalsh(T) - wr)) <= 8 * max(n, 16) * EPS * an, name
+    ctx.close()
