@@ -16,10 +16,11 @@
 namespace bsrg {
 
 // S > 1: item b = blockIdx.z / S computes the K slice blockIdx.z % S into W
-template <class C, bool TA, bool TB>
+template <class C, bool TA, bool TB, bool SYMA = false>
 __global__ void __launch_bounds__(C::NT) dgemm_kernel(DgemmBatch p, int S, int kchunk, double *W)
 {
     extern __shared__ __align__(16) double smem[];
+    if (p.lowc && (int)(blockIdx.y * C::BN) >= (int)(blockIdx.x + 1) * C::BM) return;   // wholly above the diagonal
     const int b = blockIdx.z / S, sp = blockIdx.z % S;
     const double *A = p.Ap ? p.Ap[b] : p.A + (long)b * p.sA;
     const double *B = p.Bp ? p.Bp[b] : p.B + (long)b * p.sB;
@@ -27,7 +28,7 @@ __global__ void __launch_bounds__(C::NT) dgemm_kernel(DgemmBatch p, int S, int k
     const int m0 = blockIdx.x * C::BM, n0 = blockIdx.y * C::BN;
     const int kbeg = sp * kchunk, kend = min(p.k, kbeg + kchunk);
     double acc[C::FM][C::FN][2];
-    dmma::tile_mma<C, TA, TB>(acc, smem, A, p.lda, B, p.ldb, p.m, p.n, kbeg, kend, m0, n0);
+    dmma::tile_mma<C, TA, TB, SYMA>(acc, smem, A, p.lda, B, p.ldb, p.m, p.n, kbeg, kend, m0, n0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wm = warp % C::WM, wn = warp / C::WM, r = lane >> 2, q = lane & 3;
     double *out = S > 1 ? W + (long)sp * p.m * p.n : Cm;
@@ -66,14 +67,15 @@ __global__ void splitk_reduce_kernel(int m, int n, int S, const double *__restri
     *cp = v;
 }
 
-template <class C, bool TA, bool TB>
+template <class C, bool TA, bool TB, bool SYMA = false>
 static int launch(const DgemmBatch &p, int batch, int S, int kchunk, double *W, cudaStream_t s)
 {
     constexpr int bytes = dmma::Smem<C, TA, TB>::BYTES;
-    cudaError_t e = cudaFuncSetAttribute(dgemm_kernel<C, TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e =
+        cudaFuncSetAttribute(dgemm_kernel<C, TA, TB, SYMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return cuda_fail(e, "dgemm: shared memory attribute");
     dim3 g((unsigned)((p.m + C::BM - 1) / C::BM), (unsigned)((p.n + C::BN - 1) / C::BN), (unsigned)(batch * S));
-    dgemm_kernel<C, TA, TB><<<g, C::NT, bytes, s>>>(p, S, kchunk, W);
+    dgemm_kernel<C, TA, TB, SYMA><<<g, C::NT, bytes, s>>>(p, S, kchunk, W);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "dgemm launch");
     if (S > 1) {
@@ -122,6 +124,14 @@ int dgemm_ws(bool ta, bool tb, const DgemmBatch &p, int batch, cudaStream_t s, d
         }
     }
     if (S <= 1) { S = 1; kc = std::max(p.k, 1); }
+    if (p.syma) {
+        if (ta || p.m != p.k) { set_error("dgemm: a symmetric A must be square and not transposed"); return BSRG_ERR_ARG; }
+        if (bn == 32) return tb ? launch<dmma::Tall, false, true, true>(p, batch, S, kc, work, s)
+                                : launch<dmma::Tall, false, false, true>(p, batch, S, kc, work, s);
+        return tb ? launch<dmma::Sq, false, true, true>(p, batch, S, kc, work, s)
+                  : launch<dmma::Sq, false, false, true>(p, batch, S, kc, work, s);
+    }
+    if (p.lowc && p.m != p.n) { set_error("dgemm: lower-triangle output needs a square C"); return BSRG_ERR_ARG; }
     if (bn == 32) return launch_t<dmma::Tall>(ta, tb, p, batch, S, kc, work, s);
     if (bm == 32) return launch_t<dmma::Wide>(ta, tb, p, batch, S, kc, work, s);
     return launch_t<dmma::Sq>(ta, tb, p, batch, S, kc, work, s);

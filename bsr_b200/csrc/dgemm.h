@@ -15,6 +15,8 @@ struct DgemmBatch {
     const double *const *Bp;
     double *const *Cp;
     double alpha, beta;
+    int syma;          // op(A) = A square symmetric, only its lower triangle stored (no transpose)
+    int lowc;          // compute only the tiles of C that reach the lower triangle (square C)
 };
 
 int dgemm_batched(bool ta, bool tb, const DgemmBatch &p, int batch, cudaStream_t s);

@@ -65,21 +65,26 @@ __device__ __forceinline__ void mma884(double &d0, double &d1, double a, double 
 }
 
 // stage one BK slice of the A and B tiles (zero-filled outside the matrices and
-// outside the K range [k0, kend))
-template <class C, bool TA, bool TB>
+// outside the K range [k0, kend)).  SYMA: A is square symmetric with only its lower
+// triangle stored; element (m, k) is read from (max, min), a tile wholly above the
+// diagonal with the index order that keeps the reads coalesced.
+template <class C, bool TA, bool TB, bool SYMA = false>
 __device__ __forceinline__ void load_stage(double *sA, double *sB, const double *A, long lda, const double *B,
                                            long ldb, int M, int N, int kend, int m0, int n0, int k0)
 {
     const int tid = threadIdx.x;
+    const bool upper_tile = SYMA && m0 + C::BM <= k0;
 #pragma unroll
     for (int i = 0; i < (C::BM * BK) / C::NT; i++) {
         const int idx = tid + i * C::NT;
         int ml, kl;
-        if (!TA) { ml = idx % C::BM; kl = idx / C::BM; }
+        if (!TA && !upper_tile) { ml = idx % C::BM; kl = idx / C::BM; }
         else { kl = idx % BK; ml = idx / BK; }
         const int gm = m0 + ml, gk = k0 + kl;
         const bool v = gm < M && gk < kend;
-        const double *src = v ? (TA ? A + gk + (long)gm * lda : A + gm + (long)gk * lda) : A;
+        const double *src;
+        if (SYMA) src = v ? (gm >= gk ? A + gm + (long)gk * lda : A + gk + (long)gm * lda) : A;
+        else src = v ? (TA ? A + gk + (long)gm * lda : A + gm + (long)gk * lda) : A;
         double *dst = TA ? sA + ml * (BK + PAD) + kl : sA + kl * (C::BM + PAD) + ml;
         cp_async8(dst, src, v);
     }
@@ -99,7 +104,7 @@ __device__ __forceinline__ void load_stage(double *sA, double *sB, const double 
 
 // acc[s][t][j]: row m0 + wm*TM + s*8 + (lane>>2), column n0 + wn*TN + t*8 + 2*(lane&3) + j,
 // summed over k in [kbeg, kend)
-template <class C, bool TA, bool TB>
+template <class C, bool TA, bool TB, bool SYMA = false>
 __device__ __forceinline__ void tile_mma(double (&acc)[C::FM][C::FN][2], double *smem, const double *A, long lda,
                                          const double *B, long ldb, int M, int N, int kbeg, int kend, int m0, int n0)
 {
@@ -115,8 +120,8 @@ __device__ __forceinline__ void tile_mma(double (&acc)[C::FM][C::FN][2], double 
 #pragma unroll
     for (int st = 0; st < STAGES - 1; st++) {
         if (st < ktiles)
-            load_stage<C, TA, TB>(smem + st * STG, smem + st * STG + SA, A, lda, B, ldb, M, N, kend, m0, n0,
-                                  kbeg + st * BK);
+            load_stage<C, TA, TB, SYMA>(smem + st * STG, smem + st * STG + SA, A, lda, B, ldb, M, N, kend, m0, n0,
+                                        kbeg + st * BK);
         cp_async_commit();
     }
     for (int kt = 0; kt < ktiles; kt++) {
@@ -125,7 +130,7 @@ __device__ __forceinline__ void tile_mma(double (&acc)[C::FM][C::FN][2], double 
         const int nk = kt + STAGES - 1;
         if (nk < ktiles) {
             double *base = smem + (nk % STAGES) * STG;
-            load_stage<C, TA, TB>(base, base + SA, A, lda, B, ldb, M, N, kend, m0, n0, kbeg + nk * BK);
+            load_stage<C, TA, TB, SYMA>(base, base + SA, A, lda, B, ldb, M, N, kend, m0, n0, kbeg + nk * BK);
         }
         cp_async_commit();
         const double *sA = smem + (kt % STAGES) * STG, *sB = sA + SA;

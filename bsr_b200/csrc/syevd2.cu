@@ -678,13 +678,22 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         // trailing update of A22 = A(j+NB:, j+NB:) (m x m, full symmetric storage)
         double *A22 = A + (j + NB) + lda * (long)(j + NB);
         double *Vp = w.VYV, *Yp = w.VYV + (long)m * NB;
-        int rc = dgemm(false, false, m, NB, m, 1.0, A22, lda, Vp, m, 0.0, w.X, m, st, w.gemm_ws, w.gemm_ws_doubles);
+        // X = A22 V with A22 read from its lower triangle (only the lower triangle is updated)
+        DgemmBatch gx{};
+        gx.m = m; gx.n = NB; gx.k = m;
+        gx.A = A22; gx.lda = lda; gx.B = Vp; gx.ldb = m; gx.C = w.X; gx.ldc = m;
+        gx.alpha = 1.0; gx.beta = 0.0; gx.syma = 1;
+        int rc = dgemm_ws(false, false, gx, 1, st, w.gemm_ws, w.gemm_ws_doubles);
         if (rc != BSRG_OK) return rc;
         const int nch = (m + 127) / 128;
         ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp);
         ypass2_kernel<<<nch, 128, 0, st>>>(m, nch, Vp, w.T, w.Mp, Yp);
-        // A22 -= [V Y] [Y V]^T
-        rc = dgemm(false, true, m, m, 2 * NB, -1.0, w.VYV, m, Yp, m, 1.0, A22, lda, st);
+        // A22 -= [V Y] [Y V]^T, the tiles that reach the lower triangle
+        DgemmBatch gu{};
+        gu.m = m; gu.n = m; gu.k = 2 * NB;
+        gu.A = w.VYV; gu.lda = m; gu.B = Yp; gu.ldb = m; gu.C = A22; gu.ldc = lda;
+        gu.alpha = -1.0; gu.beta = 1.0; gu.lowc = 1;
+        rc = dgemm_ws(false, true, gu, 1, st, nullptr, 0);
         if (rc != BSRG_OK) return rc;
     }
     return cuda_fail(cudaGetLastError(), "sy2sb");
@@ -763,7 +772,8 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     double fl_band = 0.0, fl_chase = 0.0, fl_q2 = 0.0, fl_q1 = 0.0, fl_dc = 0.0;
     for (int j = 0; j + NB < n; j += NB) {
         const double m = n - j - NB;
-        fl_band += 6.0 * m * m * NB + 6.0 * m * NB * NB + 4.0 * m * NB * NB;   // X, rank-2NB update; QR; Y passes
+        // X (2 m^2 NB), the lower-triangle tiles of the rank-2NB update (~2 m^2 NB), QR and Y passes
+        fl_band += 4.0 * m * m * NB + 6.0 * m * NB * NB + 4.0 * m * NB * NB;
         fl_q1 += 4.0 * m * n * NB + 2.0 * NB * NB * n;
     }
     // 1. full symmetric working copy, dense -> band
