@@ -616,6 +616,57 @@ __global__ void __launch_bounds__(Q2W_WARPS * 32) q2w_apply_kernel(int n, int S,
     }
 }
 
+// ---------------------------------------------------------------------------
+// back-transformation of the stage-1 panels, Q1_GROUP panels at a time
+// ---------------------------------------------------------------------------
+constexpr int Q1_GROUP = 4;
+constexpr int Q1W = Q1_GROUP * NB;     // columns of a merged block reflector
+
+struct Q1Panels {
+    const double *V[Q1_GROUP];   // V of each panel (m_q x NB, ld m_q), null past the last panel
+    int m[Q1_GROUP];
+};
+
+// Vg (m0 x Q1W, ld m0): panel q's V shifted down by q NB rows, zeros above
+__global__ void q1_gather_kernel(int m0, Q1Panels P, double *Vg)
+{
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= (long)m0 * Q1W) return;
+    const int r = (int)(idx % m0), c = (int)(idx / m0), q = c / NB, cc = c % NB;
+    double v = 0.0;
+    if (P.V[q] && r >= q * NB) v = P.V[q][(r - q * NB) + (long)P.m[q] * cc];
+    Vg[idx] = v;
+}
+
+// T of the merged reflector from its Gram matrix G = Vg^T Vg and the panels' taus
+// (the diagonals of their T): T(c,c) = tau_c, T(0:c, c) = -tau_c T(0:c, 0:c) G(0:c, c)
+__global__ void __launch_bounds__(Q1W) q1_tfactor_kernel(const double *__restrict__ G, Q1Panels P,
+                                                         const double *__restrict__ T1, int p0, double *Tg)
+{
+    extern __shared__ __align__(16) double q1t_sm[];
+    double (*Ts)[Q1W + 1] = (double (*)[Q1W + 1])q1t_sm;
+    __shared__ double tau[Q1W], tmp[Q1W];
+    const int t = threadIdx.x;
+    {
+        const int q = t / NB, cc = t % NB;
+        tau[t] = P.V[q] ? T1[(size_t)(p0 + q) * NB * NB + cc + NB * cc] : 0.0;
+    }
+    for (int c = 0; c < Q1W; c++) Ts[t][c] = 0.0;
+    __syncthreads();
+    for (int c = 0; c < Q1W; c++) {
+        if (t < c) {
+            double sacc = 0.0;
+            for (int l = t; l < c; l++) sacc += Ts[t][l] * G[l + (long)Q1W * c];
+            tmp[t] = sacc;
+        }
+        __syncthreads();
+        if (t < c) Ts[t][c] = -tau[c] * tmp[t];
+        if (t == 0) Ts[c][c] = tau[c];
+        __syncthreads();
+    }
+    for (int c = 0; c < Q1W; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
+}
+
 }  // namespace
 
 // ---- stage 1 driver ----
@@ -722,8 +773,8 @@ size_t syevd2_workspace_doubles(int n)
     t += (size_t)n * 3 * NB + (size_t)n * NB + 4 * NB * NB + 64;   // VYV, X, T, Mp chunk partials (below)
     t += ((size_t)n / 128 + 2) * NB * NB + 64;
     t += (size_t)(n / NB + 8) * 6 * NB + 64;       // panel partials + Gram
-    t += 2 * (size_t)NB * n + 64;                  // Q1 W1, W2
-    t += 8 * (size_t)NB * n + 64;                  // split-K slices
+    t += 3 * (size_t)4 * NB * n + 2 * (size_t)16 * NB * NB + 6 * 64;   // Q1: W1, W2, merged V, Gram, T
+    t += 8 * (size_t)4 * NB * n + 64;              // split-K slices (outputs up to 128 x n)
     t += dc_workspace_bytes(n) / 8 + 64;           // divide and conquer
     return t + 4096;
 }
@@ -760,8 +811,9 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     int *flags = (int *)take(8);                   // bar[2], err, err2
     sw.bar = (unsigned *)flags;
     sw.err = flags + 2;
-    double *W1 = take((size_t)NB * n), *W2 = take((size_t)NB * n);
-    sw.gemm_ws_doubles = 8 * (size_t)NB * n;
+    double *W1 = take((size_t)Q1W * n), *W2 = take((size_t)Q1W * n);
+    double *Vg = take((size_t)Q1W * n), *Gq = take((size_t)Q1W * Q1W), *Tg = take((size_t)Q1W * Q1W);
+    sw.gemm_ws_doubles = 8 * (size_t)Q1W * n;
     sw.gemm_ws = take(sw.gemm_ws_doubles);
     double *dcw = take(dc_workspace_bytes(n) / 8 + 8);
     if (off > ws_doubles) { set_error("dsyevd: workspace layout"); return BSRG_ERR_NOMEM; }
@@ -774,7 +826,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         const double m = n - j - NB;
         // X (2 m^2 NB), the lower-triangle tiles of the rank-2NB update (~2 m^2 NB), QR and Y passes
         fl_band += 4.0 * m * m * NB + 6.0 * m * NB * NB + 4.0 * m * NB * NB;
-        fl_q1 += 4.0 * m * n * NB + 2.0 * NB * NB * n;
+        fl_q1 += 4.0 * (m + 1.5 * NB) * n * NB + 2.0 * Q1W * NB * n + 2.0 * Q1W * NB * m;  // per panel share of a group
     }
     // 1. full symmetric working copy, dense -> band
     stage_begin(c, 9);
@@ -856,17 +908,33 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         std::vector<size_t> voff;
         size_t vo = 0;
         for (int j = 0; j + NB < n; j += NB) { voff.push_back(vo); vo += (size_t)(n - j - NB) * NB; }
-        for (int p = (int)voff.size() - 1; p >= 0; p--) {
-            const int j = p * NB, m = n - j - NB;
-            const double *Vp = V1 + voff[p], *Tp = T1 + (size_t)p * NB * NB;
-            double *Zs = Z + (j + NB);
-            rc = dgemm(true, false, NB, n, m, 1.0, Vp, m, Zs, ldz, 0.0, W1, NB, st, sw.gemm_ws, sw.gemm_ws_doubles);
-            if (rc == BSRG_OK) rc = dgemm(false, false, NB, n, NB, 1.0, Tp, NB, W1, NB, 0.0, W2, NB, st);
-            if (rc == BSRG_OK) rc = dgemm(false, false, m, n, NB, -1.0, Vp, m, W2, NB, 1.0, Zs, ldz, st);
+        const int ngrp = (np + Q1_GROUP - 1) / Q1_GROUP;
+        for (int gq = ngrp - 1; gq >= 0; gq--) {
+            const int p0 = gq * Q1_GROUP, r0 = p0 * NB + NB, m0 = n - r0;
+            Q1Panels P{};
+            for (int q = 0; q < Q1_GROUP; q++) {
+                const int p = p0 + q;
+                P.V[q] = p < np ? V1 + voff[p] : nullptr;
+                P.m[q] = p < np ? n - p * NB - NB : 0;
+            }
+            q1_gather_kernel<<<(unsigned)(((long)m0 * Q1W + 255) / 256), 256, 0, st>>>(m0, P, Vg);
+            rc = dgemm(true, false, Q1W, Q1W, m0, 1.0, Vg, m0, Vg, m0, 0.0, Gq, Q1W, st, sw.gemm_ws,
+                       sw.gemm_ws_doubles);
+            if (rc != BSRG_OK) return rc;
+            constexpr int q1t_smem = Q1W * (Q1W + 1) * (int)sizeof(double);
+            if ((e = cudaFuncSetAttribute(q1_tfactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, q1t_smem)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd Q1 smem");
+            q1_tfactor_kernel<<<1, Q1W, q1t_smem, st>>>(Gq, P, T1, p0, Tg);
+            double *Zs = Z + r0;
+            rc = dgemm(true, false, Q1W, n, m0, 1.0, Vg, m0, Zs, ldz, 0.0, W1, Q1W, st, sw.gemm_ws,
+                       sw.gemm_ws_doubles);
+            if (rc == BSRG_OK) rc = dgemm(false, false, Q1W, n, Q1W, 1.0, Tg, Q1W, W1, Q1W, 0.0, W2, Q1W, st);
+            if (rc == BSRG_OK) rc = dgemm(false, false, m0, n, Q1W, -1.0, Vg, m0, W2, Q1W, 1.0, Zs, ldz, st);
             if (rc != BSRG_OK) return rc;
         }
     }
-    stage_end(c, 13, 3 * np);
+    stage_end(c, 13, 6 * ((np + Q1_GROUP - 1) / Q1_GROUP));
     c->stage_flops[13] += fl_q1;
     c->stage_flops[6] += fl_band + fl_chase + fl_dc + fl_q2 + fl_q1;
     // device-side waits report through the flags
