@@ -337,11 +337,24 @@ __global__ void __launch_bounds__(32) sb2st_kernel(Sb2stArgs a)
             const int col = i == 0 ? j : r0 - NB;
             const int nl = r0 - col - 1;                        // left columns col+1 .. r0-1
             const int r2 = min(r1 + NB, n), nb2 = r2 - r1;      // rows below the window
-            // ---- loads (through L2: other workers write the band) ----
+            // ---- loads (through L2: other workers write the band), every load of a block
+            // issued before any is used so their latencies overlap ----
             const double x = t < L ? __ldcg(at(r0 + t, col)) : 0.0;
-            for (int c = 0; c < nl; c++) Lb[t][c] = t < L ? __ldcg(at(r0 + t, col + 1 + c)) : 0.0;
-            for (int a2 = 0; a2 < L; a2++) Ds[a2][t] = (t < L && a2 >= t) ? __ldcg(at(r0 + a2, r0 + t)) : 0.0;
-            for (int q = 0; q < nb2; q++) Bs[q][t] = t < L ? __ldcg(at(r1 + q, r0 + t)) : 0.0;
+            {
+                double rl[NB - 1], rd[NB], rb[NB];
+#pragma unroll
+                for (int c = 0; c < NB - 1; c++) rl[c] = (c < nl && t < L) ? __ldcg(at(r0 + t, col + 1 + c)) : 0.0;
+#pragma unroll
+                for (int a2 = 0; a2 < NB; a2++) rd[a2] = (a2 < L && t < L && a2 >= t) ? __ldcg(at(r0 + a2, r0 + t)) : 0.0;
+#pragma unroll
+                for (int q = 0; q < NB; q++) rb[q] = (q < nb2 && t < L) ? __ldcg(at(r1 + q, r0 + t)) : 0.0;
+#pragma unroll
+                for (int c = 0; c < NB - 1; c++) Lb[t][c] = rl[c];
+#pragma unroll
+                for (int a2 = 0; a2 < NB; a2++) Ds[a2][t] = rd[a2];
+#pragma unroll
+                for (int q = 0; q < NB; q++) Bs[q][t] = rb[q];
+            }
             // ---- the reflector ----
             double sig = (t >= 1 && t < L) ? x * x : 0.0;
             for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
@@ -539,10 +552,10 @@ __global__ void __launch_bounds__(Q2_NT) q2_apply_kernel(int n, int S, int ncol,
 // it may run once group g+1 has finished block i (or all its blocks): warps wait on the
 // previous group's progress in shared memory (bounded), lane = column, each warp keeps its
 // block's window in shared memory.
-constexpr int Q2W_WARPS = 8;
+constexpr int Q2W_WARPS = 6;
 constexpr int Q2W_SMEM = Q2W_WARPS * (2 * NB) * 33 * (int)sizeof(double);
 
-__global__ void __launch_bounds__(Q2W_WARPS * 32) q2w_apply_kernel(int n, int S, int ncol,
+__global__ void __launch_bounds__(Q2W_WARPS * 32, 2) q2w_apply_kernel(int n, int S, int ncol,
                                                                    const double *__restrict__ V2,
                                                                    const double *__restrict__ Tq, double *Z, long ldz,
                                                                    int *err)
@@ -572,8 +585,15 @@ __global__ void __launch_bounds__(Q2W_WARPS * 32) q2w_apply_kernel(int n, int S,
             const int nv = q2_nvalid(n, g, i);
             const int top = g * NB + 1 + i * NB;
             const int nrow = min(2 * NB - 1, n - top);
-            for (int r = 0; r < nrow; r++) Zw[r][lane] = cok ? Z[(top + r) + ldz * (long)c] : 0.0;
-            for (int r = nrow; r < 2 * NB; r++) Zw[r][lane] = 0.0;
+#pragma unroll
+            for (int r0w = 0; r0w < 2 * NB; r0w += 16) {     // 16 loads in flight at a time
+                double zr[16];
+#pragma unroll
+                for (int r = 0; r < 16; r++)
+                    zr[r] = (cok && r0w + r < nrow) ? Z[(top + r0w + r) + ldz * (long)c] : 0.0;
+#pragma unroll
+                for (int r = 0; r < 16; r++) Zw[r0w + r][lane] = zr[r];
+            }
             __syncwarp();
             // W = V^T Zw, then W2 = T W, then Zw -= V W2 (lane = column)
             const double *Vb = V2 + ((long)(g * NB) * S + i) * NB;     // sweep j = g NB + qq: + qq * S * NB
