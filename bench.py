@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched and serving sub-results")
+    ap.add_argument("--steps-only", action="store_true",
+                    help="run the warm-up and timed steps only and print the basic line (for a profiler's "
+                         "launch list of exactly those steps)")
     return ap.parse_args()
 
 
@@ -391,6 +394,15 @@ def run_b200(args):
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
     ms_total = float(t_max.item())
     value = world * args.steps / (ms_total * 1e-3)
+    if args.steps_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+                              "higher_is_better": True, "config": workload_desc(pw, khm), "clocks": clk,
+                              "note": "--steps-only: the timed steps without the side measurements"}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     # ---- stage breakdown (separate pass with stage events on) ----
     ctx.set_timing(True)
     ctx.stage_times()
