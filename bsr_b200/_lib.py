@@ -78,6 +78,8 @@ SIGNATURES = [
     ("bsrg_dstedc", _c_int, [_P, _c_int, _P, _P, _P, _P, _c_int]),
     ("bsrg_dsyevd", _c_int, [_P, _c_int, _P, _c_int, _P, _P, _c_int]),
     ("bsrg_dsytrd_2stage", _c_int, [_P, _c_int, _P, _c_int, _P, _P]),
+    ("bsrg_dgemm_tf32x3", _c_int, [_c_int, _c_int, _c_int, _c_double, _P, _c_int, _P, _c_int, _c_double, _P,
+                                   _c_int, _P, _P]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),
 ]

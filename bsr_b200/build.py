@@ -29,6 +29,7 @@ UNITS = {
     "refine.cu": [],
     "tridiag_dc.cu": [],
     "syevd2.cu": [],
+    "tc_mixed.cu": [],
 }
 
 

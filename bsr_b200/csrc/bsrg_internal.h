@@ -59,6 +59,8 @@ int launch_density(int ns, int ks, double *d, const double *p1, const double *p2
 int launch_convol(int ns, int ks, double *a, const double *d, const double *rkb, int ldp, int icase,
                   char si, char sj, cudaStream_t s);
 int launch_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, cudaStream_t s);
+int tf32x3_gemm(int m, int n, int k, double alpha, const double *A, long lda, const double *B, long ldb, double beta,
+                double *C, long ldc, int *err, cudaStream_t s);
 int launch_bav(int ns, int ks, const double *b, const double *v, double *y, char type, char side, cudaStream_t s);
 int launch_bvmv(int n, int k, const double *ar, char type, const double *x, const double *y, double *out,
                 cudaStream_t s);

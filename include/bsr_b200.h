@@ -312,6 +312,16 @@ int bsrg_dgemm(char transa, char transb, int m, int n, int k, double alpha, cons
                const double *B, long ldb, long strideB, double beta, double *C, long ldc, long strideC, int batch,
                void *stream);
 
+/* ---- No counterpart in the reference (which assembles in FP64): the split-
+ *      precision product of the mixed-precision form, on the 5th-generation
+ *      tensor cores (tcgen05 kind::tf32, FP32 accumulation in tensor memory).
+ *      C = alpha A B + beta C, column-major FP64 arrays (A m x k, B k x n); each
+ *      operand is split into two TF32 parts and the three leading products are
+ *      accumulated, ~22 significant bits per operand.  *err (device int) is set
+ *      to 1 if a device-side wait ran out.  Device. */
+int bsrg_dgemm_tf32x3(int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,
+                      double beta, double *C, int ldc, int *err, void *stream);
+
 /* ---- the channel solution offsets ipsol(0:nch) of the last bsrg_diag_hd on
  *      this context (module bsr_hd's ipsol, set in diag_hd.f90:100-111):
  *      channel i owns rows ipsol[i] .. ipsol[i+1]-1 of the eigenvectors. */
