@@ -361,6 +361,10 @@ class Context:
         """FP64 Rayleigh-quotient refinement of diag_hd's eigenpairs (on by default)."""
         call("bsrg_ctx_set_refine", self.handle, 1 if on else 0)
 
+    def set_precision(self, mixed=True):
+        """Mixed-precision form (tensor-core split-TF32 direct contraction) or FP64 (default)."""
+        call("bsrg_ctx_set_precision", self.handle, 1 if mixed else 0)
+
     def refine_stats(self, n):
         """(correction, residual norm) per eigenpair of the last refined diag_hd, as CUDA tensors."""
         corr = torch.empty(n, device="cuda", dtype=torch.float64)

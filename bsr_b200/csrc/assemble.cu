@@ -927,6 +927,13 @@ int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n)
     return rc;
 }
 
+int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed)
+{
+    if (!c) { set_error("ctx_set_precision: null context"); return BSRG_ERR_ARG; }
+    c->precision = mixed ? 1 : 0;
+    return BSRG_OK;
+}
+
 int bsrg_ctx_stage_flops(bsrg_ctx *c, double *flops, int n)
 {
     if (!c || !flops) { set_error("ctx_stage_flops: null argument"); return BSRG_ERR_ARG; }
@@ -1086,6 +1093,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     if (direct_blas) {
         add(sizeof(double) * nk * nk);
         add(sizeof(double) * nk * maxgd);
+        add(sizeof(int) * 4);      // the tensor-core product's wait flag (mixed precision)
     }
     add(sizeof(unsigned short) * (size_t)ncoef);
     int rc = ctx_reserve(c, need);
@@ -1111,6 +1119,12 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     unsigned short *d_zoff = ar.take<unsigned short>(std::max(ncoef, 1));
     double *R3 = direct_blas ? ar.take<double>(nk * nk) : nullptr;
     double *Cd = direct_blas ? ar.take<double>(nk * maxgd) : nullptr;
+    int *d_tcerr = direct_blas ? ar.take<int>(4) : nullptr;
+    const bool mixed = c->precision == 1;
+    if (mixed && d_tcerr) {
+        cudaError_t em = cudaMemsetAsync(d_tcerr, 0, sizeof(int) * 4, s);
+        if (em != cudaSuccess) return cuda_fail(em, "assemble: mixed flag");
+    }
     // stage host metadata through pinned memory, one copy
     char *hp = (char *)c->pinned;
     size_t o = 0;
@@ -1202,8 +1216,14 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
             if (direct_blas) {
                 direct_table_kernel<<<(unsigned)((nk * nk + 255) / 256), 256, 0, s>>>(ns, ks, rkbk, PL, R3);
-                // C = R Xd on the FP64 tensor pipe (dgemm.cu)
-                rc = dgemm(false, false, (int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd, (long)nk, s);
+                // C = R Xd on the FP64 tensor pipe (dgemm.cu), or in the mixed-precision form as the
+                // split-TF32 product on tcgen05 (tc_mixed.cu)
+                if (mixed)
+                    rc = tf32x3_gemm((int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd, (long)nk, d_tcerr,
+                                     s);
+                else
+                    rc = dgemm(false, false, (int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd,
+                               (long)nk, s);
                 if (rc != BSRG_OK) return rc;
                 dim3 g4((unsigned)(((size_t)ns * (2 * ks - 1) + 127) / 128), nd);
                 direct_update_kernel<<<g4, 128, 0, s>>>(ns, ks, nd, gdd, Cd, hcc);
@@ -1233,6 +1253,14 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             stage_end(c, 2, 1);
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "assemble k-loop");
+    }
+    if (mixed && d_tcerr) {
+        // the tensor-core product reports a device-side wait that ran out through this flag
+        int hf = 0;
+        cudaError_t em = cudaMemcpyAsync(&hf, d_tcerr, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (em == cudaSuccess) em = cudaStreamSynchronize(s);
+        if (em != cudaSuccess) return cuda_fail(em, "assemble: mixed flag");
+        if (hf) { set_error("assemble: a tensor-core wait timed out"); return BSRG_ERR_CUDA; }
     }
     // ---- target energies, overlap, symmetrisation ----
     if (!full) {

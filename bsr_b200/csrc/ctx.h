@@ -46,6 +46,7 @@ struct bsrg_ctx {
     std::vector<double> *pw_knots;           //   ks and the knots are unchanged
     int pw_ks;
     int refine;                              // FP64 refinement of the eigenpairs in diag_hd (default on)
+    int precision;                           // 0 FP64 (default), 1 mixed (tensor-core assembly contraction)
     double *rf_buf;                          // per-pair correction | residual of the last refined diag_hd
     size_t rf_cap;                           //   (doubles held)
     int rf_n;                                //   (pairs recorded)

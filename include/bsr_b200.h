@@ -301,6 +301,12 @@ int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const doub
  *      and resid (device, n <= khm doubles each, either may be NULL) on the
  *      context's stream. */
 int bsrg_ctx_set_refine(bsrg_ctx *c, int on);
+/* ---- No counterpart in the reference: the mixed-precision form for this
+ *      context (mixed = 1; 0 restores FP64, the default).  bsrg_assemble then
+ *      computes the direct contraction (convol icase 1 of every direct group,
+ *      I_data.f90:206) as bsrg_dgemm_tf32x3's split-precision tensor-core
+ *      product; everything else, the eigensolve and its refinement stay FP64. */
+int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed);
 int bsrg_diag_hd_refine_stats(bsrg_ctx *c, int n, double *corr, double *resid);
 
 /* ---- No counterpart in the reference (it links BLAS but calls no DGEMM on
