@@ -30,6 +30,7 @@
 
 #include "ctx.h"
 #include "dgemm.h"
+#include "dmma.cuh"
 
 namespace bsrg {
 
@@ -721,6 +722,197 @@ static exchange_factored_fn exchange_factored_for(int ks)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Exchange groups of every multipole in one pass: the factored form above with
+// its two contractions on the FP64 tensor pipe (m8n8k4 DMMA) and each channel
+// block's strip written once.
+//
+// One CTA per (column y', XF consecutive rows x); warp w owns row x = x0 + w.
+// For each multipole k that has exchange groups:
+//   W[e][b] = sum_f R(x,x+e,y'+f,y') p_b(y'+f)     DMMA  M = e, N = b, K = f
+//   Z[a][b] = sum_e p_a(x+e) W[e][b]               DMMA  M = a, N = b, K = e
+//   acc[blk][w] += sum_t c_t Z[a_t][b_t]           one thread per (group, row)
+// The R window of the next multipole is fetched by cp.async while Z and the
+// terms of the current one run.  After the last multipole the XF x 1 strip of
+// every channel block is written once (write mode: the kernel is the first to
+// touch H, so no separate zeroing pass) or added to the caller's blocks.  A block
+// has at most one exchange group per multipole, so the per-k updates of acc are
+// race-free.  Operand tiles in shared memory use row strides of 4 mod 16 doubles,
+// with which the fragment loads of each half-warp hit 16 distinct 8-byte banks.
+// ---------------------------------------------------------------------------
+constexpr int XF = 8;                   // rows per CTA (one warp each)
+
+__host__ __device__ constexpr int stride4mod16(int n) { return n <= 4 ? 4 : ((n - 4 + 15) / 16) * 16 + 4; }
+
+template <int KS> struct XFLayout {
+    static constexpr int HW = KS - 1, NE = 2 * KS - 1;
+    static constexpr int KT = (NE + 3) / 4;          // k-steps over f (W) and over e (Z)
+    static constexpr int EP = 4 * KT;                // padded e / f range
+    static constexpr int ME = (NE + 7) / 8;          // m-tiles over e (W)
+    static constexpr int SR = stride4mod16(EP);      // row stride of R, p_b^T and W^T
+    static constexpr int SP = stride4mod16(XF + EP - 1);   // row stride of p_a^T
+    static constexpr int REG = ((32 * SR > NORB_MAX * ZLD ? 32 * SR : NORB_MAX * ZLD)) | 1;  // W^T, then Z, per row
+    static constexpr int PY = 0;                     // p_b(y'+f-HW)      [b][f]
+    static constexpr int PX = PY + NORB_MAX * SR;    // p_a(x0-HW+r)      [a][r]
+    static constexpr int RS = PX + NORB_MAX * SP;    // R                 [w][e][f]
+    static constexpr int RG = RS + XF * NE * SR;     // per-row region    [w][REG]
+    static constexpr int ACC = RG + XF * REG;        // strip sums        [blk][w]
+    static size_t smem_bytes(int nblk) { return sizeof(double) * ((size_t)ACC + (size_t)nblk * XF); }
+};
+
+struct XKRange {
+    int k, g0, ng, pad;                  // multipole, first exchange group, group count
+};
+
+template <int KS>
+__global__ void __launch_bounds__(32 * XF, 1)
+exchange_fused_kernel(int ns, int norb, int nblk, int nact, const XKRange *__restrict__ kr, PadLayout L,
+                      const double *__restrict__ rk0, size_t tstride, const GroupDesc *__restrict__ gd,
+                      const unsigned short *__restrict__ zoff, const double *__restrict__ cv,
+                      const double *__restrict__ P, double *hcc, int accumulate)
+{
+    using Y = XFLayout<KS>;
+    constexpr int HW = Y::HW, NE = Y::NE, KT = Y::KT, EP = Y::EP, ME = Y::ME, SR = Y::SR, SP = Y::SP;
+    extern __shared__ __align__(16) double xs[];
+    double *PyT = xs + Y::PY, *PxT = xs + Y::PX, *Rs = xs + Y::RS, *acc = xs + Y::ACC;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, lr = lane >> 2, lc = lane & 3;
+    const int x0 = blockIdx.x * XF, yp = blockIdx.y;
+    const int ntb = (norb + 7) / 8;
+    double *reg = xs + Y::RG + w * Y::REG;
+    // ---- orbital windows, zeroed R tile (padding columns stay zero) and strip sums ----
+    for (int q = tid; q < NORB_MAX * SR; q += 32 * XF) {
+        const int b = q / SR, f = q % SR, y = yp + f - HW;
+        PyT[q] = (b < norb && f < NE && y >= 0 && y < ns) ? P[y + (size_t)ns * b] : 0.0;
+    }
+    for (int q = tid; q < NORB_MAX * SP; q += 32 * XF) {
+        const int a = q / SP, r = q % SP, xr = x0 - HW + r;
+        PxT[q] = (a < norb && xr >= 0 && xr < ns) ? P[xr + (size_t)ns * a] : 0.0;
+    }
+    for (int q = tid; q < XF * NE * SR; q += 32 * XF) Rs[q] = 0.0;
+    for (int q = tid; q < nblk * XF; q += 32 * XF) acc[q] = 0.0;
+    __syncthreads();
+    // R(x,x+e',y'+f',y') of multipole kr[i].k for the CTA's rows, e' = e-HW, f' = f-HW
+    auto fetch_r = [&](int i) {
+        const double *T = rk0 + tstride * (size_t)kr[i].k;
+        for (int q = tid; q < XF * NE * NE; q += 32 * XF) {
+            const int wi = q % XF, ef = q / XF, e = ef / NE - HW, f = ef % NE - HW, x = x0 + wi;
+            const int r1 = e >= 0 ? x : x + e, r2 = f >= 0 ? yp : yp + f;
+            const bool ok = x < ns;
+            const double *src = ok ? T + (size_t)(r1 + L.PL) + (size_t)L.NP * (r2 + L.PL) +
+                                         L.slice * ((e >= 0 ? e : -e) + KS * (f >= 0 ? f : -f))
+                                   : T;
+            cp_async8(Rs + (wi * NE + (e + HW)) * SR + (f + HW), src, ok);
+        }
+        cp_async_commit();
+    };
+    if (nact > 0) fetch_r(0);
+    for (int i = 0; i < nact; i++) {
+        cp_async_wait<0>();
+        __syncthreads();                 // R(i) in place; the previous multipole's terms are done
+        // ---- W = R P_y on the tensor pipe; rows e >= NE of R are zero ----
+        double aw[ME][4][2];
+#pragma unroll
+        for (int mt = 0; mt < ME; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) aw[mt][nt][0] = aw[mt][nt][1] = 0.0;
+        const double *Rw = Rs + w * NE * SR;
+#pragma unroll
+        for (int kk = 0; kk < KT; kk++) {
+            double bf[4];
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) bf[nt] = PyT[(nt * 8 + lr) * SR + kk * 4 + lc];
+#pragma unroll
+            for (int mt = 0; mt < ME; mt++) {
+                const int e = mt * 8 + lr;
+                const double af = e < NE ? Rw[e * SR + kk * 4 + lc] : 0.0;
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+                    if (nt < ntb) dmma::mma884(aw[mt][nt][0], aw[mt][nt][1], af, bf[nt]);
+            }
+        }
+        __syncthreads();                 // every warp is done with R(i)
+        if (i + 1 < nact) fetch_r(i + 1);
+        // W^T [b][e] into this row's region (rows e < EP; e >= NE are zero)
+#pragma unroll
+        for (int mt = 0; mt < ME; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int e = mt * 8 + lr, b = nt * 8 + 2 * lc + j;
+                    if (e < EP && nt < ntb) reg[b * SR + e] = aw[mt][nt][j];
+                }
+        __syncwarp();
+        // ---- Z = P_x^T W ----
+        double az[4][4][2];
+#pragma unroll
+        for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) az[mt][nt][0] = az[mt][nt][1] = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < KT; kk++) {
+            double bf[4];
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++) bf[nt] = nt < ntb ? reg[(nt * 8 + lr) * SR + kk * 4 + lc] : 0.0;
+#pragma unroll
+            for (int mt = 0; mt < 4; mt++) {
+                if (mt >= ntb) continue;
+                const double af = PxT[(mt * 8 + lr) * SP + w + kk * 4 + lc];
+#pragma unroll
+                for (int nt = 0; nt < 4; nt++)
+                    if (nt < ntb) dmma::mma884(az[mt][nt][0], az[mt][nt][1], af, bf[nt]);
+            }
+        }
+        __syncwarp();                    // W^T reads done before Z overwrites the region
+#pragma unroll
+        for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+            for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+                    if (mt < ntb && nt < ntb) reg[(mt * 8 + lr) * ZLD + nt * 8 + 2 * lc + j] = az[mt][nt][j];
+        __syncthreads();                 // Z of every row in place
+        // ---- acc[blk][row] += sum_t c_t Z[a_t][b_t] for the groups of this multipole ----
+        const XKRange K = kr[i];
+        for (int q = tid; q < K.ng * XF; q += 32 * XF) {
+            const int wi = q % XF;
+            const GroupDesc G = gd[K.g0 + q / XF];
+            const double *Z = xs + Y::RG + wi * Y::REG;
+            double s0 = 0.0, s1 = 0.0;
+            int t = G.start;
+            for (; t + 1 < G.end; t += 2) {
+                s0 = fma(__ldg(cv + t), Z[__ldg(zoff + t)], s0);
+                s1 = fma(__ldg(cv + t + 1), Z[__ldg(zoff + t + 1)], s1);
+            }
+            if (t < G.end) s0 = fma(__ldg(cv + t), Z[__ldg(zoff + t)], s0);
+            acc[G.blk * XF + wi] += s0 + s1;
+        }
+    }
+    __syncthreads();
+    // ---- each block's strip, once ----
+    const size_t nn = (size_t)ns * ns;
+    for (int q = tid; q < nblk * XF; q += 32 * XF) {
+        const int blk = q / XF, wi = q % XF, x = x0 + wi;
+        if (x >= ns) continue;
+        double *dst = hcc + (size_t)blk * nn + x + (size_t)ns * yp;
+        *dst = accumulate ? *dst + acc[q] : acc[q];
+    }
+}
+
+typedef void (*exchange_fused_fn)(int, int, int, int, const XKRange *, PadLayout, const double *, size_t,
+                                  const GroupDesc *, const unsigned short *, const double *, const double *,
+                                  double *, int);
+
+static exchange_fused_fn exchange_fused_for(int ks, size_t *smem_fixed)
+{
+#define XFCASE(K) case K: *smem_fixed = XFLayout<K>::smem_bytes(0); return exchange_fused_kernel<K>;
+    switch (ks) {
+    XFCASE(2) XFCASE(3) XFCASE(4) XFCASE(5) XFCASE(6) XFCASE(7) XFCASE(8) XFCASE(9) XFCASE(10) XFCASE(11) XFCASE(12)
+    default: *smem_fixed = 0; return nullptr;
+    }
+#undef XFCASE
+}
+
 typedef void (*rkb_pad_fn)(int, int, PadLayout, const double *, const double *, const double *, const double *,
                            const double *, double *);
 
@@ -1070,6 +1262,19 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             nchunks += xchunks[k].size();
         }
     }
+    // exchange of every multipole in one pass (exchange_fused_kernel) when the orbitals and
+    // the channel blocks' strip sums fit; BSRG_EXCHANGE_PER_K keeps one launch per multipole
+    const size_t nblk = (size_t)nch * (nch + 1) / 2;
+    size_t xfu_smem = 0;
+    exchange_fused_fn xfu = nullptr;
+    if (norb <= NORB_MAX && !getenv("BSRG_EXCHANGE_PER_K") && !getenv("BSRG_EXCHANGE_GATHER")) {
+        xfu = exchange_fused_for(ks, &xfu_smem);
+        xfu_smem += sizeof(double) * nblk * XF;
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+        if (xfu && xfu_smem > (size_t)optin) xfu = nullptr;
+    }
+    std::vector<XKRange> kact;
     // ---- workspace ----
     size_t nn = (size_t)ns * ns;
     size_t need = 0;
@@ -1084,7 +1289,10 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     add(sizeof(double) * (size_t)ik * ik * nv);
     const PadLayout PL = pad_layout(ns, ks);
     const bsrg_tables *tabs = (c->tables && c->tables->basis == b && c->tables->kmax >= kmax) ? c->tables : nullptr;
-    if (!tabs) add(sizeof(double) * PL.slice * ks * ks);
+    // the fused exchange reads every multipole's table in one launch
+    const size_t ntab = xfu ? (size_t)kmax + 1 : 1;
+    if (!tabs) add(sizeof(double) * PL.slice * ks * ks * ntab);
+    add(sizeof(XKRange) * ((size_t)kmax + 1));
     add(sizeof(double) * maxgd * ns * ks);
     add(sizeof(double) * (size_t)ns * ks * 3);
     // direct contraction by the FP64 tensor-core GEMM (unless BSRG_DIRECT_SIMT selects the register-tiled kernel)
@@ -1100,7 +1308,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     if (rc != BSRG_OK) return rc;
     size_t host_bytes = sizeof(int) * (size_t)ncoef * 2 + sizeof(double) * (size_t)ncoef +
                         sizeof(GroupDesc) * ngroups + sizeof(XChunk) * nchunks + sizeof(int) * nch +
-                        sizeof(double) * nch + 64;
+                        sizeof(double) * nch + sizeof(XKRange) * ((size_t)kmax + 1) + 64;
     rc = ctx_reserve_pinned(c, host_bytes);
     if (rc != BSRG_OK) return rc;
     Arena ar{(char *)c->ws, 0, c->ws_bytes};
@@ -1112,7 +1320,8 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     double *d_ech = ar.take<double>(nch);
     double *rkd1 = ar.take<double>((size_t)ik * nv), *rkd2 = ar.take<double>((size_t)ik * nv);
     double *rkd = ar.take<double>((size_t)ik * ik * nv);
-    double *rkbp = tabs ? nullptr : ar.take<double>(PL.slice * ks * ks);
+    double *rkbp = tabs ? nullptr : ar.take<double>(PL.slice * ks * ks * ntab);
+    XKRange *d_kr = ar.take<XKRange>((size_t)kmax + 1);
     double *Xd = ar.take<double>(std::max<size_t>(maxgd, 1) * ns * ks);
     double *rmk = ar.take<double>((size_t)ns * ks);
     double *M1 = ar.take<double>((size_t)ns * ks), *M2 = ar.take<double>((size_t)ns * ks);
@@ -1146,6 +1355,9 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         stage(xchunks[k].data(), sizeof(XChunk) * xchunks[k].size());
     }
     size_t o_lch = full ? stage(lch, sizeof(int) * nch) : 0, o_ech = full ? stage(ech, sizeof(double) * nch) : 0;
+    for (int k = 0; k <= kmax; k++)
+        if (!xgroups[k].empty()) kact.push_back(XKRange{k, (int)xoff[k], (int)xgroups[k].size(), 0});
+    size_t o_kr = stage(kact.data(), sizeof(XKRange) * kact.size());
     cudaError_t e;
 #define CP(dst, off, bytes) \
     if ((bytes) > 0 && (e = cudaMemcpyAsync(dst, hp + (off), bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) \
@@ -1159,12 +1371,50 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         CP(d_lch, o_lch, sizeof(int) * nch);
         CP(d_ech, o_ech, sizeof(double) * nch);
     }
+    if (xfu) CP(d_kr, o_kr, sizeof(XKRange) * kact.size());
 #undef CP
     cudaEventRecord(c->ev_stage, s);
+    const size_t tstride = tabs ? tabs->table_doubles : PL.slice * ks * ks;
+    const double *rk0 = tabs ? tabs->rkbp : rkbp;
+    if (xfu) {
+        // ---- the R^k tables of every multipole, then the exchange of all of them (first writer of H) ----
+        if (!tabs)
+            for (int k = 0; k <= kmax; k++) {
+                if (dgroups[k].empty() && xgroups[k].empty()) continue;
+                stage_begin(c, 0);
+                rc = launch_rk_moments(b, k, rkd1, rkd2, rkd, s);
+                if (rc != BSRG_OK) return rc;
+                stage_end(c, 0, 3);
+                stage_begin(c, 7);
+                rc = build_padded_table(b, k, rkd1, rkd2, rkd, M1, M2, rkbp + tstride * k, s);
+                if (rc != BSRG_OK) return rc;
+                stage_end(c, 7, 2);
+            }
+        if ((e = cudaFuncSetAttribute(xfu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xfu_smem)) != cudaSuccess)
+            return cuda_fail(e, "exchange (fused) smem");
+    }
+    if (xfu && (full || !kact.empty())) {
+        stage_begin(c, 2);
+        int launches = 1;
+        if (!kact.empty()) {
+            pack_terms_kernel<<<(ncoef + 255) / 256, 256, 0, s>>>(ncoef, d_ca, d_cb, d_zoff);
+            launches++;
+        }
+        dim3 gx((ns + XF - 1) / XF, ns);
+        xfu<<<gx, 32 * XF, xfu_smem, s>>>(ns, norb, (int)nblk, (int)kact.size(), d_kr, PL, rk0, tstride, d_gd,
+                                          d_zoff, d_cv, P, hcc, full ? 0 : 1);
+        stage_end(c, 2, launches);
+        // executed arithmetic: the two contractions per output and multipole, one FMA per output and record
+        const double NE = 2.0 * ks - 1.0;
+        double nxt = 0.0;
+        for (const XKRange &r : kact) nxt += (double)(xgroups[r.k].back().end - xgroups[r.k].front().start);
+        c->stage_flops[2] += 2.0 * nn * ((double)kact.size() * (NE * NE * norb + NE * norb * norb) + nxt);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "exchange (fused)");
+    }
     // ---- one-electron part ----
-    size_t nblk = (size_t)nch * (nch + 1) / 2;
     if (full) {
-        if ((e = cudaMemsetAsync(hcc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess) return cuda_fail(e, "memset hcc");
+        if (!xfu && (e = cudaMemsetAsync(hcc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess)
+            return cuda_fail(e, "memset hcc");
         if (scc && (e = cudaMemsetAsync(scc, 0, sizeof(double) * nn * nblk, s)) != cudaSuccess)
             return cuda_fail(e, "memset scc");
         if (acf && (e = cudaMemsetAsync(acf, 0, sizeof(double) * nch * nch * (kmax + 1), s)) != cudaSuccess)
@@ -1184,7 +1434,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     // the factored exchange handles up to NORB_MAX orbitals; BSRG_EXCHANGE_GATHER selects the gather kernel
     exchange_factored_fn xf = (norb <= NORB_MAX && !getenv("BSRG_EXCHANGE_GATHER")) ? exchange_factored_for(ks) : nullptr;
     const size_t xfsm = exchange_factored_smem(ks);
-    if (xf) {
+    if (xf && !xfu) {
         if ((e = cudaFuncSetAttribute(xf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xfsm)) != cudaSuccess)
             return cuda_fail(e, "exchange (factored) smem");
         if (ncoef > 0) {
@@ -1199,6 +1449,8 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         const double *rkbk = rkbp;
         if (tabs) {
             rkbk = tabs->rkbp + tabs->table_doubles * k;        // resident table of this multipole
+        } else if (xfu) {
+            rkbk = rkbp + PL.slice * ks * ks * k;               // built above with the exchange
         } else {
             stage_begin(c, 0);
             rc = launch_rk_moments(b, k, rkd1, rkd2, rkd, s);
@@ -1239,7 +1491,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             }
             stage_end(c, 1, (direct_blas ? 3 : 2) + (acf ? 2 : 0));
         }
-        if (nx > 0) {
+        if (nx > 0 && !xfu) {
             stage_begin(c, 2);
             if (xf) {
                 dim3 g3((ns + XCH - 1) / XCH, ns);
