@@ -372,6 +372,12 @@ class Context:
         call("bsrg_diag_hd_refine_stats", self.handle, n, _ptr(corr), _ptr(res))
         return corr, res
 
+    def channel_fallbacks(self):
+        """diag_hd calls on this context whose channel solves went to the cuSOLVER fallback."""
+        n = ctypes.c_int()
+        call("bsrg_ctx_channel_fallbacks", self.handle, ctypes.byref(n))
+        return n.value
+
     def set_timing(self, on=True):
         call("bsrg_ctx_set_timing", self.handle, 1 if on else 0)
 

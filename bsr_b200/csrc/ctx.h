@@ -50,6 +50,7 @@ struct bsrg_ctx {
     double *rf_buf;                          // per-pair correction | residual of the last refined diag_hd
     size_t rf_cap;                           //   (doubles held)
     int rf_n;                                //   (pairs recorded)
+    int chan_fallbacks;                      // channel solves redone on the library path (orthogonality check)
 };
 
 namespace bsrg {
@@ -87,6 +88,12 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
 size_t syevd2_workspace_doubles(int n);
 int dense_syevd(bsrg_ctx *c, int n, const double *A, long lda, double *w, double *Z, long ldz, double *ws,
                 size_t ws_doubles, void *pinned, size_t pinned_bytes, int *launches);
+
+// the channel eigenproblems of diag_hd (chan_eig.cu)
+bool chan_own_ok(int ns, int ks, int npad, int device);
+size_t chan_own_workspace_doubles(int nch, int npad, int ks);
+int chan_own_solve(bsrg_ctx *c, const bsrg_basis *b, const double *hcc, int nch, int npad, const int *d_s0,
+                   const int *d_nsol, double *AA, double *Wv, int *d_info, double *ws, int *d_flag);
 
 // eigenpair refinement (refine.cu)
 size_t refine_workspace_doubles(int n);

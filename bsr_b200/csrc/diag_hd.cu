@@ -9,7 +9,8 @@
 //   2. A = diag(bval) + bb_i^T H_ij bb_j for every stored off-diagonal block
 //      (:188-219);
 //   3. DSYEV('V','L') of A (:312, LAPACK_calls.f90:54).
-// Step 1 runs batched cuSOLVER channel solves, the filter and compaction run on
+// Step 1 runs the library's batched channel solves (chan_eig.cu; cuSOLVER's
+// batched path as the fallback), the filter and compaction run on
 // the device (one small host read of the per-channel counts fixes khm), step 2
 // is two batched FP64 tensor-core GEMMs over all blocks (dgemm.cu), step 3 is
 // cuSOLVER's syevd, followed by the FP64 Rayleigh-quotient refinement of every
@@ -444,6 +445,14 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     if (own_eig) add(sizeof(double) * syevd2_workspace_doubles(khm_max));
     size_t batched_bytes = chan_batched_bytes(c, params, ns, s0v, nsolv);
     add(batched_bytes);
+    // the library's own channel solves (chan_eig.cu); BSRG_CHANNEL_LIB selects cuSOLVER's batched path
+    const int npad = *std::max_element(nsolv.begin(), nsolv.end());
+    const bool own_chan = !getenv("BSRG_CHANNEL_LIB") && !getenv("BSRG_CHANNEL_SYGVD") &&
+                          chan_own_ok(ns, ks, npad, c->device);
+    if (own_chan) {
+        add(sizeof(double) * chan_own_workspace_doubles(nch, npad, ks));
+        add(sizeof(int) * 4);
+    }
     int rc = ctx_reserve(c, need);
     if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
     // pinned staging layout (ints): s0 | nsol | info | cnt | ipsol | final info, then block maps and pointers
@@ -468,6 +477,8 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     double *Fsym = refine ? ar.take<double>(refine_workspace_doubles(khm_max)) : nullptr;
     int *d_rflag = refine ? ar.take<int>(4) : nullptr;
     double *eig_ws = own_eig ? ar.take<double>(syevd2_workspace_doubles(khm_max)) : nullptr;
+    double *chan_ws = own_chan ? ar.take<double>(chan_own_workspace_doubles(nch, npad, ks)) : nullptr;
+    int *d_cflag = own_chan ? ar.take<int>(4) : nullptr;
     int *hi = (int *)c->pinned;
     std::memcpy(hi + o_s0, s0v.data(), sizeof(int) * nch);
     std::memcpy(hi + o_nsol, nsolv.data(), sizeof(int) * nch);
@@ -484,7 +495,25 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     // not available in the loaded cuSOLVER, each channel goes through sygvd.
     stage_begin(c, 4);
     bool batched = batched_bytes > 0 && chan_batched_ok(c, params, ns, nsolv);
-    if (batched) {
+    int chan_launches = batched ? 5 : 2;
+    bool own_done = false;
+    if (own_chan) {
+        // the own kernels; if the eigenvectors of a channel come out far from orthonormal
+        // (eigenvalues equal to working precision), the library path below redoes all channels
+        int rco = chan_own_solve(c, b, hcc, nch, npad, d_s0, d_nsol, AA, Wv, d_info, chan_ws, d_cflag);
+        if (rco != BSRG_OK) { cusolverDnDestroyParams(params); return rco; }
+        int hf[2] = {0, 0};
+        if ((e = cudaMemcpyAsync(hf, d_cflag, sizeof(hf), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+            cusolverDnDestroyParams(params);
+            return cuda_fail(e, "diag_hd channel solves");
+        }
+        own_done = hf[0] == 0 && hf[1] == 0;
+        chan_launches = 8;
+        if (!own_done) c->chan_fallbacks++;
+    }
+    if (own_done) {
+    } else if (batched) {
         int rcb = solve_channels_batched(c, params, b, hcc, nch, s0v, nsolv, d_s0, d_nsol, AA, Wv, d_info, ar);
         if (rcb != BSRG_OK) { cusolverDnDestroyParams(params); return rcb; }
     } else {
@@ -504,7 +533,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         }
     }
     keep_count_kernel<<<nch, 256, 0, s>>>(ns, nch, d_nsol, Wv, edmax, egap, d_cnt);
-    stage_end(c, 4, batched ? 5 : 2);   // own kernels: extracts, pad shift, scatter-back, keep_count
+    stage_end(c, 4, chan_launches);     // own kernels (the library path: extracts, pad shift, scatter-back)
     if ((e = cudaMemcpyAsync(hi + o_info, d_info, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(hi + o_cnt, d_cnt, sizeof(int) * nch, cudaMemcpyDeviceToHost, s)) != cudaSuccess) {
         cusolverDnDestroyParams(params);
@@ -658,6 +687,13 @@ extern "C" int bsrg_ctx_set_refine(bsrg_ctx *c, int on)
 {
     if (!c) { set_error("ctx_set_refine: null context"); return BSRG_ERR_ARG; }
     c->refine = on ? 1 : 0;
+    return BSRG_OK;
+}
+
+extern "C" int bsrg_ctx_channel_fallbacks(const bsrg_ctx *c, int *count)
+{
+    if (!c || !count) { set_error("ctx_channel_fallbacks: null argument"); return BSRG_ERR_ARG; }
+    *count = c->chan_fallbacks;
     return BSRG_OK;
 }
 

@@ -308,6 +308,12 @@ int bsrg_ctx_set_refine(bsrg_ctx *c, int on);
  *      product; everything else, the eigensolve and its refinement stay FP64. */
 int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed);
 int bsrg_diag_hd_refine_stats(bsrg_ctx *c, int n, double *corr, double *resid);
+/* ---- No counterpart in the reference: how many bsrg_diag_hd calls on this
+ *      context redid their channel problems (diag_hd.f90:82-111) on the
+ *      cuSOLVER path because the library's own batched solves flagged a pair
+ *      of eigenvectors as far from orthogonal (eigenvalues equal to working
+ *      precision).  Host int. */
+int bsrg_ctx_channel_fallbacks(const bsrg_ctx *c, int *count);
 
 /* ---- No counterpart in the reference (it links BLAS but calls no DGEMM on
  *      this path; diag_hd.f90:188-219 transforms the blocks with hand loops):
