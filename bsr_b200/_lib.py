@@ -67,6 +67,8 @@ SIGNATURES = [
                                        _IP, _DP, _P, _P]),
     ("bsrg_diag_hd", _c_int, [_P, _P, _c_int, _IP, _P, _c_int, _c_int, _c_int, _c_double, _c_double,
                               _c_int, _P, _IP, _P, _P]),
+    ("bsrg_diag_hd_gen", _c_int, [_P, _P, _c_int, _IP, _P, _P, _c_int, _c_int, _c_int, _c_double, _c_double,
+                                  _c_int, _P, _IP, _P, _P]),
     ("bsrg_bs_orth", _c_int, [_P, _P, _c_int, _c_int, _P, _IP, _IP, _P]),
     ("bsrg_diag_hd_ipsol", _c_int, [_P, _c_int, _IP]),
     ("bsrg_ctx_set_refine", _c_int, [_P, _c_int]),

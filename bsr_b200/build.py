@@ -31,6 +31,7 @@ UNITS = {
     "syevd2.cu": [],
     "tc_mixed.cu": [],
     "chan_eig.cu": [],
+    "dense_chol.cu": [],
 }
 
 

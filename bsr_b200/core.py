@@ -465,8 +465,11 @@ def add_two_electron(ctx, basis, nch, P, kmax, coefs, hcc, acf=None):
 
 
 def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001, want_vectors=True,
-            want_bb=False):
-    """bsr_hd diag_hd for a block-diagonal overlap: eigenvalues (khm,) [+ vectors (khm,khm), bb]."""
+            want_bb=False, scc=None):
+    """bsr_hd diag_hd: eigenvalues (khm,) [+ vectors (khm,khm), bb].  With scc (the channel
+    overlap blocks in hcc's layout; its off-diagonal blocks define the generalized problem,
+    the diagonal ones are the basis overlap) the generalized branch runs (DPOTRF, DSYGST,
+    DTRSM of diag_hd.f90:268-334); without it S is block diagonal."""
     lch_a = np.ascontiguousarray(lch, dtype=np.int32)
     nch = len(lch_a)
     ns = basis.ns
@@ -474,9 +477,14 @@ def diag_hd(ctx, basis, lch, hcc, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0
     vecs = torch.empty((nch * ns) ** 2, device="cuda", dtype=torch.float64) if want_vectors else None
     bb = fortran_empty((ns, nch * ns)) if want_bb else None
     khm = ctypes.c_int()
-    call("bsrg_diag_hd", ctx.handle, basis.handle, nch, _iptr(lch_a), _ptr(as_fortran(hcc)), itype, ilzero, ibzero,
-         float(Edmax), float(Egap), 1 if want_vectors else 0, _ptr(ev), ctypes.byref(khm),
-         _ptr(vecs) if want_vectors else None, _ptr(bb) if want_bb else None)
+    if scc is None:
+        call("bsrg_diag_hd", ctx.handle, basis.handle, nch, _iptr(lch_a), _ptr(as_fortran(hcc)), itype, ilzero,
+             ibzero, float(Edmax), float(Egap), 1 if want_vectors else 0, _ptr(ev), ctypes.byref(khm),
+             _ptr(vecs) if want_vectors else None, _ptr(bb) if want_bb else None)
+    else:
+        call("bsrg_diag_hd_gen", ctx.handle, basis.handle, nch, _iptr(lch_a), _ptr(as_fortran(hcc)),
+             _ptr(as_fortran(scc)), itype, ilzero, ibzero, float(Edmax), float(Egap), 1 if want_vectors else 0,
+             _ptr(ev), ctypes.byref(khm), _ptr(vecs) if want_vectors else None, _ptr(bb) if want_bb else None)
     n = khm.value
     ipsol = np.zeros(nch + 1, dtype=np.int32)
     call("bsrg_diag_hd_ipsol", ctx.handle, nch, _iptr(ipsol))

@@ -95,6 +95,15 @@ size_t chan_own_workspace_doubles(int nch, int npad, int ks);
 int chan_own_solve(bsrg_ctx *c, const bsrg_basis *b, const double *hcc, int nch, int npad, const int *d_s0,
                    const int *d_nsol, double *AA, double *Wv, int *d_info, double *ws, int *d_flag);
 
+// dense Cholesky and triangular solves (dense_chol.cu)
+size_t chol_workspace_doubles(int n);
+int dpotrf_lower(int n, double *C, long ldc, double *Linv, double *tmp, int *info, cudaStream_t s, int *launches);
+int trsm_lower_left(int n, int m, const double *L, long ldl, const double *Linv, double *B, long ldb, bool trans,
+                    double *tmp, size_t tmp_doubles, cudaStream_t s, int *launches);
+int sygst_lower(int n, double *A, long lda, const double *L, long ldl, const double *Linv, double *T, double *tmp,
+                size_t tmp_doubles, cudaStream_t s, int *launches);
+int mirror_lower(int n, double *A, long lda, cudaStream_t s);
+
 // eigenpair refinement (refine.cu)
 size_t refine_workspace_doubles(int n);
 int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s);

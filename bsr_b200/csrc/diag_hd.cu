@@ -189,6 +189,12 @@ __global__ void scatter_blocks_kernel(int ns, long lda, const BlockMap *__restri
     A[(size_t)(ipsol[m.ic] + r) + (size_t)lda * (ipsol[m.jc] + c)] = T[(size_t)b * ns * ns + tid];
 }
 
+__global__ void fill_diag_kernel(long n, double v, double *A)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) A[i + n * i] = v;
+}
+
 __global__ void set_diag_kernel(long n, const double *__restrict__ bval, double *A)
 {
     long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -361,9 +367,11 @@ static int solve_channels_batched(bsrg_ctx *c, cusolverDnParams_t params, const 
 
 using namespace bsrg;
 
-extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
-                            int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
-                            double *eval, int *khm_out, double *vecs, double *bbout)
+// scc == NULL: the block-diagonal overlap (diag_ovl /= 0); otherwise the generalized
+// branch with the channel-channel overlap blocks of scc (diag_ovl = 0)
+static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                        const double *scc, int itype, int ilzero, int ibzero, double edmax, double egap,
+                        int want_vectors, double *eval, int *khm_out, double *vecs, double *bbout)
 {
     if (!c || !b || !lch || !hcc || !eval || !khm_out) {
         set_error("diag_hd: null argument");
@@ -443,6 +451,14 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         add(sizeof(int) * 4);
     }
     if (own_eig) add(sizeof(double) * syevd2_workspace_doubles(khm_max));
+    const bool gen = scc != nullptr;
+    int nbo = 0;                          // off-diagonal overlap blocks to transform
+    if (gen) {
+        nbo = nch * (nch - 1) / 2;
+        add(sizeof(double) * (size_t)khm_max * khm_max * 2);       // C (overlap), then the DSYGST transpose
+        add(sizeof(double) * chol_workspace_doubles(khm_max));
+        add(sizeof(int) * 4);
+    }
     size_t batched_bytes = chan_batched_bytes(c, params, ns, s0v, nsolv);
     add(batched_bytes);
     // the library's own channel solves (chan_eig.cu); BSRG_CHANNEL_LIB selects cuSOLVER's batched path
@@ -458,9 +474,9 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     // pinned staging layout (ints): s0 | nsol | info | cnt | ipsol | final info, then block maps and pointers
     const size_t o_s0 = 0, o_nsol = nch, o_info = 2 * (size_t)nch, o_cnt = 3 * (size_t)nch, o_ip = 4 * (size_t)nch,
                  o_fin = 5 * (size_t)nch + 1;
-    size_t o_bm_bytes = ((o_fin + 1) * sizeof(int) + 15) & ~(size_t)15;
+    size_t o_bm_bytes = ((o_fin + 2) * sizeof(int) + 15) & ~(size_t)15;
     size_t o_ptr_bytes = (o_bm_bytes + sizeof(BlockMap) * nb + 15) & ~(size_t)15;
-    const size_t o_dc_bytes = (o_ptr_bytes + sizeof(double *) * nb * 5 + 64 + 255) & ~(size_t)255;
+    const size_t o_dc_bytes = (o_ptr_bytes + sizeof(double *) * nb * 6 + 64 + 255) & ~(size_t)255;
     rc = ctx_reserve_pinned(c, o_dc_bytes + (own_eig ? dc_pinned_bytes(khm_max) : 0) + 64);
     if (rc != BSRG_OK) { cusolverDnDestroyParams(params); return rc; }
     Arena ar{(char *)c->ws, 0, c->ws_bytes};
@@ -478,6 +494,10 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     int *d_rflag = refine ? ar.take<int>(4) : nullptr;
     double *eig_ws = own_eig ? ar.take<double>(syevd2_workspace_doubles(khm_max)) : nullptr;
     double *chan_ws = own_chan ? ar.take<double>(chan_own_workspace_doubles(nch, npad, ks)) : nullptr;
+    double *Cov = gen ? ar.take<double>((size_t)khm_max * khm_max) : nullptr;
+    double *Tgst = gen ? ar.take<double>((size_t)khm_max * khm_max) : nullptr;
+    double *chol_ws = gen ? ar.take<double>(chol_workspace_doubles(khm_max)) : nullptr;
+    int *d_cinfo = gen ? ar.take<int>(4) : nullptr;
     int *d_cflag = own_chan ? ar.take<int>(4) : nullptr;
     int *hi = (int *)c->pinned;
     std::memcpy(hi + o_s0, s0v.data(), sizeof(int) * nch);
@@ -583,6 +603,8 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         h_ptrs[2 * nb + q] = Wt + nn * q;
         h_ptrs[3 * nb + q] = BB + nn * m.ic;
         h_ptrs[4 * nb + q] = T + nn * q;
+        // overlap block S_ij of the generalized branch (the first nbo entries: the off-diagonal pairs)
+        h_ptrs[5 * nb + q] = (gen && q < nbo) ? (double *)(scc + ((size_t)(m.ic + 1) * m.ic / 2 + m.jc) * nn) : nullptr;
     }
     if ((e = cudaMemcpyAsync(d_ipsol, h_ip, sizeof(int) * (nch + 1), cudaMemcpyHostToDevice, s)) != cudaSuccess) {
         cusolverDnDestroyParams(params);
@@ -590,7 +612,7 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
     }
     if (nb > 0) {
         if ((e = cudaMemcpyAsync(d_bm, h_bm, sizeof(BlockMap) * nb, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(d_ptrs, h_ptrs, sizeof(double *) * nb * 5, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
+            (e = cudaMemcpyAsync(d_ptrs, h_ptrs, sizeof(double *) * nb * 6, cudaMemcpyHostToDevice, s)) != cudaSuccess) {
             cusolverDnDestroyParams(params);
             return cuda_fail(e, "diag_hd block upload");
         }
@@ -621,8 +643,46 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         dim3 g((unsigned)((nn + 127) / 128), nb);
         scatter_blocks_kernel<<<g, 128, 0, s>>>(ns, khm, d_bm, d_ipsol, T, A);
     }
-    stage_end(c, 5, (nb > 0 ? 4 : 1) + (refine ? 0 : 1));   // compact, [set_diag], 2 GEMMs, scatter
+    int t_launches = (nb > 0 ? 4 : 1) + (refine ? 0 : 1);   // compact, [set_diag], 2 GEMMs, scatter
     c->stage_flops[5] += 4.0 * (double)ns * ns * ns * nb;
+    if (gen) {
+        // ---- generalized branch: C = I + bb_i^T S_ij bb_j (diag_hd.f90:127-186), DPOTRF(C) and
+        //      DSYGST(1,'L') of A (:268-284) ----
+        if ((e = cudaMemsetAsync(Cov, 0, sizeof(double) * asz, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(d_cinfo, 0, sizeof(int), s)) != cudaSuccess) {
+            cusolverDnDestroyParams(params);
+            return cuda_fail(e, "diag_hd overlap");
+        }
+        fill_diag_kernel<<<(khm + 255) / 256, 256, 0, s>>>(khm, 1.0, Cov);
+        t_launches++;
+        if (nbo > 0) {
+            double **pS = d_ptrs + 5 * nb, **pBj = d_ptrs + nb, **pW = d_ptrs + 2 * nb, **pBi = d_ptrs + 3 * nb,
+                   **pT = d_ptrs + 4 * nb;
+            DgemmBatch g1{};
+            g1.m = ns; g1.n = ns; g1.k = ns;
+            g1.lda = ns; g1.ldb = ns; g1.ldc = ns;
+            g1.Ap = (const double *const *)pS; g1.Bp = (const double *const *)pBj; g1.Cp = pW;
+            g1.alpha = 1.0; g1.beta = 0.0;
+            DgemmBatch g2 = g1;
+            g2.Ap = (const double *const *)pBi; g2.Bp = (const double *const *)pW; g2.Cp = pT;
+            int rg = dgemm_batched(false, false, g1, nbo, s);
+            if (rg == BSRG_OK) rg = dgemm_batched(true, false, g2, nbo, s);
+            if (rg != BSRG_OK) { cusolverDnDestroyParams(params); return rg; }
+            dim3 g((unsigned)((nn + 127) / 128), nbo);
+            scatter_blocks_kernel<<<g, 128, 0, s>>>(ns, khm, d_bm, d_ipsol, T, Cov);
+            t_launches += 3;
+            c->stage_flops[5] += 4.0 * (double)ns * ns * ns * nbo;
+        }
+        double *Linv = chol_ws, *ctmp = chol_ws + (chol_workspace_doubles(khm_max) - (size_t)khm_max * 128 - 64);
+        const size_t ctmp_doubles = (size_t)khm_max * 128 + 64;
+        int rg = dpotrf_lower(khm, Cov, khm, Linv, ctmp, d_cinfo, s, &t_launches);
+        if (rg == BSRG_OK) rg = mirror_lower(khm, A, khm, s);
+        if (rg == BSRG_OK) rg = sygst_lower(khm, A, khm, Cov, khm, Linv, Tgst, ctmp, ctmp_doubles, s, &t_launches);
+        if (rg != BSRG_OK) { cusolverDnDestroyParams(params); return rg; }
+        t_launches++;
+        c->stage_flops[5] += (1.0 / 3.0 + 2.0) * (double)khm * khm * khm;
+    }
+    stage_end(c, 5, t_launches);
     if (refine) {
         // keep the full symmetric A for the residuals: the eigensolver overwrites A
         stage_begin(c, 8);
@@ -670,17 +730,50 @@ extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int
         if (rr != BSRG_OK) return rr;
         c->rf_n = khm;
     }
+    if (gen && want_vectors) {
+        // ---- x = L^-T y (diag_hd.f90:322-334, DTRSM('Left','L','T')) ----
+        stage_begin(c, 6);
+        int nl = 0;
+        double *ctmp = chol_ws + (chol_workspace_doubles(khm_max) - (size_t)khm_max * 128 - 64);
+        int rg = trsm_lower_left(khm, khm, Cov, khm, chol_ws, A, khm, true, ctmp, (size_t)khm_max * 128 + 64, s, &nl);
+        stage_end(c, 6, nl);
+        c->stage_flops[6] += (double)khm * khm * khm;
+        if (rg != BSRG_OK) return rg;
+    }
     if (bbout && (e = cudaMemcpyAsync(bbout, BB, sizeof(double) * nn * nch, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
         return cuda_fail(e, "diag_hd bb copy");
     if ((e = cudaMemcpyAsync(hi + o_fin, d_info + nch, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return cuda_fail(e, "diag_hd info");
+    if (gen && (e = cudaMemcpyAsync(hi + o_fin + 1, d_cinfo, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return cuda_fail(e, "diag_hd info");
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diag_hd syevd");
+    if (gen && hi[o_fin + 1] != 0) {
+        set_error("BSR_HD: Cholesky factorization failed (overlap pivot %d)", hi[o_fin + 1]);
+        return BSRG_ERR_INFO;
+    }
     int hinfo = hi[o_fin];
     if (hinfo != 0) {
         set_error("LAP_DSYEV: DSYEV(lapack) gives INFO = %d", hinfo);
         return BSRG_ERR_INFO;
     }
     return stage_collect(c);
+}
+
+extern "C" int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                            int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
+                            double *eval, int *khm_out, double *vecs, double *bbout)
+{
+    return diag_hd_impl(c, b, nch, lch, hcc, nullptr, itype, ilzero, ibzero, edmax, egap, want_vectors, eval,
+                        khm_out, vecs, bbout);
+}
+
+extern "C" int bsrg_diag_hd_gen(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                                const double *scc, int itype, int ilzero, int ibzero, double edmax, double egap,
+                                int want_vectors, double *eval, int *khm_out, double *vecs, double *bbout)
+{
+    if (!scc) { set_error("diag_hd_gen: null overlap"); return BSRG_ERR_ARG; }
+    return diag_hd_impl(c, b, nch, lch, hcc, scc, itype, ilzero, ibzero, edmax, egap, want_vectors, eval,
+                        khm_out, vecs, bbout);
 }
 
 extern "C" int bsrg_ctx_set_refine(bsrg_ctx *c, int on)

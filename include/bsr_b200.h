@@ -283,6 +283,22 @@ int bsrg_diag_hd(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, cons
                  int itype, int ilzero, int ibzero, double edmax, double egap, int want_vectors,
                  double *eval, int *khm, double *vecs, double *bb);
 
+/* ---- src/bsr/BSR_HD3/diag_hd.f90:2-340 for an overlap with channel-channel
+ *      blocks (diag_ovl = 0, "GENERALIZED eigenvalue problem", :66-69): as
+ *      bsrg_diag_hd, plus the transform of the overlap to the channel
+ *      eigenbasis, C = I + bb_i^T S_ij bb_j (:127-186), DPOTRF of C (:272),
+ *      DSYGST(1,'L') of A (:284), and after the eigensolve the back-transform
+ *      x = L^-T y (DTRSM('Left','L','T'), :322-334).  scc (device) holds the
+ *      overlap blocks in hcc's layout; its diagonal blocks are taken from b's
+ *      sb, as for bsrg_diag_hd (the reference reads the same values from the
+ *      overlap file).  Perturber rows (kcp > 0) are not part of this path.
+ *      The refinement, when on, refines the eigenpairs of the standard
+ *      problem L^-1 A L^-T.  An overlap that is not positive definite returns
+ *      BSRG_ERR_INFO ("Cholesky factorization failed"). */
+int bsrg_diag_hd_gen(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
+                     const double *scc, int itype, int ilzero, int ibzero, double edmax, double egap,
+                     int want_vectors, double *eval, int *khm, double *vecs, double *bb);
+
 /* ---- src/bsr/BSR_MAT3/bs_orth.f90:2-92 (BS_ORTH, called from sub1.f90:195):
  *      orthogonality conditions of the channels.  Channel i is made orthogonal
  *      to the orbitals ort_idx[ort_ptr[i] .. ort_ptr[i+1]-1] (host, 0-based

@@ -418,9 +418,13 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
     """Solve H c = E S c the way bsr_hd does for one partial wave.
 
     hcc, scc: (nch(nch+1)/2, ns, ns) lower-triangle channel blocks [row, col]
-    as written by Record_matrix (record_matrix.f90:2).  S must be block
-    diagonal here (diag_ovl /= 0): the reference then solves a standard
-    problem after the per-channel pre-diagonalisation (diag_hd.f90:68-71).
+    as written by Record_matrix (record_matrix.f90:2).  With a block-diagonal
+    S (diag_ovl /= 0) the reference solves a standard problem after the
+    per-channel pre-diagonalisation (diag_hd.f90:68-71); with off-diagonal
+    overlap blocks (diag_ovl = 0) it transforms them to the channel basis,
+    C = I + bb_i^T S_ij bb_j (:127-186), and runs DPOTRF(C), DSYGST(1,'L') of A
+    (:268-284), DSYEV, and the back-transform DTRSM('Left','L','T') (:322-334);
+    so does this restatement ("generalized" in the result is True then).
     Returns dict(eval, khm, bval, ipsol, [a_vectors]).
 
     refine=True restates the library's refined form: the diagonal blocks of A
@@ -436,10 +440,7 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
     nch = len(lch)
     blk = lambda i, j: hcc[i * (i + 1) // 2 + j]   # 0-based i >= j
     sblk = lambda i, j: scc[i * (i + 1) // 2 + j]
-    for i in range(nch):
-        for j in range(i):
-            if np.any(sblk(i, j) != 0):
-                raise NotImplementedError("generalized path (S with off-diagonal blocks)")
+    gen = any(np.any(sblk(i, j) != 0) for i in range(nch) for j in range(i))
     bb = []
     bval = []
     ipsol = [0]
@@ -477,7 +478,27 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
                 continue
             w = bb[ic].T @ h          # rows: solutions of ic, cols: B-splines
             a[ipsol[ic]: ipsol[ic + 1], ipsol[jc]: ipsol[jc + 1]] = w @ bb[jc]
-    out = {"khm": khm, "bval": np.array(bval), "ipsol": np.array(ipsol), "bb": bb}
+    out = {"khm": khm, "bval": np.array(bval), "ipsol": np.array(ipsol), "bb": bb, "generalized": gen}
+    Lc = None
+    if gen:
+        from scipy.linalg import solve_triangular
+        cmat = np.eye(khm, order="F")
+        for ic in range(nch):
+            for jc in range(ic):
+                sij = sblk(ic, jc)
+                if np.any(sij != 0):
+                    cmat[ipsol[ic]: ipsol[ic + 1], ipsol[jc]: ipsol[jc + 1]] = bb[ic].T @ sij @ bb[jc]
+        Lc, info = lapack.dpotrf(cmat, lower=1, clean=1)
+        if info != 0:
+            raise RuntimeError("BSR_HD: Cholesky factorization failed (info %d)" % info)
+        a, info = lapack.dsygst(a, Lc, itype=1, lower=1)
+        if info != 0:
+            raise RuntimeError("DSYGST info %d" % info)
+        a = np.asfortranarray(np.tril(a))
+        out["c"] = np.tril(cmat) + np.tril(cmat, -1).T
+        back = lambda y: solve_triangular(Lc, y, trans="T", lower=True)
+    else:
+        back = lambda y: y
     if refine:
         full = np.tril(a) + np.tril(a, -1).T
         if lowest is not None:
@@ -489,14 +510,14 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
                 raise RuntimeError("DSYEV info %d" % info)
         ev, resid = rayleigh_refine(full, ev, vec, refine_dtype)
         o = np.argsort(ev, kind="stable")
-        out.update({"eval": ev[o], "resid": resid[o], "vectors": vec[:, o], "a": full})
+        out.update({"eval": ev[o], "resid": resid[o], "vectors": back(vec[:, o]), "a": full})
         return out
     ev, vec, info = lapack.dsyev(a, compute_v=1 if want_vectors else 0, lower=1)[:3]
     if info != 0:
         raise RuntimeError("DSYEV info %d" % info)
     out["eval"] = ev
     if want_vectors:
-        out["vectors"] = vec
+        out["vectors"] = back(vec)
     return out
 
 
