@@ -143,6 +143,17 @@
         Integer(c_int) :: bsrg_diag_hd
        End Function
 
+       Function bsrg_diag_hd_gen(c, b, nch, lch, hcc, scc, itype, ilzero, ibzero, edmax, egap, &
+                want_vectors, eval, khm, vecs, bb) bind(C, name="bsrg_diag_hd_gen")
+        Import :: c_int, c_double, c_ptr
+        Type(c_ptr), value :: c, b, hcc, scc, eval, vecs, bb
+        Integer(c_int), value :: nch, itype, ilzero, ibzero, want_vectors
+        Integer(c_int), intent(in) :: lch(*)
+        Real(c_double), value :: edmax, egap
+        Integer(c_int), intent(out) :: khm
+        Integer(c_int) :: bsrg_diag_hd_gen
+       End Function
+
        Function bsrg_channel_weights(c, nch, ipsol, khm, a, wt, isol, iprm) &
                 bind(C, name="bsrg_channel_weights")
         Import :: c_int, c_ptr
@@ -364,6 +375,44 @@
       Call gpu_check(cudaFree(dH), 'cudaFree'); Call gpu_check(cudaFree(dE), 'cudaFree')
       Call gpu_check(cudaFree(dV), 'cudaFree')
       End Subroutine gpu_diag_hd
+
+!======================================================================
+      Subroutine gpu_diag_hd_gen(nch, lch, hcc, scc, itype, ilzero, ibzero, Edmax, Egap, &
+                                 khm, eval, a)
+!----------------------------------------------------------------------
+!     diag_hd for diag_ovl = 0 (diag_hd.f90:82-334 with channel-channel
+!     overlap blocks scc in hcc's layout): eigenvalues eval(1:khm) and the
+!     back-transformed eigenvectors a(1:khm,1:khm) (after DTRSM, :334)
+!----------------------------------------------------------------------
+      Use spline_param, only: ns
+      Integer, intent(in) :: nch, itype, ilzero, ibzero
+      Integer(c_int), intent(in) :: lch(nch)
+      Real(8), intent(in), target :: hcc(ns, ns, nch*(nch+1)/2), scc(ns, ns, nch*(nch+1)/2)
+      Real(8), intent(in) :: Edmax, Egap
+      Integer, intent(out) :: khm
+      Real(8), intent(out), target :: eval(nch*ns), a(*)
+      Type(c_ptr) :: dH, dS, dE, dV
+      Integer(c_size_t) :: bh, be, bv
+      Integer(c_int) :: k
+      bh = int(ns, c_size_t) * ns * (nch*(nch+1)/2) * 8
+      be = int(nch, c_size_t) * ns * 8
+      bv = int(nch, c_size_t) * ns * nch * ns * 8
+      Call gpu_check(cudaMalloc(dH, bh), 'cudaMalloc hcc')
+      Call gpu_check(cudaMalloc(dS, bh), 'cudaMalloc scc')
+      Call gpu_check(cudaMalloc(dE, be), 'cudaMalloc eval')
+      Call gpu_check(cudaMalloc(dV, bv), 'cudaMalloc vectors')
+      Call gpu_check(cudaMemcpy(dH, c_loc(hcc), bh, cudaMemcpyHostToDevice), 'upload hcc')
+      Call gpu_check(cudaMemcpy(dS, c_loc(scc), bh, cudaMemcpyHostToDevice), 'upload scc')
+      Call gpu_check(bsrg_diag_hd_gen(gpu_ctx, gpu_basis, nch, lch, dH, dS, itype, ilzero, ibzero, &
+                     Edmax, Egap, 1_c_int, dE, k, dV, c_null_ptr), 'diag_hd_gen')
+      khm = k
+      Call gpu_check(cudaMemcpy(c_loc(eval), dE, int(khm, c_size_t) * 8, cudaMemcpyDeviceToHost), &
+                     'download eval')
+      Call gpu_check(cudaMemcpy(c_loc(a), dV, int(khm, c_size_t) * khm * 8, cudaMemcpyDeviceToHost), &
+                     'download vectors')
+      Call gpu_check(cudaFree(dH), 'cudaFree'); Call gpu_check(cudaFree(dS), 'cudaFree')
+      Call gpu_check(cudaFree(dE), 'cudaFree'); Call gpu_check(cudaFree(dV), 'cudaFree')
+      End Subroutine gpu_diag_hd_gen
 
 !======================================================================
       Subroutine gpu_lap_dsyev(job, uplo, n, m, A, eval, info)
