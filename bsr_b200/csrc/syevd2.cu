@@ -777,27 +777,49 @@ namespace bsrg {
 int symmetrize_lower(int n, const double *A, long lda, double *F, long ldf, cudaStream_t s);   // refine.cu
 
 // Workspace of dense_syevd in doubles (everything but the output Z)
-size_t syevd2_workspace_doubles(int n)
+// The workspace carve-up of syevd2_impl, as offsets (doubles, 32-aligned); the size
+// function and the solver use this one layout.
+struct Syevd2Layout {
+    size_t Wk, AB, V1, T1, V2, tau2, Tq, dv, ev, progress, VYV, X, T, Mp, part, gram, flags, W1, W2, Vg, Gq, Tg,
+        gemm_ws, dcw, total;
+};
+
+static Syevd2Layout syevd2_layout(int n)
 {
+    Syevd2Layout L{};
     const size_t nn = (size_t)n * n;
     const size_t S = (size_t)sweep_steps(n, 0) + 1, ng = (size_t)(n + NB - 1) / NB + 1;
-    size_t t = 0;
-    t += nn + 64;                                  // working copy of A
-    t += (size_t)LDAB * n + 64;                    // band
-    t += sy2sb_vsave_doubles(n) + 64;              // stage-1 V
-    t += (size_t)(sy2sb_panels(n) + 1) * NB * NB + 64;   // stage-1 T
-    t += (size_t)n * S * NB + 64;                  // stage-2 V
-    t += (size_t)n * S + 64;                       // stage-2 tau
-    t += ng * S * NB * NB + 64;                    // stage-2 block T
-    t += 3 * (size_t)n + 256;                      // d, e, progress (ints fit in doubles)
-    t += (size_t)n * 3 * NB + (size_t)n * NB + 4 * NB * NB + 64;   // VYV, X, T, Mp chunk partials (below)
-    t += ((size_t)n / 128 + 2) * NB * NB + 64;
-    t += (size_t)(n / NB + 8) * 6 * NB + 64;       // panel partials + Gram
-    t += 3 * (size_t)4 * NB * n + 2 * (size_t)16 * NB * NB + 6 * 64;   // Q1: W1, W2, merged V, Gram, T
-    t += 8 * (size_t)4 * NB * n + 64;              // split-K slices (outputs up to 128 x n)
-    t += dc_workspace_bytes(n) / 8 + 64;           // divide and conquer
-    return t + 4096;
+    size_t off = 0;
+    auto take = [&](size_t cnt) { off = (off + 31) & ~(size_t)31; size_t p = off; off += cnt; return p; };
+    L.Wk = take(nn);
+    L.AB = take((size_t)LDAB * n);
+    L.V1 = take(sy2sb_vsave_doubles(n));
+    L.T1 = take((size_t)(sy2sb_panels(n) + 1) * NB * NB);
+    L.V2 = take((size_t)n * S * NB);
+    L.tau2 = take((size_t)n * S);
+    L.Tq = take(ng * S * NB * NB);
+    L.dv = take(n);
+    L.ev = take(n + 1);
+    L.progress = take(n / 2 + 8);
+    L.VYV = take((size_t)n * 3 * NB);
+    L.X = take((size_t)n * NB);
+    L.T = take(NB * NB);
+    L.Mp = take(((size_t)n / 128 + 2) * NB * NB);
+    L.part = take((size_t)(n / NB + 8) * 4 * NB);
+    L.gram = take((size_t)(n / NB + 8) * NB * NB);
+    L.flags = take(8);
+    L.W1 = take((size_t)Q1W * n);
+    L.W2 = take((size_t)Q1W * n);
+    L.Vg = take((size_t)Q1W * n);
+    L.Gq = take((size_t)Q1W * Q1W);
+    L.Tg = take((size_t)Q1W * Q1W);
+    L.gemm_ws = take(8 * (size_t)Q1W * n);
+    L.dcw = take(dc_workspace_bytes(n) / 8 + 8);
+    L.total = off + 64;
+    return L;
 }
+
+size_t syevd2_workspace_doubles(int n) { return syevd2_layout(n).total; }
 
 // Eigenvalues (ascending, w) and eigenvectors (Z, ldz) of the symmetric A (lower
 // triangle referenced).  Z may be A itself.  ws: syevd2_workspace_doubles(n).
@@ -812,31 +834,27 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     cudaError_t e;
     if (ws_doubles < syevd2_workspace_doubles(n)) { set_error("dsyevd: workspace too small"); return BSRG_ERR_NOMEM; }
     if (n > 10240) { set_error("dsyevd: n=%d above 10240", n); return BSRG_ERR_ARG; }
-    const size_t nn = (size_t)n * n;
-    const int S = sweep_steps(n, 0) + 1, ng = (n + NB - 1) / NB + 1;
-    size_t off = 0;
-    auto take = [&](size_t cnt) { off = (off + 31) & ~(size_t)31; double *p = ws + off; off += cnt; return p; };
-    double *Wk = take(nn), *AB = take((size_t)LDAB * n);
-    double *V1 = take(sy2sb_vsave_doubles(n)), *T1 = take((size_t)(sy2sb_panels(n) + 1) * NB * NB);
-    double *V2 = take((size_t)n * S * NB), *tau2 = take((size_t)n * S), *Tq = take((size_t)ng * S * NB * NB);
-    double *dv = take(n), *ev = take(n + 1);
-    int *progress = (int *)take(n / 2 + 8);
+    const int S = sweep_steps(n, 0) + 1;
+    const Syevd2Layout L = syevd2_layout(n);
+    double *Wk = ws + L.Wk, *AB = ws + L.AB, *V1 = ws + L.V1, *T1 = ws + L.T1;
+    double *V2 = ws + L.V2, *tau2 = ws + L.tau2, *Tq = ws + L.Tq;
+    double *dv = ws + L.dv, *ev = ws + L.ev;
+    int *progress = (int *)(ws + L.progress);
     Sy2sbWork sw;
-    sw.VYV = take((size_t)n * 3 * NB);
-    sw.X = take((size_t)n * NB);
-    sw.T = take(NB * NB);
-    sw.Mp = take(((size_t)n / 128 + 2) * NB * NB);
-    sw.part = take((size_t)(n / NB + 8) * 4 * NB);
-    sw.gram = take((size_t)(n / NB + 8) * NB * NB);
-    int *flags = (int *)take(8);                   // bar[2], err, err2
+    sw.VYV = ws + L.VYV;
+    sw.X = ws + L.X;
+    sw.T = ws + L.T;
+    sw.Mp = ws + L.Mp;
+    sw.part = ws + L.part;
+    sw.gram = ws + L.gram;
+    int *flags = (int *)(ws + L.flags);            // bar[2], err, err2
     sw.bar = (unsigned *)flags;
     sw.err = flags + 2;
-    double *W1 = take((size_t)Q1W * n), *W2 = take((size_t)Q1W * n);
-    double *Vg = take((size_t)Q1W * n), *Gq = take((size_t)Q1W * Q1W), *Tg = take((size_t)Q1W * Q1W);
+    double *W1 = ws + L.W1, *W2 = ws + L.W2;
+    double *Vg = ws + L.Vg, *Gq = ws + L.Gq, *Tg = ws + L.Tg;
     sw.gemm_ws_doubles = 8 * (size_t)Q1W * n;
-    sw.gemm_ws = take(sw.gemm_ws_doubles);
-    double *dcw = take(dc_workspace_bytes(n) / 8 + 8);
-    if (off > ws_doubles) { set_error("dsyevd: workspace layout"); return BSRG_ERR_NOMEM; }
+    sw.gemm_ws = ws + L.gemm_ws;
+    double *dcw = ws + L.dcw;
     if ((e = cudaMemsetAsync(flags, 0, 8 * sizeof(int), st)) != cudaSuccess ||
         (e = cudaMemsetAsync(progress, 0, sizeof(int) * n, st)) != cudaSuccess)
         return cuda_fail(e, "dsyevd init");
