@@ -637,6 +637,209 @@ __global__ void __launch_bounds__(Q2W_WARPS * 32, 2) q2w_apply_kernel(int n, int
 }
 
 // ---------------------------------------------------------------------------
+// The same application on the FP64 tensor pipe, with the strip's rows staged in
+// shared memory.  One CTA per strip of 32 columns; its Q2R_W warps take the groups
+// in rounds: round r gives warp w the group g0 - w (g0 = ng-1 - r Q2R_W), and all
+// warps of a round walk down the strip together, warp w one block behind warp w-1
+// (block (g, i) waits until group g+1 has finished its block i, as above).  The
+// rows between the last warp's window and the first warp's live in a ring of
+// Q2R_RING rows: the first warp loads the 32 new rows of each window, the last warp
+// writes back the 32 rows it leaves, and the first warp may not run more than
+// Q2R_RING / NB - 2 Q2R_W blocks ahead of the last (bounded waits).  So every
+// element of Z crosses HBM twice per round instead of twice per block.  A block
+// is three tensor-core products on the window (lane fragments of m8n8k4):
+//   W = V^T Zw (32 x 64 x 32, the band of V only), W2 = T W (T upper), Zw -= V W2.
+// ---------------------------------------------------------------------------
+constexpr int Q2R_W = 4;                    // warps (groups per round)
+constexpr int Q2R_RING = 256;               // ring rows, a power of two >= 2 NB Q2R_W
+constexpr int Q2R_LD = 36;                  // row stride of the ring and of W (4 mod 16 doubles)
+constexpr int Q2R_SMEM = (Q2R_RING + Q2R_W * NB) * Q2R_LD * (int)sizeof(double);
+static_assert(Q2R_RING >= 2 * NB * Q2R_W && (Q2R_RING & (Q2R_RING - 1)) == 0, "ring size");
+
+__device__ __forceinline__ void q2r_mma(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// rows [a, b) of the strip between Z and the ring; 4 rows x 8 columns per 32 threads
+__device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int n, int c0, int ncl, int a, int b,
+                                         bool store, int t0, int nthr)
+{
+    if (b <= a) return;
+    const int nchunk = ((b - a + 3) / 4) * 4;        // chunks of 4 rows x 8 columns
+    for (int q = t0; q < nchunk * 32; q += nthr) {
+        const int ch = q >> 5, l = q & 31;
+        const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
+        if (row >= b) continue;
+        double *rp = ring + (row & (Q2R_RING - 1)) * Q2R_LD + col;
+        const bool ok = row < n && col < ncl;
+        if (store) {
+            if (ok) Z[row + ldz * (long)(c0 + col)] = *rp;
+        } else {
+            *rp = ok ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, int ncol,
+                                                                 const double *__restrict__ V2,
+                                                                 const double *__restrict__ Tq, double *Z,
+                                                                 long ldz, int *err)
+{
+    extern __shared__ __align__(16) double q2r_sm[];
+    __shared__ volatile int prog[Q2R_W];
+    double *ring = q2r_sm;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, lr = lane >> 2, lc = lane & 3;
+    double *Wb = q2r_sm + Q2R_RING * Q2R_LD + wid * NB * Q2R_LD;
+    const int c0 = blockIdx.x * 32, ncl = min(32, ncol - c0);
+    const int ng = (n - 2 + NB - 1) / NB;
+    for (int g0 = ng - 1; g0 >= 0; g0 -= Q2R_W) {
+        const int gl = max(g0 - Q2R_W + 1, 0), nw = g0 - gl + 1;
+        __syncthreads();                              // the previous round's rows are written back
+        q2r_xfer(ring, Z, ldz, n, c0, ncl, gl * NB + 1, g0 * NB + 1 + 2 * NB, false, tid, blockDim.x);
+        if (tid < Q2R_W) prog[tid] = 0;
+        __syncthreads();
+        const int ilast = sweep_steps(n, gl * NB);
+        if (wid < nw) {
+            const int g = g0 - wid;
+            const int imax = sweep_steps(n, g * NB);
+            const int iprev = wid > 0 ? sweep_steps(n, (g + 1) * NB) : 0;
+            for (int i = 0; i < imax; i++) {
+                const unsigned long long t0 = gtime();
+                if (wid > 0) {
+                    const int need = min(i + 1, iprev);
+                    while (prog[wid - 1] < need)
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
+                } else if (nw > 1) {
+                    // the ring slots of the new rows must have been written back by the last warp
+                    const int need = min(i + nw - Q2R_RING / NB + 1, ilast);
+                    while (need > 0 && prog[nw - 1] < need)
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
+                }
+                __threadfence_block();
+                const int top = (g + i) * NB + 1;
+                const int nrow = min(2 * NB - 1, n - top);
+                if (wid == 0 && i > 0) q2r_xfer(ring, Z, ldz, n, c0, ncl, top + NB, top + 2 * NB, false, lane, 32);
+                __syncwarp();
+                const int nv = q2_nvalid(n, g, i);
+                const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;   // reflector q at + q S NB
+                const double *T = Tq + ((long)g * S + i) * NB * NB;
+                // ---- W = V^T Zw: M = q (4 tiles), N = column (4), K = window row (16 steps) ----
+                double acc[4][4][2];
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < 16; ks++) {
+                    const int r = 4 * ks + lc;
+                    double bz[4];
+                    const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD;
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++) bz[nt] = r < nrow ? rrow[8 * nt + lr] : 0.0;
+#pragma unroll
+                    for (int mt = 0; mt < 4; mt++) {
+                        if (ks < 2 * mt || ks >= 2 * mt + 10) continue;
+                        const int q = 8 * mt + lr, t = r - q;
+                        const double a = (t >= 0 && t < NB && q < nv && r < nrow) ? __ldg(Vblk + (long)q * S * NB + t) : 0.0;
+#pragma unroll
+                        for (int nt = 0; nt < 4; nt++) q2r_mma(acc[mt][nt][0], acc[mt][nt][1], a, bz[nt]);
+                    }
+                }
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++) {
+                        Wb[(8 * mt + lr) * Q2R_LD + 8 * nt + 2 * lc] = acc[mt][nt][0];
+                        Wb[(8 * mt + lr) * Q2R_LD + 8 * nt + 2 * lc + 1] = acc[mt][nt][1];
+                        acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+                    }
+                __syncwarp();
+                // ---- W2 = T W: M = q, N = column, K = l (T upper: l >= q) ----
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++) {
+                    const int l = 4 * ks + lc;
+                    double bw[4];
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++) bw[nt] = Wb[l * Q2R_LD + 8 * nt + lr];
+#pragma unroll
+                    for (int mt = 0; mt < 4; mt++) {
+                        if (ks < 2 * mt) continue;
+                        const double a = __ldg(T + (8 * mt + lr) + NB * l);
+#pragma unroll
+                        for (int nt = 0; nt < 4; nt++) q2r_mma(acc[mt][nt][0], acc[mt][nt][1], a, bw[nt]);
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 4; nt++) {
+                        Wb[(8 * mt + lr) * Q2R_LD + 8 * nt + 2 * lc] = acc[mt][nt][0];
+                        Wb[(8 * mt + lr) * Q2R_LD + 8 * nt + 2 * lc + 1] = acc[mt][nt][1];
+                    }
+                __syncwarp();
+                // ---- Zw -= V W2: M = window row (8 tiles, two halves), N = column, K = q ----
+#pragma unroll
+                for (int mh = 0; mh < 2; mh++) {
+#pragma unroll
+                    for (int a = 0; a < 4; a++) {
+                        const int r = 8 * (4 * mh + a) + lr;
+                        const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD;
+#pragma unroll
+                        for (int nt = 0; nt < 4; nt++) {
+                            acc[a][nt][0] = r < nrow ? rrow[8 * nt + 2 * lc] : 0.0;
+                            acc[a][nt][1] = r < nrow ? rrow[8 * nt + 2 * lc + 1] : 0.0;
+                        }
+                    }
+#pragma unroll
+                    for (int ks = 0; ks < 8; ks++) {
+                        const int q = 4 * ks + lc;
+                        double bw[4];
+#pragma unroll
+                        for (int nt = 0; nt < 4; nt++) bw[nt] = Wb[q * Q2R_LD + 8 * nt + lr];
+#pragma unroll
+                        for (int a = 0; a < 4; a++) {
+                            const int mt = 4 * mh + a;
+                            const int klo = 2 * mt - 8 > 0 ? 2 * mt - 8 : 0, khi = 2 * mt + 1 < 7 ? 2 * mt + 1 : 7;
+                            if (ks < klo || ks > khi) continue;
+                            const int r = 8 * mt + lr, t = r - q;
+                            const double v = (t >= 0 && t < NB && q < nv && r < nrow) ? __ldg(Vblk + (long)q * S * NB + t) : 0.0;
+#pragma unroll
+                            for (int nt = 0; nt < 4; nt++) q2r_mma(acc[a][nt][0], acc[a][nt][1], -v, bw[nt]);
+                        }
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; a++) {
+                        const int r = 8 * (4 * mh + a) + lr;
+                        if (r < nrow) {
+                            double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD;
+#pragma unroll
+                            for (int nt = 0; nt < 4; nt++) {
+                                rrow[8 * nt + 2 * lc] = acc[a][nt][0];
+                                rrow[8 * nt + 2 * lc + 1] = acc[a][nt][1];
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                // the last warp leaves the window's first NB rows for good this round
+                if (wid == nw - 1) q2r_xfer(ring, Z, ldz, n, c0, ncl, top, top + NB, true, lane, 32);
+                __threadfence_block();
+                __syncwarp();
+                if (lane == 0) prog[wid] = i + 1;
+            }
+        }
+        __syncthreads();
+        // rows below the last warp's last block
+        const int rdone = ilast > 0 ? (gl + ilast) * NB + 1 : gl * NB + 1;
+        q2r_xfer(ring, Z, ldz, n, c0, ncl, rdone, n, true, tid, blockDim.x);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // back-transformation of the stage-1 panels, Q1_GROUP panels at a time
 // ---------------------------------------------------------------------------
 constexpr int Q1_GROUP = 4;
@@ -927,12 +1130,17 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             return cuda_fail(e, "dsyevd Q2 smem");
         if (getenv("BSRG_Q2_SIMPLE")) {
             q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
-        } else {
+        } else if (getenv("BSRG_Q2_WAVE")) {
             if ((e = cudaFuncSetAttribute(q2w_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2W_SMEM)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2w_apply_kernel<<<(unsigned)((n + 31) / 32), Q2W_WARPS * 32, Q2W_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz,
                                                                                           sw.err);
+        } else {
+            if ((e = cudaFuncSetAttribute(q2r_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2R_SMEM)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd Q2 smem");
+            q2r_apply_kernel<<<(unsigned)((n + 31) / 32), Q2R_W * 32, Q2R_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
         }
         // per block and column: W = V^T Z (2 NB nv), T W (~NB nv), Z -= V W (2 NB nv)
         double nvsum = 0.0;
