@@ -2,8 +2,8 @@
 DSYGST, DSYEV, DTRSM of diag_hd.f90:268-334) on the GPU against the oracle's
 restatement of the same steps (scipy LAPACK dpotrf/dsygst/dsyev/solve_triangular).
 
-The overlap blocks between channels are a seeded banded perturbation of size
-2e-3 added to the assembled S of config 1.  Refined eigenvalues (Rayleigh
+The overlap blocks between channels are seeded multiples (|eps_ij| <= 0.05) of the
+B-spline overlap added to the assembled S of config 1.  Refined eigenvalues (Rayleigh
 quotients of the standard problem L^-1 A L^-T on both sides) are compared per
 eigenvalue; the rounding of forming L^-1 A L^-T differs between the two
 reductions, so the bar is 1e-10 (floor 1e-3) rather than the block-diagonal
@@ -18,15 +18,17 @@ from tests.gpu_helpers import to_np
 pytestmark = pytest.mark.gpu
 
 
-def _perturbed_overlap(scc, ns, ks, eps=2e-3, seed=11):
+def _perturbed_overlap(scc, ns, ks, eps=0.05, seed=11):
+    """Channel-channel overlap blocks eps_ij S (S the B-spline overlap, eps_ij in [-eps, eps]):
+    in the S-orthonormal channel bases they become eps_ij bb_i^T S bb_j, of norm <= eps, so the
+    transformed overlap C = I + ... stays positive definite."""
     rng = np.random.default_rng(seed)
     nb = scc.shape[0]
     nch = int(round((np.sqrt(8 * nb + 1) - 1) / 2))
-    band = lambda M: np.triu(np.tril(M, ks - 1), -(ks - 1))
     out = scc.copy()
     for i in range(nch):
         for j in range(i):
-            out[i * (i + 1) // 2 + j] += eps * band(rng.standard_normal((ns, ns)))
+            out[i * (i + 1) // 2 + j] += rng.uniform(-eps, eps) * scc[0]
     return out
 
 
