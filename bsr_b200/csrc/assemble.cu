@@ -756,7 +756,7 @@ template <int KS> struct XFLayout {
     static constexpr int PX = PY + NORB_MAX * SR;    // p_a(x0-HW+r)      [a][r]
     static constexpr int RS = PX + NORB_MAX * SP;    // R                 [w][e][f]
     static constexpr int RG = RS + XF * NE * SR;     // per-row region    [w][REG]
-    static constexpr int ACC = RG + XF * REG;        // strip sums        [blk][w]
+    static constexpr int ACC = RG + XF * REG;        // strip sums        [w][blk]
     static size_t smem_bytes(int nblk) { return sizeof(double) * ((size_t)ACC + (size_t)nblk * XF); }
 };
 
@@ -774,7 +774,7 @@ exchange_fused_kernel(int ns, int norb, int nblk, int nact, const XKRange *__res
     using Y = XFLayout<KS>;
     constexpr int HW = Y::HW, NE = Y::NE, KT = Y::KT, EP = Y::EP, ME = Y::ME, SR = Y::SR, SP = Y::SP;
     extern __shared__ __align__(16) double xs[];
-    double *PyT = xs + Y::PY, *PxT = xs + Y::PX, *Rs = xs + Y::RS, *acc = xs + Y::ACC;
+    double *PyT = xs + Y::PY, *PxT = xs + Y::PX, *Rs = xs + Y::RS, *acc = xs + Y::ACC;   // acc [row][blk]
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, lr = lane >> 2, lc = lane & 3;
     const int x0 = blockIdx.x * XF, yp = blockIdx.y;
     const int ntb = (norb + 7) / 8;
@@ -872,20 +872,31 @@ exchange_fused_kernel(int ns, int norb, int nblk, int nact, const XKRange *__res
                 for (int j = 0; j < 2; j++)
                     if (mt < ntb && nt < ntb) reg[(mt * 8 + lr) * ZLD + nt * 8 + 2 * lc + j] = az[mt][nt][j];
         __syncthreads();                 // Z of every row in place
-        // ---- acc[blk][row] += sum_t c_t Z[a_t][b_t] for the groups of this multipole ----
+        // ---- acc[row][blk] += sum_t c_t Z_row[a_t][b_t]: a thread per group, all XF rows at once,
+        //      so each coefficient record is read once per CTA ----
         const XKRange K = kr[i];
-        for (int q = tid; q < K.ng * XF; q += 32 * XF) {
-            const int wi = q % XF;
-            const GroupDesc G = gd[K.g0 + q / XF];
-            const double *Z = xs + Y::RG + wi * Y::REG;
-            double s0 = 0.0, s1 = 0.0;
+        const double *Z0 = xs + Y::RG;
+        for (int gi = tid; gi < K.ng; gi += 32 * XF) {
+            const GroupDesc G = gd[K.g0 + gi];
+            double s[XF];
+#pragma unroll
+            for (int wi = 0; wi < XF; wi++) s[wi] = 0.0;
             int t = G.start;
             for (; t + 1 < G.end; t += 2) {
-                s0 = fma(__ldg(cv + t), Z[__ldg(zoff + t)], s0);
-                s1 = fma(__ldg(cv + t + 1), Z[__ldg(zoff + t + 1)], s1);
+                const double c0 = __ldg(cv + t), c1 = __ldg(cv + t + 1);
+                const int z0 = __ldg(zoff + t), z1 = __ldg(zoff + t + 1);
+#pragma unroll
+                for (int wi = 0; wi < XF; wi++)
+                    s[wi] = fma(c1, Z0[wi * Y::REG + z1], fma(c0, Z0[wi * Y::REG + z0], s[wi]));
             }
-            if (t < G.end) s0 = fma(__ldg(cv + t), Z[__ldg(zoff + t)], s0);
-            acc[G.blk * XF + wi] += s0 + s1;
+            if (t < G.end) {
+                const double c0 = __ldg(cv + t);
+                const int z0 = __ldg(zoff + t);
+#pragma unroll
+                for (int wi = 0; wi < XF; wi++) s[wi] = fma(c0, Z0[wi * Y::REG + z0], s[wi]);
+            }
+#pragma unroll
+            for (int wi = 0; wi < XF; wi++) acc[wi * nblk + G.blk] += s[wi];
         }
     }
     __syncthreads();
@@ -895,7 +906,8 @@ exchange_fused_kernel(int ns, int norb, int nblk, int nact, const XKRange *__res
         const int blk = q / XF, wi = q % XF, x = x0 + wi;
         if (x >= ns) continue;
         double *dst = hcc + (size_t)blk * nn + x + (size_t)ns * yp;
-        *dst = accumulate ? *dst + acc[q] : acc[q];
+        const double a = acc[wi * nblk + blk];
+        *dst = accumulate ? *dst + a : a;
     }
 }
 
