@@ -23,6 +23,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ctx.h"
 #include "dgemm.h"
 
@@ -201,6 +203,128 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_kernel(PanelArgs a)
         a.T[q] = Tt[q % NB][q / NB];
         a.Ts[q] = Tt[q % NB][q / NB];
     }
+}
+
+// The same factorisation on one thread-block cluster (up to 16 CTAs, PQC_ROWS rows each):
+// the per-column partial dot products stay in each CTA's shared memory and are read
+// by every CTA through distributed shared memory after a hardware cluster barrier,
+// instead of a grid barrier over global memory.
+constexpr int PQC_ROWS = 640;
+constexpr int PQC_MAXG = 16;
+
+__global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) double ps[];       // rpc x (NB + 1) | partials [2][2 NB] | Gram NB x NB
+    __shared__ double tot[NB], piv[NB], wv[NB], tau_s[NB];
+    __shared__ double sc_tau, sc_scale, sc_beta;
+    const int cta = (int)cl.block_rank(), G = (int)cl.num_blocks(), tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int m = a.m, r0 = cta * a.rpc, nr = max(0, min(a.rpc, m - r0));
+    constexpr int LD = NB + 1;
+    double *part = ps + (size_t)a.rpc * LD;
+    double *gram = part + 4 * NB;
+    for (int q = tid; q < nr * NB; q += PQ_NT) {
+        const int r = q % nr, c = q / nr;
+        ps[r * LD + c] = a.P[(r0 + r) + a.ldp * (long)c];
+    }
+    const int kb = min(m, NB);
+    __syncthreads();
+    for (int c = 0; c < kb; c++) {
+        double *buf = part + (c & 1) * 2 * NB;
+        for (int k = c + warp; k < NB; k += PQ_NT / 32) {
+            double s = 0.0;
+            for (int r = lane; r < nr; r += 32)
+                if (r0 + r > c) s += ps[r * LD + c] * ps[r * LD + k];
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) buf[k] = s;
+        }
+        if (cta == 0)
+            for (int k = c + tid; k < NB; k += PQ_NT) buf[NB + k] = ps[c * LD + k];
+        cl.sync();
+        for (int k = c + tid; k < NB; k += PQ_NT) {
+            double s = 0.0;
+            for (int q = 0; q < G; q++) s += cl.map_shared_rank(buf, q)[k];
+            tot[k] = s;
+            piv[k] = cl.map_shared_rank(buf, 0)[NB + k];
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const double alpha = piv[c], sigma = tot[c];
+            if (sigma == 0.0) { sc_tau = 0.0; sc_scale = 0.0; sc_beta = alpha; }
+            else {
+                const double beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+                sc_tau = (beta - alpha) / beta;
+                sc_scale = 1.0 / (alpha - beta);
+                sc_beta = beta;
+            }
+            tau_s[c] = sc_tau;
+        }
+        __syncthreads();
+        const double tau = sc_tau, scale = sc_scale;
+        for (int k = c + 1 + tid; k < NB; k += PQ_NT) wv[k] = piv[k] + scale * tot[k];
+        __syncthreads();
+        for (int q = tid; q < nr * (NB - c - 1); q += PQ_NT) {
+            const int r = q % nr, k = c + 1 + q / nr;
+            if (r0 + r > c) ps[r * LD + k] -= tau * scale * ps[r * LD + c] * wv[k];
+        }
+        if (cta == 0)
+            for (int k = c + 1 + tid; k < NB; k += PQ_NT) ps[c * LD + k] -= tau * wv[k];
+        __syncthreads();
+        for (int r = tid; r < nr; r += PQ_NT)
+            if (r0 + r > c) ps[r * LD + c] *= scale;
+        if (cta == 0 && tid == 0) ps[c * LD + c] = sc_beta;
+        __syncthreads();
+    }
+    for (int q = tid; q < NB * NB; q += PQ_NT) {
+        const int i = q % NB, j = q / NB;
+        double s = 0.0;
+        if (i <= j && j < kb)
+            for (int r = 0; r < nr; r++) {
+                const int gr = r0 + r;
+                const double vi = gr > i ? ps[r * LD + i] : (gr == i ? 1.0 : 0.0);
+                const double vj = gr > j ? ps[r * LD + j] : (gr == j ? 1.0 : 0.0);
+                s += vi * vj;
+            }
+        gram[q] = s;
+    }
+    for (int q = tid; q < nr * NB; q += PQ_NT) {
+        const int r = q % nr, c = q / nr, gr = r0 + r;
+        const double v = c < kb ? (gr > c ? ps[r * LD + c] : (gr == c ? 1.0 : 0.0)) : 0.0;
+        a.V[gr + (long)m * c] = v;
+        a.V[gr + (long)m * (2 * NB + c)] = v;
+        a.Vs[gr + (long)m * c] = v;
+        a.P[gr + a.ldp * (long)c] = gr <= c ? ps[r * LD + c] : 0.0;
+    }
+    cl.sync();                                          // every CTA's Gram partial is complete
+    if (cta == 0) {
+        __shared__ double Gs[NB * NB];
+        __shared__ double Tt[NB][NB + 1];
+        for (int q = tid; q < NB * NB; q += PQ_NT) {
+            double s = 0.0;
+            for (int g = 0; g < G; g++) s += cl.map_shared_rank(gram, g)[q];
+            Gs[q] = s;
+            Tt[q % NB][q / NB] = 0.0;
+        }
+        __syncthreads();
+        for (int c = 0; c < kb; c++) {
+            if (tid < c) {
+                double s = 0.0;
+                for (int l = tid; l < c; l++) s += Tt[tid][l] * Gs[l + NB * c];
+                wv[tid] = s;
+            }
+            __syncthreads();
+            if (tid < c) Tt[tid][c] = -tau_s[c] * wv[tid];
+            if (tid == 0) Tt[c][c] = tau_s[c];
+            __syncthreads();
+        }
+        for (int q = tid; q < NB * NB; q += PQ_NT) {
+            a.T[q] = Tt[q % NB][q / NB];
+            a.Ts[q] = Tt[q % NB][q / NB];
+        }
+    }
+    cl.sync();                                          // CTA 0 has read every Gram partial
 }
 
 // Y = X T (rows), partial M = V^T Y per chunk of 128 rows.  X, V, Y: ld m.
@@ -404,6 +528,137 @@ __global__ void __launch_bounds__(32) sb2st_kernel(Sb2stArgs a)
                 for (int q = 0; q < nb2; q++)
                     if (t < L) *at(r1 + q, r0 + t) = Bs[q][t];
             }
+            __threadfence();
+            __syncwarp();
+            if (t == 0) *(volatile int *)(a.progress + j) = i + 1;
+        }
+    }
+}
+
+// The same tasks with every block held row-wise in registers (lane = row, so the
+// band is read and written coalesced), the reductions across rows through shared
+// memory, and the x column and left block of step i > 0 taken from step i-1's
+// updated lower block (the same rows and columns; no other sweep writes them in
+// between: sweep j-1 is at least three steps ahead, sweep j+1 behind).
+__global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
+{
+    __shared__ double Ts[NB][NB + 1];          // transpose of the diagonal block
+    __shared__ double Cs[NB][NB + 1];          // the previous step's lower block (row-major): x and left block
+    __shared__ double vs[NB], ws2[NB];
+    const int t = threadIdx.x, n = a.n;
+    double *AB = a.AB;
+    auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
+    for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
+        const int nst = sweep_steps(n, j);
+        const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
+        for (int i = 0; i < nst; i++) {
+            if (j > 0) {
+                const int need = min(i + 3, nprev);
+                if (t == 0) {
+                    volatile int *pg = a.progress + (j - 1);
+                    const unsigned long long t0 = gtime();
+                    while (*pg < need) {
+                        if (*(volatile int *)a.err) break;
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                    }
+                    __threadfence();
+                }
+                __syncwarp();
+                if (*(volatile int *)a.err) return;
+            }
+            const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+            const int col = i == 0 ? j : r0 - NB;
+            const int nl = r0 - col - 1;
+            const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+            // ---- loads, lane = row (all issued before use) ----
+            double Dr[NB], Br[NB];
+            const double xl = i == 0 ? (t < L ? __ldcg(at(r0 + t, col)) : 0.0) : Cs[t][0];
+#pragma unroll
+            for (int c = 0; c < NB; c++) Dr[c] = (t < L && c <= t) ? __ldcg(at(r0 + t, r0 + c)) : 0.0;
+#pragma unroll
+            for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
+            // ---- the reflector ----
+            double sig = (t >= 1 && t < L) ? xl * xl : 0.0;
+            for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+            const double alpha = __shfl_sync(0xffffffffu, xl, 0);
+            double tau = 0.0, scale = 0.0, beta = alpha;
+            if (sig != 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+                tau = (beta - alpha) / beta;
+                scale = 1.0 / (alpha - beta);
+            }
+            const double v = t == 0 ? 1.0 : (t < L ? xl * scale : 0.0);
+            vs[t] = v;
+            a.V2[((long)j * a.S + i) * NB + t] = v;
+            if (t == 0) a.tau2[(long)j * a.S + i] = tau;
+            if (t < L) *at(r0 + t, col) = t == 0 ? beta : 0.0;
+            __syncwarp();
+            if (tau != 0.0) {
+                // left: columns col+1 .. r0-1 = columns 1.. of the carried block; w_c across rows
+                if (nl > 0) {
+                    if (t < nl) {
+                        double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+                        for (int q = 0; q < NB; q += 2) {
+                            w0 = fma(vs[q], Cs[q][t + 1], w0);
+                            w1 = fma(vs[q + 1], Cs[q + 1][t + 1], w1);
+                        }
+                        ws2[t] = tau * (w0 + w1);
+                    }
+                    __syncwarp();
+                    if (t < L) {
+#pragma unroll
+                        for (int c = 0; c < NB - 1; c++)
+                            if (c < nl) *at(r0 + t, col + 1 + c) = fma(-v, ws2[c], Cs[t][c + 1]);
+                    }
+                    __syncwarp();
+                }
+                // two-sided on the diagonal block: p = tau D v, w = p - tau/2 (v^T p) v
+#pragma unroll
+                for (int c = 0; c < NB; c++) Ts[t][c] = Dr[c];
+                __syncwarp();
+                double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NB; c += 2) {
+                    const double d0 = c <= t ? Dr[c] : Ts[c][t];           // D(t, c) from the lower triangle
+                    const double d1 = c + 1 <= t ? Dr[c + 1] : Ts[c + 1][t];
+                    p0 = fma(d0, vs[c], p0);
+                    p1 = fma(d1, vs[c + 1], p1);
+                }
+                const double p = t < L ? tau * (p0 + p1) : 0.0;
+                double vp = v * p;
+                for (int o = 16; o > 0; o >>= 1) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+                const double w = p - 0.5 * tau * vp * v;
+                ws2[t] = w;
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < NB; c++)
+                    if (c <= t) Dr[c] -= v * ws2[c] + w * vs[c];
+                // right: rows below the window, s_q = sum_c B(q, c) v_c
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NB; c += 2) {
+                    s0 = fma(Br[c], vs[c], s0);
+                    s1 = fma(Br[c + 1], vs[c + 1], s1);
+                }
+                const double sr = tau * (s0 + s1);
+#pragma unroll
+                for (int c = 0; c < NB; c++) Br[c] = fma(-sr, vs[c], Br[c]);
+                // ---- stores, lane = row ----
+                if (t < L) {
+#pragma unroll
+                    for (int c = 0; c < NB; c++)
+                        if (c <= t) *at(r0 + t, r0 + c) = Dr[c];
+                }
+                if (t < nb2) {
+#pragma unroll
+                    for (int c = 0; c < NB; c++)
+                        if (c < L) *at(r1 + t, r0 + c) = Br[c];
+                }
+            }
+            // the next window's x column and left block are this step's lower block
+#pragma unroll
+            for (int c = 0; c < NB; c++) Cs[t][c] = Br[c];
             __threadfence();
             __syncwarp();
             if (t == 0) *(volatile int *)(a.progress + j) = i + 1;
@@ -652,8 +907,10 @@ __global__ void __launch_bounds__(Q2W_WARPS * 32, 2) q2w_apply_kernel(int n, int
 // ---------------------------------------------------------------------------
 constexpr int Q2R_W = 4;                    // warps (groups per round)
 constexpr int Q2R_RING = 256;               // ring rows, a power of two >= 2 NB Q2R_W
-constexpr int Q2R_LD = 36;                  // row stride of the ring and of W (4 mod 16 doubles)
-constexpr int Q2R_SMEM = (Q2R_RING + Q2R_W * NB) * Q2R_LD * (int)sizeof(double);
+constexpr int Q2R_LD = 36;                  // row stride of the ring, of W and of T (4 mod 16 doubles)
+constexpr int Q2R_LDV = 37;                 // row stride of a block's V (reflector q: V(q, t) at q LDV + t)
+constexpr int Q2R_WARP = NB * (2 * Q2R_LD + Q2R_LDV);   // doubles per warp: W, T, V
+constexpr int Q2R_SMEM = (Q2R_RING * Q2R_LD + Q2R_W * Q2R_WARP) * (int)sizeof(double);
 static_assert(Q2R_RING >= 2 * NB * Q2R_W && (Q2R_RING & (Q2R_RING - 1)) == 0, "ring size");
 
 __device__ __forceinline__ void q2r_mma(double &d0, double &d1, double a, double b)
@@ -683,7 +940,7 @@ __device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int 
     }
 }
 
-__global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, int ncol,
+__global__ void __launch_bounds__(Q2R_W * 32, 1) q2r_apply_kernel(int n, int S, int ncol,
                                                                  const double *__restrict__ V2,
                                                                  const double *__restrict__ Tq, double *Z,
                                                                  long ldz, int *err)
@@ -692,7 +949,9 @@ __global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, 
     __shared__ volatile int prog[Q2R_W];
     double *ring = q2r_sm;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, lr = lane >> 2, lc = lane & 3;
-    double *Wb = q2r_sm + Q2R_RING * Q2R_LD + wid * NB * Q2R_LD;
+    double *Wb = q2r_sm + Q2R_RING * Q2R_LD + wid * Q2R_WARP;       // W, then W2
+    double *Tsm = Wb + NB * Q2R_LD;                                  // T(q, l) at q + LD l
+    double *Vsm = Tsm + NB * Q2R_LD;                                 // V(q, t) at q LDV + t
     const int c0 = blockIdx.x * 32, ncl = min(32, ncol - c0);
     const int ng = (n - 2 + NB - 1) / NB;
     for (int g0 = ng - 1; g0 >= 0; g0 -= Q2R_W) {
@@ -724,8 +983,21 @@ __global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, 
                 if (wid == 0 && i > 0) q2r_xfer(ring, Z, ldz, n, c0, ncl, top + NB, top + 2 * NB, false, lane, 32);
                 __syncwarp();
                 const int nv = q2_nvalid(n, g, i);
-                const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;   // reflector q at + q S NB
-                const double *T = Tq + ((long)g * S + i) * NB * NB;
+                {
+                    // the block's reflectors and T into shared memory: 64 coalesced loads per lane in flight
+                    const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;   // reflector q at + q S NB
+                    const double *T = Tq + ((long)g * S + i) * NB * NB;
+                    double vr[NB], tr[NB];
+#pragma unroll
+                    for (int q = 0; q < NB; q++) vr[q] = q < nv ? __ldg(Vblk + (long)q * S * NB + lane) : 0.0;
+#pragma unroll
+                    for (int l = 0; l < NB; l++) tr[l] = __ldg(T + lane + NB * l);
+#pragma unroll
+                    for (int q = 0; q < NB; q++) Vsm[q * Q2R_LDV + lane] = vr[q];
+#pragma unroll
+                    for (int l = 0; l < NB; l++) Tsm[lane + Q2R_LD * l] = tr[l];
+                }
+                __syncwarp();
                 // ---- W = V^T Zw: M = q (4 tiles), N = column (4), K = window row (16 steps) ----
                 double acc[4][4][2];
 #pragma unroll
@@ -743,7 +1015,7 @@ __global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, 
                     for (int mt = 0; mt < 4; mt++) {
                         if (ks < 2 * mt || ks >= 2 * mt + 10) continue;
                         const int q = 8 * mt + lr, t = r - q;
-                        const double a = (t >= 0 && t < NB && q < nv && r < nrow) ? __ldg(Vblk + (long)q * S * NB + t) : 0.0;
+                        const double a = (t >= 0 && t < NB && q < nv && r < nrow) ? Vsm[q * Q2R_LDV + t] : 0.0;
 #pragma unroll
                         for (int nt = 0; nt < 4; nt++) q2r_mma(acc[mt][nt][0], acc[mt][nt][1], a, bz[nt]);
                     }
@@ -767,7 +1039,7 @@ __global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, 
 #pragma unroll
                     for (int mt = 0; mt < 4; mt++) {
                         if (ks < 2 * mt) continue;
-                        const double a = __ldg(T + (8 * mt + lr) + NB * l);
+                        const double a = Tsm[(8 * mt + lr) + Q2R_LD * l];
 #pragma unroll
                         for (int nt = 0; nt < 4; nt++) q2r_mma(acc[mt][nt][0], acc[mt][nt][1], a, bw[nt]);
                     }
@@ -806,7 +1078,7 @@ __global__ void __launch_bounds__(Q2R_W * 32, 2) q2r_apply_kernel(int n, int S, 
                             const int klo = 2 * mt - 8 > 0 ? 2 * mt - 8 : 0, khi = 2 * mt + 1 < 7 ? 2 * mt + 1 : 7;
                             if (ks < klo || ks > khi) continue;
                             const int r = 8 * mt + lr, t = r - q;
-                            const double v = (t >= 0 && t < NB && q < nv && r < nrow) ? __ldg(Vblk + (long)q * S * NB + t) : 0.0;
+                            const double v = (t >= 0 && t < NB && q < nv && r < nrow) ? Vsm[q * Q2R_LDV + t] : 0.0;
 #pragma unroll
                             for (int nt = 0; nt < 4; nt++) q2r_mma(acc[a][nt][0], acc[a][nt][1], -v, bw[nt]);
                         }
@@ -924,6 +1196,35 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
     if ((e = cudaFuncSetAttribute(panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(ypass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, YP1_SMEM)) != cudaSuccess)
         return cuda_fail(e, "sy2sb smem");
+    // the cluster form of the panel factorisation when a 16-CTA cluster with its shared memory fits
+    // (BSRG_PANEL_GRID selects the grid-barrier form)
+    bool use_cluster = !getenv("BSRG_PANEL_GRID");
+    if (use_cluster) {
+        const int smem_c = (PQC_ROWS * (NB + 1) + 4 * NB + NB * NB) * (int)sizeof(double);
+        if (cudaFuncSetAttribute(panel_qr_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(panel_qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_c) !=
+                cudaSuccess) {
+            use_cluster = false;
+        } else {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(PQC_MAXG);
+            cfg.blockDim = dim3(PQ_NT);
+            cfg.dynamicSmemBytes = (size_t)smem_c;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = PQC_MAXG;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, panel_qr_cluster_kernel, &cfg) != cudaSuccess ||
+                nclusters < 1)
+                use_cluster = false;
+        }
+        cudaGetLastError();
+    }
     size_t voff = 0;
     int p = 0;
     for (int j = 0; j + NB < n; j += NB, p++) {
@@ -945,9 +1246,31 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         a.gram = w.gram;
         a.bar = w.bar;
         a.err = w.err;
-        void *args[] = {&a};
-        if ((e = cudaLaunchCooperativeKernel((const void *)panel_qr_kernel, G, PQ_NT, args, smem, st)) != cudaSuccess)
-            return cuda_fail(e, "sy2sb panel");
+        const int Gc = std::max(1, (m + PQC_ROWS - 1) / PQC_ROWS);
+        if (use_cluster && Gc <= PQC_MAXG) {
+            // one cluster of Gc CTAs (m / Gc rows each)
+            a.rpc = (m + Gc - 1) / Gc;
+            const int smem_c = (a.rpc * (NB + 1) + 4 * NB + NB * NB) * (int)sizeof(double);
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3((unsigned)Gc);
+            cfg.blockDim = dim3(PQ_NT);
+            cfg.dynamicSmemBytes = (size_t)smem_c;
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)Gc;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            if ((e = cudaLaunchKernelEx(&cfg, panel_qr_cluster_kernel, a)) != cudaSuccess)
+                return cuda_fail(e, "sy2sb panel (cluster)");
+        } else {
+            void *args[] = {&a};
+            if ((e = cudaLaunchCooperativeKernel((const void *)panel_qr_kernel, G, PQ_NT, args, smem, st)) !=
+                cudaSuccess)
+                return cuda_fail(e, "sy2sb panel");
+        }
         voff += (size_t)m * NB;
         // trailing update of A22 = A(j+NB:, j+NB:) (m x m, full symmetric storage)
         double *A22 = A + (j + NB) + lda * (long)(j + NB);
@@ -1082,12 +1405,14 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     if (n > 2) {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+        // the register form (sb2st2_kernel) by default; BSRG_SB2ST_SHARED keeps the shared-memory form
+        const void *kfn = getenv("BSRG_SB2ST_SHARED") ? (const void *)sb2st_kernel : (const void *)sb2st2_kernel;
         int per = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st_kernel, 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, 32, 0);
         const int workers = std::max(1, std::min(n - 2, std::min(nsm * std::max(per, 1), 2 * nsm)));
         Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
         void *args[] = {&a2};
-        if ((e = cudaLaunchCooperativeKernel((const void *)sb2st_kernel, workers, 32, args, 0, st)) != cudaSuccess)
+        if ((e = cudaLaunchCooperativeKernel(kfn, workers, 32, args, 0, st)) != cudaSuccess)
             return cuda_fail(e, "dsyevd bulge chasing");
     }
     tridiag_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, AB, dv, ev);

@@ -398,19 +398,55 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(const DcMerge *__restri
         o = j; lo = 0.0; hi = rho * znrm;
     }
     const double dov = sd[o];
-    // bracketed Newton on tau (every iterate inside [lo, hi], bisection when Newton leaves it)
+    // Iterate on tau with the two-pole model of the secular function (the "middle way" of
+    // R.-C. Li, 1993, as LAPACK dlaed4 uses it): psi (poles up to j) and phi (poles above j)
+    // are each replaced by a constant plus their nearest pole, matched in value and slope;
+    // the model's root in the bracket is the next iterate (the last root: one pole).  Every
+    // iterate stays inside [lo, hi]; a step that would leave it bisects instead.
     double t = 0.5 * (lo + hi);
-    for (int it = 0; it < 200; it++) {
-        double f = 1.0, fp = 0.0;
-        for (int i = 0; i < K; i++) {
-            const double del = (sd[i] - dov) - t;
-            const double q = sz[i] / del;
-            f += rho * q;
-            fp += rho * q / del;
+    const double dj = sd[j] - dov, dj1 = j < K - 1 ? sd[j + 1] - dov : 0.0;
+    for (int it = 0; it < 100; it++) {
+        double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0, eabs = 0.0;
+        for (int i = 0; i <= j; i++) {
+            const double r = 1.0 / ((sd[i] - dov) - t);
+            const double q = sz[i] * r;
+            psi += q;
+            dpsi += q * r;
         }
+        for (int i = j + 1; i < K; i++) {
+            const double r = 1.0 / ((sd[i] - dov) - t);
+            const double q = sz[i] * r;
+            phi += q;
+            dphi += q * r;
+        }
+        eabs = 1.0 + rho * (fabs(psi) + fabs(phi));
+        const double f = 1.0 + rho * (psi + phi);
         if (f < 0.0) lo = t; else hi = t;
-        if (f == 0.0) break;
-        double tn = t - f / fp;
+        if (f == 0.0 || fabs(f) <= 8.0 * 2.220446049250313e-16 * K * eabs) break;
+        const double Dj = dj - t;                      // distances to the two nearest poles
+        double eta;
+        if (j < K - 1) {
+            const double Dj1 = dj1 - t;
+            const double sj = rho * dpsi * Dj * Dj, sj1 = rho * dphi * Dj1 * Dj1;
+            const double c = f - sj / Dj - sj1 / Dj1;
+            // c eta^2 - (c (Dj + Dj1) + sj + sj1) eta + (c Dj Dj1 + sj Dj1 + sj1 Dj) = 0
+            const double qa = c, qb = c * (Dj + Dj1) + sj + sj1, qc = c * Dj * Dj1 + sj * Dj1 + sj1 * Dj;
+            // the model's root between the two poles, eta in (Dj, Dj1); both roots formed stably
+            eta = 0.5 * (lo + hi) - t;
+            if (qa == 0.0) {
+                if (qb != 0.0) eta = qc / qb;
+            } else {
+                const double disc = sqrt(fmax(qb * qb - 4.0 * qa * qc, 0.0));
+                const double w1 = 0.5 * (qb + copysign(disc, qb));
+                const double e1 = w1 / qa, e2 = w1 != 0.0 ? qc / w1 : e1;
+                if (e1 > Dj && e1 < Dj1) eta = e1;
+                else if (e2 > Dj && e2 < Dj1) eta = e2;
+            }
+        } else {
+            const double sj = rho * dpsi * Dj * Dj, c = f - sj / Dj;
+            eta = c != 0.0 ? Dj + sj / c : 0.5 * (hi - t);
+        }
+        double tn = t + eta;
         if (!(tn > lo && tn < hi)) tn = 0.5 * (lo + hi);
         const double step = fabs(tn - t);
         t = tn;

@@ -71,7 +71,9 @@ def test_generalized_config1(refine):
             A[ip[i]:ip[i + 1], ip[j]:ip[j + 1]] = ref["bb"][i].T @ hcc[i * (i + 1) // 2 + j] @ ref["bb"][j]
     A = np.tril(A) + np.tril(A, -1).T
     C = ref["c"]
-    assert np.max(np.abs(Xs.T @ C @ Xs - np.eye(khm))) < 1e-10
+    # C here is the oracle's, built in the oracle's channel bases; the GPU's channel eigenvectors
+    # differ from them by ~eps ||C_ch|| / gap (1e-10 measured), which bounds this check
+    assert np.max(np.abs(Xs.T @ C @ Xs - np.eye(khm))) < 1e-8
     assert np.max(np.abs(A @ Xs - C @ Xs * ev[None, :])) < 1e-11 * np.max(np.abs(A))
 
 
