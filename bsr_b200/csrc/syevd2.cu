@@ -225,10 +225,8 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
     constexpr int LD = NB + 1;
     double *part = ps + (size_t)a.rpc * LD;
     double *gram = part + 4 * NB;
-    for (int q = tid; q < nr * NB; q += PQ_NT) {
-        const int r = q % nr, c = q / nr;
-        ps[r * LD + c] = a.P[(r0 + r) + a.ldp * (long)c];
-    }
+    for (int c = warp; c < NB; c += PQ_NT / 32)
+        for (int r = lane; r < nr; r += 32) ps[r * LD + c] = a.P[(r0 + r) + a.ldp * (long)c];
     const int kb = min(m, NB);
     __syncthreads();
     for (int c = 0; c < kb; c++) {
@@ -265,9 +263,13 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
         const double tau = sc_tau, scale = sc_scale;
         for (int k = c + 1 + tid; k < NB; k += PQ_NT) wv[k] = piv[k] + scale * tot[k];
         __syncthreads();
-        for (int q = tid; q < nr * (NB - c - 1); q += PQ_NT) {
-            const int r = q % nr, k = c + 1 + q / nr;
-            if (r0 + r > c) ps[r * LD + k] -= tau * scale * ps[r * LD + c] * wv[k];
+        // a thread per row (stride 33 doubles: conflict-free), columns k > c in registers' reach
+        const double ts_ = tau * scale;
+        for (int r = tid; r < nr; r += PQ_NT) {
+            if (r0 + r <= c) continue;
+            double *row = ps + r * LD;
+            const double f = ts_ * row[c];
+            for (int k = c + 1; k < NB; k++) row[k] -= f * wv[k];
         }
         if (cta == 0)
             for (int k = c + 1 + tid; k < NB; k += PQ_NT) ps[c * LD + k] -= tau * wv[k];
@@ -277,25 +279,32 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
         if (cta == 0 && tid == 0) ps[c * LD + c] = sc_beta;
         __syncthreads();
     }
-    for (int q = tid; q < NB * NB; q += PQ_NT) {
+    // V in place (unit diagonal, zeros above; columns beyond kb zero), the R part kept aside
+    for (int c = warp; c < NB; c += PQ_NT / 32)
+        for (int r = lane; r < nr; r += 32) {
+            const int gr = r0 + r;
+            const double x = ps[r * LD + c];
+            const double v = c < kb ? (gr > c ? x : (gr == c ? 1.0 : 0.0)) : 0.0;
+            a.V[gr + (long)m * c] = v;
+            a.V[gr + (long)m * (2 * NB + c)] = v;
+            a.Vs[gr + (long)m * c] = v;
+            a.P[gr + a.ldp * (long)c] = gr <= c ? x : 0.0;
+        }
+    __syncthreads();
+    for (int c = warp; c < NB; c += PQ_NT / 32)
+        for (int r = lane; r < nr; r += 32) {
+            const int gr = r0 + r;
+            ps[r * LD + c] = c < kb ? (gr > c ? ps[r * LD + c] : (gr == c ? 1.0 : 0.0)) : 0.0;
+        }
+    __syncthreads();
+    // Gram partial of V over my rows: warp per (i, j) pairs, lanes over rows
+    for (int q = warp; q < NB * NB; q += PQ_NT / 32) {
         const int i = q % NB, j = q / NB;
-        double s = 0.0;
-        if (i <= j && j < kb)
-            for (int r = 0; r < nr; r++) {
-                const int gr = r0 + r;
-                const double vi = gr > i ? ps[r * LD + i] : (gr == i ? 1.0 : 0.0);
-                const double vj = gr > j ? ps[r * LD + j] : (gr == j ? 1.0 : 0.0);
-                s += vi * vj;
-            }
-        gram[q] = s;
-    }
-    for (int q = tid; q < nr * NB; q += PQ_NT) {
-        const int r = q % nr, c = q / nr, gr = r0 + r;
-        const double v = c < kb ? (gr > c ? ps[r * LD + c] : (gr == c ? 1.0 : 0.0)) : 0.0;
-        a.V[gr + (long)m * c] = v;
-        a.V[gr + (long)m * (2 * NB + c)] = v;
-        a.Vs[gr + (long)m * c] = v;
-        a.P[gr + a.ldp * (long)c] = gr <= c ? ps[r * LD + c] : 0.0;
+        double sacc = 0.0;
+        if (i <= j)
+            for (int r = lane; r < nr; r += 32) sacc += ps[r * LD + i] * ps[r * LD + j];
+        for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+        if (lane == 0) gram[q] = sacc;
     }
     cl.sync();                                          // every CTA's Gram partial is complete
     if (cta == 0) {
@@ -1162,6 +1171,52 @@ __global__ void __launch_bounds__(Q1W) q1_tfactor_kernel(const double *__restric
     for (int c = 0; c < Q1W; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
 }
 
+// The same T from the panels' own T factors (T1) and the Gram blocks, merging pairs as
+// Q_a Q_b = I - [V_a V_b] [[T_a, -T_a G_ab T_b], [0, T_b]] [V_a V_b]^T (the block form of the
+// recurrence above): two 32 x 32 merges, then one of the 64-column halves; small products in
+// shared memory instead of 128 dependent column steps.
+constexpr int Q1M_SMEM = (Q1W * (Q1W + 1) + 64 * 65) * (int)sizeof(double);
+
+__global__ void __launch_bounds__(Q1W) q1_tmerge_kernel(const double *__restrict__ G, Q1Panels P,
+                                                        const double *__restrict__ T1, int p0, double *Tg)
+{
+    extern __shared__ __align__(16) double q1m_sm[];
+    double (*Ts)[Q1W + 1] = (double (*)[Q1W + 1])q1m_sm;               // Ts[r][c]
+    double (*W)[65] = (double (*)[65])(q1m_sm + Q1W * (Q1W + 1));
+    const int t = threadIdx.x;
+    for (int c = 0; c < Q1W; c++) Ts[t][c] = 0.0;
+    __syncthreads();
+    for (int q = 0; q < Q1_GROUP; q++) {
+        if (!P.V[q]) continue;
+        const double *Tp = T1 + (size_t)(p0 + q) * NB * NB;             // column-major NB x NB
+        for (int e = t; e < NB * NB; e += Q1W) Ts[q * NB + e % NB][q * NB + e / NB] = Tp[e];
+    }
+    __syncthreads();
+    // merges: width w = NB (pairs 0|1, 2|3), then 2 NB (halves)
+    for (int w = NB; w < Q1W; w *= 2) {
+        for (int a0 = 0; a0 < Q1W; a0 += 2 * w) {
+            const int b0 = a0 + w;
+            // W = G(a rows, b cols) T_b
+            for (int e = t; e < w * w; e += Q1W) {
+                const int r = e % w, c = e / w;
+                double sacc = 0.0;
+                for (int k = 0; k <= c; k++) sacc += __ldg(G + (a0 + r) + (long)Q1W * (b0 + k)) * Ts[b0 + k][b0 + c];
+                W[r][c] = sacc;
+            }
+            __syncthreads();
+            // T(a rows, b cols) = -T_a W
+            for (int e = t; e < w * w; e += Q1W) {
+                const int r = e % w, c = e / w;
+                double sacc = 0.0;
+                for (int k = r; k < w; k++) sacc += Ts[a0 + r][a0 + k] * W[k][c];
+                Ts[a0 + r][b0 + c] = -sacc;
+            }
+            __syncthreads();
+        }
+    }
+    for (int c = 0; c < Q1W; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
+}
+
 }  // namespace
 
 // ---- stage 1 driver ----
@@ -1492,11 +1547,18 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             rc = dgemm(true, false, Q1W, Q1W, m0, 1.0, Vg, m0, Vg, m0, 0.0, Gq, Q1W, st, sw.gemm_ws,
                        sw.gemm_ws_doubles);
             if (rc != BSRG_OK) return rc;
-            constexpr int q1t_smem = Q1W * (Q1W + 1) * (int)sizeof(double);
-            if ((e = cudaFuncSetAttribute(q1_tfactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, q1t_smem)) !=
-                cudaSuccess)
-                return cuda_fail(e, "dsyevd Q1 smem");
-            q1_tfactor_kernel<<<1, Q1W, q1t_smem, st>>>(Gq, P, T1, p0, Tg);
+            if (getenv("BSRG_Q1_RECURRENCE")) {
+                constexpr int q1t_smem = Q1W * (Q1W + 1) * (int)sizeof(double);
+                if ((e = cudaFuncSetAttribute(q1_tfactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              q1t_smem)) != cudaSuccess)
+                    return cuda_fail(e, "dsyevd Q1 smem");
+                q1_tfactor_kernel<<<1, Q1W, q1t_smem, st>>>(Gq, P, T1, p0, Tg);
+            } else {
+                if ((e = cudaFuncSetAttribute(q1_tmerge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              Q1M_SMEM)) != cudaSuccess)
+                    return cuda_fail(e, "dsyevd Q1 smem");
+                q1_tmerge_kernel<<<1, Q1W, Q1M_SMEM, st>>>(Gq, P, T1, p0, Tg);
+            }
             double *Zs = Z + r0;
             rc = dgemm(true, false, Q1W, n, m0, 1.0, Vg, m0, Zs, ldz, 0.0, W1, Q1W, st, sw.gemm_ws,
                        sw.gemm_ws_doubles);
