@@ -557,35 +557,45 @@ __global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
     const int t = threadIdx.x, n = a.n;
     double *AB = a.AB;
     auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
+    // wait until sweep j-1 has completed `need` steps (bounded; false: give up, the flag is set)
+    auto wait_prev = [&](int j, int need) -> bool {
+        if (j > 0 && need > 0) {
+            if (t == 0) {
+                volatile int *pg = a.progress + (j - 1);
+                const unsigned long long t0 = gtime();
+                while (*pg < need) {
+                    if (*(volatile int *)a.err) break;
+                    if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                }
+                __threadfence();
+            }
+            __syncwarp();
+            if (*(volatile int *)a.err) return false;
+        }
+        return true;
+    };
+    // the diagonal and lower blocks of step i of sweep j, lane = row
+    auto load_blocks = [&](int j, int i, double *Dr, double *Br) {
+        const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+        const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+#pragma unroll
+        for (int c = 0; c < NB; c++) Dr[c] = (t < L && c <= t) ? __ldcg(at(r0 + t, r0 + c)) : 0.0;
+#pragma unroll
+        for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
+    };
     for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
         const int nst = sweep_steps(n, j);
         const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
+        double Dr[NB], Br[NB];
+        if (!wait_prev(j, min(3, nprev))) return;
+        load_blocks(j, 0, Dr, Br);
         for (int i = 0; i < nst; i++) {
-            if (j > 0) {
-                const int need = min(i + 3, nprev);
-                if (t == 0) {
-                    volatile int *pg = a.progress + (j - 1);
-                    const unsigned long long t0 = gtime();
-                    while (*pg < need) {
-                        if (*(volatile int *)a.err) break;
-                        if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
-                    }
-                    __threadfence();
-                }
-                __syncwarp();
-                if (*(volatile int *)a.err) return;
-            }
             const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
             const int col = i == 0 ? j : r0 - NB;
             const int nl = r0 - col - 1;
             const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
-            // ---- loads, lane = row (all issued before use) ----
-            double Dr[NB], Br[NB];
+            // the blocks of this step were loaded at the end of the previous one (or above)
             const double xl = i == 0 ? (t < L ? __ldcg(at(r0 + t, col)) : 0.0) : Cs[t][0];
-#pragma unroll
-            for (int c = 0; c < NB; c++) Dr[c] = (t < L && c <= t) ? __ldcg(at(r0 + t, r0 + c)) : 0.0;
-#pragma unroll
-            for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
             // ---- the reflector ----
             double sig = (t >= 1 && t < L) ? xl * xl : 0.0;
             for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
@@ -668,6 +678,12 @@ __global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
             // the next window's x column and left block are this step's lower block
 #pragma unroll
             for (int c = 0; c < NB; c++) Cs[t][c] = Br[c];
+            // the next step's blocks (written by nobody in this step; sweep j-1 must be three steps
+            // ahead of it) are requested before this step's stores are fenced, so the two overlap
+            if (i + 1 < nst) {
+                if (!wait_prev(j, min(i + 4, nprev))) return;
+                load_blocks(j, i + 1, Dr, Br);
+            }
             __threadfence();
             __syncwarp();
             if (t == 0) *(volatile int *)(a.progress + j) = i + 1;
