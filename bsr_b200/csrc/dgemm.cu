@@ -33,6 +33,30 @@ __global__ void __launch_bounds__(C::NT) dgemm_kernel(DgemmBatch p, int S, int k
     const int wm = warp % C::WM, wn = warp / C::WM, r = lane >> 2, q = lane & 3;
     double *out = S > 1 ? W + (long)sp * p.m * p.n : Cm;
     const long ldo = S > 1 ? p.m : p.ldc;
+    if (S == 1 && p.beta != 0.0) {
+        // C is read here: every load of a row of tiles is issued before any is used, so the
+        // epilogue waits for one memory latency per row of tiles instead of one per element
+#pragma unroll
+        for (int s = 0; s < C::FM; s++) {
+            const int row = m0 + wm * C::TM + s * 8 + r;
+            double old[C::FN][2];
+#pragma unroll
+            for (int t = 0; t < C::FN; t++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int col = n0 + wn * C::TN + t * 8 + 2 * q + j;
+                    old[t][j] = (row < p.m && col < p.n) ? out[row + (long)col * ldo] : 0.0;
+                }
+#pragma unroll
+            for (int t = 0; t < C::FN; t++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int col = n0 + wn * C::TN + t * 8 + 2 * q + j;
+                    if (row < p.m && col < p.n) out[row + (long)col * ldo] = p.alpha * acc[s][t][j] + p.beta * old[t][j];
+                }
+        }
+        return;
+    }
 #pragma unroll
     for (int s = 0; s < C::FM; s++) {
         const int row = m0 + wm * C::TM + s * 8 + r;
@@ -44,10 +68,7 @@ __global__ void __launch_bounds__(C::NT) dgemm_kernel(DgemmBatch p, int S, int k
                 const int col = n0 + wn * C::TN + t * 8 + 2 * q + j;
                 if (col >= p.n) continue;
                 double *cp = out + row + (long)col * ldo;
-                if (S > 1) { *cp = acc[s][t][j]; continue; }
-                double v = p.alpha * acc[s][t][j];
-                if (p.beta != 0.0) v += p.beta * *cp;
-                *cp = v;
+                *cp = S > 1 ? acc[s][t][j] : p.alpha * acc[s][t][j];
             }
     }
 }

@@ -1137,6 +1137,211 @@ __global__ void __launch_bounds__(Q2R_W * 32, 1) q2r_apply_kernel(int n, int S, 
 }
 
 // ---------------------------------------------------------------------------
+// The ring application with two warps per group: warp h of a pair owns columns
+// 16h .. 16h+15 of the strip, so 8 warps run 4 groups and every scheduler has two
+// warps to switch between.  The pair shares its block's reflectors, staged as the
+// dense band V(r, q) (r = window row, zeros outside the band and below the window)
+// so that no fragment load needs a mask, and T; the two halves depend only on the
+// same half of the neighbouring groups (their columns are disjoint).
+// ---------------------------------------------------------------------------
+constexpr int Q2P_G = 4;                                        // groups (pairs) per round
+constexpr int Q2P_PAIR = (2 * NB + 2 * NB) * Q2R_LD;            // doubles per pair: V band (64 rows), T, W
+constexpr int Q2P_SMEM = (Q2R_RING * Q2R_LD + Q2P_G * Q2P_PAIR) * (int)sizeof(double);
+static_assert(Q2R_RING >= 2 * NB * Q2P_G, "ring size");
+
+__device__ __forceinline__ void pair_sync(int p) { asm volatile("bar.sync %0, 64;" ::"r"(p + 1)); }
+
+// rows [a, b) of the 16 columns of half h between Z and the ring (one warp)
+__device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int n, int c0, int ncl, int h, int a,
+                                         int b, bool store, int lane)
+{
+    if (b <= a) return;
+    const int nchunk = ((b - a + 3) / 4) * 2;          // chunks of 4 rows x 8 columns, 2 column chunks
+    for (int q = lane; q < nchunk * 32; q += 32) {
+        const int ch = q >> 5, l = q & 31;
+        const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
+        if (row >= b) continue;
+        double *rp = ring + (row & (Q2R_RING - 1)) * Q2R_LD + col;
+        const bool ok = row < n && col < ncl;
+        if (store) {
+            if (ok) Z[row + ldz * (long)(c0 + col)] = *rp;
+        } else {
+            *rp = ok ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, int ncol,
+                                                                 const double *__restrict__ V2,
+                                                                 const double *__restrict__ Tq, double *Z,
+                                                                 long ldz, int *err)
+{
+    extern __shared__ __align__(16) double q2p_sm[];
+    __shared__ volatile int prog[Q2P_G][2];
+    double *ring = q2p_sm;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, lr = lane >> 2, lc = lane & 3;
+    const int pr = wid >> 1, h = wid & 1;                        // pair (group slot), half
+    double *Vd = q2p_sm + Q2R_RING * Q2R_LD + pr * Q2P_PAIR;     // V(r, q) at r LD + q, 64 rows
+    double *Tsm = Vd + 2 * NB * Q2R_LD;                          // T(q, l) at q + LD l
+    double *Wb = Tsm + NB * Q2R_LD;                              // W(q, c) at q LD + c, this half's columns
+    const int c0 = blockIdx.x * 32, ncl = min(32, ncol - c0);
+    const int ng = (n - 2 + NB - 1) / NB;
+    for (int g0 = ng - 1; g0 >= 0; g0 -= Q2P_G) {
+        const int gl = max(g0 - Q2P_G + 1, 0), nw = g0 - gl + 1;
+        __syncthreads();
+        q2r_xfer(ring, Z, ldz, n, c0, ncl, gl * NB + 1, g0 * NB + 1 + 2 * NB, false, tid, blockDim.x);
+        if (tid < 2 * Q2P_G) prog[tid >> 1][tid & 1] = 0;
+        __syncthreads();
+        const int ilast = sweep_steps(n, gl * NB);
+        if (pr < nw) {
+            const int g = g0 - pr;
+            const int imax = sweep_steps(n, g * NB);
+            const int iprev = pr > 0 ? sweep_steps(n, (g + 1) * NB) : 0;
+            for (int i = 0; i < imax; i++) {
+                const unsigned long long t0 = gtime();
+                if (pr > 0) {
+                    const int need = min(i + 1, iprev);
+                    while (prog[pr - 1][h] < need)
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
+                } else if (nw > 1) {
+                    const int need = min(i + nw - Q2R_RING / NB + 1, ilast);
+                    while (need > 0 && prog[nw - 1][h] < need)
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
+                }
+                __threadfence_block();
+                const int top = (g + i) * NB + 1;
+                const int nrow = min(2 * NB - 1, n - top);
+                if (pr == 0 && i > 0) q2p_xfer(ring, Z, ldz, n, c0, ncl, h, top + NB, top + 2 * NB, false, lane);
+                // ---- the pair stages the block's V band and T (after both finished the previous block) ----
+                pair_sync(pr);
+                {
+                    const int nv = q2_nvalid(n, g, i);
+                    const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;
+                    const double *T = Tq + ((long)g * S + i) * NB * NB;
+                    double vq[NB / 2], tl[NB / 2];
+#pragma unroll
+                    for (int u = 0; u < NB / 2; u++) {
+                        const int q = 16 * h + u;
+                        vq[u] = q < nv ? __ldg(Vblk + (long)q * S * NB + lane) : 0.0;
+                        tl[u] = __ldg(T + lane + NB * q);               // column l = q of T
+                    }
+#pragma unroll
+                    for (int u = 0; u < NB / 2; u++) {
+                        const int q = 16 * h + u;
+#pragma unroll
+                        for (int half = 0; half < 2; half++) {
+                            const int rr = lane + 32 * half, t = rr - q;
+                            const double x = __shfl_sync(0xffffffffu, vq[u], t & 31);
+                            Vd[rr * Q2R_LD + q] = (t >= 0 && t < NB && rr < nrow) ? x : 0.0;
+                        }
+                        Tsm[lane + Q2R_LD * q] = tl[u];
+                    }
+                }
+                pair_sync(pr);
+                // ---- W = V^T Zw on this half's columns: M = q (4), N = column (2), K = row (16) ----
+                double acc[4][2][2];
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < 16; ks++) {
+                    const int r = 4 * ks + lc;
+                    const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+                    const double bz0 = rrow[lr], bz1 = rrow[8 + lr];
+#pragma unroll
+                    for (int mt = 0; mt < 4; mt++) {
+                        if (ks < 2 * mt || ks >= 2 * mt + 10) continue;
+                        const double a = Vd[r * Q2R_LD + 8 * mt + lr];
+                        q2r_mma(acc[mt][0][0], acc[mt][0][1], a, bz0);
+                        q2r_mma(acc[mt][1][0], acc[mt][1][1], a, bz1);
+                    }
+                }
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 2; nt++) {
+                        Wb[(8 * mt + lr) * Q2R_LD + 16 * h + 8 * nt + 2 * lc] = acc[mt][nt][0];
+                        Wb[(8 * mt + lr) * Q2R_LD + 16 * h + 8 * nt + 2 * lc + 1] = acc[mt][nt][1];
+                        acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+                    }
+                __syncwarp();
+                // ---- W2 = T W ----
+#pragma unroll
+                for (int ks = 0; ks < 8; ks++) {
+                    const int l = 4 * ks + lc;
+                    const double bw0 = Wb[l * Q2R_LD + 16 * h + lr], bw1 = Wb[l * Q2R_LD + 16 * h + 8 + lr];
+#pragma unroll
+                    for (int mt = 0; mt < 4; mt++) {
+                        if (ks < 2 * mt) continue;
+                        const double a = Tsm[(8 * mt + lr) + Q2R_LD * l];
+                        q2r_mma(acc[mt][0][0], acc[mt][0][1], a, bw0);
+                        q2r_mma(acc[mt][1][0], acc[mt][1][1], a, bw1);
+                    }
+                }
+                __syncwarp();
+#pragma unroll
+                for (int mt = 0; mt < 4; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < 2; nt++) {
+                        Wb[(8 * mt + lr) * Q2R_LD + 16 * h + 8 * nt + 2 * lc] = acc[mt][nt][0];
+                        Wb[(8 * mt + lr) * Q2R_LD + 16 * h + 8 * nt + 2 * lc + 1] = acc[mt][nt][1];
+                    }
+                __syncwarp();
+                // ---- Zw -= V W2: M = window row (8 tiles in two halves), N = column (2), K = q (8) ----
+#pragma unroll
+                for (int mh = 0; mh < 2; mh++) {
+#pragma unroll
+                    for (int a = 0; a < 4; a++) {
+                        const int r = 8 * (4 * mh + a) + lr;
+                        const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+#pragma unroll
+                        for (int nt = 0; nt < 2; nt++) {
+                            acc[a][nt][0] = rrow[8 * nt + 2 * lc];
+                            acc[a][nt][1] = rrow[8 * nt + 2 * lc + 1];
+                        }
+                    }
+#pragma unroll
+                    for (int ks = 0; ks < 8; ks++) {
+                        const int q = 4 * ks + lc;
+                        const double bw0 = Wb[q * Q2R_LD + 16 * h + lr], bw1 = Wb[q * Q2R_LD + 16 * h + 8 + lr];
+#pragma unroll
+                        for (int a = 0; a < 4; a++) {
+                            const int mt = 4 * mh + a;
+                            const int klo = 2 * mt - 8 > 0 ? 2 * mt - 8 : 0, khi = 2 * mt + 1 < 7 ? 2 * mt + 1 : 7;
+                            if (ks < klo || ks > khi) continue;
+                            const double v = -Vd[(8 * mt + lr) * Q2R_LD + q];
+                            q2r_mma(acc[a][0][0], acc[a][0][1], v, bw0);
+                            q2r_mma(acc[a][1][0], acc[a][1][1], v, bw1);
+                        }
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; a++) {
+                        const int r = 8 * (4 * mh + a) + lr;
+                        if (r < nrow) {
+                            double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+#pragma unroll
+                            for (int nt = 0; nt < 2; nt++) {
+                                rrow[8 * nt + 2 * lc] = acc[a][nt][0];
+                                rrow[8 * nt + 2 * lc + 1] = acc[a][nt][1];
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if (pr == nw - 1) q2p_xfer(ring, Z, ldz, n, c0, ncl, h, top, top + NB, true, lane);
+                __threadfence_block();
+                __syncwarp();
+                if (lane == 0) prog[pr][h] = i + 1;
+            }
+        }
+        __syncthreads();
+        const int rdone = ilast > 0 ? (gl + ilast) * NB + 1 : gl * NB + 1;
+        q2r_xfer(ring, Z, ldz, n, c0, ncl, rdone, n, true, tid, blockDim.x);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // back-transformation of the stage-1 panels, Q1_GROUP panels at a time
 // ---------------------------------------------------------------------------
 constexpr int Q1_GROUP = 4;
@@ -1532,11 +1737,16 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2w_apply_kernel<<<(unsigned)((n + 31) / 32), Q2W_WARPS * 32, Q2W_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz,
                                                                                           sw.err);
-        } else {
+        } else if (getenv("BSRG_Q2_RING1")) {
             if ((e = cudaFuncSetAttribute(q2r_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2R_SMEM)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2r_apply_kernel<<<(unsigned)((n + 31) / 32), Q2R_W * 32, Q2R_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
+        } else {
+            if ((e = cudaFuncSetAttribute(q2p_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2P_SMEM)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd Q2 smem");
+            q2p_apply_kernel<<<(unsigned)((n + 31) / 32), Q2P_G * 64, Q2P_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
         }
         // per block and column: W = V^T Z (2 NB nv), T W (~NB nv), Z -= V W (2 NB nv)
         double nvsum = 0.0;
