@@ -43,7 +43,51 @@ def parse():
     ap.add_argument("--steps-only", action="store_true",
                     help="run the warm-up and timed steps only and print the basic line (for a profiler's "
                          "launch list of exactly those steps)")
+    ap.add_argument("--dense-eig", type=int, default=0, metavar="N",
+                    help="time only the library's dense eigensolver (bsrg_dsyevd) on a seeded symmetric N x N "
+                         "matrix, with its stage times, beside cuSOLVER's (torch.linalg.eigh); for profiling")
     return ap.parse_args()
+
+
+def run_dense_eig(args):
+    """The dense eigensolver alone: --warmup untimed calls, then --steps timed calls (CUDA events)."""
+    import torch
+    import bsr_b200 as bsr
+    from bsr_b200._lib import call
+    from bsr_b200.core import _ptr
+    n = args.dense_eig
+    ctx = bsr.Context()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    M = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g)
+    A = (M + M.T) / 2
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    Z = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    for _ in range(max(args.warmup, 0)):
+        call("bsrg_dsyevd", ctx.handle, n, _ptr(A), n, _ptr(w), _ptr(Z), n)
+    torch.cuda.synchronize()
+    ctx.set_timing(True)
+    ctx.stage_times()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        call("bsrg_dsyevd", ctx.handle, n, _ptr(A), n, _ptr(w), _ptr(Z), n)
+    s1.record()
+    s1.synchronize()
+    own = s0.elapsed_time(s1) / args.steps
+    st = ctx.stage_times()
+    ctx.set_timing(False)
+    wl = torch.linalg.eigh(A)[0]
+    torch.cuda.synchronize()
+    s0.record()
+    for _ in range(args.steps):
+        torch.linalg.eigh(A)
+    s1.record()
+    s1.synchronize()
+    lib = s0.elapsed_time(s1) / args.steps
+    err = float(((w - wl).abs().max() / wl.abs().max()).item())
+    print(json.dumps({"dense_eig_n": n, "own_ms": own, "cusolver_ms": lib, "max_rel_eig_diff": err,
+                      "stages_ms": {k: round(v[0] / args.steps, 3) for k, v in st.items() if k.startswith("eig_")}}),
+          flush=True)
 
 
 def dist_env():
@@ -766,7 +810,9 @@ def _group_counts(c, ty):
 
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.dense_eig > 0:
+        run_dense_eig(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
