@@ -951,16 +951,30 @@ __device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int 
 {
     if (b <= a) return;
     const int nchunk = ((b - a + 3) / 4) * 4;        // chunks of 4 rows x 8 columns
-    for (int q = t0; q < nchunk * 32; q += nthr) {
-        const int ch = q >> 5, l = q & 31;
-        const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
-        if (row >= b) continue;
-        double *rp = ring + (row & (Q2R_RING - 1)) * Q2R_LD + col;
-        const bool ok = row < n && col < ncl;
-        if (store) {
-            if (ok) Z[row + ldz * (long)(c0 + col)] = *rp;
-        } else {
-            *rp = ok ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+    const int total = nchunk * 32;
+    if (store) {
+        for (int q = t0; q < total; q += nthr) {
+            const int ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
+            if (row < b && row < n && col < ncl)
+                Z[row + ldz * (long)(c0 + col)] = ring[(row & (Q2R_RING - 1)) * Q2R_LD + col];
+        }
+        return;
+    }
+    // loads in batches of 16 per thread, all issued before any is stored
+    for (int q0 = t0; q0 < total; q0 += 16 * nthr) {
+        double v[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int q = q0 + u * nthr, ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
+            v[u] = (q < total && row < b && row < n && col < ncl) ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int q = q0 + u * nthr, ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
+            if (q < total && row < b) ring[(row & (Q2R_RING - 1)) * Q2R_LD + col] = v[u];
         }
     }
 }
@@ -1157,16 +1171,30 @@ __device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int 
 {
     if (b <= a) return;
     const int nchunk = ((b - a + 3) / 4) * 2;          // chunks of 4 rows x 8 columns, 2 column chunks
-    for (int q = lane; q < nchunk * 32; q += 32) {
-        const int ch = q >> 5, l = q & 31;
-        const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
-        if (row >= b) continue;
-        double *rp = ring + (row & (Q2R_RING - 1)) * Q2R_LD + col;
-        const bool ok = row < n && col < ncl;
-        if (store) {
-            if (ok) Z[row + ldz * (long)(c0 + col)] = *rp;
-        } else {
-            *rp = ok ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+    const int total = nchunk * 32;
+    if (store) {
+        for (int q = lane; q < total; q += 32) {
+            const int ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
+            if (row < b && row < n && col < ncl)
+                Z[row + ldz * (long)(c0 + col)] = ring[(row & (Q2R_RING - 1)) * Q2R_LD + col];
+        }
+        return;
+    }
+    // loads in batches of 16 per lane (a 32-row window half is exactly one batch), issued before use
+    for (int q0 = lane; q0 < total; q0 += 16 * 32) {
+        double v[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int q = q0 + u * 32, ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
+            v[u] = (q < total && row < b && row < n && col < ncl) ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const int q = q0 + u * 32, ch = q >> 5, l = q & 31;
+            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
+            if (q < total && row < b) ring[(row & (Q2R_RING - 1)) * Q2R_LD + col] = v[u];
         }
     }
 }
