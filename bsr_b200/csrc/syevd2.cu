@@ -1253,16 +1253,20 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
                         vq[u] = q < nv ? __ldg(Vblk + (long)q * S * NB + lane) : 0.0;
                         tl[u] = __ldg(T + lane + NB * q);               // column l = q of T
                     }
+                    // compact V(q, t) into the W area first (free until W is formed): consecutive stores
+                    double *Vc = Wb;
 #pragma unroll
                     for (int u = 0; u < NB / 2; u++) {
                         const int q = 16 * h + u;
-#pragma unroll
-                        for (int half = 0; half < 2; half++) {
-                            const int rr = lane + 32 * half, t = rr - q;
-                            const double x = __shfl_sync(0xffffffffu, vq[u], t & 31);
-                            Vd[rr * Q2R_LD + q] = (t >= 0 && t < NB && rr < nrow) ? x : 0.0;
-                        }
+                        Vc[q * 34 + lane] = vq[u];
                         Tsm[lane + Q2R_LD * q] = tl[u];
+                    }
+                    pair_sync(pr);
+                    // the dense band V(r, q) = Vc(q, r - q), a row's 32 entries by 32 consecutive threads
+                    // (reads Vc at 33 q + r: distinct banks)
+                    for (int e = 32 * h + lane; e < 2 * NB * NB; e += 64) {
+                        const int rr = e >> 5, q = e & 31, t = rr - q;
+                        Vd[rr * Q2R_LD + q] = (t >= 0 && t < NB && rr < nrow) ? Vc[q * 34 + t] : 0.0;
                     }
                 }
                 pair_sync(pr);
