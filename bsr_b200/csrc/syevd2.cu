@@ -552,23 +552,43 @@ __global__ void __launch_bounds__(32) sb2st_kernel(Sb2stArgs a)
 // memory, and the x column and left block of step i > 0 taken from step i-1's
 // updated lower block (the same rows and columns; no other sweep writes them in
 // between: sweep j-1 is at least three steps ahead, sweep j+1 behind).
-__global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
+// K warps per CTA: CTA b takes the groups of K consecutive sweeps g = b, b + gridDim.x, ...,
+// warp w sweep g K + w.  A warp waits for its predecessor sweep through a counter in shared
+// memory when the predecessor is a warp of the same CTA (w > 0) and through the global
+// progress array otherwise; the band itself is exchanged through global memory (L2) as before.
+constexpr int SB_WSM = 2 * NB * (NB + 1) + 2 * NB;       // doubles of shared memory per warp
+
+template <int K>
+__global__ void __launch_bounds__(32 * K) sb2st2_kernel(Sb2stArgs a)
 {
-    __shared__ double Ts[NB][NB + 1];          // transpose of the diagonal block
-    __shared__ double Cs[NB][NB + 1];          // the previous step's lower block (row-major): x and left block
-    __shared__ double vs[NB], ws2[NB];
-    const int t = threadIdx.x, n = a.n;
+    extern __shared__ __align__(16) double sbsm[];
+    __shared__ volatile int sprog[K];          // it * 4096 + completed steps of warp w's sweep
+    const int t = threadIdx.x & 31, w = threadIdx.x >> 5, n = a.n;
+    double (*Ts)[NB + 1] = (double (*)[NB + 1])(sbsm + w * SB_WSM);            // transpose of D
+    double (*Cs)[NB + 1] = (double (*)[NB + 1])(sbsm + w * SB_WSM + NB * (NB + 1));   // carried block
+    double *vs = sbsm + w * SB_WSM + 2 * NB * (NB + 1), *ws2 = vs + NB;
     double *AB = a.AB;
+    if (threadIdx.x < K) sprog[threadIdx.x] = 0;
+    __syncthreads();
+    int it = 0;
     auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
     // wait until sweep j-1 has completed `need` steps (bounded; false: give up, the flag is set)
     auto wait_prev = [&](int j, int need) -> bool {
         if (j > 0 && need > 0) {
             if (t == 0) {
-                volatile int *pg = a.progress + (j - 1);
                 const unsigned long long t0 = gtime();
-                while (*pg < need) {
-                    if (*(volatile int *)a.err) break;
-                    if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                if (w > 0) {
+                    const int target = it * 4096 + need;
+                    while (sprog[w - 1] < target) {
+                        if (*(volatile int *)a.err) break;
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                    }
+                } else {
+                    volatile int *pg = a.progress + (j - 1);
+                    while (*pg < need) {
+                        if (*(volatile int *)a.err) break;
+                        if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); break; }
+                    }
                 }
                 __threadfence();
             }
@@ -586,7 +606,9 @@ __global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
 #pragma unroll
         for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
     };
-    for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
+    for (int g = blockIdx.x; g * K < n - 2; g += gridDim.x, it++) {
+        const int j = g * K + w;
+        if (j >= n - 2) break;
         const int nst = sweep_steps(n, j);
         const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
         double Dr[NB], Br[NB];
@@ -689,7 +711,10 @@ __global__ void __launch_bounds__(32) sb2st2_kernel(Sb2stArgs a)
             }
             __threadfence();
             __syncwarp();
-            if (t == 0) *(volatile int *)(a.progress + j) = i + 1;
+            if (t == 0) {
+                *(volatile int *)(a.progress + j) = i + 1;
+                sprog[w] = it * 4096 + i + 1;
+            }
         }
     }
 }
@@ -1717,14 +1742,30 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
         // the register form (sb2st2_kernel) by default; BSRG_SB2ST_SHARED keeps the shared-memory form
-        const void *kfn = getenv("BSRG_SB2ST_SHARED") ? (const void *)sb2st_kernel : (const void *)sb2st2_kernel;
-        int per = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kfn, 32, 0);
-        const int workers = std::max(1, std::min(n - 2, std::min(nsm * std::max(per, 1), 2 * nsm)));
+        // groups of SB_K consecutive sweeps per CTA (sb2st2_kernel<SB_K>); BSRG_SB2ST_SHARED keeps the
+        // shared-memory form with one sweep per CTA
+        constexpr int SB_K = 8;
         Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
         void *args[] = {&a2};
-        if ((e = cudaLaunchCooperativeKernel(kfn, workers, 32, args, 0, st)) != cudaSuccess)
-            return cuda_fail(e, "dsyevd bulge chasing");
+        if (getenv("BSRG_SB2ST_SHARED")) {
+            int per = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st_kernel, 32, 0);
+            const int workers = std::max(1, std::min(n - 2, std::min(nsm * std::max(per, 1), 2 * nsm)));
+            if ((e = cudaLaunchCooperativeKernel((const void *)sb2st_kernel, workers, 32, args, 0, st)) != cudaSuccess)
+                return cuda_fail(e, "dsyevd bulge chasing");
+        } else {
+            const int smem = SB_K * SB_WSM * (int)sizeof(double);
+            if ((e = cudaFuncSetAttribute(sb2st2_kernel<SB_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd bulge chasing smem");
+            int per = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st2_kernel<SB_K>, 32 * SB_K, smem);
+            const int groups = (n - 2 + SB_K - 1) / SB_K;
+            const int ctas = std::max(1, std::min(groups, nsm * std::max(per, 1)));
+            if ((e = cudaLaunchCooperativeKernel((const void *)sb2st2_kernel<SB_K>, ctas, 32 * SB_K, args, smem, st)) !=
+                cudaSuccess)
+                return cuda_fail(e, "dsyevd bulge chasing");
+        }
     }
     tridiag_extract_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, AB, dv, ev);
     for (int j = 0; j < n - 2; j++)
