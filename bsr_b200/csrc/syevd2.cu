@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
 
 // Y = X T (rows), partial M = V^T Y per chunk of 128 rows.  X, V, Y: ld m.
 __global__ void __launch_bounds__(128) ypass1_kernel(int m, const double *__restrict__ X, const double *__restrict__ V,
-                                                     const double *__restrict__ T, double *Y, double *Mp)
+                                                     const double *__restrict__ T, double *Y, double *Mp,
+                                                     unsigned *tick)
 {
     __shared__ double Ts[NB][NB + 1];
     extern __shared__ __align__(16) double ysm[];        // Vs, Ys: 128 x (NB + 1) each
@@ -369,28 +370,39 @@ __global__ void __launch_bounds__(128) ypass1_kernel(int m, const double *__rest
         for (int rr = 0; rr < 128; rr++) s += Vs[rr][i] * Ys[rr][j];
         Mp[(long)blockIdx.x * NB * NB + q] = s;
     }
-}
-
-// M = sum of the chunk partials, M2 = 1/2 T^T M, Y -= V M2 (rows)
-__global__ void __launch_bounds__(128) ypass2_kernel(int m, int nchunk, const double *__restrict__ V,
-                                                     const double *__restrict__ T, const double *__restrict__ Mp,
-                                                     double *Y)
-{
-    __shared__ double Ms[NB][NB + 1], M2[NB][NB + 1], Ts[NB][NB + 1];
-    const int tid = threadIdx.x;
+    // the last CTA to finish sums the partials in chunk order and forms M2 = 1/2 T^T M once
+    // (at Mp + gridDim.x NB^2) for ypass2; it resets the ticket for the next panel
+    __shared__ unsigned ticket;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) ticket = atomicAdd(tick, 1u);
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return;
+    __threadfence();
+    double (*Ms)[NB + 1] = Vs;                     // reuse
     for (int q = tid; q < NB * NB; q += 128) {
         double s = 0.0;
-        for (int ch = 0; ch < nchunk; ch++) s += Mp[(long)ch * NB * NB + q];
+        for (int ch = 0; ch < (int)gridDim.x; ch++) s += __ldcg(Mp + (long)ch * NB * NB + q);
         Ms[q % NB][q / NB] = s;
-        Ts[q % NB][q / NB] = T[q];
     }
     __syncthreads();
+    double *M2 = Mp + (long)gridDim.x * NB * NB;
     for (int q = tid; q < NB * NB; q += 128) {
         const int i = q % NB, j = q / NB;
         double s = 0.0;
         for (int l = 0; l <= i; l++) s += Ts[l][i] * Ms[l][j];     // T upper: T^T(i,l) = T(l,i), l <= i
-        M2[i][j] = 0.5 * s;
+        M2[q] = 0.5 * s;                                            // column-major M2(i, j)
     }
+    if (tid == 0) *tick = 0u;
+}
+
+// Y -= V M2 (rows), M2 formed by the last CTA of ypass1
+__global__ void __launch_bounds__(128) ypass2_kernel(int m, const double *__restrict__ V, const double *__restrict__ M2g,
+                                                     double *Y)
+{
+    __shared__ double M2[NB][NB + 1];
+    const int tid = threadIdx.x;
+    for (int q = tid; q < NB * NB; q += 128) M2[q % NB][q / NB] = M2g[q];
     __syncthreads();
     const int r = blockIdx.x * 128 + tid;
     if (r >= m) return;
@@ -1509,6 +1521,7 @@ struct Sy2sbWork {
     double *part;      // PQ CTAs x 4NB
     double *gram;      // PQ CTAs x NB x NB
     unsigned *bar;     // 2
+    unsigned *ticket;  // ypass1's last-CTA counter (zero between panels)
     int *err;
     double *gemm_ws;   // split-K workspace
     size_t gemm_ws_doubles;
@@ -1619,8 +1632,8 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         int rc = dgemm_ws(false, false, gx, 1, st, w.gemm_ws, w.gemm_ws_doubles);
         if (rc != BSRG_OK) return rc;
         const int nch = (m + 127) / 128;
-        ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp);
-        ypass2_kernel<<<nch, 128, 0, st>>>(m, nch, Vp, w.T, w.Mp, Yp);
+        ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp, w.ticket);
+        ypass2_kernel<<<nch, 128, 0, st>>>(m, Vp, w.Mp + (size_t)nch * NB * NB, Yp);
         // A22 -= [V Y] [Y V]^T, the tiles that reach the lower triangle
         DgemmBatch gu{};
         gu.m = m; gu.n = m; gu.k = 2 * NB;
@@ -1712,6 +1725,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     int *flags = (int *)(ws + L.flags);            // bar[2], err, err2
     sw.bar = (unsigned *)flags;
     sw.err = flags + 2;
+    sw.ticket = (unsigned *)(flags + 4);
     double *W1 = ws + L.W1, *W2 = ws + L.W2;
     double *Vg = ws + L.Vg, *Gq = ws + L.Gq, *Tg = ws + L.Tg;
     sw.gemm_ws_doubles = 8 * (size_t)Q1W * n;
