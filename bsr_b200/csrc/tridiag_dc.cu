@@ -363,16 +363,25 @@ __global__ void dc_rotate_kernel(const DcMerge *__restrict__ mg, const int *__re
 // merge step 2: secular equation, one thread per root
 // ---------------------------------------------------------------------------
 // root j in (dd_j, dd_{j+1}) (the last in (dd_K, dd_K + rho |z|^2)) as origin index + offset
-__global__ void __launch_bounds__(128) dc_secular_kernel(const DcMerge *__restrict__ mg, const int *__restrict__ scal,
-                                                         double *ws, int *iws, int kcap)
+constexpr int SEC_WARPS = 16;          // roots per CTA of the secular kernel (a warp each)
+
+__device__ __forceinline__ double warp_sum(double x)
+{
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// one warp per root: the lanes split the sums over the poles, every lane then takes the same step
+__global__ void __launch_bounds__(32 * SEC_WARPS) dc_secular_kernel(const DcMerge *__restrict__ mg,
+                                                                    const int *__restrict__ scal, double *ws,
+                                                                    int *iws, int kcap)
 {
     extern __shared__ __align__(16) double sm2[];
     const int mi = blockIdx.y;
     const DcMerge M = mg[mi];
     const int k = M.k1 + M.k2;
     const int K = scal[DC_NS * mi];
-    const int j0 = blockIdx.x * blockDim.x;
-    if (j0 >= K) return;
+    if ((int)blockIdx.x * SEC_WARPS >= K) return;
     double *V = ws + M.off_v;
     const double *dd = V, *zz = V + k;
     double *tau = V + 5 * (long)k;
@@ -381,21 +390,22 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(const DcMerge *__restri
     double *sd = sm2, *sz = sm2 + kcap;
     for (int i = threadIdx.x; i < K; i += blockDim.x) { sd[i] = dd[i]; sz[i] = zz[i] * zz[i]; }
     __syncthreads();
-    const int j = j0 + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.x * SEC_WARPS + (threadIdx.x >> 5);
     if (j >= K) return;
-    double znrm = 0.0;
     int o;
     double lo, hi;
     if (j < K - 1) {
-        const double del = sd[j + 1] - sd[j];
-        const double mid = 0.5 * del;
-        double f = 1.0;
-        for (int i = 0; i < K; i++) f += rho * sz[i] / ((sd[i] - sd[j]) - mid);
+        const double mid = 0.5 * (sd[j + 1] - sd[j]);
+        double fp = 0.0;
+        for (int i = lane; i < K; i += 32) fp += sz[i] / ((sd[i] - sd[j]) - mid);
+        const double f = 1.0 + rho * warp_sum(fp);
         if (f >= 0.0) { o = j; lo = 0.0; hi = mid; }
         else { o = j + 1; lo = -mid; hi = 0.0; }
     } else {
-        for (int i = 0; i < K; i++) znrm += sz[i];
-        o = j; lo = 0.0; hi = rho * znrm;
+        double zp = 0.0;
+        for (int i = lane; i < K; i += 32) zp += sz[i];
+        o = j; lo = 0.0; hi = rho * warp_sum(zp);
     }
     const double dov = sd[o];
     // Iterate on tau with the two-pole model of the secular function (the "middle way" of
@@ -406,20 +416,18 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(const DcMerge *__restri
     double t = 0.5 * (lo + hi);
     const double dj = sd[j] - dov, dj1 = j < K - 1 ? sd[j + 1] - dov : 0.0;
     for (int it = 0; it < 100; it++) {
-        double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0, eabs = 0.0;
-        for (int i = 0; i <= j; i++) {
+        double psi = 0.0, dpsi = 0.0, phi = 0.0, dphi = 0.0;
+        for (int i = lane; i < K; i += 32) {
             const double r = 1.0 / ((sd[i] - dov) - t);
             const double q = sz[i] * r;
-            psi += q;
-            dpsi += q * r;
+            if (i <= j) { psi += q; dpsi += q * r; }
+            else { phi += q; dphi += q * r; }
         }
-        for (int i = j + 1; i < K; i++) {
-            const double r = 1.0 / ((sd[i] - dov) - t);
-            const double q = sz[i] * r;
-            phi += q;
-            dphi += q * r;
-        }
-        eabs = 1.0 + rho * (fabs(psi) + fabs(phi));
+        psi = warp_sum(psi);
+        dpsi = warp_sum(dpsi);
+        phi = warp_sum(phi);
+        dphi = warp_sum(dphi);
+        const double eabs = 1.0 + rho * (fabs(psi) + fabs(phi));
         const double f = 1.0 + rho * (psi + phi);
         if (f < 0.0) lo = t; else hi = t;
         if (f == 0.0 || fabs(f) <= 8.0 * 2.220446049250313e-16 * K * eabs) break;
@@ -453,8 +461,10 @@ __global__ void __launch_bounds__(128) dc_secular_kernel(const DcMerge *__restri
         if (step <= 2.220446049250313e-16 * fabs(t) || hi - lo <= 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)))
             break;
     }
-    tau[j] = t;
-    org[j] = o;
+    if (lane == 0) {
+        tau[j] = t;
+        org[j] = o;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -697,8 +707,9 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
             if ((err = cudaFuncSetAttribute(dc_secular_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             smem_sec)) != cudaSuccess)
                 return cuda_fail(err, "dstedc secular smem");
+            dim3 gsec((unsigned)((Kmax + SEC_WARPS - 1) / SEC_WARPS), nm);
+            dc_secular_kernel<<<gsec, 32 * SEC_WARPS, smem_sec, st>>>(d_mg, d_scal, wsd, wsi, Kmax);
             dim3 gs((unsigned)((Kmax + 127) / 128), nm);
-            dc_secular_kernel<<<gs, 128, smem_sec, st>>>(d_mg, d_scal, wsd, wsi, Kmax);
             dc_zhat_kernel<<<gs, 128, 0, st>>>(d_mg, d_scal, wsd, wsi);
             dim3 gv((unsigned)((Kmax + 7) / 8), nm);
             dc_vec_kernel<<<gv, 256, 0, st>>>(d_mg, d_scal, wsd, wsi);
