@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ __align__(16) double ps[];       // rpc x (NB + 1) | partials [2][2 NB] | Gram NB x NB
     __shared__ double tot[NB], piv[NB], wv[NB], tau_s[NB];
+    __shared__ double sc_tau, sc_scale, sc_beta;
     const int cta = (int)cl.block_rank(), G = (int)cl.num_blocks(), tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int m = a.m, r0 = cta * a.rpc, nr = max(0, min(a.rpc, m - r0));
@@ -247,39 +248,35 @@ __global__ void __launch_bounds__(PQ_NT) panel_qr_cluster_kernel(PanelArgs a)
             piv[k] = cl.map_shared_rank(buf, 0)[NB + k];
         }
         __syncthreads();
-        // every thread forms the reflector's scalars and w_k = v^T P(:, k) itself (no barrier), then
-        // updates and scales its own rows in one pass
-        double tau = 0.0, scale = 0.0, beta = piv[c];
-        {
+        if (tid == 0) {
             const double alpha = piv[c], sigma = tot[c];
-            if (sigma != 0.0) {
-                beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
-                tau = (beta - alpha) / beta;
-                scale = 1.0 / (alpha - beta);
+            if (sigma == 0.0) { sc_tau = 0.0; sc_scale = 0.0; sc_beta = alpha; }
+            else {
+                const double beta = -copysign(sqrt(alpha * alpha + sigma), alpha);
+                sc_tau = (beta - alpha) / beta;
+                sc_scale = 1.0 / (alpha - beta);
+                sc_beta = beta;
             }
+            tau_s[c] = sc_tau;
         }
-        if (tid == 0) tau_s[c] = tau;
-        double wk[NB];
-#pragma unroll
-        for (int k = 0; k < NB; k++) wk[k] = k > c ? piv[k] + scale * tot[k] : 0.0;
+        __syncthreads();
+        const double tau = sc_tau, scale = sc_scale;
+        for (int k = c + 1 + tid; k < NB; k += PQ_NT) wv[k] = piv[k] + scale * tot[k];
+        __syncthreads();
+        // a thread per row (stride 33 doubles: conflict-free), columns k > c in registers' reach
         const double ts_ = tau * scale;
         for (int r = tid; r < nr; r += PQ_NT) {
-            const int gr = r0 + r;
-            if (gr < c) continue;
+            if (r0 + r <= c) continue;
             double *row = ps + r * LD;
-            if (gr > c) {
-                const double f = ts_ * row[c];
-#pragma unroll
-                for (int k = 0; k < NB; k++)
-                    if (k > c) row[k] -= f * wk[k];
-                row[c] *= scale;
-            } else {                                        // the pivot row (v = 1 there)
-#pragma unroll
-                for (int k = 0; k < NB; k++)
-                    if (k > c) row[k] -= tau * wk[k];
-                row[c] = beta;
-            }
+            const double f = ts_ * row[c];
+            for (int k = c + 1; k < NB; k++) row[k] -= f * wv[k];
         }
+        if (cta == 0)
+            for (int k = c + 1 + tid; k < NB; k += PQ_NT) ps[c * LD + k] -= tau * wv[k];
+        __syncthreads();
+        for (int r = tid; r < nr; r += PQ_NT)
+            if (r0 + r > c) ps[r * LD + c] *= scale;
+        if (cta == 0 && tid == 0) ps[c * LD + c] = sc_beta;
         __syncthreads();
     }
     // V in place (unit diagonal, zeros above; columns beyond kb zero), the R part kept aside
