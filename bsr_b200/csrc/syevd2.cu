@@ -1755,7 +1755,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         // the register form (sb2st2_kernel) by default; BSRG_SB2ST_SHARED keeps the shared-memory form
         // groups of SB_K consecutive sweeps per CTA (sb2st2_kernel<SB_K>); BSRG_SB2ST_SHARED keeps the
         // shared-memory form with one sweep per CTA
-        constexpr int SB_K = 8;
+        constexpr int SB_K = 1;              // eight sweeps per CTA measured slower (152 vs 121 ms at n = 7810)
         Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
         void *args[] = {&a2};
         if (getenv("BSRG_SB2ST_SHARED")) {
@@ -1772,7 +1772,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             int per = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st2_kernel<SB_K>, 32 * SB_K, smem);
             const int groups = (n - 2 + SB_K - 1) / SB_K;
-            const int ctas = std::max(1, std::min(groups, nsm * std::max(per, 1)));
+            const int ctas = std::max(1, std::min(groups, std::min(nsm * std::max(per, 1), 2 * nsm)));
             if ((e = cudaLaunchCooperativeKernel((const void *)sb2st2_kernel<SB_K>, ctas, 32 * SB_K, args, smem, st)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd bulge chasing");
