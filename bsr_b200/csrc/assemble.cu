@@ -1170,6 +1170,12 @@ int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
     cusolverDnSetStream(c->solver, c->stream);
     cudaEventCreateWithFlags(&c->ev_stage, cudaEventDisableTiming);
     cudaEventRecord(c->ev_stage, c->stream);
+    if (cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->aux_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->aux_ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        c->aux_stream = nullptr;              // the band reduction then runs on one stream
+    }
     c->events = new std::vector<bsrg_stage_event>();
     c->pool = new std::vector<cudaEvent_t>();
     c->last_ipsol = new std::vector<int>();
@@ -1186,6 +1192,12 @@ int bsrg_ctx_destroy(bsrg_ctx *c)
     if (c->ws) cudaFree(c->ws);
     if (c->pinned) cudaFreeHost(c->pinned);
     cudaEventDestroy(c->ev_stage);
+    if (c->aux_stream) {
+        cudaStreamSynchronize(c->aux_stream);
+        cudaStreamDestroy(c->aux_stream);
+        cudaEventDestroy(c->aux_ev[0]);
+        cudaEventDestroy(c->aux_ev[1]);
+    }
     for (auto &e : *c->events) { cudaEventDestroy(e.start); cudaEventDestroy(e.stop); }
     for (auto ev : *c->pool) cudaEventDestroy(ev);
     delete c->events;

@@ -1512,6 +1512,9 @@ __global__ void __launch_bounds__(Q1W) q1_tmerge_kernel(const double *__restrict
 // ---- stage 1 driver ----
 struct Sy2sbWork {
     double *VYV;       // m x 3NB
+    double *VYV2;      // the second [V | Y | V] buffer (panels alternate while the look-ahead runs)
+    cudaStream_t aux;  // the look-ahead's second stream (null: one stream)
+    cudaEvent_t ev_y, ev_c2;
     double *X;         // m x NB
     double *T;         // NB x NB
     double *Mp;        // chunks x NB x NB
@@ -1579,12 +1582,13 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         G = std::max(1, std::min(G, std::max(1, m / NB)));      // CTA 0 holds the NB pivot rows
         const int rpc = (m + G - 1) / G;
         if (rpc > PQ_ROWS) { set_error("sy2sb: panel of %d rows does not fit", m); return BSRG_ERR_ARG; }
+        double *VYV = (p & 1) && w.aux ? w.VYV2 : w.VYV;
         PanelArgs a;
         a.P = A + (j + NB) + lda * (long)j;
         a.ldp = lda;
         a.m = m;
         a.rpc = rpc;
-        a.V = w.VYV;
+        a.V = VYV;
         a.Vs = Vsave + voff;
         a.T = w.T;
         a.Ts = Tsave + (size_t)p * NB * NB;
@@ -1620,7 +1624,10 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         voff += (size_t)m * NB;
         // trailing update of A22 = A(j+NB:, j+NB:) (m x m, full symmetric storage)
         double *A22 = A + (j + NB) + lda * (long)(j + NB);
-        double *Vp = w.VYV, *Yp = w.VYV + (long)m * NB;
+        double *Vp = VYV, *Yp = VYV + (long)m * NB;
+        // X = A22 V needs the previous panel's trailing update, which may still run on the aux stream
+        if (w.aux && p > 0 && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
+            return cuda_fail(e, "sy2sb look-ahead wait");
         // X = A22 V with A22 read from its lower triangle (only the lower triangle is updated)
         DgemmBatch gx{};
         gx.m = m; gx.n = NB; gx.k = m;
@@ -1632,13 +1639,37 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp, w.ticket);
         ypass2_kernel<<<nch, 128, 0, st>>>(m, Vp, w.Mp + (size_t)nch * NB * NB, Yp);
         // A22 -= [V Y] [Y V]^T, the tiles that reach the lower triangle
-        DgemmBatch gu{};
-        gu.m = m; gu.n = m; gu.k = 2 * NB;
-        gu.A = w.VYV; gu.lda = m; gu.B = Yp; gu.ldb = m; gu.C = A22; gu.ldc = lda;
-        gu.alpha = -1.0; gu.beta = 1.0; gu.lowc = 1;
-        rc = dgemm_ws(false, true, gu, 1, st, nullptr, 0);
-        if (rc != BSRG_OK) return rc;
+        if (!w.aux || m <= NB) {
+            DgemmBatch gu{};
+            gu.m = m; gu.n = m; gu.k = 2 * NB;
+            gu.A = VYV; gu.lda = m; gu.B = Yp; gu.ldb = m; gu.C = A22; gu.ldc = lda;
+            gu.alpha = -1.0; gu.beta = 1.0; gu.lowc = 1;
+            rc = dgemm_ws(false, true, gu, 1, st, nullptr, 0);
+            if (rc != BSRG_OK) return rc;
+        } else {
+            // look-ahead: the next panel's NB columns first, on this stream (the next panel QR follows
+            // them here), the rest of the trailing matrix on the aux stream, concurrently with that QR
+            if ((e = cudaEventRecord(w.ev_y, st)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(w.aux, w.ev_y, 0)) != cudaSuccess)
+                return cuda_fail(e, "sy2sb look-ahead");
+            DgemmBatch g1{};
+            g1.m = m; g1.n = NB; g1.k = 2 * NB;
+            g1.A = VYV; g1.lda = m; g1.B = Yp; g1.ldb = m; g1.C = A22; g1.ldc = lda;
+            g1.alpha = -1.0; g1.beta = 1.0;
+            rc = dgemm_ws(false, true, g1, 1, st, nullptr, 0);
+            if (rc != BSRG_OK) return rc;
+            const int m2 = m - NB;
+            DgemmBatch g2{};
+            g2.m = m2; g2.n = m2; g2.k = 2 * NB;
+            g2.A = VYV + NB; g2.lda = m; g2.B = Yp + NB; g2.ldb = m; g2.C = A22 + NB + lda * (long)NB; g2.ldc = lda;
+            g2.alpha = -1.0; g2.beta = 1.0; g2.lowc = 1;
+            rc = dgemm_ws(false, true, g2, 1, w.aux, nullptr, 0);
+            if (rc != BSRG_OK) return rc;
+            if ((e = cudaEventRecord(w.ev_c2, w.aux)) != cudaSuccess) return cuda_fail(e, "sy2sb look-ahead");
+        }
     }
+    if (w.aux && n > 2 * NB && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
+        return cuda_fail(e, "sy2sb look-ahead join");
     return cuda_fail(cudaGetLastError(), "sy2sb");
 }
 
@@ -1673,7 +1704,7 @@ static Syevd2Layout syevd2_layout(int n)
     L.dv = take(n);
     L.ev = take(n + 1);
     L.progress = take(n / 2 + 8);
-    L.VYV = take((size_t)n * 3 * NB);
+    L.VYV = take((size_t)n * 6 * NB);               // two [V | Y | V] buffers
     L.X = take((size_t)n * NB);
     L.T = take(NB * NB);
     L.Mp = take(((size_t)n / 128 + 2) * NB * NB);
@@ -1714,6 +1745,10 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     int *progress = (int *)(ws + L.progress);
     Sy2sbWork sw;
     sw.VYV = ws + L.VYV;
+    sw.VYV2 = sw.VYV + (size_t)n * 3 * NB;
+    sw.aux = getenv("BSRG_NO_LOOKAHEAD") ? nullptr : c->aux_stream;
+    sw.ev_y = c->aux_ev[0];
+    sw.ev_c2 = c->aux_ev[1];
     sw.X = ws + L.X;
     sw.T = ws + L.T;
     sw.Mp = ws + L.Mp;
