@@ -1413,8 +1413,9 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
 // ---------------------------------------------------------------------------
 // back-transformation of the stage-1 panels, Q1_GROUP panels at a time
 // ---------------------------------------------------------------------------
-constexpr int Q1_GROUP = 4;
+constexpr int Q1_GROUP = 8;
 constexpr int Q1W = Q1_GROUP * NB;     // columns of a merged block reflector
+constexpr int Q1H = 4 * NB;            // the unit of q1_tmerge_kernel: four panels
 
 struct Q1Panels {
     const double *V[Q1_GROUP];   // V of each panel (m_q x NB, ld m_q), null past the last panel
@@ -1432,70 +1433,41 @@ __global__ void q1_gather_kernel(int m0, Q1Panels P, double *Vg)
     Vg[idx] = v;
 }
 
-// T of the merged reflector from its Gram matrix G = Vg^T Vg and the panels' taus
-// (the diagonals of their T): T(c,c) = tau_c, T(0:c, c) = -tau_c T(0:c, 0:c) G(0:c, c)
-__global__ void __launch_bounds__(Q1W) q1_tfactor_kernel(const double *__restrict__ G, Q1Panels P,
-                                                         const double *__restrict__ T1, int p0, double *Tg)
-{
-    extern __shared__ __align__(16) double q1t_sm[];
-    double (*Ts)[Q1W + 1] = (double (*)[Q1W + 1])q1t_sm;
-    __shared__ double tau[Q1W], tmp[Q1W];
-    const int t = threadIdx.x;
-    {
-        const int q = t / NB, cc = t % NB;
-        tau[t] = P.V[q] ? T1[(size_t)(p0 + q) * NB * NB + cc + NB * cc] : 0.0;
-    }
-    for (int c = 0; c < Q1W; c++) Ts[t][c] = 0.0;
-    __syncthreads();
-    for (int c = 0; c < Q1W; c++) {
-        if (t < c) {
-            double sacc = 0.0;
-            for (int l = t; l < c; l++) sacc += Ts[t][l] * G[l + (long)Q1W * c];
-            tmp[t] = sacc;
-        }
-        __syncthreads();
-        if (t < c) Ts[t][c] = -tau[c] * tmp[t];
-        if (t == 0) Ts[c][c] = tau[c];
-        __syncthreads();
-    }
-    for (int c = 0; c < Q1W; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
-}
-
 // The same T from the panels' own T factors (T1) and the Gram blocks, merging pairs as
 // Q_a Q_b = I - [V_a V_b] [[T_a, -T_a G_ab T_b], [0, T_b]] [V_a V_b]^T (the block form of the
 // recurrence above): two 32 x 32 merges, then one of the 64-column halves; small products in
 // shared memory instead of 128 dependent column steps.
-constexpr int Q1M_SMEM = (Q1W * (Q1W + 1) + 64 * 65) * (int)sizeof(double);
+constexpr int Q1M_SMEM = (Q1H * (Q1H + 1) + 64 * 65) * (int)sizeof(double);
 
-__global__ void __launch_bounds__(Q1W) q1_tmerge_kernel(const double *__restrict__ G, Q1Panels P,
+// T of the merged reflector of four consecutive panels (q0 .. q0+3 of the group): G and the
+// output block T are Q1H x Q1H with leading dimension Q1W
+__global__ void __launch_bounds__(Q1H) q1_tmerge_kernel(const double *__restrict__ G, Q1Panels P, int q0,
                                                         const double *__restrict__ T1, int p0, double *Tg)
 {
     extern __shared__ __align__(16) double q1m_sm[];
-    double (*Ts)[Q1W + 1] = (double (*)[Q1W + 1])q1m_sm;               // Ts[r][c]
-    double (*W)[65] = (double (*)[65])(q1m_sm + Q1W * (Q1W + 1));
+    double (*Ts)[Q1H + 1] = (double (*)[Q1H + 1])q1m_sm;               // Ts[r][c]
+    double (*W)[65] = (double (*)[65])(q1m_sm + Q1H * (Q1H + 1));
     const int t = threadIdx.x;
-    for (int c = 0; c < Q1W; c++) Ts[t][c] = 0.0;
+    for (int c = 0; c < Q1H; c++) Ts[t][c] = 0.0;
     __syncthreads();
-    for (int q = 0; q < Q1_GROUP; q++) {
-        if (!P.V[q]) continue;
-        const double *Tp = T1 + (size_t)(p0 + q) * NB * NB;             // column-major NB x NB
-        for (int e = t; e < NB * NB; e += Q1W) Ts[q * NB + e % NB][q * NB + e / NB] = Tp[e];
+    for (int q = 0; q < 4; q++) {
+        if (!P.V[q0 + q]) continue;
+        const double *Tp = T1 + (size_t)(p0 + q0 + q) * NB * NB;        // column-major NB x NB
+        for (int e = t; e < NB * NB; e += Q1H) Ts[q * NB + e % NB][q * NB + e / NB] = Tp[e];
     }
     __syncthreads();
     // merges: width w = NB (pairs 0|1, 2|3), then 2 NB (halves)
-    for (int w = NB; w < Q1W; w *= 2) {
-        for (int a0 = 0; a0 < Q1W; a0 += 2 * w) {
+    for (int w = NB; w < Q1H; w *= 2) {
+        for (int a0 = 0; a0 < Q1H; a0 += 2 * w) {
             const int b0 = a0 + w;
-            // W = G(a rows, b cols) T_b
-            for (int e = t; e < w * w; e += Q1W) {
+            for (int e = t; e < w * w; e += Q1H) {
                 const int r = e % w, c = e / w;
                 double sacc = 0.0;
                 for (int k = 0; k <= c; k++) sacc += __ldg(G + (a0 + r) + (long)Q1W * (b0 + k)) * Ts[b0 + k][b0 + c];
                 W[r][c] = sacc;
             }
             __syncthreads();
-            // T(a rows, b cols) = -T_a W
-            for (int e = t; e < w * w; e += Q1W) {
+            for (int e = t; e < w * w; e += Q1H) {
                 const int r = e % w, c = e / w;
                 double sacc = 0.0;
                 for (int k = r; k < w; k++) sacc += Ts[a0 + r][a0 + k] * W[k][c];
@@ -1504,7 +1476,7 @@ __global__ void __launch_bounds__(Q1W) q1_tmerge_kernel(const double *__restrict
             __syncthreads();
         }
     }
-    for (int c = 0; c < Q1W; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
+    for (int c = 0; c < Q1H; c++) Tg[t + (long)Q1W * c] = Ts[t][c];
 }
 
 }  // namespace
@@ -1895,18 +1867,28 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             rc = dgemm(true, false, Q1W, Q1W, m0, 1.0, Vg, m0, Vg, m0, 0.0, Gq, Q1W, st, sw.gemm_ws,
                        sw.gemm_ws_doubles);
             if (rc != BSRG_OK) return rc;
-            if (getenv("BSRG_Q1_RECURRENCE")) {
-                constexpr int q1t_smem = Q1W * (Q1W + 1) * (int)sizeof(double);
-                if ((e = cudaFuncSetAttribute(q1_tfactor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              q1t_smem)) != cudaSuccess)
-                    return cuda_fail(e, "dsyevd Q1 smem");
-                q1_tfactor_kernel<<<1, Q1W, q1t_smem, st>>>(Gq, P, T1, p0, Tg);
-            } else {
-                if ((e = cudaFuncSetAttribute(q1_tmerge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              Q1M_SMEM)) != cudaSuccess)
-                    return cuda_fail(e, "dsyevd Q1 smem");
-                q1_tmerge_kernel<<<1, Q1W, Q1M_SMEM, st>>>(Gq, P, T1, p0, Tg);
+            // T of the merged 256-column reflector: each 128-column half by pairwise merges of its
+            // panels' T (q1_tmerge_kernel), then the off-diagonal block -T_a G_ab T_b by two GEMMs
+            if ((e = cudaFuncSetAttribute(q1_tmerge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          Q1M_SMEM)) != cudaSuccess)
+                return cuda_fail(e, "dsyevd Q1 smem");
+            if ((e = cudaMemsetAsync(Tg, 0, sizeof(double) * Q1W * Q1W, st)) != cudaSuccess)
+                return cuda_fail(e, "dsyevd Q1 T");
+            for (int hq = 0; hq < Q1_GROUP / 4; hq++) {
+                const long o = (long)hq * Q1H * (Q1W + 1);
+                q1_tmerge_kernel<<<1, Q1H, Q1M_SMEM, st>>>(Gq + o, P, 4 * hq, T1, p0, Tg + o);
             }
+            for (int w = Q1H; w < Q1W; w *= 2)
+                for (int a0 = 0; a0 < Q1W; a0 += 2 * w) {
+                    const int b0 = a0 + w;
+                    // Wq = G(a, b) T_b (w x w), then T(a, b) = -T_a Wq
+                    rc = dgemm(false, false, w, w, w, 1.0, Gq + a0 + (long)Q1W * b0, Q1W, Tg + b0 + (long)Q1W * b0,
+                               Q1W, 0.0, W2, w, st);
+                    if (rc == BSRG_OK)
+                        rc = dgemm(false, false, w, w, w, -1.0, Tg + a0 + (long)Q1W * a0, Q1W, W2, w, 0.0,
+                                   Tg + a0 + (long)Q1W * b0, Q1W, st);
+                    if (rc != BSRG_OK) return rc;
+                }
             double *Zs = Z + r0;
             rc = dgemm(true, false, Q1W, n, m0, 1.0, Vg, m0, Zs, ldz, 0.0, W1, Q1W, st, sw.gemm_ws,
                        sw.gemm_ws_doubles);
@@ -1915,7 +1897,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             if (rc != BSRG_OK) return rc;
         }
     }
-    stage_end(c, 13, 6 * ((np + Q1_GROUP - 1) / Q1_GROUP));
+    stage_end(c, 13, 10 * ((np + Q1_GROUP - 1) / Q1_GROUP));
     c->stage_flops[13] += fl_q1;
     c->stage_flops[6] += fl_band + fl_chase + fl_dc + fl_q2 + fl_q1;
     // device-side waits report through the flags
