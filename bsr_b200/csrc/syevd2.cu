@@ -983,6 +983,7 @@ __device__ __forceinline__ void q2r_mma(double &d0, double &d1, double a, double
 }
 
 // rows [a, b) of the strip between Z and the ring; 4 rows x 8 columns per 32 threads
+template <int RING = Q2R_RING>
 __device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int n, int c0, int ncl, int a, int b,
                                          bool store, int t0, int nthr)
 {
@@ -994,7 +995,7 @@ __device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int 
             const int ch = q >> 5, l = q & 31;
             const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
             if (row < b && row < n && col < ncl)
-                Z[row + ldz * (long)(c0 + col)] = ring[(row & (Q2R_RING - 1)) * Q2R_LD + col];
+                Z[row + ldz * (long)(c0 + col)] = ring[(row & (RING - 1)) * Q2R_LD + col];
         }
         return;
     }
@@ -1011,7 +1012,7 @@ __device__ __forceinline__ void q2r_xfer(double *ring, double *Z, long ldz, int 
         for (int u = 0; u < 16; u++) {
             const int q = q0 + u * nthr, ch = q >> 5, l = q & 31;
             const int row = a + (ch >> 2) * 4 + (l >> 3), col = (ch & 3) * 8 + (l & 7);
-            if (q < total && row < b) ring[(row & (Q2R_RING - 1)) * Q2R_LD + col] = v[u];
+            if (q < total && row < b) ring[(row & (RING - 1)) * Q2R_LD + col] = v[u];
         }
     }
 }
@@ -1195,14 +1196,13 @@ __global__ void __launch_bounds__(Q2R_W * 32, 1) q2r_apply_kernel(int n, int S, 
 // so that no fragment load needs a mask, and T; the two halves depend only on the
 // same half of the neighbouring groups (their columns are disjoint).
 // ---------------------------------------------------------------------------
-constexpr int Q2P_G = 4;                                        // groups (pairs) per round
 constexpr int Q2P_PAIR = (2 * NB + 2 * NB) * Q2R_LD;            // doubles per pair: V band (64 rows), T, W
-constexpr int Q2P_SMEM = (Q2R_RING * Q2R_LD + Q2P_G * Q2P_PAIR) * (int)sizeof(double);
-static_assert(Q2R_RING >= 2 * NB * Q2P_G, "ring size");
+template <int G, int RING> constexpr int q2p_smem() { return (RING * Q2R_LD + G * Q2P_PAIR) * (int)sizeof(double); }
 
 __device__ __forceinline__ void pair_sync(int p) { asm volatile("bar.sync %0, 64;" ::"r"(p + 1)); }
 
 // rows [a, b) of the 16 columns of half h between Z and the ring (one warp)
+template <int RING>
 __device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int n, int c0, int ncl, int h, int a,
                                          int b, bool store, int lane)
 {
@@ -1214,7 +1214,7 @@ __device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int 
             const int ch = q >> 5, l = q & 31;
             const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
             if (row < b && row < n && col < ncl)
-                Z[row + ldz * (long)(c0 + col)] = ring[(row & (Q2R_RING - 1)) * Q2R_LD + col];
+                Z[row + ldz * (long)(c0 + col)] = ring[(row & (RING - 1)) * Q2R_LD + col];
         }
         return;
     }
@@ -1231,31 +1231,34 @@ __device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int 
         for (int u = 0; u < 16; u++) {
             const int q = q0 + u * 32, ch = q >> 5, l = q & 31;
             const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
-            if (q < total && row < b) ring[(row & (Q2R_RING - 1)) * Q2R_LD + col] = v[u];
+            if (q < total && row < b) ring[(row & (RING - 1)) * Q2R_LD + col] = v[u];
         }
     }
 }
 
-__global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, int ncol,
+// G groups per round, a ring of RING rows (a power of two >= 2 NB G)
+template <int G, int RING>
+__global__ void __launch_bounds__(G * 64, 1) q2p_apply_kernel(int n, int S, int ncol,
                                                                  const double *__restrict__ V2,
                                                                  const double *__restrict__ Tq, double *Z,
                                                                  long ldz, int *err)
 {
+    static_assert(RING >= 2 * NB * G && (RING & (RING - 1)) == 0, "ring size");
     extern __shared__ __align__(16) double q2p_sm[];
-    __shared__ volatile int prog[Q2P_G][2];
+    __shared__ volatile int prog[G][2];
     double *ring = q2p_sm;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, lr = lane >> 2, lc = lane & 3;
     const int pr = wid >> 1, h = wid & 1;                        // pair (group slot), half
-    double *Vd = q2p_sm + Q2R_RING * Q2R_LD + pr * Q2P_PAIR;     // V(r, q) at r LD + q, 64 rows
+    double *Vd = q2p_sm + RING * Q2R_LD + pr * Q2P_PAIR;     // V(r, q) at r LD + q, 64 rows
     double *Tsm = Vd + 2 * NB * Q2R_LD;                          // T(q, l) at q + LD l
     double *Wb = Tsm + NB * Q2R_LD;                              // W(q, c) at q LD + c, this half's columns
     const int c0 = blockIdx.x * 32, ncl = min(32, ncol - c0);
     const int ng = (n - 2 + NB - 1) / NB;
-    for (int g0 = ng - 1; g0 >= 0; g0 -= Q2P_G) {
-        const int gl = max(g0 - Q2P_G + 1, 0), nw = g0 - gl + 1;
+    for (int g0 = ng - 1; g0 >= 0; g0 -= G) {
+        const int gl = max(g0 - G + 1, 0), nw = g0 - gl + 1;
         __syncthreads();
-        q2r_xfer(ring, Z, ldz, n, c0, ncl, gl * NB + 1, g0 * NB + 1 + 2 * NB, false, tid, blockDim.x);
-        if (tid < 2 * Q2P_G) prog[tid >> 1][tid & 1] = 0;
+        q2r_xfer<RING>(ring, Z, ldz, n, c0, ncl, gl * NB + 1, g0 * NB + 1 + 2 * NB, false, tid, blockDim.x);
+        if (tid < 2 * G) prog[tid >> 1][tid & 1] = 0;
         __syncthreads();
         const int ilast = sweep_steps(n, gl * NB);
         if (pr < nw) {
@@ -1269,14 +1272,14 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
                     while (prog[pr - 1][h] < need)
                         if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
                 } else if (nw > 1) {
-                    const int need = min(i + nw - Q2R_RING / NB + 1, ilast);
+                    const int need = min(i + nw - RING / NB + 1, ilast);
                     while (need > 0 && prog[nw - 1][h] < need)
                         if (gtime() - t0 > WAIT_NS) { atomicExch(err, 3); break; }
                 }
                 __threadfence_block();
                 const int top = (g + i) * NB + 1;
                 const int nrow = min(2 * NB - 1, n - top);
-                if (pr == 0 && i > 0) q2p_xfer(ring, Z, ldz, n, c0, ncl, h, top + NB, top + 2 * NB, false, lane);
+                if (pr == 0 && i > 0) q2p_xfer<RING>(ring, Z, ldz, n, c0, ncl, h, top + NB, top + 2 * NB, false, lane);
                 // ---- the pair stages the block's V band and T (after both finished the previous block) ----
                 pair_sync(pr);
                 {
@@ -1316,7 +1319,7 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
 #pragma unroll
                 for (int ks = 0; ks < 16; ks++) {
                     const int r = 4 * ks + lc;
-                    const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+                    const double *rrow = ring + ((top + r) & (RING - 1)) * Q2R_LD + 16 * h;
                     const double bz0 = rrow[lr], bz1 = rrow[8 + lr];
 #pragma unroll
                     for (int mt = 0; mt < 4; mt++) {
@@ -1363,7 +1366,7 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
 #pragma unroll
                     for (int a = 0; a < 4; a++) {
                         const int r = 8 * (4 * mh + a) + lr;
-                        const double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+                        const double *rrow = ring + ((top + r) & (RING - 1)) * Q2R_LD + 16 * h;
 #pragma unroll
                         for (int nt = 0; nt < 2; nt++) {
                             acc[a][nt][0] = rrow[8 * nt + 2 * lc];
@@ -1388,7 +1391,7 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
                     for (int a = 0; a < 4; a++) {
                         const int r = 8 * (4 * mh + a) + lr;
                         if (r < nrow) {
-                            double *rrow = ring + ((top + r) & (Q2R_RING - 1)) * Q2R_LD + 16 * h;
+                            double *rrow = ring + ((top + r) & (RING - 1)) * Q2R_LD + 16 * h;
 #pragma unroll
                             for (int nt = 0; nt < 2; nt++) {
                                 rrow[8 * nt + 2 * lc] = acc[a][nt][0];
@@ -1398,7 +1401,7 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
                     }
                 }
                 __syncwarp();
-                if (pr == nw - 1) q2p_xfer(ring, Z, ldz, n, c0, ncl, h, top, top + NB, true, lane);
+                if (pr == nw - 1) q2p_xfer<RING>(ring, Z, ldz, n, c0, ncl, h, top, top + NB, true, lane);
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0) prog[pr][h] = i + 1;
@@ -1406,7 +1409,7 @@ __global__ void __launch_bounds__(Q2P_G * 64, 1) q2p_apply_kernel(int n, int S, 
         }
         __syncthreads();
         const int rdone = ilast > 0 ? (gl + ilast) * NB + 1 : gl * NB + 1;
-        q2r_xfer(ring, Z, ldz, n, c0, ncl, rdone, n, true, tid, blockDim.x);
+        q2r_xfer<RING>(ring, Z, ldz, n, c0, ncl, rdone, n, true, tid, blockDim.x);
     }
 }
 
@@ -1837,10 +1840,22 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2r_apply_kernel<<<(unsigned)((n + 31) / 32), Q2R_W * 32, Q2R_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
         } else {
-            if ((e = cudaFuncSetAttribute(q2p_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2P_SMEM)) !=
-                cudaSuccess)
-                return cuda_fail(e, "dsyevd Q2 smem");
-            q2p_apply_kernel<<<(unsigned)((n + 31) / 32), Q2P_G * 64, Q2P_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
+            // four groups per round and one CTA per SM, or (BSRG_Q2_TWO) two groups and two CTAs per SM
+            if (getenv("BSRG_Q2_TWO")) {
+                constexpr int sm2 = q2p_smem<2, 128>();
+                if ((e = cudaFuncSetAttribute(q2p_apply_kernel<2, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              sm2)) != cudaSuccess)
+                    return cuda_fail(e, "dsyevd Q2 smem");
+                q2p_apply_kernel<2, 128><<<(unsigned)((n + 31) / 32), 2 * 64, sm2, st>>>(n, S, n, V2, Tq, Z, ldz,
+                                                                                        sw.err);
+            } else {
+                constexpr int sm4 = q2p_smem<4, 256>();
+                if ((e = cudaFuncSetAttribute(q2p_apply_kernel<4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              sm4)) != cudaSuccess)
+                    return cuda_fail(e, "dsyevd Q2 smem");
+                q2p_apply_kernel<4, 256><<<(unsigned)((n + 31) / 32), 4 * 64, sm4, st>>>(n, S, n, V2, Tq, Z, ldz,
+                                                                                        sw.err);
+            }
         }
         // per block and column: W = V^T Z (2 NB nv), T W (~NB nv), Z -= V W (2 NB nv)
         double nvsum = 0.0;
