@@ -367,6 +367,9 @@ static int solve_channels_batched(bsrg_ctx *c, cusolverDnParams_t params, const 
 
 using namespace bsrg;
 
+// smallest dense problem for which diag_hd uses the library's eigensolver by default
+constexpr int kOwnEigMin = 1 << 30;
+
 // scc == NULL: the block-diagonal overlap (diag_ovl /= 0); otherwise the generalized
 // branch with the channel-channel overlap blocks of scc (diag_ovl = 0)
 static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lch, const double *hcc,
@@ -401,8 +404,12 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
     // the eigenvalues, which the Rayleigh quotients below then resolve.
     const bool refine = want_vectors && c->refine;
     const char *eig_env = getenv("BSRG_EIG");
-    // the library's two-stage eigensolver (syevd2.cu) or cuSOLVER's syevd
-    const bool own_eig = want_vectors && eig_env && strcmp(eig_env, "own") == 0;
+    // the library's two-stage eigensolver (syevd2.cu) or cuSOLVER's syevd: BSRG_EIG=own or =lib
+    // chooses; otherwise the library's from kOwnEigMin rows up (where it was measured faster)
+    int khm_bound = 0;
+    for (int ich = 0; ich < nch; ich++) khm_bound += nsolv[ich];
+    const bool own_eig = want_vectors && khm_bound <= 10240 &&
+                         (eig_env ? strcmp(eig_env, "own") == 0 : khm_bound >= kOwnEigMin);
     std::vector<BlockMap> bmap;
     for (int ic = 1; ic < nch; ic++)
         for (int jc = 0; jc < ic; jc++) bmap.push_back({ic, jc});
