@@ -1170,7 +1170,9 @@ int bsrg_ctx_create(int device, void *stream, bsrg_ctx **out)
     cusolverDnSetStream(c->solver, c->stream);
     cudaEventCreateWithFlags(&c->ev_stage, cudaEventDisableTiming);
     cudaEventRecord(c->ev_stage, c->stream);
-    if (cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking) != cudaSuccess ||
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&c->aux_stream, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->aux_ev[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->aux_ev[1], cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();

@@ -51,7 +51,7 @@ struct bsrg_ctx {
     size_t rf_cap;                           //   (doubles held)
     int rf_n;                                //   (pairs recorded)
     int chan_fallbacks;                      // channel solves redone on the library path (orthogonality check)
-    cudaStream_t aux_stream;                 // second stream of the band reduction's look-ahead (or 0)
+    cudaStream_t aux_stream;                 // high-priority second stream (the band reduction's panels), or 0
     cudaEvent_t aux_ev[2];                   //   its hand-off events
 };
 

@@ -1549,21 +1549,19 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         }
         cudaGetLastError();
     }
-    size_t voff = 0;
-    int p = 0;
-    for (int j = 0; j + NB < n; j += NB, p++) {
-        const int m = n - j - NB;
+    // factorise panel p (columns j = p NB ..) on stream sq; its V goes to the [V | Y | V] buffer of p's parity
+    auto factor_panel = [&](int p, size_t voff, cudaStream_t sq) -> int {
+        const int j = p * NB, m = n - j - NB;
         int G = (m + PQ_ROWS - 1) / PQ_ROWS;
         G = std::max(1, std::min(G, std::max(1, m / NB)));      // CTA 0 holds the NB pivot rows
         const int rpc = (m + G - 1) / G;
         if (rpc > PQ_ROWS) { set_error("sy2sb: panel of %d rows does not fit", m); return BSRG_ERR_ARG; }
-        double *VYV = (p & 1) && w.aux ? w.VYV2 : w.VYV;
         PanelArgs a;
         a.P = A + (j + NB) + lda * (long)j;
         a.ldp = lda;
         a.m = m;
         a.rpc = rpc;
-        a.V = VYV;
+        a.V = (p & 1) && w.aux ? w.VYV2 : w.VYV;
         a.Vs = Vsave + voff;
         a.T = w.T;
         a.Ts = Tsave + (size_t)p * NB * NB;
@@ -1580,7 +1578,7 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
             cfg.gridDim = dim3((unsigned)Gc);
             cfg.blockDim = dim3(PQ_NT);
             cfg.dynamicSmemBytes = (size_t)smem_c;
-            cfg.stream = st;
+            cfg.stream = sq;
             cudaLaunchAttribute attr[1];
             attr[0].id = cudaLaunchAttributeClusterDimension;
             attr[0].val.clusterDim.x = (unsigned)Gc;
@@ -1592,23 +1590,32 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
                 return cuda_fail(e, "sy2sb panel (cluster)");
         } else {
             void *args[] = {&a};
-            if ((e = cudaLaunchCooperativeKernel((const void *)panel_qr_kernel, G, PQ_NT, args, smem, st)) !=
+            if ((e = cudaLaunchCooperativeKernel((const void *)panel_qr_kernel, G, PQ_NT, args, smem, sq)) !=
                 cudaSuccess)
                 return cuda_fail(e, "sy2sb panel");
         }
-        voff += (size_t)m * NB;
-        // trailing update of A22 = A(j+NB:, j+NB:) (m x m, full symmetric storage)
+        return BSRG_OK;
+    };
+    size_t voff = 0;
+    int rc = n > NB ? factor_panel(0, 0, st) : BSRG_OK;
+    if (rc != BSRG_OK) return rc;
+    bool qr_on_aux = false;                       // the current panel was factorised on the aux stream
+    int p = 0;
+    for (int j = 0; j + NB < n; j += NB, p++) {
+        const int m = n - j - NB;
+        double *VYV = (p & 1) && w.aux ? w.VYV2 : w.VYV;
         double *A22 = A + (j + NB) + lda * (long)(j + NB);
         double *Vp = VYV, *Yp = VYV + (long)m * NB;
-        // X = A22 V needs the previous panel's trailing update, which may still run on the aux stream
-        if (w.aux && p > 0 && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
+        const size_t voff_next = voff + (size_t)m * NB;
+        const bool has_next = j + 2 * NB < n;
+        if (qr_on_aux && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
             return cuda_fail(e, "sy2sb look-ahead wait");
         // X = A22 V with A22 read from its lower triangle (only the lower triangle is updated)
         DgemmBatch gx{};
         gx.m = m; gx.n = NB; gx.k = m;
         gx.A = A22; gx.lda = lda; gx.B = Vp; gx.ldb = m; gx.C = w.X; gx.ldc = m;
         gx.alpha = 1.0; gx.beta = 0.0; gx.syma = 1;
-        int rc = dgemm_ws(false, false, gx, 1, st, w.gemm_ws, w.gemm_ws_doubles);
+        rc = dgemm_ws(false, false, gx, 1, st, w.gemm_ws, w.gemm_ws_doubles);
         if (rc != BSRG_OK) return rc;
         const int nch = (m + 127) / 128;
         ypass1_kernel<<<nch, 128, YP1_SMEM, st>>>(m, w.X, Vp, w.T, Yp, w.Mp, w.ticket);
@@ -1620,30 +1627,40 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
             gu.A = VYV; gu.lda = m; gu.B = Yp; gu.ldb = m; gu.C = A22; gu.ldc = lda;
             gu.alpha = -1.0; gu.beta = 1.0; gu.lowc = 1;
             rc = dgemm_ws(false, true, gu, 1, st, nullptr, 0);
+            if (rc == BSRG_OK && has_next) rc = factor_panel(p + 1, voff_next, st);
             if (rc != BSRG_OK) return rc;
+            qr_on_aux = false;
         } else {
-            // look-ahead: the next panel's NB columns first, on this stream (the next panel QR follows
-            // them here), the rest of the trailing matrix on the aux stream, concurrently with that QR
-            if ((e = cudaEventRecord(w.ev_y, st)) != cudaSuccess ||
-                (e = cudaStreamWaitEvent(w.aux, w.ev_y, 0)) != cudaSuccess)
-                return cuda_fail(e, "sy2sb look-ahead");
+            // look-ahead: the next panel's NB columns first; the next panel is then factorised on the
+            // high-priority aux stream while the rest of the trailing matrix is updated here, so the
+            // panel's few CTAs are placed before the update's fill the machine
             DgemmBatch g1{};
             g1.m = m; g1.n = NB; g1.k = 2 * NB;
             g1.A = VYV; g1.lda = m; g1.B = Yp; g1.ldb = m; g1.C = A22; g1.ldc = lda;
             g1.alpha = -1.0; g1.beta = 1.0;
             rc = dgemm_ws(false, true, g1, 1, st, nullptr, 0);
             if (rc != BSRG_OK) return rc;
+            qr_on_aux = false;
+            if (has_next) {
+                if ((e = cudaEventRecord(w.ev_y, st)) != cudaSuccess ||
+                    (e = cudaStreamWaitEvent(w.aux, w.ev_y, 0)) != cudaSuccess)
+                    return cuda_fail(e, "sy2sb look-ahead");
+                rc = factor_panel(p + 1, voff_next, w.aux);
+                if (rc != BSRG_OK) return rc;
+                if ((e = cudaEventRecord(w.ev_c2, w.aux)) != cudaSuccess) return cuda_fail(e, "sy2sb look-ahead");
+                qr_on_aux = true;
+            }
             const int m2 = m - NB;
             DgemmBatch g2{};
             g2.m = m2; g2.n = m2; g2.k = 2 * NB;
             g2.A = VYV + NB; g2.lda = m; g2.B = Yp + NB; g2.ldb = m; g2.C = A22 + NB + lda * (long)NB; g2.ldc = lda;
             g2.alpha = -1.0; g2.beta = 1.0; g2.lowc = 1;
-            rc = dgemm_ws(false, true, g2, 1, w.aux, nullptr, 0);
+            rc = dgemm_ws(false, true, g2, 1, st, nullptr, 0);
             if (rc != BSRG_OK) return rc;
-            if ((e = cudaEventRecord(w.ev_c2, w.aux)) != cudaSuccess) return cuda_fail(e, "sy2sb look-ahead");
         }
+        voff = voff_next;
     }
-    if (w.aux && n > 2 * NB && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
+    if (qr_on_aux && (e = cudaStreamWaitEvent(st, w.ev_c2, 0)) != cudaSuccess)
         return cuda_fail(e, "sy2sb look-ahead join");
     return cuda_fail(cudaGetLastError(), "sy2sb");
 }
