@@ -1201,38 +1201,39 @@ template <int G, int RING> constexpr int q2p_smem() { return (RING * Q2R_LD + G 
 
 __device__ __forceinline__ void pair_sync(int p) { asm volatile("bar.sync %0, 64;" ::"r"(p + 1)); }
 
-// rows [a, b) of the 16 columns of half h between Z and the ring (one warp)
+// rows [a, a + 32) (cut at b) of the 16 columns of half h: chunks of 4 rows x 8 columns, lane l of
+// chunk u holds row a + 4 (u >> 1) + (l >> 3), column 16 h + 8 (u & 1) + (l & 7)
+__device__ __forceinline__ void q2p_fetch(double (&v)[16], const double *Z, long ldz, int n, int c0, int ncl, int h,
+                                          int a, int b, int lane)
+{
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int row = a + (u >> 1) * 4 + (lane >> 3), col = 16 * h + (u & 1) * 8 + (lane & 7);
+        v[u] = (row < b && row < n && col < ncl) ? Z[row + ldz * (long)(c0 + col)] : 0.0;
+    }
+}
+
 template <int RING>
-__device__ __forceinline__ void q2p_xfer(double *ring, double *Z, long ldz, int n, int c0, int ncl, int h, int a,
-                                         int b, bool store, int lane)
+__device__ __forceinline__ void q2p_put(const double (&v)[16], double *ring, int h, int a, int b, int lane)
+{
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+        const int row = a + (u >> 1) * 4 + (lane >> 3), col = 16 * h + (u & 1) * 8 + (lane & 7);
+        if (row < b) ring[(row & (RING - 1)) * Q2R_LD + col] = v[u];
+    }
+}
+
+// rows [a, b) of the 16 columns of half h from the ring back to Z (one warp)
+template <int RING>
+__device__ __forceinline__ void q2p_store(const double *ring, double *Z, long ldz, int n, int c0, int ncl, int h,
+                                          int a, int b, int lane)
 {
     if (b <= a) return;
-    const int nchunk = ((b - a + 3) / 4) * 2;          // chunks of 4 rows x 8 columns, 2 column chunks
-    const int total = nchunk * 32;
-    if (store) {
-        for (int q = lane; q < total; q += 32) {
-            const int ch = q >> 5, l = q & 31;
-            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
-            if (row < b && row < n && col < ncl)
-                Z[row + ldz * (long)(c0 + col)] = ring[(row & (RING - 1)) * Q2R_LD + col];
-        }
-        return;
-    }
-    // loads in batches of 16 per lane (a 32-row window half is exactly one batch), issued before use
-    for (int q0 = lane; q0 < total; q0 += 16 * 32) {
-        double v[16];
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-            const int q = q0 + u * 32, ch = q >> 5, l = q & 31;
-            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
-            v[u] = (q < total && row < b && row < n && col < ncl) ? Z[row + ldz * (long)(c0 + col)] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 16; u++) {
-            const int q = q0 + u * 32, ch = q >> 5, l = q & 31;
-            const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
-            if (q < total && row < b) ring[(row & (RING - 1)) * Q2R_LD + col] = v[u];
-        }
+    const int total = ((b - a + 3) / 4) * 2 * 32;      // chunks of 4 rows x 8 columns, 2 column chunks
+    for (int q = lane; q < total; q += 32) {
+        const int ch = q >> 5, l = q & 31;
+        const int row = a + (ch >> 1) * 4 + (l >> 3), col = 16 * h + (ch & 1) * 8 + (l & 7);
+        if (row < b && row < n && col < ncl) Z[row + ldz * (long)(c0 + col)] = ring[(row & (RING - 1)) * Q2R_LD + col];
     }
 }
 
@@ -1254,6 +1255,8 @@ __global__ void __launch_bounds__(G * 64, 1) q2p_apply_kernel(int n, int S, int 
     double *Wb = Tsm + NB * Q2R_LD;                              // W(q, c) at q LD + c, this half's columns
     const int c0 = blockIdx.x * 32, ncl = min(32, ncol - c0);
     const int ng = (n - 2 + NB - 1) / NB;
+    // entries of the dense band outside the parallelogram stay zero; the band is rewritten per block
+    for (int e = 32 * h + lane; e < 2 * NB * Q2R_LD; e += 64) Vd[e] = 0.0;
     for (int g0 = ng - 1; g0 >= 0; g0 -= G) {
         const int gl = max(g0 - G + 1, 0), nw = g0 - gl + 1;
         __syncthreads();
@@ -1265,6 +1268,25 @@ __global__ void __launch_bounds__(G * 64, 1) q2p_apply_kernel(int n, int S, int 
             const int g = g0 - pr;
             const int imax = sweep_steps(n, g * NB);
             const int iprev = pr > 0 ? sweep_steps(n, (g + 1) * NB) : 0;
+            // the next block's reflectors and T, and (pair 0) the next step's new rows of Z, are loaded
+            // one step ahead into registers so that their latency hides behind the current block
+            double vq[NB / 2], tl[NB / 2], zn[16];
+            auto fetch_vt = [&](int i) {
+                const int nv = q2_nvalid(n, g, i);
+                const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;
+                const double *T = Tq + ((long)g * S + i) * NB * NB;
+#pragma unroll
+                for (int u = 0; u < NB / 2; u++) {
+                    const int q = 16 * h + u;
+                    vq[u] = q < nv ? __ldg(Vblk + (long)q * S * NB + lane) : 0.0;
+                    tl[u] = __ldg(T + lane + NB * q);               // column l = q of T
+                }
+            };
+            if (imax > 0) fetch_vt(0);
+            if (pr == 0 && imax > 1) {
+                const int t1 = (g + 1) * NB + 1;
+                q2p_fetch(zn, Z, ldz, n, c0, ncl, h, t1 + NB, t1 + 2 * NB, lane);
+            }
             for (int i = 0; i < imax; i++) {
                 const unsigned long long t0 = gtime();
                 if (pr > 0) {
@@ -1279,34 +1301,29 @@ __global__ void __launch_bounds__(G * 64, 1) q2p_apply_kernel(int n, int S, int 
                 __threadfence_block();
                 const int top = (g + i) * NB + 1;
                 const int nrow = min(2 * NB - 1, n - top);
-                if (pr == 0 && i > 0) q2p_xfer<RING>(ring, Z, ldz, n, c0, ncl, h, top + NB, top + 2 * NB, false, lane);
+                if (pr == 0 && i > 0) {
+                    q2p_put<RING>(zn, ring, h, top + NB, top + 2 * NB, lane);
+                    if (i + 1 < imax) q2p_fetch(zn, Z, ldz, n, c0, ncl, h, top + 2 * NB, top + 3 * NB, lane);
+                }
                 // ---- the pair stages the block's V band and T (after both finished the previous block) ----
                 pair_sync(pr);
                 {
-                    const int nv = q2_nvalid(n, g, i);
-                    const double *Vblk = V2 + ((long)(g * NB) * S + i) * NB;
-                    const double *T = Tq + ((long)g * S + i) * NB * NB;
-                    double vq[NB / 2], tl[NB / 2];
-#pragma unroll
-                    for (int u = 0; u < NB / 2; u++) {
-                        const int q = 16 * h + u;
-                        vq[u] = q < nv ? __ldg(Vblk + (long)q * S * NB + lane) : 0.0;
-                        tl[u] = __ldg(T + lane + NB * q);               // column l = q of T
-                    }
                     // compact V(q, t) into the W area first (free until W is formed): consecutive stores
                     double *Vc = Wb;
 #pragma unroll
                     for (int u = 0; u < NB / 2; u++) {
                         const int q = 16 * h + u;
-                        Vc[q * 34 + lane] = vq[u];
+                        Vc[q * 33 + lane] = vq[u];
                         Tsm[lane + Q2R_LD * q] = tl[u];
                     }
+                    if (i + 1 < imax) fetch_vt(i + 1);
                     pair_sync(pr);
-                    // the dense band V(r, q) = Vc(q, r - q), a row's 32 entries by 32 consecutive threads
-                    // (reads Vc at 33 q + r: distinct banks)
-                    for (int e = 32 * h + lane; e < 2 * NB * NB; e += 64) {
-                        const int rr = e >> 5, q = e & 31, t = rr - q;
-                        Vd[rr * Q2R_LD + q] = (t >= 0 && t < NB && rr < nrow) ? Vc[q * 34 + t] : 0.0;
+                    // the band V(q + t, q) = Vc(q, t): lane q, 16 values of t per warp (Vc at 33 q + t and
+                    // Vd at 37 q + 36 t are distinct banks across a half-warp)
+#pragma unroll
+                    for (int u = 0; u < NB / 2; u++) {
+                        const int t = 16 * h + u, rr = lane + t;
+                        Vd[rr * Q2R_LD + lane] = rr < nrow ? Vc[lane * 33 + t] : 0.0;
                     }
                 }
                 pair_sync(pr);
@@ -1401,7 +1418,7 @@ __global__ void __launch_bounds__(G * 64, 1) q2p_apply_kernel(int n, int S, int 
                     }
                 }
                 __syncwarp();
-                if (pr == nw - 1) q2p_xfer<RING>(ring, Z, ldz, n, c0, ncl, h, top, top + NB, true, lane);
+                if (pr == nw - 1) q2p_store<RING>(ring, Z, ldz, n, c0, ncl, h, top, top + NB, lane);
                 __threadfence_block();
                 __syncwarp();
                 if (lane == 0) prog[pr][h] = i + 1;
