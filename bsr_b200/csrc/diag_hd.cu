@@ -367,8 +367,10 @@ static int solve_channels_batched(bsrg_ctx *c, cusolverDnParams_t params, const 
 
 using namespace bsrg;
 
-// smallest dense problem for which diag_hd uses the library's eigensolver by default
-constexpr int kOwnEigMin = 1 << 30;
+// smallest dense problem (by its row bound) for which diag_hd uses the library's eigensolver by
+// default: measured against cuSOLVER's syevd on a B200, 399 vs 421 ms at 7810 rows, 258 vs 228 ms
+// at 6000 and 154 vs 114 ms at 4500
+constexpr int kOwnEigMin = 7000;
 
 // scc == NULL: the block-diagonal overlap (diag_ovl /= 0); otherwise the generalized
 // branch with the channel-channel overlap blocks of scc (diag_ovl = 0)

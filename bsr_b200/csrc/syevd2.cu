@@ -728,6 +728,184 @@ __global__ void __launch_bounds__(32 * K) sb2st2_kernel(Sb2stArgs a)
     }
 }
 
+// The register form with a helper warp: warp 0 computes and stores each step, warp 1 publishes
+// the step (fence, then the progress counter) and polls the previous sweep's counter, so that
+// neither the release fence nor the poll's round trip to L2 sits between two steps of warp 0.
+// Warp 0 hands a step over through the shared counter `done` after a block-scope fence; warp 1
+// observes it, and its device-scope fence orders warp 0's stores before the progress counter
+// (the fence is cumulative over what warp 1 has observed).  The previous sweep's progress goes
+// the other way: warp 1 reads it, fences, and posts it in `seen`.  (A sleep between polls, of
+// even 8 ns, measured slower: the sleep's granularity is coarse.)
+__global__ void __launch_bounds__(64) sb2st3_kernel(Sb2stArgs a)
+{
+    __shared__ double Ts[NB][NB + 1], Cs[NB][NB + 1];
+    __shared__ double vs[NB], ws2[NB];
+    __shared__ volatile int done, seen, quit;
+    const int t = threadIdx.x & 31, w = threadIdx.x >> 5, n = a.n;
+    double *AB = a.AB;
+    auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
+    for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
+        const int nst = sweep_steps(n, j);
+        const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
+        if (threadIdx.x == 0) { done = 0; seen = j > 0 ? 0 : 1 << 30; quit = 0; }
+        __syncthreads();
+        if (w == 1) {
+            // ---- helper: publish warp 0's steps, watch the previous sweep ----
+            if (t == 0) {
+                int pub = 0, sv = j > 0 ? 0 : 1 << 30;
+                unsigned long long t0 = gtime();
+                while (pub < nst) {
+                    const int d = done;
+                    if (d > pub) {
+                        __threadfence();
+                        *(volatile int *)(a.progress + j) = d;
+                        pub = d;
+                        t0 = gtime();
+                        continue;
+                    }
+                    if (quit) break;
+                    if (sv < nprev) {
+                        const int v = *(volatile int *)(a.progress + (j - 1));
+                        if (v > sv) {
+                            __threadfence();
+                            sv = v;
+                            seen = v;
+                            t0 = gtime();
+                            continue;
+                        }
+                    }
+                    if (*(volatile int *)a.err) { quit = 1; break; }
+                    if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); quit = 1; break; }
+                }
+            }
+            __syncthreads();
+            if (*(volatile int *)a.err) return;
+            continue;
+        }
+        // ---- warp 0: the steps ----
+        // wait until the helper has seen the previous sweep complete `need` steps
+        auto wait_prev = [&](int need) -> bool {
+            if (t == 0) {
+                const unsigned long long t0 = gtime();
+                while (seen < need) {
+                    if (quit) break;
+                    if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); quit = 1; break; }
+                }
+                __threadfence_block();
+            }
+            __syncwarp();
+            return !quit;
+        };
+        auto load_blocks = [&](int i, double *Dr, double *Br) {
+            const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+            const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+#pragma unroll
+            for (int c = 0; c < NB; c++) Dr[c] = (t < L && c <= t) ? __ldcg(at(r0 + t, r0 + c)) : 0.0;
+#pragma unroll
+            for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
+        };
+        double Dr[NB], Br[NB];
+        bool ok = wait_prev(min(3, nprev));
+        if (ok) load_blocks(0, Dr, Br);
+        for (int i = 0; ok && i < nst; i++) {
+            const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+            const int col = i == 0 ? j : r0 - NB;
+            const int nl = r0 - col - 1;
+            const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+            const double xl = i == 0 ? (t < L ? __ldcg(at(r0 + t, col)) : 0.0) : Cs[t][0];
+            // ---- the reflector ----
+            double sig = (t >= 1 && t < L) ? xl * xl : 0.0;
+            for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+            const double alpha = __shfl_sync(0xffffffffu, xl, 0);
+            double tau = 0.0, scale = 0.0, beta = alpha;
+            if (sig != 0.0) {
+                beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+                tau = (beta - alpha) / beta;
+                scale = 1.0 / (alpha - beta);
+            }
+            const double v = t == 0 ? 1.0 : (t < L ? xl * scale : 0.0);
+            vs[t] = v;
+            a.V2[((long)j * a.S + i) * NB + t] = v;
+            if (t == 0) a.tau2[(long)j * a.S + i] = tau;
+            if (t < L) *at(r0 + t, col) = t == 0 ? beta : 0.0;
+            __syncwarp();
+            if (tau != 0.0) {
+                if (nl > 0) {
+                    if (t < nl) {
+                        double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+                        for (int q = 0; q < NB; q += 2) {
+                            w0 = fma(vs[q], Cs[q][t + 1], w0);
+                            w1 = fma(vs[q + 1], Cs[q + 1][t + 1], w1);
+                        }
+                        ws2[t] = tau * (w0 + w1);
+                    }
+                    __syncwarp();
+                    if (t < L) {
+#pragma unroll
+                        for (int c = 0; c < NB - 1; c++)
+                            if (c < nl) *at(r0 + t, col + 1 + c) = fma(-v, ws2[c], Cs[t][c + 1]);
+                    }
+                    __syncwarp();
+                }
+#pragma unroll
+                for (int c = 0; c < NB; c++) Ts[t][c] = Dr[c];
+                __syncwarp();
+                double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NB; c += 2) {
+                    const double d0 = c <= t ? Dr[c] : Ts[c][t];
+                    const double d1 = c + 1 <= t ? Dr[c + 1] : Ts[c + 1][t];
+                    p0 = fma(d0, vs[c], p0);
+                    p1 = fma(d1, vs[c + 1], p1);
+                }
+                const double p = t < L ? tau * (p0 + p1) : 0.0;
+                double vp = v * p;
+                for (int o = 16; o > 0; o >>= 1) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+                const double wv = p - 0.5 * tau * vp * v;
+                ws2[t] = wv;
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < NB; c++)
+                    if (c <= t) Dr[c] -= v * ws2[c] + wv * vs[c];
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int c = 0; c < NB; c += 2) {
+                    s0 = fma(Br[c], vs[c], s0);
+                    s1 = fma(Br[c + 1], vs[c + 1], s1);
+                }
+                const double sr = tau * (s0 + s1);
+#pragma unroll
+                for (int c = 0; c < NB; c++) Br[c] = fma(-sr, vs[c], Br[c]);
+                if (t < L) {
+#pragma unroll
+                    for (int c = 0; c < NB; c++)
+                        if (c <= t) *at(r0 + t, r0 + c) = Dr[c];
+                }
+                if (t < nb2) {
+#pragma unroll
+                    for (int c = 0; c < NB; c++)
+                        if (c < L) *at(r1 + t, r0 + c) = Br[c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NB; c++) Cs[t][c] = Br[c];
+            // hand the step to the helper, then fetch the next step's blocks once the previous sweep
+            // is three steps ahead of it
+            __threadfence_block();
+            __syncwarp();
+            if (t == 0) done = i + 1;
+            if (i + 1 < nst) {
+                ok = wait_prev(min(i + 4, nprev));
+                if (ok) load_blocks(i + 1, Dr, Br);
+            }
+        }
+        if (!ok && t == 0) quit = 1;
+        __syncthreads();
+        if (*(volatile int *)a.err) return;
+    }
+}
+
 // d(c) = A(c, c), e(c) = A(c+1, c)
 __global__ void tridiag_extract_kernel(int n, const double *__restrict__ AB, double *d, double *e)
 {
@@ -1796,13 +1974,20 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     if (n > 2) {
         int nsm = 148;
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-        // the register form (sb2st2_kernel) by default; BSRG_SB2ST_SHARED keeps the shared-memory form
-        // groups of SB_K consecutive sweeps per CTA (sb2st2_kernel<SB_K>); BSRG_SB2ST_SHARED keeps the
-        // shared-memory form with one sweep per CTA
+        // the register form with a helper warp (sb2st3_kernel) by default; BSRG_SB2ST_ONEWARP selects the
+        // register form without it, groups of SB_K consecutive sweeps per CTA (sb2st2_kernel<SB_K>), and
+        // BSRG_SB2ST_SHARED the shared-memory form with one sweep per CTA
         constexpr int SB_K = 1;              // eight sweeps per CTA measured slower (152 vs 121 ms at n = 7810)
         Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
         void *args[] = {&a2};
-        if (getenv("BSRG_SB2ST_SHARED")) {
+        if (!getenv("BSRG_SB2ST_SHARED") && !getenv("BSRG_SB2ST_ONEWARP")) {
+            // one sweep per CTA at a time, a helper warp beside the computing one (sb2st3_kernel);
+            // one CTA per SM: about n / (3.4 NB) sweeps are active at once, so nsm CTAs never make a
+            // sweep wait for its CTA, and no waiting CTA shares an SM with a working one
+            const int ctas = std::max(1, std::min(n - 2, nsm));
+            if ((e = cudaLaunchCooperativeKernel((const void *)sb2st3_kernel, ctas, 64, args, 0, st)) != cudaSuccess)
+                return cuda_fail(e, "dsyevd bulge chasing");
+        } else if (getenv("BSRG_SB2ST_SHARED")) {
             int per = 1;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sb2st_kernel, 32, 0);
             const int workers = std::max(1, std::min(n - 2, std::min(nsm * std::max(per, 1), 2 * nsm)));
