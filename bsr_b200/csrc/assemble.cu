@@ -1416,7 +1416,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
                 if (rc != BSRG_OK) return rc;
                 stage_end(c, 7, 2);
             }
-        if ((e = cudaFuncSetAttribute(xfu, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xfu_smem)) != cudaSuccess)
+        if ((e = smem_attr(xfu, (int)xfu_smem)) != cudaSuccess)
             return cuda_fail(e, "exchange (fused) smem");
     }
     if (xfu && (full || !kact.empty())) {
@@ -1455,13 +1455,13 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     const int xg = exchange_groups_per_cta(ks);
     exchange_fn xk = exchange_kernel_for(ks);
     if (!xk) { set_error("assemble: ks=%d unsupported", ks); return BSRG_ERR_ARG; }
-    if ((e = cudaFuncSetAttribute(xk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm)) != cudaSuccess)
+    if ((e = smem_attr(xk, (int)xsm)) != cudaSuccess)
         return cuda_fail(e, "exchange smem");
     // the factored exchange handles up to NORB_MAX orbitals; BSRG_EXCHANGE_GATHER selects the gather kernel
     exchange_factored_fn xf = (norb <= NORB_MAX && !getenv("BSRG_EXCHANGE_GATHER")) ? exchange_factored_for(ks) : nullptr;
     const size_t xfsm = exchange_factored_smem(ks);
     if (xf && !xfu) {
-        if ((e = cudaFuncSetAttribute(xf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xfsm)) != cudaSuccess)
+        if ((e = smem_attr(xf, (int)xfsm)) != cudaSuccess)
             return cuda_fail(e, "exchange (factored) smem");
         if (ncoef > 0) {
             stage_begin(c, 2);

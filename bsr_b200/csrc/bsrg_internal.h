@@ -29,6 +29,15 @@ namespace bsrg {
 void set_error(const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *where);
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device and never lowers
+// it: threads that launch the same kernel with different sizes on their own streams cannot undo
+// one another's limit between setting it and launching.
+cudaError_t smem_attr_raw(const void *func, int bytes);
+template <typename F> inline cudaError_t smem_attr(F *func, size_t bytes)
+{
+    return smem_attr_raw((const void *)func, (int)bytes);
+}
+
 inline int ik_of(int ks) { return ks * (ks + 1) / 2; }
 
 // Gauss-Legendre nodes/weights on [0,1], ascending (Newton on P_k).

@@ -6,6 +6,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "bsrg_internal.h"
@@ -27,6 +30,21 @@ int cuda_fail(cudaError_t e, const char *where)
     if (e == cudaSuccess) return BSRG_OK;
     set_error("%s: %s", where, cudaGetErrorString(e));
     return e == cudaErrorMemoryAllocation ? BSRG_ERR_NOMEM : BSRG_ERR_CUDA;
+}
+
+cudaError_t smem_attr_raw(const void *func, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, int> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    int &cur = limit[{dev, func}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
 }
 
 // Gauss-Legendre rule on [0,1] by Newton iteration on the Legendre polynomial

@@ -518,8 +518,8 @@ int chan_own_solve(bsrg_ctx *c, const bsrg_basis *b, const double *hcc, int nch,
     double *Lg = Gm + np2 * nch, *Vg = Lg + (size_t)npad * ks * nch, *dg = Vg + tri(npad) * nch;
     double *eg = dg + (size_t)npad * nch, *tg = eg + (size_t)npad * nch, *scr = tg + (size_t)npad * nch;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(ktri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(kback, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm4)) != cudaSuccess)
+    if ((e = smem_attr(ktri, (int)sm1)) != cudaSuccess ||
+        (e = smem_attr(kback, (int)sm4)) != cudaSuccess)
         return cuda_fail(e, "channel solves: shared memory");
     if ((e = cudaMemsetAsync(d_flag, 0, 2 * sizeof(int), s)) != cudaSuccess) return cuda_fail(e, "channel solves: flag");
     ktri<<<nch, CH_THREADS, sm1, s>>>(ns, npad, d_s0, d_nsol, hcc, b->sb, X, Lg, Vg, dg, eg, tg, d_info);

@@ -109,7 +109,7 @@ int mirror_lower(int n, double *A, long lda, cudaStream_t s);
 // eigenpair refinement (refine.cu)
 size_t refine_workspace_doubles(int n);
 int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s);
-int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *P, double *corr, double *resid,
+int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *work, double *corr, double *resid,
                  int *flag, cudaStream_t s);
 
 }  // namespace bsrg

@@ -148,7 +148,7 @@ static int copy2d(int m, int n, const double *src, long lds, double *dst, long l
 int dpotrf_lower(int n, double *C, long ldc, double *Linv, double *tmp, int *info, cudaStream_t s, int *launches)
 {
     const size_t smem = sizeof(double) * ((size_t)CH_NB * CH_LD + CH_NB);
-    cudaError_t e = cudaFuncSetAttribute(chol_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_attr(chol_diag_kernel, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "dpotrf: shared memory");
     int nl = 0;
     for (int j0 = 0, jb = 0; j0 < n; j0 += CH_NB, jb++) {

@@ -92,8 +92,7 @@ template <class C, bool TA, bool TB, bool SYMA = false>
 static int launch(const DgemmBatch &p, int batch, int S, int kchunk, double *W, cudaStream_t s)
 {
     constexpr int bytes = dmma::Smem<C, TA, TB>::BYTES;
-    cudaError_t e =
-        cudaFuncSetAttribute(dgemm_kernel<C, TA, TB, SYMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = smem_attr(dgemm_kernel<C, TA, TB, SYMA>, bytes);
     if (e != cudaSuccess) return cuda_fail(e, "dgemm: shared memory attribute");
     dim3 g((unsigned)((p.m + C::BM - 1) / C::BM), (unsigned)((p.n + C::BN - 1) / C::BN), (unsigned)(batch * S));
     dgemm_kernel<C, TA, TB, SYMA><<<g, C::NT, bytes, s>>>(p, S, kchunk, W);

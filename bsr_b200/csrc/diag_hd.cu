@@ -721,7 +721,7 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
         }
     }
     if (refine) {
-        // ---- FP64 refinement of the eigenpairs (Rayleigh quotients) ----
+        // ---- FP64 refinement of the eigenpairs (windowed Rayleigh-Ritz values) ----
         if (c->rf_cap < 2 * (size_t)khm) {
             if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diag_hd refine sync");
             if (c->rf_buf) cudaFree(c->rf_buf);
@@ -735,7 +735,8 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
         int rr = refine_apply(khm, Fsym, A, khm, eval, Fsym + (size_t)khm * khm, c->rf_buf, c->rf_buf + khm,
                               d_rflag, s);
         stage_end(c, 8, 3);
-        c->stage_flops[8] += 2.0 * (double)khm * khm * khm + 6.0 * (double)khm * khm;
+        // A V, the residuals and their sums, and the banded products of the Rayleigh-Ritz windows
+        c->stage_flops[8] += 2.0 * (double)khm * khm * khm + 6.0 * (double)khm * khm + 132.0 * (double)khm * khm;
         if (rr != BSRG_OK) return rr;
         c->rf_n = khm;
     }

@@ -565,7 +565,7 @@ int trd_reduce(bsrg_ctx *c, int n, double *A, int lda, double *d, double *e, dou
     if ((er = cudaMemsetAsync(L.bar, 0, flag_bytes, s)) != cudaSuccess) return cuda_fail(er, "tridiagonal reduction");
     int dev = c->device, nsm = 0, occ = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if ((er = cudaFuncSetAttribute(trd_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TRD_SMEM)) !=
+    if ((er = smem_attr(trd_panel_kernel, TRD_SMEM)) !=
         cudaSuccess)
         return cuda_fail(er, "tridiagonal reduction smem");
     if ((er = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, trd_panel_kernel, TRD_NT, TRD_SMEM)) != cudaSuccess)

@@ -162,7 +162,7 @@ extern "C" int bsrg_channel_weights(bsrg_ctx *c, int nch, const int *ipsol, int 
         return cuda_fail(e, "channel_weights upload");
     cudaEventRecord(c->ev_stage, s);
     if (shm > 48 * 1024 &&
-        (e = cudaFuncSetAttribute(channel_weights_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm)) !=
+        (e = smem_attr(channel_weights_kernel, (int)shm)) !=
             cudaSuccess)
         return cuda_fail(e, "channel_weights smem");
     channel_weights_kernel<<<khm, 128, shm, s>>>(nch, d_ip, khm, a, wt, isol, iprm);

@@ -1015,8 +1015,7 @@ int launch_rk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
     if (rkd) {
         size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + 2 * (size_t)ks * ik + (size_t)ik * ik);
         if (shm > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)shm);
+            cudaError_t e = smem_attr(diag_cell_kernel, (int)shm);
             if (e != cudaSuccess) return cuda_fail(e, "diag_cell smem");
         }
         diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
@@ -1057,8 +1056,7 @@ int launch_nkmk_moments(const bsrg_basis *b, int k, int sym, double *rkd1, doubl
     if (rkd) {
         size_t shm = sizeof(double) * ((size_t)ks * ks * ks + ks * ks + (size_t)ks * ik + (sym ? (size_t)ik * ik : 0));
         if (shm > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(nk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)shm);
+            cudaError_t e = smem_attr(nk_diag_cell_kernel, (int)shm);
             if (e != cudaSuccess) return cuda_fail(e, "nk diag_cell smem");
         }
         nk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, sym, b->t, rule_of(b), b->gr,
@@ -1099,7 +1097,7 @@ int launch_tk_moments(const bsrg_basis *b, int k, double *rkd1, double *rkd2, do
                       shm, optin);
             return BSRG_ERR_ARG;
         }
-        cudaError_t e = cudaFuncSetAttribute(tk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        cudaError_t e = smem_attr(tk_diag_cell_kernel, (int)shm);
         if (e != cudaSuccess) return cuda_fail(e, "tk diag_cell smem");
         tk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, b->t, rule_of(b), b->gr,
                                                 b->grm, b->grw, b->bsp, b->bsq, rkd);
@@ -1162,8 +1160,7 @@ int launch_vw_moments(const bsrg_basis *b, int k, int mode, double *rkd1, double
     if (rkd) {
         const size_t shm = sizeof(double) * (4 * (size_t)ks * ks * ks + 2 * (size_t)ks * ks);
         if (shm > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(vk_diag_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)shm);
+            cudaError_t e = smem_attr(vk_diag_cell_kernel, (int)shm);
             if (e != cudaSuccess) return cuda_fail(e, "vk diag_cell smem");
         }
         vk_diag_cell_kernel<<<nv, 256, shm, s>>>(ks, nv, b->ml, b->me, b->h + 1.0, k, mode, b->t, rule_of(b), b->gr,

@@ -1712,8 +1712,8 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
 {
     cudaError_t e;
     const int smem = PQ_ROWS * (NB + 1) * (int)sizeof(double);
-    if ((e = cudaFuncSetAttribute(panel_qr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(ypass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, YP1_SMEM)) != cudaSuccess)
+    if ((e = smem_attr(panel_qr_kernel, smem)) != cudaSuccess ||
+        (e = smem_attr(ypass1_kernel, YP1_SMEM)) != cudaSuccess)
         return cuda_fail(e, "sy2sb smem");
     // the cluster form of the panel factorisation when a 16-CTA cluster with its shared memory fits
     // (BSRG_PANEL_GRID selects the grid-barrier form)
@@ -1722,7 +1722,7 @@ int sy2sb(cudaStream_t st, int n, double *A, long lda, double *Vsave, double *Ts
         const int smem_c = (PQC_ROWS * (NB + 1) + 4 * NB + NB * NB) * (int)sizeof(double);
         if (cudaFuncSetAttribute(panel_qr_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                 cudaSuccess ||
-            cudaFuncSetAttribute(panel_qr_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_c) !=
+            smem_attr(panel_qr_cluster_kernel, smem_c) !=
                 cudaSuccess) {
             use_cluster = false;
         } else {
@@ -1995,7 +1995,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
                 return cuda_fail(e, "dsyevd bulge chasing");
         } else {
             const int smem = SB_K * SB_WSM * (int)sizeof(double);
-            if ((e = cudaFuncSetAttribute(sb2st2_kernel<SB_K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) !=
+            if ((e = smem_attr(sb2st2_kernel<SB_K>, smem)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd bulge chasing smem");
             int per = 1;
@@ -2042,19 +2042,19 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
     if (n > 2) {
         dim3 gt((unsigned)S, (unsigned)((n - 2 + NB - 1) / NB));
         q2_tfactor_kernel<<<gt, 32, 0, st>>>(n, S, V2, tau2, Tq);
-        if ((e = cudaFuncSetAttribute(q2_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2_SMEM)) !=
+        if ((e = smem_attr(q2_apply_kernel, Q2_SMEM)) !=
             cudaSuccess)
             return cuda_fail(e, "dsyevd Q2 smem");
         if (getenv("BSRG_Q2_SIMPLE")) {
             q2_apply_kernel<<<(unsigned)((n + Q2_COLS - 1) / Q2_COLS), Q2_NT, Q2_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz);
         } else if (getenv("BSRG_Q2_WAVE")) {
-            if ((e = cudaFuncSetAttribute(q2w_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2W_SMEM)) !=
+            if ((e = smem_attr(q2w_apply_kernel, Q2W_SMEM)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2w_apply_kernel<<<(unsigned)((n + 31) / 32), Q2W_WARPS * 32, Q2W_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz,
                                                                                           sw.err);
         } else if (getenv("BSRG_Q2_RING1")) {
-            if ((e = cudaFuncSetAttribute(q2r_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, Q2R_SMEM)) !=
+            if ((e = smem_attr(q2r_apply_kernel, Q2R_SMEM)) !=
                 cudaSuccess)
                 return cuda_fail(e, "dsyevd Q2 smem");
             q2r_apply_kernel<<<(unsigned)((n + 31) / 32), Q2R_W * 32, Q2R_SMEM, st>>>(n, S, n, V2, Tq, Z, ldz, sw.err);
@@ -2062,15 +2062,13 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             // four groups per round and one CTA per SM, or (BSRG_Q2_TWO) two groups and two CTAs per SM
             if (getenv("BSRG_Q2_TWO")) {
                 constexpr int sm2 = q2p_smem<2, 128>();
-                if ((e = cudaFuncSetAttribute(q2p_apply_kernel<2, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              sm2)) != cudaSuccess)
+                if ((e = smem_attr(q2p_apply_kernel<2, 128>, sm2)) != cudaSuccess)
                     return cuda_fail(e, "dsyevd Q2 smem");
                 q2p_apply_kernel<2, 128><<<(unsigned)((n + 31) / 32), 2 * 64, sm2, st>>>(n, S, n, V2, Tq, Z, ldz,
                                                                                         sw.err);
             } else {
                 constexpr int sm4 = q2p_smem<4, 256>();
-                if ((e = cudaFuncSetAttribute(q2p_apply_kernel<4, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              sm4)) != cudaSuccess)
+                if ((e = smem_attr(q2p_apply_kernel<4, 256>, sm4)) != cudaSuccess)
                     return cuda_fail(e, "dsyevd Q2 smem");
                 q2p_apply_kernel<4, 256><<<(unsigned)((n + 31) / 32), 4 * 64, sm4, st>>>(n, S, n, V2, Tq, Z, ldz,
                                                                                         sw.err);
@@ -2103,8 +2101,7 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
             if (rc != BSRG_OK) return rc;
             // T of the merged 256-column reflector: each 128-column half by pairwise merges of its
             // panels' T (q1_tmerge_kernel), then the off-diagonal block -T_a G_ab T_b by two GEMMs
-            if ((e = cudaFuncSetAttribute(q1_tmerge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          Q1M_SMEM)) != cudaSuccess)
+            if ((e = smem_attr(q1_tmerge_kernel, Q1M_SMEM)) != cudaSuccess)
                 return cuda_fail(e, "dsyevd Q1 smem");
             if ((e = cudaMemsetAsync(Tg, 0, sizeof(double) * Q1W * Q1W, st)) != cudaSuccess)
                 return cuda_fail(e, "dsyevd Q1 T");

@@ -202,7 +202,7 @@ int tf32x3_gemm(int m, int n, int k, double alpha, const double *A, long lda, co
                 double *C, long ldc, int *err, cudaStream_t s)
 {
     if (m <= 0 || n <= 0) return BSRG_OK;
-    cudaError_t e = cudaFuncSetAttribute(tf32x3_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    cudaError_t e = smem_attr(tf32x3_gemm_kernel, TC_SMEM);
     if (e != cudaSuccess) return cuda_fail(e, "tf32x3 gemm smem");
     dim3 g((unsigned)((m + TC_M - 1) / TC_M), (unsigned)((n + TC_N - 1) / TC_N));
     tf32x3_gemm_kernel<<<g, TC_NT, TC_SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, err);

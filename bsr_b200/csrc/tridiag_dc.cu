@@ -661,7 +661,7 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
         (err = cudaMemcpyAsync(d_lk, h_lk, sizeof(int) * leaves.size(), cudaMemcpyHostToDevice, st)) != cudaSuccess)
         return cuda_fail(err, "dstedc upload");
     const int smem_leaf = 2 * DC_LEAF * (DC_LEAF + 1) * (int)sizeof(double);
-    if ((err = cudaFuncSetAttribute(dc_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_leaf)) !=
+    if ((err = smem_attr(dc_leaf_kernel, smem_leaf)) !=
         cudaSuccess)
         return cuda_fail(err, "dstedc leaf smem");
     dc_leaf_kernel<<<(unsigned)leaves.size(), 256, smem_leaf, st>>>(d_ls, d_lk, d, e, w, Z, ldz);
@@ -686,7 +686,7 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
         if ((err = cudaMemcpyAsync(d_mg, h_mg, sizeof(DcMerge) * nm, cudaMemcpyHostToDevice, st)) != cudaSuccess)
             return cuda_fail(err, "dstedc merge upload");
         const int smem_prep = kmax * 21 + 64;
-        if ((err = cudaFuncSetAttribute(dc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_prep)) !=
+        if ((err = smem_attr(dc_prep_kernel, smem_prep)) !=
             cudaSuccess)
             return cuda_fail(err, "dstedc prep smem");
         dc_prep_kernel<<<nm, 512, smem_prep, st>>>(d_mg, e, w, Z, ldz, wsd, wsi, d_scal);
@@ -704,8 +704,7 @@ int tridiag_dc(cudaStream_t st, int n, double *d, const double *e, double *w, do
         for (int q = 0; q < nm; q++) Kmax = std::max(Kmax, h_scal[DC_NS * q]);
         if (Kmax > 0) {
             const int smem_sec = 16 * Kmax;
-            if ((err = cudaFuncSetAttribute(dc_secular_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            smem_sec)) != cudaSuccess)
+            if ((err = smem_attr(dc_secular_kernel, smem_sec)) != cudaSuccess)
                 return cuda_fail(err, "dstedc secular smem");
             dim3 gsec((unsigned)((Kmax + SEC_WARPS - 1) / SEC_WARPS), nm);
             dc_secular_kernel<<<gsec, 32 * SEC_WARPS, smem_sec, st>>>(d_mg, d_scal, wsd, wsi, Kmax);

@@ -401,16 +401,76 @@ def assemble(basis, z, lch, ech, P, kmax, rkb_all, coefs, want_s=True, want_acf=
 # ---------------------------------------------------------------------------
 # diag_hd restatement (src/bsr/BSR_HD3/diag_hd.f90:2-340) with scipy LAPACK
 # ---------------------------------------------------------------------------
-def rayleigh_refine(A, ev, V, dtype=np.longdouble):
-    """Rayleigh quotients lambda + v^T (A v - lambda v) / v^T v of the eigenpairs
-    (ev, V) of the symmetric A, evaluated in `dtype` (long double: ~1e-19 relative
-    rounding, so the result is the exact quotient of the FP64 pair to working
-    precision).  Returns (refined eigenvalues, residual norms ||A v - lambda v|| / ||v||)."""
+RR_HW = 8   # half-width of the Rayleigh-Ritz window of rayleigh_refine
+
+
+def jacobi_eigvals(M, sweeps=10):
+    """Eigenvalues of the small symmetric M by cyclic Jacobi rotations (each zeroes one
+    off-diagonal pair; tan of its angle = the smaller root of t^2 + 2 theta t - 1 = 0,
+    theta = (a_qq - a_pp) / (2 a_pq)), unsorted.  Rotations keep small eigenvalues of a
+    graded matrix to relative accuracy, where a tridiagonalising solver is off by
+    ~eps ||M||.  The sequence of rotations is the library's (refine.cu)."""
+    A = np.array(M, dtype=np.float64)
+    w = A.shape[0]
+    for _ in range(sweeps):
+        rotated = False
+        for p in range(w - 1):
+            for q in range(p + 1, w):
+                apq, app, aqq = A[p, q], A[p, p], A[q, q]
+                if not (abs(apq) > 1e-19 * (abs(app) + abs(aqq))) or abs(apq) < 1e-300:
+                    continue
+                rotated = True
+                th = (aqq - app) / (2.0 * apq)
+                t = 0.5 / th if abs(th) > 1e150 else np.copysign(1.0, th) / (abs(th) + np.sqrt(1.0 + th * th))
+                c = 1.0 / np.sqrt(1.0 + t * t)
+                s = t * c
+                k = np.array([i for i in range(w) if i != p and i != q], dtype=int)
+                akp, akq = A[k, p].copy(), A[k, q].copy()
+                A[k, p] = A[p, k] = c * akp - s * akq
+                A[k, q] = A[q, k] = s * akp + c * akq
+                A[p, p] = app - t * apq
+                A[q, q] = aqq + t * apq
+                A[p, q] = A[q, p] = 0.0
+        if not rotated:
+            break
+    return np.diag(A).copy()
+
+
+def rayleigh_refine(A, ev, V, dtype=np.longdouble, window=RR_HW):
+    """Refined eigenvalues of the eigenpairs (ev, V) of the symmetric A, evaluated in `dtype`
+    (long double: ~1e-19 relative rounding).  The Rayleigh quotient lambda + v^T r / v^T v
+    (r = A v - lambda v) leaves an error ~||r||^2 / gap, which close pairs feel; so, as the
+    library does (refine.cu), each lambda_j becomes the Rayleigh-Ritz value in j's place of
+    the window of pairs [j - window, j + window] (cut to the pairs given):
+    M(k, l) = (v_k^T r_l + lambda_l v_k^T v_l) / (|v_k| |v_l|), symmetrised, its eigenvalues
+    by jacobi_eigvals.  window=0 gives the plain quotients.
+    Returns (refined eigenvalues in the order of ev, residual norms ||A v - lambda v|| / ||v||)."""
     Al, Vl, el = A.astype(dtype), V.astype(dtype), ev.astype(dtype)
     R = Al @ Vl - Vl * el[None, :]
     vv = np.sum(Vl * Vl, axis=0)
-    ref = el + np.sum(Vl * R, axis=0) / vv
-    return np.asarray(ref, dtype=np.float64), np.sqrt(np.asarray(np.sum(R * R, axis=0) / vv, dtype=np.float64))
+    resid = np.sqrt(np.asarray(np.sum(R * R, axis=0) / vv, dtype=np.float64))
+    m = len(ev)
+    if window <= 0:
+        return np.asarray(el + np.sum(Vl * R, axis=0) / vv, dtype=np.float64), resid
+    bw = 2 * window
+    # B[j, d + bw] = v_{j+d}^T r_j, G[j, d + bw] = v_{j+d}^T v_j
+    B = np.zeros((m, 2 * bw + 1), dtype=dtype)
+    G = np.zeros((m, 2 * bw + 1), dtype=dtype)
+    for d in range(-bw, bw + 1):
+        j = np.arange(max(0, -d), min(m, m - d))
+        if len(j):
+            B[j, d + bw] = np.sum(Vl[:, j + d] * R[:, j], axis=0)
+            G[j, d + bw] = np.sum(Vl[:, j + d] * Vl[:, j], axis=0)
+    out = np.empty(m)
+    for j in range(m):
+        lo, hi = max(0, j - window), min(m - 1, j + window)
+        idx = np.arange(lo, hi + 1)
+        kk, ll = np.meshgrid(idx, idx, indexing="ij")
+        mkl = B[ll, kk - ll + bw] + el[ll] * G[ll, kk - ll + bw]
+        nrm = np.sqrt(G[kk, bw] * G[ll, bw])
+        M = np.asarray((0.5 * (mkl + mkl.T)) / nrm, dtype=np.float64)
+        out[j] = np.sort(jacobi_eigvals(M))[j - lo]
+    return out, resid
 
 
 def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=0.001,
@@ -429,10 +489,10 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
 
     refine=True restates the library's refined form: the diagonal blocks of A
     are bb_i^T H_ii bb_i (diag(bval) in exact arithmetic, diag_hd.f90:188-219)
-    and every eigenvalue is replaced by its Rayleigh quotient in refine_dtype
+    and every eigenvalue is replaced by its windowed Rayleigh-Ritz value in refine_dtype
     (rayleigh_refine); the eigenvectors come from LAPACK DSYEV as in the
     reference (:312), or, with lowest=m, from DSYEVR for the m lowest pairs
-    only (the quotient makes the result independent of the driver).  Also
+    only (the refinement makes the result independent of the driver).  Also
     returns "a" (the symmetric A) and "resid".
     """
     from scipy.linalg import lapack
@@ -502,13 +562,17 @@ def diag_hd(hcc, scc, lch, ns, ks, itype=0, ilzero=1, ibzero=1, Edmax=0.0, Egap=
     if refine:
         full = np.tril(a) + np.tril(a, -1).T
         if lowest is not None:
+            # the Rayleigh-Ritz windows of the lowest pairs reach RR_HW pairs beyond them
             from scipy.linalg import eigh
-            ev, vec = eigh(full, subset_by_index=[0, min(lowest, khm) - 1], driver="evr")
+            ev, vec = eigh(full, subset_by_index=[0, min(lowest + RR_HW, khm) - 1], driver="evr")
         else:
             ev, vec, info = lapack.dsyev(a, compute_v=1, lower=1)[:3]
             if info != 0:
                 raise RuntimeError("DSYEV info %d" % info)
         ev, resid = rayleigh_refine(full, ev, vec, refine_dtype)
+        if lowest is not None:
+            keep = min(lowest, khm)
+            ev, resid, vec = ev[:keep], resid[:keep], vec[:, :keep]
         o = np.argsort(ev, kind="stable")
         out.update({"eval": ev[o], "resid": resid[o], "vectors": back(vec[:, o]), "a": full})
         return out
