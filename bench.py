@@ -743,11 +743,14 @@ def bench_batched_serving(torch, bsr):
 
     for s in syms[:2]:
         plain(s)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    seq = [plain(s) for s in syms]
-    torch.cuda.synchronize()
-    t_seq = time.perf_counter() - t0
+    t_seqs = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        seq = [plain(s) for s in syms]
+        torch.cuda.synchronize()
+        t_seqs.append(time.perf_counter() - t0)
+    t_seq = float(np.median(t_seqs))
     del ctx
     torch.cuda.empty_cache()
 
@@ -759,22 +762,31 @@ def bench_batched_serving(torch, bsr):
     srv = make(n_best)
     try:
         serve.run_stream(srv, syms[:2], [0.0, 0.0])
-        reqs = serve.run_stream(srv, syms, [0.0] * len(syms))
-        st = srv.stats(reqs)
-        res = [r.wait() for r in reqs]
+        rates = []
+        for _ in range(3):
+            reqs = serve.run_stream(srv, syms, [0.0] * len(syms))
+            st = srv.stats(reqs)
+            res = [r.wait() for r in reqs]
+            rates.append(st["solves_per_s"])
     finally:
         srv.close()
-    same = all(np.array_equal(r["eval"], e) for r, e in zip(res, seq))
-    maxrel = max(float(np.max(np.abs(r["eval"] - e)) / np.max(np.abs(e))) for r, e in zip(res, seq))
+    plain_rates = [len(syms) / t for t in t_seqs]
+    # per eigenvalue (floor 1e-3, diag_hd's Egap): the batched workers may use the other dense
+    # eigensolver than the plain path at a given size, so agreement is to the refined form's accuracy
+    maxrel = max(float(np.max(np.abs(r["eval"] - e) / np.maximum(np.abs(e), 1e-3))) for r, e in zip(res, seq))
+    same = maxrel <= 1e-11
     nchs = [s["nch"] for s in syms]
     batched = {
         "workload": "config4: %d symmetries, channels %d..%d (log-uniform 4..60), ks=%d ns=%d k=0..%d, FP64 with "
                     "eigenvectors, all submitted at t=0" % (len(syms), min(nchs), max(nchs), b["ks"], b["ns"], b["kmax"]),
-        "solves_per_s": st["solves_per_s"], "plain_solves_per_s": len(syms) / t_seq,
-        "speedup_vs_plain": st["solves_per_s"] * t_seq / len(syms),
+        "solves_per_s": float(np.median(rates)), "plain_solves_per_s": len(syms) / t_seq,
+        "speedup_vs_plain": float(np.median(rates)) * t_seq / len(syms),
+        "repeats": {"batched_solves_per_s": rates, "plain_solves_per_s": plain_rates,
+                    "min_batched_over_max_plain": min(rates) / max(plain_rates)},
         "p50_s": st["p50_s"], "p99_s": st["p99_s"], "n_streams": n_best,
+        "eigensolver": "library two-stage on every worker (several streams)" if n_best > 1 else "by size",
         "autotune_solves_per_s": tune["config4"]["solves_per_s"],
-        "eigenvalues_equal_plain": same, "max_rel_diff_vs_plain": maxrel,
+        "eigenvalues_match_plain_1e-11": same, "max_rel_diff_vs_plain_per_eigenvalue": maxrel,
         "timing": "host wall clock, first submit to last result; resident R^k tables; HBM-budget admission",
     }
     del srv

@@ -73,6 +73,7 @@ SIGNATURES = [
     ("bsrg_diag_hd_ipsol", _c_int, [_P, _c_int, _IP]),
     ("bsrg_ctx_set_refine", _c_int, [_P, _c_int]),
     ("bsrg_ctx_set_precision", _c_int, [_P, _c_int]),
+    ("bsrg_ctx_set_eigensolver", _c_int, [_P, _c_int]),
     ("bsrg_diag_hd_refine_stats", _c_int, [_P, _c_int, _P, _P]),
     ("bsrg_ctx_channel_fallbacks", _c_int, [_P, _P]),
     ("bsrg_dgemm", _c_int, [_c_char, _c_char, _c_int, _c_int, _c_int, _c_double, _P, _c_long, _c_long, _P,

@@ -365,6 +365,11 @@ class Context:
         """Mixed-precision form (tensor-core split-TF32 direct contraction) or FP64 (default)."""
         call("bsrg_ctx_set_precision", self.handle, 1 if mixed else 0)
 
+    def set_eigensolver(self, which="auto"):
+        """diag_hd's dense eigensolver: "auto" (the library's from 7000 rows, cuSOLVER's below),
+        "own" (the library's two-stage solver) or "lib" (cuSOLVER's syevd)."""
+        call("bsrg_ctx_set_eigensolver", self.handle, {"auto": 0, "own": 1, "lib": 2}[which])
+
     def refine_stats(self, n):
         """(correction, residual norm) per eigenpair of the last refined diag_hd, as CUDA tensors."""
         corr = torch.empty(n, device="cuda", dtype=torch.float64)

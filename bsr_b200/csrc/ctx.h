@@ -47,6 +47,7 @@ struct bsrg_ctx {
     int pw_ks;
     int refine;                              // FP64 refinement of the eigenpairs in diag_hd (default on)
     int precision;                           // 0 FP64 (default), 1 mixed (tensor-core assembly contraction)
+    int eig_mode;                            // dense eigensolver of diag_hd: 0 by size, 1 library's, 2 cuSOLVER's
     double *rf_buf;                          // per-pair correction | residual of the last refined diag_hd
     size_t rf_cap;                           //   (doubles held)
     int rf_n;                                //   (pairs recorded)

@@ -407,11 +407,13 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
     const bool refine = want_vectors && c->refine;
     const char *eig_env = getenv("BSRG_EIG");
     // the library's two-stage eigensolver (syevd2.cu) or cuSOLVER's syevd: BSRG_EIG=own or =lib
-    // chooses; otherwise the library's from kOwnEigMin rows up (where it was measured faster)
+    // chooses, else the context's setting; by default the library's from kOwnEigMin rows up (where
+    // it was measured faster)
     int khm_bound = 0;
     for (int ich = 0; ich < nch; ich++) khm_bound += nsolv[ich];
     const bool own_eig = want_vectors && khm_bound <= 10240 &&
-                         (eig_env ? strcmp(eig_env, "own") == 0 : khm_bound >= kOwnEigMin);
+                         (eig_env ? strcmp(eig_env, "own") == 0
+                                  : (c->eig_mode == 1 || (c->eig_mode == 0 && khm_bound >= kOwnEigMin)));
     std::vector<BlockMap> bmap;
     for (int ic = 1; ic < nch; ic++)
         for (int jc = 0; jc < ic; jc++) bmap.push_back({ic, jc});
@@ -790,6 +792,14 @@ extern "C" int bsrg_ctx_set_refine(bsrg_ctx *c, int on)
 {
     if (!c) { set_error("ctx_set_refine: null context"); return BSRG_ERR_ARG; }
     c->refine = on ? 1 : 0;
+    return BSRG_OK;
+}
+
+extern "C" int bsrg_ctx_set_eigensolver(bsrg_ctx *c, int which)
+{
+    if (!c) { set_error("ctx_set_eigensolver: null context"); return BSRG_ERR_ARG; }
+    if (which < 0 || which > 2) { set_error("ctx_set_eigensolver: which=%d (0, 1 or 2)", which); return BSRG_ERR_ARG; }
+    c->eig_mode = which;
     return BSRG_OK;
 }
 

@@ -51,16 +51,23 @@ class Request:
         return None if self.t_done is None else self.t_done - self.t_submit
 
 
-def request_bytes(nch, ns, lch, ks, want_vectors=True):
+OWN_EIG_MIN = 7000      # diag_hd's default crossover to the library's dense eigensolver (rows)
+
+
+def request_bytes(nch, ns, lch, ks, want_vectors=True, own_eig=False):
     """Device bytes one solve needs beyond the shared state (H blocks, the dense
     problem with vectors and its eigensolver workspace, block-transform buffers;
-    with vectors also the eigenvectors and the refinement's copy of A)."""
+    with vectors also the eigenvectors and the refinement's copy of A and its
+    residuals; with the library's two-stage eigensolver its workspace: the band
+    reduction's copy, both stages' reflectors and block factors, the divide and
+    conquer's merge buffers, ~6.5 khm^2 + 3000 khm doubles)."""
     khm, hb, db = shard.symmetry_dims(nch, ns, lch, ks)
     nch, ns = int(nch), int(ns)
     nb = nch * (nch + 1) // 2
     transform = 2 * nb * ns * ns * 8
     channel = 4 * nch * ns * ns * 8
-    return hb + db + transform + channel + (2 * khm * khm * 8 if want_vectors else 0)
+    own = int((6.5 * khm * khm + 3000 * khm) * 8) if (own_eig and want_vectors) else 0
+    return hb + db + transform + channel + (3 * khm * khm * 8 if want_vectors else 0) + own
 
 
 class AdmissionQueue:
@@ -111,7 +118,13 @@ class AdmissionQueue:
 class PartialWaveServer:
     """Device-resident request loop for partial waves sharing one basis and orbital set."""
 
-    def __init__(self, t, ks, z, P, kmax, n_streams=2, hbm_budget_bytes=None, device=0):
+    def __init__(self, t, ks, z, P, kmax, n_streams=2, hbm_budget_bytes=None, device=0, eigensolver=None):
+        """eigensolver: diag_hd's dense eigensolver per worker ("auto", "own" or "lib", see
+        Context.set_eigensolver).  Default: "own" with more than one stream -- concurrent
+        solves overlap with the library's two-stage solver, whose bulge chasing and panel
+        factorisations leave most of the GPU to the other streams, where cuSOLVER's
+        per-column reduction serialises them (config 4 on a B200: 14.9 solves/s on four
+        streams against 9.5 to 14.2 from run to run with cuSOLVER) -- and "auto" with one."""
         import torch
 
         from . import core
@@ -119,6 +132,7 @@ class PartialWaveServer:
         torch.cuda.set_device(device)
         self.device = device
         self.ks, self.ns, self.z, self.kmax = ks, len(t) - ks, float(z), kmax
+        self.eigensolver = eigensolver or ("own" if n_streams > 1 else "auto")
         self.basis = core.define_spline(t, ks)
         self.P = core.as_fortran(P)
         self._setup_ctx = core.Context()
@@ -139,7 +153,9 @@ class PartialWaveServer:
     # ---- client side ----
     def submit(self, sym, want_vectors=True):
         """sym: dict with nch, lch, ech, coefs.  Returns a Request (wait() for the result)."""
-        nb = request_bytes(sym["nch"], self.ns, sym["lch"], self.ks, want_vectors)
+        khm = shard.symmetry_dims(sym["nch"], self.ns, sym["lch"], self.ks)[0]
+        own = self.eigensolver == "own" or (self.eigensolver == "auto" and khm >= OWN_EIG_MIN)
+        nb = request_bytes(sym["nch"], self.ns, sym["lch"], self.ks, want_vectors, own_eig=own)
         with self._lock:
             r = Request(self._next_id, sym, want_vectors)
             self._next_id += 1
@@ -182,6 +198,7 @@ class PartialWaveServer:
         with torch.cuda.stream(stream):
             ctx = core.Context(stream=stream)
             ctx.use_tables(self.tables)
+            ctx.set_eigensolver(self.eigensolver)
             while True:
                 r = self.queue.take()
                 if r is None:

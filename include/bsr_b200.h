@@ -323,6 +323,16 @@ int bsrg_ctx_set_refine(bsrg_ctx *c, int on);
  *      I_data.f90:206) as bsrg_dgemm_tf32x3's split-precision tensor-core
  *      product; everything else, the eigensolve and its refinement stay FP64. */
 int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed);
+/* ---- No counterpart in the reference (its DSYEV call is diag_hd.f90:312):
+ *      which dense eigensolver bsrg_diag_hd uses on this context.  which = 0
+ *      (default): the library's two-stage solver from 7000 rows of the dense
+ *      problem (where it was measured faster than cuSOLVER's syevd on a B200)
+ *      and cuSOLVER's below; 1: the library's at every size up to 10240 rows;
+ *      2: cuSOLVER's at every size.  Contexts that solve concurrently on
+ *      several streams do better with 1: the library's solver leaves most of
+ *      the GPU to the other streams where cuSOLVER's reduction serialises
+ *      them.  The environment variable BSRG_EIG=own|lib overrides it. */
+int bsrg_ctx_set_eigensolver(bsrg_ctx *c, int which);
 int bsrg_diag_hd_refine_stats(bsrg_ctx *c, int n, double *corr, double *resid);
 /* ---- No counterpart in the reference: how many bsrg_diag_hd calls on this
  *      context redid their channel problems (diag_hd.f90:82-111) on the

@@ -170,3 +170,24 @@ def test_own_channel_solves_match_library(monkeypatch, name):
     dv = np.max(np.abs(ba * sg[None, :] - bl), axis=0) / np.maximum(np.max(np.abs(bl), axis=0), 1e-300)
     print("%s channel eigenvectors: max relative difference %.2e" % (name, dv.max()))
     assert np.max(dv) < 1e-4      # eigenvector error ~ eps ||C|| / gap on both sides
+
+
+def test_eigensolver_choice_config1():
+    """The library's two-stage eigensolver and cuSOLVER's syevd, chosen per context, give the
+    same refined spectrum per eigenvalue (config 1, khm 480), and a bad choice is rejected."""
+    import bsr_b200 as bsr
+    pw = W.partial_wave("config1")
+    gb = bsr.define_spline(pw["t"], pw["ks"])
+    ctx = bsr.Context()
+    H = bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], pw["P"], pw["kmax"], pw["coefs"])
+    out = {}
+    for which in ("own", "lib", "auto"):
+        ctx.set_eigensolver(which)
+        out[which] = to_np(bsr.diag_hd(ctx, gb, pw["lch"], H["hcc"], want_vectors=True)["eval"])
+    rel = per_eig_rel(out["own"], out["lib"])
+    print("config1 own vs cuSOLVER dense eigensolver, refined: max rel %.2e" % rel.max())
+    assert np.max(rel) <= TOL_E
+    assert np.array_equal(out["auto"], out["lib"])       # 480 rows: below the crossover
+    with pytest.raises(Exception):
+        bsr._lib.call("bsrg_ctx_set_eigensolver", ctx.handle, 3)
+

@@ -108,3 +108,26 @@ def test_budget_rejects(batch):
             r.wait(5)
     finally:
         srv.close()
+
+
+def test_alone_equals_mix_with_vectors(batch):
+    """With eigenvectors the workers of a multi-stream server use the library's two-stage
+    eigensolver; a request's eigenvalues are still bitwise those of the same request alone
+    on a one-stream server using that eigensolver."""
+    from bsr_b200 import serve
+    b, small = batch
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=1, eigensolver="own")
+    try:
+        alone = [serve.run_stream(srv, [s], [0.0])[0].wait(120) for s in small]
+    finally:
+        srv.close()
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=3)
+    assert srv.eigensolver == "own"
+    try:
+        order = list(range(len(small)))[::-1] + list(range(len(small)))
+        mixed = [r.wait(120) for r in serve.run_stream(srv, [small[q] for q in order], [0.0] * len(order))]
+    finally:
+        srv.close()
+    for q, res in zip(order, mixed):
+        assert res["khm"] == alone[q]["khm"]
+        assert np.array_equal(res["eval"], alone[q]["eval"]), "symmetry %d differs in a mix" % q

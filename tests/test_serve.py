@@ -115,3 +115,14 @@ def test_autotune_prefers_more_streams_within_margin(monkeypatch):
         assert cache["k"] == {"n_streams": want, "solves_per_s": rates}
         assert serve.autotune_streams(make, sample, candidates=(1, 2, 4), cache=cache, key="k") == want
         assert len(made) == 3                   # the cached choice runs nothing
+
+
+def test_request_bytes_counts_the_library_eigensolver():
+    lch = [c % 7 for c in range(40)]
+    a = serve.request_bytes(40, 150, lch, 8)
+    b = serve.request_bytes(40, 150, lch, 8, own_eig=True)
+    khm = 40 * 150 - sum(min(l, 6) + 1 for l in lch)
+    assert b - a == int((6.5 * khm * khm + 3000 * khm) * 8)
+    # without eigenvectors neither eigensolver workspace nor the refinement is counted
+    assert serve.request_bytes(40, 150, lch, 8, want_vectors=False, own_eig=True) == \
+        serve.request_bytes(40, 150, lch, 8, want_vectors=False)
