@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--dense-eig", type=int, default=0, metavar="N",
                     help="time only the library's dense eigensolver (bsrg_dsyevd) on a seeded symmetric N x N "
                          "matrix, with its stage times, beside cuSOLVER's (torch.linalg.eigh); for profiling")
+    ap.add_argument("--assemble-only", action="store_true",
+                    help="time only the assembly of the workload's partial wave (R^k tables, exchange, "
+                         "direct and one-electron parts; no eigensolve), with its stage times; for profiling")
     return ap.parse_args()
 
 
@@ -88,6 +91,33 @@ def run_dense_eig(args):
     print(json.dumps({"dense_eig_n": n, "own_ms": own, "cusolver_ms": lib, "max_rel_eig_diff": err,
                       "stages_ms": {k: round(v[0] / args.steps, 3) for k, v in st.items() if k.startswith("eig_")}}),
           flush=True)
+
+
+def run_assemble_only(args):
+    """The assembly alone (bsrg_assemble on the workload's partial wave): --warmup untimed
+    calls, then --steps timed calls (CUDA events), with the library's stage times."""
+    import torch
+    import bsr_b200 as bsr
+    from bsr_b200 import workload as W
+    pw = W.partial_wave(args.workload)
+    gb = bsr.define_spline(pw["t"], pw["ks"])
+    ctx = bsr.Context()
+    P = bsr.as_fortran(pw["P"])
+    for _ in range(max(args.warmup, 0)):
+        bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], P, pw["kmax"], pw["coefs"])
+    torch.cuda.synchronize()
+    ctx.set_timing(True)
+    ctx.stage_times()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        bsr.assemble(ctx, gb, pw["z"], pw["lch"], pw["ech"], P, pw["kmax"], pw["coefs"])
+    s1.record()
+    s1.synchronize()
+    st = ctx.stage_times()
+    ctx.set_timing(False)
+    print(json.dumps({"assemble_workload": args.workload, "ms_per_call": s0.elapsed_time(s1) / args.steps,
+                      "stages_ms": {k: round(v[0] / args.steps, 4) for k, v in st.items() if v[0] > 0}}), flush=True)
 
 
 def dist_env():
@@ -824,6 +854,8 @@ def main():
     args = parse()
     if args.dense_eig > 0:
         run_dense_eig(args)
+    elif args.assemble_only:
+        run_assemble_only(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
