@@ -1899,7 +1899,7 @@ static Syevd2Layout syevd2_layout(int n)
     L.gram = take((size_t)(n / NB + 8) * NB * NB);
     L.flags = take(8);
     L.W1 = take((size_t)Q1W * n);
-    L.W2 = take((size_t)Q1W * n);
+    L.W2 = take(std::max((size_t)Q1W * n, (size_t)(Q1W / 2) * (Q1W / 2)));   // also the T merges' temporary
     L.Vg = take((size_t)Q1W * n);
     L.Gq = take((size_t)Q1W * Q1W);
     L.Tg = take((size_t)Q1W * Q1W);

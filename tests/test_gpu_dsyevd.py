@@ -14,7 +14,7 @@ EPS = np.finfo(float).eps
 def _cases():
     rng = np.random.default_rng(21)
     out = []
-    for n in (1, 2, 3, 31, 33, 64, 97, 300, 1000, 2047):
+    for n in (1, 2, 3, 31, 33, 40, 57, 64, 97, 300, 1000, 2047):
         M = rng.standard_normal((n, n))
         out.append(("random%d" % n, (M + M.T) / 2))
     n = 800
