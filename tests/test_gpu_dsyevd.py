@@ -80,3 +80,33 @@ def test_dsytrd_2stage(case):
     an = np.max(np.abs(wr))
     assert np.max(np.abs(np.linalg.eigvalsh(T) - wr)) <= 8 * max(n, 16) * EPS * an, name
     ctx.close()
+
+
+def test_dsyevd_size_sweep():
+    """Every size from 1 to 300 in steps of 7, plus the panel, leaf and merged-reflector
+    boundaries (32, 64, 128, 256, 257 and one more): eigenvalues, residuals and orthogonality
+    at the same bar, one context reused across sizes (the workspace only grows)."""
+    import torch
+    import bsr_b200 as bsr
+    from bsr_b200._lib import call
+    from bsr_b200.core import _ptr
+    rng = np.random.default_rng(5)
+    ctx = bsr.Context()
+    sizes = sorted(set(range(1, 301, 7)) | {32, 63, 64, 65, 128, 129, 256, 257, 258, 289})
+    for n in sizes:
+        M = rng.standard_normal((n, n))
+        A = (M + M.T) / 2
+        dA = torch.from_numpy(np.tril(A).T.copy()).cuda()
+        w = torch.empty(n, dtype=torch.float64, device="cuda")
+        Z = torch.empty(n * n, dtype=torch.float64, device="cuda")
+        call("bsrg_dsyevd", ctx.handle, n, _ptr(dA), n, _ptr(w), _ptr(Z), n)
+        torch.cuda.synchronize()
+        W = w.cpu().numpy()
+        V = Z.cpu().numpy().reshape(n, n).T
+        wr = np.linalg.eigvalsh(A)
+        an = max(np.max(np.abs(wr)), 1e-300)
+        tol = 8 * max(n, 16) * EPS
+        assert np.max(np.abs(W - wr)) <= tol * an, (n, np.max(np.abs(W - wr)) / an)
+        assert np.max(np.abs(A @ V - V * W[None, :])) <= tol * an, n
+        assert np.max(np.abs(V.T @ V - np.eye(n))) <= tol, n
+    ctx.close()
