@@ -363,9 +363,15 @@ __global__ void __launch_bounds__(128) ypass1_kernel(int m, const double *__rest
     __syncthreads();
     for (int q = tid; q < NB * NB; q += 128) {
         const int i = q % NB, j = q / NB;
-        double s = 0.0;
-        for (int rr = 0; rr < 128; rr++) s += Vs[rr][i] * Ys[rr][j];
-        Mp[(long)blockIdx.x * NB * NB + q] = s;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;     // four chains over the rows
+#pragma unroll 4
+        for (int rr = 0; rr < 128; rr += 4) {
+            s0 = fma(Vs[rr][i], Ys[rr][j], s0);
+            s1 = fma(Vs[rr + 1][i], Ys[rr + 1][j], s1);
+            s2 = fma(Vs[rr + 2][i], Ys[rr + 2][j], s2);
+            s3 = fma(Vs[rr + 3][i], Ys[rr + 3][j], s3);
+        }
+        Mp[(long)blockIdx.x * NB * NB + q] = (s0 + s1) + (s2 + s3);
     }
     // the last CTA to finish sums the partials in chunk order and forms M2 = 1/2 T^T M once
     // (at Mp + gridDim.x NB^2) for ypass2; it resets the ticket for the next panel
