@@ -614,7 +614,7 @@ def run_b200(args):
     dom_own = max(cand, key=lambda k: cand[k])
     r = dict(by_stage[dom_own])
     r["kernel"] = {"rk_expand": "rkb_pad_kernel", "exchange": "exchange_fused_kernel",
-                   "eig_chase": "sb2st3_kernel", "eig_q2": "q2p_apply_kernel",
+                   "eig_chase": "sb2st5_kernel", "eig_q2": "q2p_apply_kernel",
                    "refine": "refine_gemm_kernel"}[dom_own]
     r["stage"] = dom_own
     r["traffic"] = None

@@ -912,6 +912,222 @@ __global__ void __launch_bounds__(64) sb2st3_kernel(Sb2stArgs a)
     }
 }
 
+// sb2st3_kernel with each step's two-sided update of the diagonal block and its left update of
+// the previous bulge moved to warps of their own (sb2st5_kernel).  Warp 0 keeps the chain from
+// step to step -- the reflector from x, the right update of B, and B's new first column as the
+// next x -- which reads neither.  Warp 2 loads D of step i itself (once the previous sweep has
+// completed step i+2) and updates and stores it; warp 3 applies step i's reflector from the left
+// to the previous step's updated B (warp 0 leaves it in one of two shared buffers) and stores
+// it; both take v_i and tau_i from a ring of four in shared memory and run behind warp 0.  The
+// helper (warp 1) publishes step i once warp 0 has stored step i and warps 2 and 3 step i-1:
+// sweep j+1's step i-2, the first to wait for it, reads the first column of D_{i-1} and of the
+// previous bulge but neither D_i nor step i's left update.  The arithmetic is sb2st3's.
+__global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
+{
+    __shared__ double Ts[NB][NB + 1], Cs[2][NB][NB + 1];
+    __shared__ double vring[4][NB], tauring[4], ws2[NB], wsd[NB];
+    __shared__ volatile int done, doneD, doneL, vready, seen, quit;
+    const int t = threadIdx.x & 31, w = threadIdx.x >> 5, n = a.n;
+    double *AB = a.AB;
+    auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
+    // bounded wait of lane 0 until *flag >= need (false: gave up; the error flag is set)
+    auto wait_ge = [&](volatile int *flag, int need) -> bool {
+        if (t == 0) {
+            const unsigned long long t0 = gtime();
+            while (*flag < need) {
+                if (quit) break;
+                if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); quit = 1; break; }
+            }
+            __threadfence_block();
+        }
+        __syncwarp();
+        return !quit;
+    };
+    for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
+        const int nst = sweep_steps(n, j);
+        const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
+        if (threadIdx.x == 0) { done = 0; doneD = 0; doneL = 0; vready = 0; seen = j > 0 ? 0 : 1 << 30; quit = 0; }
+        __syncthreads();
+        if (w == 1) {
+            // ---- helper: publish what both workers have stored, watch the previous sweep ----
+            if (t == 0) {
+                int pub = 0, sv = j > 0 ? 0 : 1 << 30;
+                unsigned long long t0 = gtime();
+                while (pub < nst) {
+                    const int d0 = done, dd = doneD, dl = doneL;
+                    const int ready = (d0 == nst && dd == nst && dl == nst) ? nst
+                                                                          : min(min(d0, min(dd, dl) + 1), nst - 1);
+                    if (ready > pub) {
+                        __threadfence();
+                        *(volatile int *)(a.progress + j) = ready;
+                        pub = ready;
+                        t0 = gtime();
+                        continue;
+                    }
+                    if (quit) break;
+                    if (sv < nprev) {
+                        const int v = *(volatile int *)(a.progress + (j - 1));
+                        if (v > sv) {
+                            __threadfence();
+                            sv = v;
+                            seen = v;
+                            t0 = gtime();
+                            continue;
+                        }
+                    }
+                    if (*(volatile int *)a.err) { quit = 1; break; }
+                    if (gtime() - t0 > WAIT_NS) { atomicExch(a.err, 2); quit = 1; break; }
+                }
+            }
+        } else if (w == 2) {
+            // ---- the diagonal blocks, one step behind warp 0 ----
+            for (int i = 0; i < nst; i++) {
+                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+                if (!wait_ge(&seen, min(i + 3, nprev))) break;
+                double Dr[NB];
+#pragma unroll
+                for (int c = 0; c < NB; c++) Dr[c] = (t < L && c <= t) ? __ldcg(at(r0 + t, r0 + c)) : 0.0;
+                if (!wait_ge(&vready, i + 1)) break;
+                const double *vs = vring[i & 3];
+                const double tau = tauring[i & 3], v = vs[t];
+                if (tau != 0.0) {
+#pragma unroll
+                    for (int c = 0; c < NB; c++) Ts[t][c] = Dr[c];
+                    __syncwarp();
+                    double p0 = 0.0, p1 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < NB; c += 2) {
+                        const double d0 = c <= t ? Dr[c] : Ts[c][t];
+                        const double d1 = c + 1 <= t ? Dr[c + 1] : Ts[c + 1][t];
+                        p0 = fma(d0, vs[c], p0);
+                        p1 = fma(d1, vs[c + 1], p1);
+                    }
+                    const double p = t < L ? tau * (p0 + p1) : 0.0;
+                    double vp = v * p;
+                    for (int o = 16; o > 0; o >>= 1) vp += __shfl_xor_sync(0xffffffffu, vp, o);
+                    const double wv = p - 0.5 * tau * vp * v;
+                    wsd[t] = wv;
+                    __syncwarp();
+#pragma unroll
+                    for (int c = 0; c < NB; c++)
+                        if (c <= t) Dr[c] -= v * wsd[c] + wv * vs[c];
+                    if (t < L) {
+#pragma unroll
+                        for (int c = 0; c < NB; c++)
+                            if (c <= t) *at(r0 + t, r0 + c) = Dr[c];
+                    }
+                }
+                __threadfence_block();
+                __syncwarp();
+                if (t == 0) doneD = i + 1;
+            }
+        } else if (w == 3) {
+            // ---- the left updates: step i's reflector on the previous step's updated B ----
+            for (int i = 0; i < nst; i++) {
+                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+                const int col = i == 0 ? j : r0 - NB;
+                const int nl = r0 - col - 1;
+                if (!wait_ge(&vready, i + 1)) break;
+                const double *vs = vring[i & 3];
+                const double tau = tauring[i & 3], v = vs[t];
+                if (tau != 0.0 && nl > 0) {
+                    double (*C)[NB + 1] = Cs[(i - 1) & 1];
+                    if (t < nl) {
+                        double w0 = 0.0, w1 = 0.0;
+#pragma unroll
+                        for (int q = 0; q < NB; q += 2) {
+                            w0 = fma(vs[q], C[q][t + 1], w0);
+                            w1 = fma(vs[q + 1], C[q + 1][t + 1], w1);
+                        }
+                        ws2[t] = tau * (w0 + w1);
+                    }
+                    __syncwarp();
+                    if (t < L) {
+#pragma unroll
+                        for (int c = 0; c < NB - 1; c++)
+                            if (c < nl) *at(r0 + t, col + 1 + c) = fma(-v, ws2[c], C[t][c + 1]);
+                    }
+                    __syncwarp();
+                }
+                __threadfence_block();
+                __syncwarp();
+                if (t == 0) doneL = i + 1;
+            }
+        } else {
+            // ---- warp 0: reflectors and right updates ----
+            auto load_b = [&](int i, double *Br) {
+                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+                const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+#pragma unroll
+                for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
+            };
+            double Br[NB], xnext = 0.0;
+            bool ok = wait_ge(&seen, min(3, nprev));
+            if (ok) load_b(0, Br);
+            for (int i = 0; ok && i < nst; i++) {
+                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+                const int col = i == 0 ? j : r0 - NB;
+                const int nl = r0 - col - 1;
+                const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+                const double xl = i == 0 ? (t < L ? __ldcg(at(r0 + t, col)) : 0.0) : xnext;
+                // ---- the reflector, into ring slot i & 3 once warp 2 has finished step i-4 ----
+                double sig = (t >= 1 && t < L) ? xl * xl : 0.0;
+                for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+                const double alpha = __shfl_sync(0xffffffffu, xl, 0);
+                double tau = 0.0, scale = 0.0, beta = alpha;
+                if (sig != 0.0) {
+                    beta = -copysign(sqrt(alpha * alpha + sig), alpha);
+                    tau = (beta - alpha) / beta;
+                    scale = 1.0 / (alpha - beta);
+                }
+                const double v = t == 0 ? 1.0 : (t < L ? xl * scale : 0.0);
+                if (i >= 4 && (!(ok = wait_ge(&doneD, i - 3)) || !(ok = wait_ge(&doneL, i - 3)))) break;
+                double *vs = vring[i & 3];
+                vs[t] = v;
+                if (t == 0) tauring[i & 3] = tau;
+                a.V2[((long)j * a.S + i) * NB + t] = v;
+                if (t == 0) a.tau2[(long)j * a.S + i] = tau;
+                if (t < L) *at(r0 + t, col) = t == 0 ? beta : 0.0;
+                __threadfence_block();
+                __syncwarp();
+                if (t == 0) vready = i + 1;
+                if (tau != 0.0) {
+                    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                    for (int c = 0; c < NB; c += 2) {
+                        s0 = fma(Br[c], vs[c], s0);
+                        s1 = fma(Br[c + 1], vs[c + 1], s1);
+                    }
+                    const double sr = tau * (s0 + s1);
+#pragma unroll
+                    for (int c = 0; c < NB; c++) Br[c] = fma(-sr, vs[c], Br[c]);
+                    if (t < nb2) {
+#pragma unroll
+                        for (int c = 0; c < NB; c++)
+                            if (c < L) *at(r1 + t, r0 + c) = Br[c];
+                    }
+                }
+                // B goes to buffer i & 1 for warp 3's left update of step i+1, once warp 3 is done
+                // with the buffer's last use (step i-1)
+                xnext = Br[0];
+                if (i >= 1 && !(ok = wait_ge(&doneL, i))) break;
+#pragma unroll
+                for (int c = 0; c < NB; c++) Cs[i & 1][t][c] = Br[c];
+                __threadfence_block();
+                __syncwarp();
+                if (t == 0) done = i + 1;
+                if (i + 1 < nst) {
+                    ok = wait_ge(&seen, min(i + 4, nprev));
+                    if (ok) load_b(i + 1, Br);
+                }
+            }
+            if (!ok && t == 0) quit = 1;
+        }
+        __syncthreads();
+        if (*(volatile int *)a.err) return;
+    }
+}
+
 // d(c) = A(c, c), e(c) = A(c+1, c)
 __global__ void tridiag_extract_kernel(int n, const double *__restrict__ AB, double *d, double *e)
 {
@@ -1987,11 +2203,15 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         Sb2stArgs a2{AB, n, V2, tau2, S, progress, sw.err};
         void *args[] = {&a2};
         if (!getenv("BSRG_SB2ST_SHARED") && !getenv("BSRG_SB2ST_ONEWARP")) {
-            // one sweep per CTA at a time, a helper warp beside the computing one (sb2st3_kernel);
-            // one CTA per SM: about n / (3.4 NB) sweeps are active at once, so nsm CTAs never make a
-            // sweep wait for its CTA, and no waiting CTA shares an SM with a working one
+            // one sweep per CTA at a time: the chain of reflectors and right updates on one warp, the
+            // diagonal blocks and the left updates on two more, a helper warp that publishes the steps
+            // (sb2st5_kernel; BSRG_SB2ST_TWOWARP: sb2st3_kernel, computing warp and helper only).  One
+            // CTA per SM: about n / (3.4 NB) sweeps are active at once, so nsm CTAs never make a sweep
+            // wait for its CTA, and no waiting CTA shares an SM with a working one
             const int ctas = std::max(1, std::min(n - 2, nsm));
-            if ((e = cudaLaunchCooperativeKernel((const void *)sb2st3_kernel, ctas, 64, args, 0, st)) != cudaSuccess)
+            const bool two = getenv("BSRG_SB2ST_TWOWARP") != nullptr;
+            if ((e = cudaLaunchCooperativeKernel(two ? (const void *)sb2st3_kernel : (const void *)sb2st5_kernel, ctas,
+                                                 two ? 64 : 128, args, 0, st)) != cudaSuccess)
                 return cuda_fail(e, "dsyevd bulge chasing");
         } else if (getenv("BSRG_SB2ST_SHARED")) {
             int per = 1;
