@@ -924,9 +924,9 @@ __global__ void __launch_bounds__(64) sb2st3_kernel(Sb2stArgs a)
 // previous bulge but neither D_i nor step i's left update.  The arithmetic is sb2st3's.
 __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
 {
-    __shared__ double Ts[NB][NB + 1], Cs[2][NB][NB + 1];
+    __shared__ double Ts[NB][NB + 1], Cs[2][NB][NB + 1], Bsm[2][NB][NB + 1];
     __shared__ double vring[4][NB], tauring[4], ws2[NB], wsd[NB];
-    __shared__ volatile int done, doneD, doneL, vready, seen, quit;
+    __shared__ volatile int done, doneD, doneL, vready, bready, seen, quit;
     const int t = threadIdx.x & 31, w = threadIdx.x >> 5, n = a.n;
     double *AB = a.AB;
     auto at = [&](int r, int c) -> double * { return AB + (r - c) + (long)LDAB * c; };
@@ -946,7 +946,9 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
     for (int j = blockIdx.x; j < n - 2; j += gridDim.x) {
         const int nst = sweep_steps(n, j);
         const int nprev = j > 0 ? sweep_steps(n, j - 1) : 0;
-        if (threadIdx.x == 0) { done = 0; doneD = 0; doneL = 0; vready = 0; seen = j > 0 ? 0 : 1 << 30; quit = 0; }
+        if (threadIdx.x == 0) {
+            done = 0; doneD = 0; doneL = 0; vready = 0; bready = 0; seen = j > 0 ? 0 : 1 << 30; quit = 0;
+        }
         __syncthreads();
         if (w == 1) {
             // ---- helper: publish what both workers have stored, watch the previous sweep ----
@@ -1022,7 +1024,22 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
                 if (t == 0) doneD = i + 1;
             }
         } else if (w == 3) {
-            // ---- the left updates: step i's reflector on the previous step's updated B ----
+            // ---- the left updates: step i's reflector on the previous step's updated B; and the
+            //      B block of step i+1 into shared buffer (i+1) & 1 for warp 0, once the previous
+            //      sweep has completed step i+3 ----
+            auto stage_b = [&](int i) -> bool {
+                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
+                const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
+                if (!wait_ge(&seen, min(i + 3, nprev))) return false;
+                double (*B)[NB + 1] = Bsm[i & 1];
+#pragma unroll
+                for (int c = 0; c < NB; c++) B[t][c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
+                __threadfence_block();
+                __syncwarp();
+                if (t == 0) bready = i + 1;
+                return true;
+            };
+            if (nst > 0 && !stage_b(0)) goto sweep_end;
             for (int i = 0; i < nst; i++) {
                 const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
                 const int col = i == 0 ? j : r0 - NB;
@@ -1052,18 +1069,12 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
                 __threadfence_block();
                 __syncwarp();
                 if (t == 0) doneL = i + 1;
+                if (i + 1 < nst && !stage_b(i + 1)) break;
             }
         } else {
             // ---- warp 0: reflectors and right updates ----
-            auto load_b = [&](int i, double *Br) {
-                const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
-                const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
-#pragma unroll
-                for (int c = 0; c < NB; c++) Br[c] = (t < nb2 && c < L) ? __ldcg(at(r1 + t, r0 + c)) : 0.0;
-            };
             double Br[NB], xnext = 0.0;
             bool ok = wait_ge(&seen, min(3, nprev));
-            if (ok) load_b(0, Br);
             for (int i = 0; ok && i < nst; i++) {
                 const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
                 const int col = i == 0 ? j : r0 - NB;
@@ -1085,12 +1096,18 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
                 double *vs = vring[i & 3];
                 vs[t] = v;
                 if (t == 0) tauring[i & 3] = tau;
+                __threadfence_block();                   // (before the global stores: it need not wait for them)
+                __syncwarp();
+                if (t == 0) vready = i + 1;
                 a.V2[((long)j * a.S + i) * NB + t] = v;
                 if (t == 0) a.tau2[(long)j * a.S + i] = tau;
                 if (t < L) *at(r0 + t, col) = t == 0 ? beta : 0.0;
-                __threadfence_block();
-                __syncwarp();
-                if (t == 0) vready = i + 1;
+                if (!(ok = wait_ge(&bready, i + 1))) break;
+                {
+                    const double (*B)[NB + 1] = Bsm[i & 1];
+#pragma unroll
+                    for (int c = 0; c < NB; c++) Br[c] = B[t][c];
+                }
                 if (tau != 0.0) {
                     double s0 = 0.0, s1 = 0.0;
 #pragma unroll
@@ -1116,13 +1133,10 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
                 __threadfence_block();
                 __syncwarp();
                 if (t == 0) done = i + 1;
-                if (i + 1 < nst) {
-                    ok = wait_ge(&seen, min(i + 4, nprev));
-                    if (ok) load_b(i + 1, Br);
-                }
             }
             if (!ok && t == 0) quit = 1;
         }
+    sweep_end:
         __syncthreads();
         if (*(volatile int *)a.err) return;
     }
