@@ -675,14 +675,17 @@ def run_b200(args):
 
 
 def bench_mixed(torch, bsr, pw, steps=2):
-    """Config 3: the config-2 partial wave in the mixed-precision form (direct contraction as
-    the tcgen05 split-TF32 product; FP64 eigensolve and refinement) beside the FP64 path:
-    solves/s of both by CUDA events and the mixed eigenvalues' error per eigenvalue."""
+    """Config 3: the config-2 partial wave in the mixed-precision forms beside the FP64 path --
+    "i8": the direct contraction from 8-bit digits on tcgen05 with exact int32 accumulation
+    (bsrg_dgemm_ozaki), "tf32": the split-TF32 product with FP32 accumulation; the eigensolve and
+    its refinement FP64 in all three.  Solves/s of each by CUDA events, the direct stage's time,
+    and each mixed form's eigenvalue error per eigenvalue against the FP64 path."""
     out = {}
     evs = {}
-    for name, mixed in (("fp64", False), ("mixed", True)):
+    forms = (("fp64", False, "i8"), ("mixed", True, "i8"), ("mixed_tf32", True, "tf32"))
+    for name, mixed, form in forms:
         ctx = bsr.Context()
-        ctx.set_precision(mixed)
+        ctx.set_precision(mixed, form)
         basis = bsr.define_spline(pw["t"], pw["ks"])
         P = bsr.as_fortran(pw["P"])
 
@@ -702,16 +705,25 @@ def bench_mixed(torch, bsr, pw, steps=2):
         evs[name] = res["eval"].cpu().numpy()
         if mixed:
             corr, resid = ctx.refine_stats(res["khm"])
-            out["mixed_residual_norm_max"] = float(resid.max().item())
+            out[name + "_residual_norm_max"] = float(resid.max().item())
+        ctx.set_timing(True)
+        ctx.stage_times()
+        step()
+        torch.cuda.synchronize()
+        out[name + "_direct_ms"] = round(ctx.stage_times()["direct"], 4)
         ctx.close()
-    e64, emx = evs["fp64"], evs["mixed"]
-    rel = np.abs(emx - e64) / np.maximum(np.abs(e64), 1e-3)
-    out.update({"workload": "config3: the config2 partial wave, direct contraction in split TF32 on tcgen05 "
-                            "(FP32 accumulation in tensor memory), FP64 eigensolve and Rayleigh refinement",
-                "eig_rel_err_vs_fp64": {"max": float(rel.max()), "p99": float(np.percentile(rel, 99)),
-                                        "median": float(np.median(rel)),
-                                        "what": "|E_mixed - E_fp64| / max(|E_fp64|, 1e-3) per eigenvalue"},
-                "meets_1e-10": bool(rel.max() <= 1e-10),
+    e64 = evs["fp64"]
+    for name in ("mixed", "mixed_tf32"):
+        rel = np.abs(evs[name] - e64) / np.maximum(np.abs(e64), 1e-3)
+        out["eig_rel_err_vs_fp64" + ("" if name == "mixed" else "_tf32")] = {
+            "max": float(rel.max()), "p99": float(np.percentile(rel, 99)), "median": float(np.median(rel)),
+            "max_lowest_1100": float(rel[:1100].max()),
+            "what": "|E_mixed - E_fp64| / max(|E_fp64|, 1e-3) per eigenvalue"}
+    rel = out["eig_rel_err_vs_fp64"]
+    out.update({"workload": "config3: the config2 partial wave; mixed = direct contraction from 8-bit digits on "
+                            "tcgen05 (kind::i8, exact int32 accumulation, 8 digits), mixed_tf32 = split TF32 on "
+                            "tcgen05 (FP32 accumulation); FP64 eigensolve and Rayleigh refinement in every form",
+                "meets_1e-10": bool(rel["max"] <= 1e-10),
                 "speedup_vs_fp64": out["mixed_solves_per_s"] / out["fp64_solves_per_s"]})
     return out
 

@@ -85,6 +85,9 @@ SIGNATURES = [
     ("bsrg_dsytrd_2stage", _c_int, [_P, _c_int, _P, _c_int, _P, _P]),
     ("bsrg_dgemm_tf32x3", _c_int, [_c_int, _c_int, _c_int, _c_double, _P, _c_int, _P, _c_int, _c_double, _P,
                                    _c_int, _P, _P]),
+    ("bsrg_dgemm_ozaki_work_bytes", _c_size_t, [_c_int, _c_int, _c_int, _c_int]),
+    ("bsrg_dgemm_ozaki", _c_int, [_c_int, _c_int, _c_int, _c_double, _P, _c_int, _P, _c_int, _c_double, _P, _c_int,
+                                  _c_int, _P, _c_size_t, _P, _P]),
     ("bsrg_partial_wave_solve", _c_int, [_P, _c_int, _c_int, _DP, _c_double, _c_int, _IP, _DP, _c_int, _DP,
                                          _c_int, _c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP, _c_int, _DP, _IP]),
 ]

@@ -30,6 +30,7 @@ UNITS = {
     "tridiag_dc.cu": [],
     "syevd2.cu": [],
     "tc_mixed.cu": [],
+    "tc_ozaki.cu": [],
     "chan_eig.cu": [],
     "dense_chol.cu": [],
 }

@@ -361,9 +361,11 @@ class Context:
         """FP64 Rayleigh-quotient refinement of diag_hd's eigenpairs (on by default)."""
         call("bsrg_ctx_set_refine", self.handle, 1 if on else 0)
 
-    def set_precision(self, mixed=True):
-        """Mixed-precision form (tensor-core split-TF32 direct contraction) or FP64 (default)."""
-        call("bsrg_ctx_set_precision", self.handle, 1 if mixed else 0)
+    def set_precision(self, mixed=True, form="i8"):
+        """FP64 (mixed=False, the default) or the mixed-precision form: the direct contraction on
+        the tensor cores from 8-bit digits with exact integer accumulation (form "i8", FP64
+        accuracy) or as the split-TF32 product with FP32 accumulation (form "tf32")."""
+        call("bsrg_ctx_set_precision", self.handle, {"i8": 1, "tf32": 2}[form] if mixed else 0)
 
     def set_eigensolver(self, which="auto"):
         """diag_hd's dense eigensolver: "auto" (the library's from 7000 rows, cuSOLVER's below),

@@ -1134,7 +1134,8 @@ int bsrg_ctx_stage_times(bsrg_ctx *c, double *ms, int *launches, int n)
 int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed)
 {
     if (!c) { set_error("ctx_set_precision: null context"); return BSRG_ERR_ARG; }
-    c->precision = mixed ? 1 : 0;
+    if (mixed < 0 || mixed > 2) { set_error("ctx_set_precision: form %d is not 0, 1 or 2", mixed); return BSRG_ERR_ARG; }
+    c->precision = mixed;
     return BSRG_OK;
 }
 
@@ -1328,6 +1329,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         add(sizeof(double) * nk * nk);
         add(sizeof(double) * nk * maxgd);
         add(sizeof(int) * 4);      // the tensor-core product's wait flag (mixed precision)
+        if (c->precision == 1) add(ozaki_ws_bytes((int)nk, (int)maxgd, (int)nk, 8));   // its digit planes
     }
     add(sizeof(unsigned short) * (size_t)ncoef);
     int rc = ctx_reserve(c, need);
@@ -1355,7 +1357,9 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
     double *R3 = direct_blas ? ar.take<double>(nk * nk) : nullptr;
     double *Cd = direct_blas ? ar.take<double>(nk * maxgd) : nullptr;
     int *d_tcerr = direct_blas ? ar.take<int>(4) : nullptr;
-    const bool mixed = c->precision == 1;
+    const bool mixed = c->precision != 0;
+    const size_t oz_bytes = direct_blas && c->precision == 1 ? ozaki_ws_bytes((int)nk, (int)maxgd, (int)nk, 8) : 0;
+    char *oz_ws = oz_bytes ? ar.take<char>(oz_bytes) : nullptr;
     if (mixed && d_tcerr) {
         cudaError_t em = cudaMemsetAsync(d_tcerr, 0, sizeof(int) * 4, s);
         if (em != cudaSuccess) return cuda_fail(em, "assemble: mixed flag");
@@ -1494,9 +1498,12 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
             direct_density_kernel<<<g1, 128, 0, s>>>(ns, ks, nd, gdd, d_ca, d_cb, d_cv, P, Xd);
             if (direct_blas) {
                 direct_table_kernel<<<(unsigned)((nk * nk + 255) / 256), 256, 0, s>>>(ns, ks, rkbk, PL, R3);
-                // C = R Xd on the FP64 tensor pipe (dgemm.cu), or in the mixed-precision form as the
-                // split-TF32 product on tcgen05 (tc_mixed.cu)
-                if (mixed)
+                // C = R Xd on the FP64 tensor pipe (dgemm.cu), or in the mixed-precision form from 8-bit
+                // digits on tcgen05 (tc_ozaki.cu), or as the split-TF32 product (tc_mixed.cu)
+                if (oz_ws)
+                    rc = ozaki_gemm((int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd, (long)nk, 8,
+                                    oz_ws, oz_bytes, d_tcerr, s);
+                else if (mixed)
                     rc = tf32x3_gemm((int)nk, nd, (int)nk, 1.0, R3, (long)nk, Xd, (long)nk, 0.0, Cd, (long)nk, d_tcerr,
                                      s);
                 else
@@ -1538,6 +1545,7 @@ static int assemble_impl(bsrg_ctx *c, const bsrg_basis *b, double z, int nch, co
         cudaError_t em = cudaMemcpyAsync(&hf, d_tcerr, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (em == cudaSuccess) em = cudaStreamSynchronize(s);
         if (em != cudaSuccess) return cuda_fail(em, "assemble: mixed flag");
+        if (hf == 2) { set_error("assemble: non-finite value in the direct contraction"); return BSRG_ERR_ARG; }
         if (hf) { set_error("assemble: a tensor-core wait timed out"); return BSRG_ERR_CUDA; }
     }
     // ---- target energies, overlap, symmetrisation ----

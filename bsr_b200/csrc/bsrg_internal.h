@@ -70,6 +70,9 @@ int launch_convol(int ns, int ks, double *a, const double *d, const double *rkb,
 int launch_sum_amb(int ns, int ks, const double *a, const double *b, char sym, double *out, cudaStream_t s);
 int tf32x3_gemm(int m, int n, int k, double alpha, const double *A, long lda, const double *B, long ldb, double beta,
                 double *C, long ldc, int *err, cudaStream_t s);
+size_t ozaki_ws_bytes(int m, int n, int k, int slices);
+int ozaki_gemm(int m, int n, int k, double alpha, const double *A, long lda, const double *B, long ldb, double beta,
+               double *C, long ldc, int slices, void *ws, size_t ws_bytes, int *err, cudaStream_t s);
 int launch_bav(int ns, int ks, const double *b, const double *v, double *y, char type, char side, cudaStream_t s);
 int launch_bvmv(int n, int k, const double *ar, char type, const double *x, const double *y, double *out,
                 cudaStream_t s);

@@ -1078,7 +1078,6 @@ __global__ void __launch_bounds__(128) sb2st5_kernel(Sb2stArgs a)
             for (int i = 0; ok && i < nst; i++) {
                 const int r0 = j + 1 + i * NB, r1 = min(r0 + NB, n), L = r1 - r0;
                 const int col = i == 0 ? j : r0 - NB;
-                const int nl = r0 - col - 1;
                 const int r2 = min(r1 + NB, n), nb2 = r2 - r1;
                 const double xl = i == 0 ? (t < L ? __ldcg(at(r0 + t, col)) : 0.0) : xnext;
                 // ---- the reflector, into ring slot i & 3 once warp 2 has finished step i-4 ----

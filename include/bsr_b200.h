@@ -317,11 +317,14 @@ int bsrg_bs_orth(bsrg_ctx *c, const bsrg_basis *b, int nch, int norb, const doub
  *      and resid (device, n <= khm doubles each, either may be NULL) on the
  *      context's stream. */
 int bsrg_ctx_set_refine(bsrg_ctx *c, int on);
-/* ---- No counterpart in the reference: the mixed-precision form for this
- *      context (mixed = 1; 0 restores FP64, the default).  bsrg_assemble then
- *      computes the direct contraction (convol icase 1 of every direct group,
- *      I_data.f90:206) as bsrg_dgemm_tf32x3's split-precision tensor-core
- *      product; everything else, the eigensolve and its refinement stay FP64. */
+/* ---- No counterpart in the reference: the precision form of this context.
+ *      mixed = 0: FP64 (the default).  mixed = 1: the mixed-precision form --
+ *      bsrg_assemble computes the direct contraction (convol icase 1 of every
+ *      direct group, I_data.f90:206) as bsrg_dgemm_ozaki's product from 8-bit
+ *      digits on the tensor cores (8 digits, exact int32 accumulation: FP64
+ *      accuracy).  mixed = 2: the same contraction as bsrg_dgemm_tf32x3's
+ *      split-TF32 product (FP32 accumulation, ~1e-6 relative).  Everything
+ *      else, the eigensolve and its refinement stay FP64. */
 int bsrg_ctx_set_precision(bsrg_ctx *c, int mixed);
 /* ---- No counterpart in the reference (its DSYEV call is diag_hd.f90:312):
  *      which dense eigensolver bsrg_diag_hd uses on this context.  which = 0
@@ -359,6 +362,24 @@ int bsrg_dgemm(char transa, char transb, int m, int n, int k, double alpha, cons
  *      to 1 if a device-side wait ran out.  Device. */
 int bsrg_dgemm_tf32x3(int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,
                       double beta, double *C, int ldc, int *err, void *stream);
+
+/* ---- No counterpart in the reference (which assembles in FP64): the product
+ *      of the mixed-precision form, C = alpha A B + beta C (column-major FP64,
+ *      A m x k, B k x n), computed on the 5th-generation tensor cores from 8-bit
+ *      integer digits with exact int32 accumulation (the Ozaki splitting): each
+ *      row of A and column of B is scaled by a power of two and cut into
+ *      `slices` signed 7-bit digits (6..8, 0 = 8), and the digit products of
+ *      order below slices are summed.  With 8 digits the result agrees with an
+ *      FP64 GEMM to ~1e-16 k max|A(i,:)| max|B(:,j)|.  k <= BSRG_OZAKI_KMAX.
+ *      work (device, 256-byte aligned) holds the digits:
+ *      bsrg_dgemm_ozaki_work_bytes(m, n, k, slices) bytes.  *err (device int)
+ *      is set to 1 if a device-side wait ran out and to 2 if A or B holds a
+ *      non-finite value (C is then undefined).  Device. */
+#define BSRG_OZAKI_KMAX 16384
+size_t bsrg_dgemm_ozaki_work_bytes(int m, int n, int k, int slices);
+int bsrg_dgemm_ozaki(int m, int n, int k, double alpha, const double *A, int lda, const double *B, int ldb,
+                     double beta, double *C, int ldc, int slices, void *work, size_t work_bytes, int *err,
+                     void *stream);
 
 /* ---- the channel solution offsets ipsol(0:nch) of the last bsrg_diag_hd on
  *      this context (module bsr_hd's ipsol, set in diag_hd.f90:100-111):
