@@ -710,7 +710,7 @@ def bench_mixed(torch, bsr, pw, steps=2):
         ctx.stage_times()
         step()
         torch.cuda.synchronize()
-        out[name + "_direct_ms"] = round(ctx.stage_times()["direct"], 4)
+        out[name + "_direct_ms"] = round(ctx.stage_times()["direct"][0], 4)
         ctx.close()
     e64 = evs["fp64"]
     for name in ("mixed", "mixed_tf32"):

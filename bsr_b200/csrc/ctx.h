@@ -111,6 +111,6 @@ int mirror_lower(int n, double *A, long lda, cudaStream_t s);
 size_t refine_workspace_doubles(int n);
 int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s);
 int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *work, double *corr, double *resid,
-                 int *flag, cudaStream_t s);
+                 int *flag, cudaStream_t s, void *oz_ws = nullptr, size_t oz_bytes = 0, int *oz_err = nullptr);
 
 }  // namespace bsrg

@@ -457,9 +457,13 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
     add(sizeof(double) * nn * std::max(nb, 1) * 2);   // Wt, T
     if (!vecs) add(sizeof(double) * (size_t)khm_max * khm_max);
     add(dws + 16);
+    // the mixed-precision form's A V from 8-bit digits (its K limit: the FP64 GEMM beyond)
+    const bool oz_refine = refine && c->precision == 1 && khm_max <= BSRG_OZAKI_KMAX;
+    const size_t oz_bytes = oz_refine ? ozaki_ws_bytes(khm_max, khm_max, khm_max, 8) : 0;
     if (refine) {
         add(sizeof(double) * refine_workspace_doubles(khm_max));   // mirrored A, then the tile partial sums
         add(sizeof(int) * 4);
+        if (oz_refine) add(oz_bytes);
     }
     if (own_eig) add(sizeof(double) * syevd2_workspace_doubles(khm_max));
     const bool gen = scc != nullptr;
@@ -503,6 +507,7 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
     void *dwork = ar.take<char>(dws + 16);
     double *Fsym = refine ? ar.take<double>(refine_workspace_doubles(khm_max)) : nullptr;
     int *d_rflag = refine ? ar.take<int>(4) : nullptr;
+    char *oz_ws = oz_refine ? ar.take<char>(oz_bytes) : nullptr;
     double *eig_ws = own_eig ? ar.take<double>(syevd2_workspace_doubles(khm_max)) : nullptr;
     double *chan_ws = own_chan ? ar.take<double>(chan_own_workspace_doubles(nch, npad, ks)) : nullptr;
     double *Cov = gen ? ar.take<double>((size_t)khm_max * khm_max) : nullptr;
@@ -733,10 +738,21 @@ static int diag_hd_impl(bsrg_ctx *c, const bsrg_basis *b, int nch, const int *lc
                 return cuda_fail(e, "diag_hd refine buffer");
             c->rf_cap = 2 * (size_t)khm;
         }
+        if (oz_ws && (e = cudaMemsetAsync(d_rflag + 1, 0, sizeof(int), s)) != cudaSuccess)
+            return cuda_fail(e, "diag_hd refine flag");
         stage_begin(c, 8);
         int rr = refine_apply(khm, Fsym, A, khm, eval, Fsym + (size_t)khm * khm, c->rf_buf, c->rf_buf + khm,
-                              d_rflag, s);
+                              d_rflag, s, oz_ws, oz_bytes, oz_ws ? d_rflag + 1 : nullptr);
         stage_end(c, 8, 3);
+        if (rr == BSRG_OK && oz_ws) {
+            // the digit product reports a wait that ran out (1) or a non-finite input (2)
+            int hf = 0;
+            if ((e = cudaMemcpyAsync(&hf, d_rflag + 1, sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess)
+                return cuda_fail(e, "diag_hd refine flag");
+            if (hf == 2) { set_error("diag_hd: non-finite value in the refinement product"); return BSRG_ERR_ARG; }
+            if (hf) { set_error("diag_hd: a tensor-core wait timed out"); return BSRG_ERR_CUDA; }
+        }
         // A V, the residuals and their sums, and the banded products of the Rayleigh-Ritz windows
         c->stage_flops[8] += 2.0 * (double)khm * khm * khm + 6.0 * (double)khm * khm + 132.0 * (double)khm * khm;
         if (rr != BSRG_OK) return rr;

@@ -113,6 +113,44 @@ __global__ void __launch_bounds__(dmma::Sq::NT) refine_gemm_kernel(int n, const 
     }
 }
 
+// The residual epilogue of the mixed-precision form, whose A V comes from the digit product
+// (tc_ozaki.cu) in R: R(i,j) -= lambda_j V(i,j) and the same per-tile partial sums as
+// refine_gemm_kernel, P[(tm*3 + w)*n + j] over rows of 128-row tile tm.  One warp per column
+// and tile (lanes over rows, shuffles in a fixed order), eight columns per CTA.
+__global__ void __launch_bounds__(256) refine_resid_kernel(int n, const double *__restrict__ V, long ldv,
+                                                           const double *__restrict__ lam, double *__restrict__ P,
+                                                           double *__restrict__ R)
+{
+    const int lane = threadIdx.x & 31, col = blockIdx.y * 8 + (threadIdx.x >> 5), tm = blockIdx.x;
+    if (col >= n) return;
+    const double lj = lam[col];
+    double svr = 0.0, srr = 0.0, svv = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int row = tm * 128 + q * 32 + lane;
+        if (row < n) {
+            const double v = V[row + (long)ldv * col];
+            double *rp = R + row + (long)n * col;
+            const double res = *rp - lj * v;
+            *rp = res;
+            svr += v * res;
+            srr += res * res;
+            svv += v * v;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        svr += __shfl_xor_sync(0xffffffffu, svr, o);
+        srr += __shfl_xor_sync(0xffffffffu, srr, o);
+        svv += __shfl_xor_sync(0xffffffffu, svv, o);
+    }
+    if (lane == 0) {
+        P[((long)tm * 3 + 0) * n + col] = svr;
+        P[((long)tm * 3 + 1) * n + col] = srr;
+        P[((long)tm * 3 + 2) * n + col] = svv;
+    }
+}
+
 // resid_j = ||r_j|| / ||v_j|| (tiles added in order)
 __global__ void refine_finalize_kernel(int n, int ntm, const double *__restrict__ P, double *resid)
 {
@@ -331,8 +369,10 @@ int refine_prepare(int n, const double *A, long lda, double *F, cudaStream_t s)
 
 // After the eigensolver: lam (n) refined in place, V (ldv) reordered if needed;
 // corr/resid (n, device) may be NULL.  work: refine_work_doubles(n); flag one int.
+// oz_ws (ozaki_ws_bytes(n, n, n, 8) bytes) selects the mixed-precision form's A V
+// (digit product, wait and input errors in *oz_err); NULL the FP64 tensor-core GEMM.
 int refine_apply(int n, const double *F, double *V, long ldv, double *lam, double *work, double *corr, double *resid,
-                 int *flag, cudaStream_t s)
+                 int *flag, cudaStream_t s, void *oz_ws, size_t oz_bytes, int *oz_err)
 {
     constexpr int bytes = dmma::Smem<dmma::Sq, false, false>::BYTES;
     static_assert(bytes >= 2 * 128 * 3 * 8, "epilogue reduction fits the pipeline's shared memory");
@@ -342,7 +382,15 @@ int refine_apply(int n, const double *F, double *V, long ldv, double *lam, doubl
     dim3 g((unsigned)ntm, (unsigned)((n + dmma::Sq::BN - 1) / dmma::Sq::BN));
     double *P = work, *R = P + (size_t)ntm * 3 * n, *Bd = R + (size_t)n * n, *Gd = Bd + (size_t)RR_ND * n;
     double *lamw = Gd + (size_t)RR_ND * n;
-    refine_gemm_kernel<<<g, dmma::Sq::NT, bytes, s>>>(n, F, n, V, ldv, lam, P, R);
+    if (oz_ws) {
+        // mixed-precision form: A V from 8-bit digits on the tensor cores, then the residual epilogue
+        static_assert(dmma::Sq::BM == 128, "the residual epilogue's tiles are the GEMM's");
+        int rc = ozaki_gemm(n, n, n, 1.0, F, n, V, ldv, 0.0, R, n, 8, oz_ws, oz_bytes, oz_err, s);
+        if (rc != BSRG_OK) return rc;
+        refine_resid_kernel<<<dim3((unsigned)ntm, (unsigned)((n + 7) / 8)), 256, 0, s>>>(n, V, ldv, lam, P, R);
+    } else {
+        refine_gemm_kernel<<<g, dmma::Sq::NT, bytes, s>>>(n, F, n, V, ldv, lam, P, R);
+    }
     refine_finalize_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, ntm, P, resid);
     refine_band_kernel<<<(n + 31) / 32, 256, 0, s>>>(n, V, ldv, R, Bd, Gd);
     refine_window_kernel<<<(n + 7) / 8, 256, 0, s>>>(n, lam, Bd, Gd, lamw);
