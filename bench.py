@@ -49,7 +49,55 @@ def parse():
     ap.add_argument("--assemble-only", action="store_true",
                     help="time only the assembly of the workload's partial wave (R^k tables, exchange, "
                          "direct and one-electron parts; no eigensolve), with its stage times; for profiling")
+    ap.add_argument("--gemm", default="", metavar="M,N,K",
+                    help="time only the library's products C = A B on seeded FP64 M x K and K x N operands: "
+                         "from 8-bit digits on tcgen05 (8 and 7 digits), split TF32 on tcgen05 and the FP64 "
+                         "DMMA GEMM; --gemm-forms picks which; for profiling")
+    ap.add_argument("--gemm-forms", default="i8,i8s7,tf32,dmma")
     return ap.parse_args()
+
+
+def run_gemm(args):
+    """The library's GEMMs alone: --warmup untimed calls, then --steps timed calls (CUDA events)."""
+    import torch
+    from bsr_b200._lib import call, lib
+    from bsr_b200.core import _ptr, _stream
+    m, n, k = (int(x) for x in args.gemm.split(","))
+    g = torch.Generator(device="cuda").manual_seed(5)
+    dA = torch.randn(m * k, dtype=torch.float64, device="cuda", generator=g)
+    dB = torch.randn(k * n, dtype=torch.float64, device="cuda", generator=g)
+    dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
+    err = torch.zeros(4, dtype=torch.int32, device="cuda")
+    nb = lib().bsrg_dgemm_ozaki_work_bytes(m, n, k, 8)
+    ws = torch.empty(nb + 256, dtype=torch.uint8, device="cuda")
+    wp = (ws.data_ptr() + 255) // 256 * 256
+
+    def oz(S):
+        return lambda: call("bsrg_dgemm_ozaki", m, n, k, 1.0, _ptr(dA), m, _ptr(dB), k, 0.0, _ptr(dC), m, S, wp, nb,
+                            _ptr(err), _stream())
+    forms = {"i8": oz(8), "i8s7": oz(7),
+             "tf32": lambda: call("bsrg_dgemm_tf32x3", m, n, k, 1.0, _ptr(dA), m, _ptr(dB), k, 0.0, _ptr(dC), m,
+                                  _ptr(err), _stream()),
+             "dmma": lambda: call("bsrg_dgemm", b"N", b"N", m, n, k, 1.0, _ptr(dA), m, 0, _ptr(dB), k, 0, 0.0,
+                                  _ptr(dC), m, 0, 1, _stream())}
+    out = {"gemm": [m, n, k], "ms": {}, "fp64_equivalent_tflops": {}}
+    for name in args.gemm_forms.split(","):
+        f = forms[name]
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.steps):
+            f()
+        s1.record()
+        s1.synchronize()
+        if int(err[0].item()) != 0:
+            raise SystemExit("gemm %s: device flag %d" % (name, int(err[0].item())))
+        ms = s0.elapsed_time(s1) / max(args.steps, 1)
+        out["ms"][name] = round(ms, 4)
+        out["fp64_equivalent_tflops"][name] = round(2.0 * m * n * k / (ms * 1e-3) / 1e12, 2)
+    print(json.dumps(out), flush=True)
 
 
 def run_dense_eig(args):
@@ -676,10 +724,11 @@ def run_b200(args):
 
 def bench_mixed(torch, bsr, pw, steps=2):
     """Config 3: the config-2 partial wave in the mixed-precision forms beside the FP64 path --
-    "i8": the direct contraction from 8-bit digits on tcgen05 with exact int32 accumulation
-    (bsrg_dgemm_ozaki), "tf32": the split-TF32 product with FP32 accumulation; the eigensolve and
-    its refinement FP64 in all three.  Solves/s of each by CUDA events, the direct stage's time,
-    and each mixed form's eigenvalue error per eigenvalue against the FP64 path."""
+    "i8": the direct contraction and the refinement's A V from 8-bit digits on tcgen05 with exact
+    int32 accumulation (bsrg_dgemm_ozaki), "tf32": the direct contraction as the split-TF32 product
+    with FP32 accumulation; the eigensolve FP64 in all three.  Solves/s of each by CUDA events, the
+    direct and refinement stages' times, and each mixed form's eigenvalue error per eigenvalue
+    against the FP64 path."""
     out = {}
     evs = {}
     forms = (("fp64", False, "i8"), ("mixed", True, "i8"), ("mixed_tf32", True, "tf32"))
@@ -710,7 +759,9 @@ def bench_mixed(torch, bsr, pw, steps=2):
         ctx.stage_times()
         step()
         torch.cuda.synchronize()
-        out[name + "_direct_ms"] = round(ctx.stage_times()["direct"][0], 4)
+        st = ctx.stage_times()
+        out[name + "_direct_ms"] = round(st["direct"][0], 4)
+        out[name + "_refine_ms"] = round(st["refine"][0], 4)
         ctx.close()
     e64 = evs["fp64"]
     for name in ("mixed", "mixed_tf32"):
@@ -720,9 +771,10 @@ def bench_mixed(torch, bsr, pw, steps=2):
             "max_lowest_1100": float(rel[:1100].max()),
             "what": "|E_mixed - E_fp64| / max(|E_fp64|, 1e-3) per eigenvalue"}
     rel = out["eig_rel_err_vs_fp64"]
-    out.update({"workload": "config3: the config2 partial wave; mixed = direct contraction from 8-bit digits on "
-                            "tcgen05 (kind::i8, exact int32 accumulation, 8 digits), mixed_tf32 = split TF32 on "
-                            "tcgen05 (FP32 accumulation); FP64 eigensolve and Rayleigh refinement in every form",
+    out.update({"workload": "config3: the config2 partial wave; mixed = direct contraction and the refinement's "
+                            "A V from 8-bit digits on tcgen05 (kind::i8, exact int32 accumulation, 8 digits), "
+                            "mixed_tf32 = direct contraction in split TF32 on tcgen05 (FP32 accumulation); FP64 "
+                            "eigensolve and residuals in every form",
                 "meets_1e-10": bool(rel["max"] <= 1e-10),
                 "speedup_vs_fp64": out["mixed_solves_per_s"] / out["fp64_solves_per_s"]})
     return out
@@ -864,7 +916,9 @@ def _group_counts(c, ty):
 
 def main():
     args = parse()
-    if args.dense_eig > 0:
+    if args.gemm:
+        run_gemm(args)
+    elif args.dense_eig > 0:
         run_dense_eig(args)
     elif args.assemble_only:
         run_assemble_only(args)

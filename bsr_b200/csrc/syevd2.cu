@@ -2218,10 +2218,14 @@ static int syevd2_impl(bsrg_ctx *c, int n, const double *A, long lda, double *w,
         if (!getenv("BSRG_SB2ST_SHARED") && !getenv("BSRG_SB2ST_ONEWARP")) {
             // one sweep per CTA at a time: the chain of reflectors and right updates on one warp, the
             // diagonal blocks and the left updates on two more, a helper warp that publishes the steps
-            // (sb2st5_kernel; BSRG_SB2ST_TWOWARP: sb2st3_kernel, computing warp and helper only).  One
-            // CTA per SM: about n / (3.4 NB) sweeps are active at once, so nsm CTAs never make a sweep
-            // wait for its CTA, and no waiting CTA shares an SM with a working one
-            const int ctas = std::max(1, std::min(n - 2, nsm));
+            // (sb2st5_kernel; BSRG_SB2ST_TWOWARP: sb2st3_kernel, computing warp and helper only).  A sweep
+            // starts three steps behind its predecessor, so about sweep_steps / 3 sweeps are active at
+            // once; sweep_steps / 2.5 + 4 CTAs (at most one per SM) never make a sweep wait for its CTA,
+            // and the SMs left over stay free for work on other streams instead of polling
+            // (BSRG_SB2ST_CTAS overrides the count)
+            int want = (int)(sweep_steps(n, 0) / 2.5) + 4;
+            if (const char *ov = getenv("BSRG_SB2ST_CTAS")) want = std::max(1, atoi(ov));
+            const int ctas = std::max(1, std::min(n - 2, std::min(nsm, want)));
             const bool two = getenv("BSRG_SB2ST_TWOWARP") != nullptr;
             if ((e = cudaLaunchCooperativeKernel(two ? (const void *)sb2st3_kernel : (const void *)sb2st5_kernel, ctas,
                                                  two ? 64 : 128, args, 0, st)) != cudaSuccess)
