@@ -170,6 +170,31 @@
         Integer(c_int) :: bsrg_dsyevd
        End Function
 
+       Function bsrg_ctx_set_precision(c, mixed) bind(C, name="bsrg_ctx_set_precision")
+        Import :: c_int, c_ptr
+        Type(c_ptr), value :: c
+        Integer(c_int), value :: mixed
+        Integer(c_int) :: bsrg_ctx_set_precision
+       End Function
+
+       Function bsrg_dgemm_ozaki_work_bytes(m, n, k, slices)             &
+                bind(C, name="bsrg_dgemm_ozaki_work_bytes")
+        Import :: c_int, c_size_t
+        Integer(c_int), value :: m, n, k, slices
+        Integer(c_size_t) :: bsrg_dgemm_ozaki_work_bytes
+       End Function
+
+       Function bsrg_dgemm_ozaki(m, n, k, alpha, A, lda, B, ldb, beta,    &
+                C, ldc, slices, work, work_bytes, err, stream)          &
+                bind(C, name="bsrg_dgemm_ozaki")
+        Import :: c_int, c_ptr, c_size_t, c_double
+        Integer(c_int), value :: m, n, k, lda, ldb, ldc, slices
+        Real(c_double), value :: alpha, beta
+        Type(c_ptr), value :: A, B, C, work, err, stream
+        Integer(c_size_t), value :: work_bytes
+        Integer(c_int) :: bsrg_dgemm_ozaki
+       End Function
+
        Function cudaMalloc(p, bytes) bind(C, name="cudaMalloc")
         Import :: c_int, c_ptr, c_size_t
         Type(c_ptr) :: p
