@@ -54,20 +54,26 @@ class Request:
 OWN_EIG_MIN = 7000      # diag_hd's default crossover to the library's dense eigensolver (rows)
 
 
-def request_bytes(nch, ns, lch, ks, want_vectors=True, own_eig=False):
+def request_bytes(nch, ns, lch, ks, want_vectors=True, own_eig=False, mixed=False):
     """Device bytes one solve needs beyond the shared state (H blocks, the dense
     problem with vectors and its eigensolver workspace, block-transform buffers;
     with vectors also the eigenvectors and the refinement's copy of A and its
     residuals; with the library's two-stage eigensolver its workspace: the band
     reduction's copy, both stages' reflectors and block factors, the divide and
-    conquer's merge buffers, ~6.5 khm^2 + 3000 khm doubles)."""
+    conquer's merge buffers, ~6.5 khm^2 + 3000 khm doubles; in the mixed-precision
+    form the 8-bit digit planes of the refinement's product, 16 bytes per element of
+    A rounded up to the product's tiles, and of the direct contraction)."""
     khm, hb, db = shard.symmetry_dims(nch, ns, lch, ks)
     nch, ns = int(nch), int(ns)
     nb = nch * (nch + 1) // 2
     transform = 2 * nb * ns * ns * 8
     channel = 4 * nch * ns * ns * 8
     own = int((6.5 * khm * khm + 3000 * khm) * 8) if (own_eig and want_vectors) else 0
-    return hb + db + transform + channel + (3 * khm * khm * 8 if want_vectors else 0) + own
+    digits = 0
+    if mixed:
+        nk = ns * ks          # the direct contraction: (nk x nk) times (nk x direct groups <= nb)
+        digits = 8 * (nk + 128 + nb + 64) * (nk + 32) + (16 * (khm + 128) * (khm + 32) if want_vectors else 0)
+    return hb + db + transform + channel + (3 * khm * khm * 8 if want_vectors else 0) + own + digits
 
 
 class AdmissionQueue:
@@ -118,8 +124,12 @@ class AdmissionQueue:
 class PartialWaveServer:
     """Device-resident request loop for partial waves sharing one basis and orbital set."""
 
-    def __init__(self, t, ks, z, P, kmax, n_streams=2, hbm_budget_bytes=None, device=0, eigensolver=None):
-        """eigensolver: diag_hd's dense eigensolver per worker ("auto", "own" or "lib", see
+    def __init__(self, t, ks, z, P, kmax, n_streams=2, hbm_budget_bytes=None, device=0, eigensolver=None,
+                 mixed=False):
+        """mixed: every worker solves in the mixed-precision form (Context.set_precision:
+        the direct contraction and the refinement's A V from 8-bit digits on the tensor
+        cores); FP64 by default.
+        eigensolver: diag_hd's dense eigensolver per worker ("auto", "own" or "lib", see
         Context.set_eigensolver).  Default: "own" with more than one stream -- concurrent
         solves overlap with the library's two-stage solver, whose bulge chasing and panel
         factorisations leave most of the GPU to the other streams, where cuSOLVER's
@@ -133,6 +143,7 @@ class PartialWaveServer:
         self.device = device
         self.ks, self.ns, self.z, self.kmax = ks, len(t) - ks, float(z), kmax
         self.eigensolver = eigensolver or ("own" if n_streams > 1 else "auto")
+        self.mixed = bool(mixed)
         self.basis = core.define_spline(t, ks)
         self.P = core.as_fortran(P)
         self._setup_ctx = core.Context()
@@ -155,7 +166,7 @@ class PartialWaveServer:
         """sym: dict with nch, lch, ech, coefs.  Returns a Request (wait() for the result)."""
         khm = shard.symmetry_dims(sym["nch"], self.ns, sym["lch"], self.ks)[0]
         own = self.eigensolver == "own" or (self.eigensolver == "auto" and khm >= OWN_EIG_MIN)
-        nb = request_bytes(sym["nch"], self.ns, sym["lch"], self.ks, want_vectors, own_eig=own)
+        nb = request_bytes(sym["nch"], self.ns, sym["lch"], self.ks, want_vectors, own_eig=own, mixed=self.mixed)
         with self._lock:
             r = Request(self._next_id, sym, want_vectors)
             self._next_id += 1
@@ -199,6 +210,7 @@ class PartialWaveServer:
             ctx = core.Context(stream=stream)
             ctx.use_tables(self.tables)
             ctx.set_eigensolver(self.eigensolver)
+            ctx.set_precision(self.mixed)
             while True:
                 r = self.queue.take()
                 if r is None:

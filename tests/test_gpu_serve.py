@@ -131,3 +131,36 @@ def test_alone_equals_mix_with_vectors(batch):
     for q, res in zip(order, mixed):
         assert res["khm"] == alone[q]["khm"]
         assert np.array_equal(res["eval"], alone[q]["eval"]), "symmetry %d differs in a mix" % q
+
+
+def test_mixed_form_alone_equals_mix(batch):
+    """The mixed-precision form served: a request's eigenvalues alone and in a concurrent
+    mix are bitwise the same (the digit products sum in integers, so their order does not
+    matter), and within 1e-10 per eigenvalue (floor 1e-3) of the FP64 form of the same
+    request."""
+    from bsr_b200 import serve
+    b, small = batch
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=1, eigensolver="own")
+    try:
+        fp64 = [serve.run_stream(srv, [s], [0.0])[0].wait(120) for s in small]
+    finally:
+        srv.close()
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=1, eigensolver="own",
+                                  mixed=True)
+    try:
+        alone = [serve.run_stream(srv, [s], [0.0])[0].wait(120) for s in small]
+    finally:
+        srv.close()
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=3, mixed=True)
+    assert srv.eigensolver == "own" and srv.mixed
+    try:
+        order = list(range(len(small)))[::-1] + list(range(len(small)))
+        mix = [r.wait(120) for r in serve.run_stream(srv, [small[q] for q in order], [0.0] * len(order))]
+    finally:
+        srv.close()
+    for q, res in zip(order, mix):
+        assert res["khm"] == alone[q]["khm"]
+        assert np.array_equal(res["eval"], alone[q]["eval"]), "symmetry %d differs in a mix" % q
+    for a, f in zip(alone, fp64):
+        rel = np.abs(a["eval"] - f["eval"]) / np.maximum(np.abs(f["eval"]), 1e-3)
+        assert rel.max() <= 1e-10

@@ -126,3 +126,16 @@ def test_request_bytes_counts_the_library_eigensolver():
     # without eigenvectors neither eigensolver workspace nor the refinement is counted
     assert serve.request_bytes(40, 150, lch, 8, want_vectors=False, own_eig=True) == \
         serve.request_bytes(40, 150, lch, 8, want_vectors=False)
+
+
+def test_request_bytes_counts_the_mixed_form_digits():
+    """The mixed-precision form holds the 8-bit digit planes of the refinement's product
+    (16 bytes per element of A, rounded up to the product's tiles) and of the direct
+    contraction on top of the FP64 form's buffers."""
+    lch = [c % 7 for c in range(40)]
+    khm = serve.shard.symmetry_dims(40, 150, lch, 8)[0]
+    a = serve.request_bytes(40, 150, lch, 8)
+    b = serve.request_bytes(40, 150, lch, 8, mixed=True)
+    assert b - a >= 16 * khm * khm
+    c = serve.request_bytes(40, 150, lch, 8, want_vectors=False, mixed=True)
+    assert c - serve.request_bytes(40, 150, lch, 8, want_vectors=False) < 16 * khm * khm
