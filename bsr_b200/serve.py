@@ -30,7 +30,8 @@ from . import shard
 
 
 class Request:
-    __slots__ = ("rid", "sym", "want_vectors", "t_submit", "t_start", "t_done", "result", "error", "event", "nbytes")
+    __slots__ = ("rid", "sym", "want_vectors", "t_submit", "t_start", "t_done", "result", "error", "event", "nbytes",
+                 "barrier")
 
     def __init__(self, rid, sym, want_vectors):
         self.rid, self.sym, self.want_vectors = rid, sym, want_vectors
@@ -38,6 +39,7 @@ class Request:
         self.result = self.error = None
         self.event = threading.Event()
         self.nbytes = 0
+        self.barrier = None       # warm-up requests: the worker waits here after releasing it
 
     def wait(self, timeout=None):
         if not self.event.wait(timeout):
@@ -180,6 +182,24 @@ class PartialWaveServer:
         self.queue.put(r)
         return r
 
+    def warm(self, sym, want_vectors=True, timeout=600.0):
+        """Solve `sym` once on every worker, untimed and outside the served results, so that
+        each worker's context has grown its device workspace to that problem's size (a
+        workspace that grows during service synchronises the device and stalls every
+        stream).  Give it the largest symmetry expected.  A worker that has finished its
+        copy waits until every worker has taken one, so each worker solves exactly one."""
+        n = len(self.workers)
+        barrier = threading.Barrier(n, timeout=timeout)
+        reqs = []
+        for _ in range(n):
+            r = self.submit(sym, want_vectors)
+            r.barrier = barrier
+            reqs.append(r)
+        for r in reqs:
+            r.wait(timeout)
+        with self._lock:
+            self.done = [d for d in self.done if d not in reqs]
+
     def close(self):
         self.queue.close()
         for th in self.workers:
@@ -228,6 +248,11 @@ class PartialWaveServer:
                 r.t_done = time.perf_counter()
                 r.event.set()
                 self._release(r)
+                if r.barrier is not None:
+                    try:
+                        r.barrier.wait()
+                    except threading.BrokenBarrierError:
+                        pass
             ctx.close()
 
 
@@ -254,8 +279,8 @@ def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=
     """Pick the worker-stream count with the highest solves/s on a sample batch.
 
     make_server(n_streams) -> PartialWaveServer; sample: list of symmetries.  Each
-    candidate server first gets one request per worker, so every worker's context has
-    met the problem sizes before the timed run.  A short sample's rates are noisy and
+    candidate server's workers first solve the sample's largest symmetry once
+    (PartialWaveServer.warm), so no worker grows its workspace in the timed run.  A short sample's rates are noisy and
     close together, while on a full batch more workers also overlap each other's host
     work (record grouping, uploads, result reads), so the most streams whose rate is
     within `margin` of the best is chosen.  The choice is kept in `cache` (a dict, e.g.
@@ -266,9 +291,7 @@ def autotune_streams(make_server, sample, candidates=(1, 2, 4), cache=None, key=
     for n in candidates:
         srv = make_server(n)
         try:
-            warm = list(sample[:n]) or list(sample[:1])
-            run_stream(srv, warm, [0.0] * len(warm), want_vectors=True)
-            srv.done.clear()
+            srv.warm(max(sample, key=lambda s: s["nch"]))
             reqs = run_stream(srv, sample, [0.0] * len(sample), want_vectors=True)
             rates[n] = srv.stats(reqs)["solves_per_s"]
         finally:

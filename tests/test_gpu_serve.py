@@ -164,3 +164,26 @@ def test_mixed_form_alone_equals_mix(batch):
     for a, f in zip(alone, fp64):
         rel = np.abs(a["eval"] - f["eval"]) / np.maximum(np.abs(f["eval"]), 1e-3)
         assert rel.max() <= 1e-10
+
+
+def test_warm_then_serve(batch):
+    """PartialWaveServer.warm solves one symmetry on every worker outside the served
+    results; what is served afterwards is unchanged."""
+    from bsr_b200 import serve
+    b, small = batch
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=3)
+    try:
+        srv.warm(max(small, key=lambda s: s["nch"]))
+        assert srv.done == []
+        got = serve.run_stream(srv, small[:2], [0.0, 0.0])
+        res = [r.wait(120) for r in got]
+        assert len(srv.done) == 2
+    finally:
+        srv.close()
+    srv = serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=1, eigensolver="own")
+    try:
+        alone = [serve.run_stream(srv, [s], [0.0])[0].wait(120) for s in small[:2]]
+    finally:
+        srv.close()
+    for a, r in zip(alone, res):
+        assert np.array_equal(a["eval"], r["eval"])

@@ -80,7 +80,10 @@ def test_request_bytes_numpy_ints():
 
 class _FakeServer:
     def __init__(self, n, rate):
-        self.n, self.rate, self.done, self.warm, self.closed = n, rate, [], [], False
+        self.n, self.rate, self.done, self.warmed, self.closed = n, rate, [], [], False
+
+    def warm(self, sym, want_vectors=True, timeout=600.0):
+        self.warmed.append(sym)
 
     def stats(self, reqs):
         return {"solves_per_s": self.rate}
@@ -90,17 +93,17 @@ class _FakeServer:
 
 
 def test_autotune_prefers_more_streams_within_margin(monkeypatch):
-    """The most streams within 5 % of the best rate win; every worker is warmed first;
-    the choice and the measured rates go to the cache."""
+    """The most streams within 5 % of the best rate win; every candidate's workers are
+    warmed first with the sample's largest symmetry; the choice and the measured rates go
+    to the cache."""
     made = []
 
     def fake_run(srv, syms, arrivals, want_vectors=True):
-        if not srv.warm:
-            srv.warm.append(len(syms))
+        assert srv.warmed, "timed before the warm-up"
         return list(syms)
 
     monkeypatch.setattr(serve, "run_stream", fake_run)
-    sample = list(range(8))
+    sample = [{"nch": c} for c in (4, 9, 30, 7, 12, 5, 8, 6)]
     for rates, want in (({1: 10.0, 2: 10.3, 4: 9.0}, 2), ({1: 12.5, 2: 11.0, 4: 9.0}, 1),
                         ({1: 10.0, 2: 10.0, 4: 13.0}, 4), ({1: 9.7, 2: 9.9, 4: 9.95}, 4)):
         made.clear()
@@ -111,7 +114,7 @@ def test_autotune_prefers_more_streams_within_margin(monkeypatch):
 
         cache = {}
         assert serve.autotune_streams(make, sample, candidates=(1, 2, 4), cache=cache, key="k") == want
-        assert [s.warm[0] for s in made] == [1, 2, 4] and all(s.closed for s in made)
+        assert [s.warmed for s in made] == [[{"nch": 30}]] * 3 and all(s.closed for s in made)
         assert cache["k"] == {"n_streams": want, "solves_per_s": rates}
         assert serve.autotune_streams(make, sample, candidates=(1, 2, 4), cache=cache, key="k") == want
         assert len(made) == 3                   # the cached choice runs nothing
