@@ -853,7 +853,7 @@ def bench_batched_serving(torch, bsr):
         return serve.PartialWaveServer(b["t"], b["ks"], b["z"], b["P"], b["kmax"], n_streams=n)
 
     tune = {}
-    n_best = serve.autotune_streams(make, syms[::2], candidates=(1, 2, 3, 4), cache=tune, key="config4")
+    n_best = serve.autotune_streams(make, syms[::2], candidates=(1, 2, 3, 4, 6), cache=tune, key="config4")
     srv = make(n_best)
     try:
         srv.warm(max(syms, key=lambda q: q["nch"]))
