@@ -320,19 +320,52 @@ __global__ void band_moment_kernel(int ks, int ns, int nv, const double *__restr
 
 constexpr int PAD_TI = 32, PAD_TJ = 32, PAD_JT = PAD_TJ / 8;      // block tile, columns per thread
 
+// Element (i, j) of one (ip, jp) slice whose interval ranges [iv_lo, iv_hi] and [jv_lo, jv_hi]
+// overlap (only pairs with |i - j| < ks can): the diagonal cells rkd(ii,jj,jv) of the shared
+// range, then sum_jv [ rkd2(jj,jv) sum_{iv<jv} rkd1(ii,iv) + rkd1(jj,jv) sum_{iv>jv} rkd2(ii,iv) ]
+// with the iv sums running (ascending for iv < jv, descending for iv > jv).
+template <int KS>
+__device__ __forceinline__ double rkb_overlap(int i, int j, int ip, int jp, int iv_lo, int iv_hi, int jv_lo,
+                                              int jv_hi, const double *__restrict__ rkd1,
+                                              const double *__restrict__ rkd2, const double *__restrict__ rkd)
+{
+    constexpr int ks = KS, ik = KS * (KS + 1) / 2;
+    auto cell = [&](int h, int p, int v) { return h * ks - h * (h - 1) / 2 + p + ik * v; };
+    double v = 0.0;
+    // the diagonal cells first: independent loads, unrolled so they overlap
+    const int ov_lo = iv_lo > jv_lo ? iv_lo : jv_lo, ov_hi = iv_hi < jv_hi ? iv_hi : jv_hi;
+#pragma unroll 4
+    for (int jv = ov_lo; jv <= ov_hi; jv++) {
+        const int ih = i - jv, jh = j - jv;
+        v += __ldg(rkd + ih * ks - ih * (ih - 1) / 2 + ip +
+                   (size_t)ik * (jh * ks - jh * (jh - 1) / 2 + jp + (size_t)ik * jv));
+    }
+    double lo_sum = 0.0;               // sum of rkd1(ii,iv) over iv < jv
+    int ivn = iv_lo;
+    for (int jv = jv_lo; jv <= jv_hi; jv++) {
+        for (; ivn < jv && ivn <= iv_hi; ivn++) lo_sum += __ldg(rkd1 + cell(i - ivn, ip, ivn));
+        v += lo_sum * __ldg(rkd2 + cell(j - jv, jp, jv));
+    }
+    double hi_sum = 0.0;               // sum of rkd2(ii,iv) over iv > jv
+    ivn = iv_hi;
+    for (int jv = jv_hi; jv >= jv_lo; jv--) {
+        for (; ivn > jv && ivn >= iv_lo; ivn--) hi_sum += __ldg(rkd2 + cell(i - ivn, ip, ivn));
+        v += hi_sum * __ldg(rkd1 + cell(j - jv, jp, jv));
+    }
+    return v;
+}
+
+// Everything of the table but the band |i - j| < ks of valid elements: the factorised products
+// M1(i,ip) M2(j,jp) (or M1(j,jp) M2(i,ip)) and the zero margins.  rkb_band_kernel writes the band.
 template <int KS>
 __global__ void __launch_bounds__(256)
-rkb_pad_kernel(int ns, int nv, PadLayout L, const double *__restrict__ rkd1, const double *__restrict__ rkd2,
-               const double *__restrict__ rkd, const double *__restrict__ M1, const double *__restrict__ M2,
+rkb_pad_kernel(int ns, int nv, PadLayout L, const double *__restrict__ M1, const double *__restrict__ M2,
                double *__restrict__ rkbp)
 {
     constexpr int ks = KS;
-    // the block's band moments (A: M1(i,ip), M2(i,ip) of its rows; B: M1(j,jp), M2(j,jp) of
-    // its columns) and, near the diagonal, its cell moments [ih][r] / [jh][c], iv = i - ih
+    // the block's band moments (A: M1(i,ip), M2(i,ip) of its rows; B: M1(j,jp), M2(j,jp) of its columns)
     __shared__ double A1[PAD_TI], A2[PAD_TI], B1[PAD_TJ], B2[PAD_TJ];
-    __shared__ double S1[KS][PAD_TI], S2[KS][PAD_TI], T1[KS][PAD_TJ], T2[KS][PAD_TJ];
     const int ipjp = blockIdx.z, ip = ipjp % ks, jp = ipjp / ks;
-    constexpr int ik = KS * (KS + 1) / 2;
     const int i0 = (int)blockIdx.x * PAD_TI - L.PL, j0 = (int)blockIdx.y * PAD_TJ - L.PL;
     const int t = threadIdx.x + 32 * threadIdx.y;
     if (t < PAD_TI) {
@@ -346,29 +379,10 @@ rkb_pad_kernel(int ns, int nv, PadLayout L, const double *__restrict__ rkd1, con
         B1[t - PAD_TI] = ok ? M1[j + (size_t)ns * jp] : 0.0;
         B2[t - PAD_TI] = ok ? M2[j + (size_t)ns * jp] : 0.0;
     }
-    // overlapping interval ranges need |i - j| < ks; a block with none skips the staging
-    const bool near = !(i0 > j0 + PAD_TJ - 1 + ks - 1 || j0 > i0 + PAD_TI - 1 + ks - 1);
-    if (near) {
-        for (int q = t; q < ks * PAD_TI; q += 256) {
-            const int ih = q / PAD_TI, r = q % PAD_TI, i = i0 + r, iv = i - ih;
-            const bool ok = i >= 0 && i < ns && iv >= 0 && iv < nv && ih + ip < ks;
-            const int idx = ih * ks - ih * (ih - 1) / 2 + ip + ik * iv;
-            S1[ih][r] = ok ? rkd1[idx] : 0.0;
-            S2[ih][r] = ok ? rkd2[idx] : 0.0;
-        }
-        for (int q = t; q < ks * PAD_TJ; q += 256) {
-            const int jh = q / PAD_TJ, c = q % PAD_TJ, j = j0 + c, jv = j - jh;
-            const bool ok = j >= 0 && j < ns && jv >= 0 && jv < nv && jh + jp < ks;
-            const int idx = jh * ks - jh * (jh - 1) / 2 + jp + ik * jv;
-            T1[jh][c] = ok ? rkd1[idx] : 0.0;
-            T2[jh][c] = ok ? rkd2[idx] : 0.0;
-        }
-    }
     __syncthreads();
     const int r = threadIdx.x, pr = blockIdx.x * PAD_TI + r, i = pr - L.PL;
     if (pr >= L.NP) return;
     const bool irow = i >= 0 && i + ip < ns;
-    int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
     const int iv_hi = i < nv - 1 ? i : nv - 1;
     double *out = rkbp + (size_t)pr + L.slice * ipjp;
 #pragma unroll
@@ -377,39 +391,38 @@ rkb_pad_kernel(int ns, int nv, PadLayout L, const double *__restrict__ rkd1, con
         if (pc >= L.NP) break;
         double v = 0.0;
         if (irow && j >= 0 && j + jp < ns) {
+            if (j - i < ks && i - j < ks) continue;        // the band: rkb_band_kernel
             int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
-            const int jv_hi = j < nv - 1 ? j : nv - 1;
-            if (iv_hi < jv_lo) v = A1[r] * B2[c];
-            else if (jv_hi < iv_lo) v = B1[c] * A2[r];
-            else {
-                // overlapping interval ranges: sum over the cells jv both ranges share of
-                // rkd(ii,jj,jv), then sum_jv [ rkd2(jj,jv) sum_{iv<jv} rkd1(ii,iv) +
-                // rkd1(jj,jv) sum_{iv>jv} rkd2(ii,iv) ], the iv sums running (ascending for
-                // iv < jv, descending for iv > jv)
-                // the diagonal cells first: independent loads, unrolled so they overlap
-                const int ov_lo = iv_lo > jv_lo ? iv_lo : jv_lo, ov_hi = iv_hi < jv_hi ? iv_hi : jv_hi;
-#pragma unroll 4
-                for (int jv = ov_lo; jv <= ov_hi; jv++) {
-                    const int ih = i - jv, jh = j - jv;
-                    v += __ldg(rkd + ih * ks - ih * (ih - 1) / 2 + ip +
-                               (size_t)ik * (jh * ks - jh * (jh - 1) / 2 + jp + (size_t)ik * jv));
-                }
-                double lo_sum = 0.0;               // sum of rkd1(ii,iv) over iv < jv
-                int ivn = iv_lo;
-                for (int jv = jv_lo; jv <= jv_hi; jv++) {
-                    for (; ivn < jv && ivn <= iv_hi; ivn++) lo_sum += S1[i - ivn][r];
-                    v += lo_sum * T2[j - jv][c];
-                }
-                double hi_sum = 0.0;               // sum of rkd2(ii,iv) over iv > jv
-                ivn = iv_hi;
-                for (int jv = jv_hi; jv >= jv_lo; jv--) {
-                    for (; ivn > jv && ivn >= iv_lo; ivn--) hi_sum += S2[i - ivn][r];
-                    v += hi_sum * T1[j - jv][c];
-                }
-            }
+            v = iv_hi < jv_lo ? A1[r] * B2[c] : B1[c] * A2[r];
         }
         out[(size_t)L.NP * pc] = v;
     }
+}
+
+// The band |i - j| < ks of one (ip, jp) slice: one warp per 32 consecutive i of one diagonal
+// d = j - i, so the lanes of a warp share their loop structure (a tile of rkb_pad_kernel mixed
+// band and factorised elements in one warp and waited on its slowest lane).  Same arithmetic, in
+// the same order, as the product of the cells.
+template <int KS>
+__global__ void __launch_bounds__(256)
+rkb_band_kernel(int ns, int nv, PadLayout L, const double *__restrict__ rkd1, const double *__restrict__ rkd2,
+                const double *__restrict__ rkd, const double *__restrict__ M1, const double *__restrict__ M2,
+                double *__restrict__ rkbp)
+{
+    constexpr int ks = KS;
+    const int ipjp = blockIdx.z, ip = ipjp % ks, jp = ipjp / ks;
+    const int d = (int)blockIdx.y - (ks - 1);
+    const int i = ((int)blockIdx.x * 8 + (int)threadIdx.y) * 32 + (int)threadIdx.x, j = i + d;
+    if (i >= ns || j < 0 || j >= ns || i + ip >= ns || j + jp >= ns) return;
+    int iv_lo = i + ip - (ks - 1); if (iv_lo < 0) iv_lo = 0;
+    const int iv_hi = i < nv - 1 ? i : nv - 1;
+    int jv_lo = j + jp - (ks - 1); if (jv_lo < 0) jv_lo = 0;
+    const int jv_hi = j < nv - 1 ? j : nv - 1;
+    double v;
+    if (iv_hi < jv_lo) v = M1[i + (size_t)ns * ip] * M2[j + (size_t)ns * jp];
+    else if (jv_hi < iv_lo) v = M1[j + (size_t)ns * jp] * M2[i + (size_t)ns * ip];
+    else v = rkb_overlap<KS>(i, j, ip, jp, iv_lo, iv_hi, jv_lo, jv_hi, rkd1, rkd2, rkd);
+    rkbp[L.at(i, j, ip, jp, ks)] = v;
 }
 
 // ---------------------------------------------------------------------------
@@ -925,30 +938,21 @@ static exchange_fused_fn exchange_fused_for(int ks, size_t *smem_fixed)
 #undef XFCASE
 }
 
-typedef void (*rkb_pad_fn)(int, int, PadLayout, const double *, const double *, const double *, const double *,
-                           const double *, double *);
+typedef void (*rkb_pad_fn)(int, int, PadLayout, const double *, const double *, double *);
+typedef void (*rkb_band_fn)(int, int, PadLayout, const double *, const double *, const double *, const double *,
+                            const double *, double *);
 
-static rkb_pad_fn rkb_pad_for(int ks)
+#define PADCASE(K) \
+    case K: *band = rkb_band_kernel<K>; return rkb_pad_kernel<K>;
+static rkb_pad_fn rkb_pad_for(int ks, rkb_band_fn *band)
 {
     switch (ks) {
-    case 2: return rkb_pad_kernel<2>;
-    case 3: return rkb_pad_kernel<3>;
-    case 4: return rkb_pad_kernel<4>;
-    case 5: return rkb_pad_kernel<5>;
-    case 6: return rkb_pad_kernel<6>;
-    case 7: return rkb_pad_kernel<7>;
-    case 8: return rkb_pad_kernel<8>;
-    case 9: return rkb_pad_kernel<9>;
-    case 10: return rkb_pad_kernel<10>;
-    case 11: return rkb_pad_kernel<11>;
-    case 12: return rkb_pad_kernel<12>;
-    case 13: return rkb_pad_kernel<13>;
-    case 14: return rkb_pad_kernel<14>;
-    case 15: return rkb_pad_kernel<15>;
-    case 16: return rkb_pad_kernel<16>;
-    default: return nullptr;
+    PADCASE(2) PADCASE(3) PADCASE(4) PADCASE(5) PADCASE(6) PADCASE(7) PADCASE(8) PADCASE(9)
+    PADCASE(10) PADCASE(11) PADCASE(12) PADCASE(13) PADCASE(14) PADCASE(15) PADCASE(16)
+    default: *band = nullptr; return nullptr;
     }
 }
+#undef PADCASE
 
 // band moments + zero-margined R^k table of multipole k (from its cell moments)
 static int build_padded_table(const bsrg_basis *b, int k, const double *rkd1, const double *rkd2, const double *rkd,
@@ -958,12 +962,15 @@ static int build_padded_table(const bsrg_basis *b, int k, const double *rkd1, co
     const PadLayout PL = pad_layout(ns, ks);
     band_moment_kernel<<<(ns * ks + 127) / 128, 128, 0, s>>>(ks, ns, nv, rkd1, rkd2, M1, M2);
     dim3 gp((PL.NP + PAD_TI - 1) / PAD_TI, (PL.NP + PAD_TJ - 1) / PAD_TJ, ks * ks);
-    rkb_pad_fn fn = rkb_pad_for(ks);
-    if (!fn) {
+    rkb_band_fn band = nullptr;
+    rkb_pad_fn fn = rkb_pad_for(ks, &band);
+    if (!fn || !band) {
         set_error("R^k table: ks=%d outside the compiled range 2..%d", ks, BSRG_MAXKS);
         return BSRG_ERR_ARG;
     }
-    fn<<<gp, dim3(32, 8), 0, s>>>(ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
+    fn<<<gp, dim3(32, 8), 0, s>>>(ns, nv, PL, M1, M2, rkbp);
+    dim3 gb((unsigned)((ns + 255) / 256), (unsigned)(2 * ks - 1), (unsigned)(ks * ks));
+    band<<<gb, dim3(32, 8), 0, s>>>(ns, nv, PL, rkd1, rkd2, rkd, M1, M2, rkbp);
     (void)k;
     return cuda_fail(cudaGetLastError(), "R^k table");
 }

@@ -27,7 +27,8 @@
 // A block and the B block) is then two contiguous bulk copies (cp.async.bulk, no
 // tensor map, no multicast) completed on an mbarrier.
 //
-// GEMM: one CTA per 128 x 64 tile of C, 128 threads, a 4-stage ring in shared memory.
+// GEMM: one CTA per 128 x 64 tile of C (tiles in groups of 8 row blocks, so CTAs in flight share
+// digit blocks in L2), 128 threads, a 4-stage ring in shared memory.
 // Thread 0 issues the bulk copies, thread 32 the S(S+1)/2 MMAs (M = 128, N = 64,
 // K = 32) of each stage into the S level accumulators (64 TMEM columns each, 512 for
 // S = 8) and commits each stage's MMAs to the stage's "empty" mbarrier.  Every wait is
@@ -47,6 +48,7 @@ constexpr int OZ_ASTEP = OZ_M * OZ_K;          // bytes of one digit plane of a 
 constexpr int OZ_BSTEP = OZ_N * OZ_K;          // ... of a 64-column block of B
 constexpr int OZ_NST = 4;                      // stages of the shared-memory ring
 constexpr int OZ_KPER = 256;                   // K range of one thread of the exponent pass
+constexpr int OZ_GM = 8;                       // row blocks per group of the tile order
 constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
 constexpr int OZ_ZERO_EXP = -4000;             // below: an all-zero line (exponents start at 0x80808080)
 
@@ -173,7 +175,7 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
 }
 
 template <int S>
-__global__ void __launch_bounds__(OZ_NT, 1) oz_gemm_kernel(int M, int N, int kst, double alpha,
+__global__ void __launch_bounds__(OZ_NT, 1) oz_gemm_kernel(int M, int N, int kst, int mblk, int nblk, double alpha,
                                                           const int8_t *__restrict__ Asl,
                                                           const int8_t *__restrict__ Bsl, const int *__restrict__ ea,
                                                           const int *__restrict__ eb, double beta, double *C, long ldc,
@@ -189,7 +191,11 @@ __global__ void __launch_bounds__(OZ_NT, 1) oz_gemm_kernel(int M, int N, int kst
     volatile int *issued_s = fail_s + 1;           // stages whose copies were issued
     volatile int *used_s = fail_s + 2;             // stages whose MMAs were issued
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int mb = blockIdx.x, nb = blockIdx.y;
+    // tile order: groups of OZ_GM row blocks, walked column block by column block, so that the CTAs
+    // in flight share a few blocks of A's and B's digits in L2
+    const int per = OZ_GM * nblk, grp = (int)blockIdx.x / per, m0b = grp * OZ_GM;
+    const int gs = min(mblk - m0b, OZ_GM), rr = (int)blockIdx.x - grp * per;
+    const int mb = m0b + rr % gs, nb = rr / gs;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(osm);
     const uint32_t full_a = (uint32_t)__cvta_generic_to_shared(full);
     const uint32_t empty_a = (uint32_t)__cvta_generic_to_shared(empty);
@@ -333,14 +339,15 @@ OzLayout oz_layout(int m, int n, int k, int S)
     return L;
 }
 
-template <int S> int oz_launch(dim3 g, int m, int n, int kst, double alpha, const int8_t *As, const int8_t *Bs,
-                               const int *ea, const int *eb, double beta, double *C, long ldc, int *err,
-                               cudaStream_t s)
+template <int S> int oz_launch(int mblk, int nblk, int m, int n, int kst, double alpha, const int8_t *As,
+                               const int8_t *Bs, const int *ea, const int *eb, double beta, double *C, long ldc,
+                               int *err, cudaStream_t s)
 {
     const int smem = OZ_NST * S * (OZ_ASTEP + OZ_BSTEP) + 128;
     cudaError_t e = smem_attr(oz_gemm_kernel<S>, smem);
     if (e != cudaSuccess) return cuda_fail(e, "ozaki gemm smem");
-    oz_gemm_kernel<S><<<g, OZ_NT, smem, s>>>(m, n, kst, alpha, As, Bs, ea, eb, beta, C, ldc, err);
+    oz_gemm_kernel<S><<<(unsigned)(mblk * nblk), OZ_NT, smem, s>>>(m, n, kst, mblk, nblk, alpha, As, Bs, ea, eb, beta,
+                                                                   C, ldc, err);
     return cuda_fail(cudaGetLastError(), "ozaki gemm");
 }
 
@@ -389,11 +396,11 @@ int ozaki_gemm(int m, int n, int k, double alpha, const double *A, long lda, con
     oz_slice_kernel<<<dim3((unsigned)((L.np + 127) / 128), kc), 128, 0, s>>>(n, (int)L.np, k, B, ldb, 1, eb, slices,
                                                                              OZ_N, (int)L.kst, Bs);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "ozaki digits");
-    const dim3 g((unsigned)(L.mp / OZ_M), (unsigned)(L.np / OZ_N));
+    const int mblk = (int)(L.mp / OZ_M), nblk = (int)(L.np / OZ_N);
     switch (slices) {
-    case 6: return oz_launch<6>(g, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
-    case 7: return oz_launch<7>(g, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
-    default: return oz_launch<8>(g, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
+    case 6: return oz_launch<6>(mblk, nblk, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
+    case 7: return oz_launch<7>(mblk, nblk, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
+    default: return oz_launch<8>(mblk, nblk, m, n, (int)L.kst, alpha, As, Bs, ea, eb, beta, C, ldc, err, s);
     }
 }
 
