@@ -11,6 +11,13 @@ eigensolve with eigenvectors (bsr_hd).  Inputs are seeded synthetic data.
 Under torchrun every rank solves its own partial wave (different seed): the
 work shards by partial wave with no collective in the data path (weak
 scaling); rank 0 prints one JSON line.
+
+At N = 1 the line also carries side results: the mixed-precision form of the
+same partial wave (direct contraction and refinement product from 8-bit digits
+on the tensor cores) beside FP64, config 1 solved whole on the GPU and on the
+host, the batched (config 4) and served (config 5) forms in FP64 and mixed
+precision, and the CPU baseline.  --gemm, --dense-eig and --assemble-only time
+one piece alone for profiling.
 """
 import argparse
 import json
