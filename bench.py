@@ -704,26 +704,37 @@ def run_b200(args):
         "gpu_launches": int(round(own_launches * args.steps)),
         "clocks": clk,
     }
+    def side(name, fn):
+        # a side result that fails is reported in the line instead of ending the run before the line
+        try:
+            return fn()
+        except Exception as ex:          # noqa: BLE001 -- recorded, not hidden
+            print("bench: side result %s failed: %s: %s" % (name, type(ex).__name__, ex), file=sys.stderr)
+            return {"error": "%s: %s" % (type(ex).__name__, ex)}
+
     if world == 1 and not args.no_batched:
         del ctx, basis, P, res
         torch.cuda.empty_cache()
-        line["batched"], line["serving"] = bench_batched_serving(torch, bsr)
+        bs = side("batched/serving", lambda: bench_batched_serving(torch, bsr))
+        line["batched"], line["serving"] = bs if isinstance(bs, tuple) else (bs, bs)
     if world == 1:
-        line["config1"] = bench_config1(torch, bsr, with_cpu=not args.no_cpu_baseline)
-        line["mixed"] = bench_mixed(torch, bsr, pw)
+        line["config1"] = side("config1", lambda: bench_config1(torch, bsr, with_cpu=not args.no_cpu_baseline))
+        line["mixed"] = side("mixed", lambda: bench_mixed(torch, bsr, pw))
     if world == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
-        ref = CpuReference(pw, procs=cores, threads=None)
-        try:
-            ref.sample()
-            wall, total, st, sc = ref.sample()
-        finally:
-            ref.close()
-        line["cpu_baseline"] = {"value": 1.0 / total, "unit": "solves/s", "cores": cores, "kind": "port",
-                                "sample": ref.describe(), "extrapolated_seconds_per_solve": total,
-                                "sample_seconds": wall,
-                                "stage_seconds_sampled": {k: round(v, 4) for k, v in st.items()},
-                                "stage_scale_to_one_solve": {k: round(v, 3) for k, v in sc.items()}}
+        def cpu_baseline():
+            cores = os.cpu_count() or 1
+            ref = CpuReference(pw, procs=cores, threads=None)
+            try:
+                ref.sample()
+                wall, total, st, sc = ref.sample()
+            finally:
+                ref.close()
+            return {"value": 1.0 / total, "unit": "solves/s", "cores": cores, "kind": "port",
+                    "sample": ref.describe(), "extrapolated_seconds_per_solve": total,
+                    "sample_seconds": wall,
+                    "stage_seconds_sampled": {k: round(v, 4) for k, v in st.items()},
+                    "stage_scale_to_one_solve": {k: round(v, 3) for k, v in sc.items()}}
+        line["cpu_baseline"] = side("cpu_baseline", cpu_baseline)
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
