@@ -249,8 +249,12 @@ class PartialWaveServer:
                 r.event.set()
                 self._release(r)
                 if r.barrier is not None:
+                    # a failed warm-up releases the other workers at once instead of at the timeout
                     try:
-                        r.barrier.wait()
+                        if r.error is not None:
+                            r.barrier.abort()
+                        else:
+                            r.barrier.wait()
                     except threading.BrokenBarrierError:
                         pass
             ctx.close()
